@@ -1,0 +1,318 @@
+#!/usr/bin/env python
+"""Headline benchmark: PM steps per second of particles at 512^3.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One process per GPU (torchrun for N > 1).  Each rank advances its own
+independent box (replicas: the step itself has no collective), so scaling
+is weak.  The timed region is exactly K whole DKD steps on the device
+(CUDA events on the box's stream, barrier + synchronize on both sides, max
+over ranks).  value = particle updates of all ranks / that time.
+
+Also reported (rank 0): per-kernel timings and the roofline of the dominant
+kernel against the measured HBM peak, the end-to-end number through the
+C-ABI with host buffers (hgpm_step_host: H2D of the state, one step, D2H of
+the state, every step), the CPU baseline (the OpenMP C++ transcription of
+the reference's serial step on this host's cores), kernel launch count and
+SM clocks sampled during the timed region.
+
+--impl reference times the reference's algorithm on the host cores (the
+reference has no CPU path; oracle/_bin/cpu_pm is its OpenMP transcription).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-updates/s at 512^3"
+UNIT = "particle-updates/s"
+NG = NP = 512
+RL = 512.0
+Z_INI = 50.0
+NSTEPS_RUN = 100  # step size of the run the timed steps belong to (z 50 -> 0 in 100 steps)
+
+# Algorithmic bytes per launch of each kernel (precision-form state:
+# x = 12 B offset + 4 B cell, v = 12 B; FP32 grids).  Sum = 72 Np + 64 Ng.
+def alg_bytes(np3, ng3):
+    return {
+        "deposit": 16 * np3 + 4 * ng3,
+        "fft_z_fwd": 8 * ng3,
+        "fft_y_fwd": 0,
+        "poisson_x": 16 * ng3,
+        "fft_y_inv": 0,
+        "fft_z_inv": 24 * ng3,
+        "kick_drift": 56 * np3 + 12 * ng3,
+    }
+
+
+KERNEL_NAMES = {
+    "deposit": "deposit_kernel",
+    "fft_z_fwd": "zpass_r2c_kernel<512,true>",
+    "fft_y_fwd": "strided_kernel<512,false>",
+    "poisson_x": "xfused_kernel<512,PoissonOp>",
+    "fft_y_inv": "strided_kernel<512,true>",
+    "fft_z_inv": "zpass_c2r_kernel<512>",
+    "kick_drift": "kick_drift_kernel",
+}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for nm, val in zip(names, r[5:9]):
+                    if val.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(steps=1, warmup=0, ng=NG, np_side=NP):
+    exe = os.path.join(ROOT, "oracle", "_bin", "cpu_pm")
+    if not os.path.exists(exe):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "cpu"], check=True)
+    out = subprocess.run([exe, "--ng", str(ng), "--np", str(np_side), "--rl", str(RL), "--zini", str(Z_INI),
+                          "--nsteps-total", str(NSTEPS_RUN), "--steps", str(steps), "--warmup", str(warmup)],
+                         capture_output=True, text=True, check=True)
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 3))
+    r = cpu_baseline(steps=steps, warmup=1 if args.warmup > 0 else 0)
+    v = NP ** 3 / r["sec_per_step"]
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": r["steps"],
+        "warmup": 1 if args.warmup > 0 else 0, "ms_per_step": r["sec_per_step"] * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic: seeded perturbed lattice",
+        "config": {"workload": "PM step, 512^3 particles on a 512^3 grid, L=512 Mpc/h", "np": NP, "ng": NG,
+                   "rl": RL, "parallelism": "host cores (OpenMP)"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["threads"], "kind": "port",
+                         "sample": "%d full 512^3 step(s) of the OpenMP C++ transcription of the reference's serial "
+                                   "step (float3 layout, float atomics, C2C FFTs), after 1 warm-up" % r["steps"]},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def allmax(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    import hacc_gpm_b200 as H
+    from hacc_gpm_b200 import ipk as ipkmod
+
+    txt = ipkmod.lcdm_params_text(NG, NP, RL, Z_INI, NSTEPS_RUN, seed=21082001 + rank)
+    params = H.parse_params(txt)
+    header, table = ipkmod.make_ipk(ipkmod.cosmo_from_params(params), Z_INI, k_max=20.0, k_bins=20000)
+    sim = H.Simulation(params, device=local)
+    sim.generate_ic(table, header[3])
+    ts = H.Timestepper(params)
+    ts.set_initial_z(params.z_ini)
+    ts.reverse_half_step()
+    ts.advance_half_step()
+    stream = torch.cuda.ExternalStream(sim.stream)
+
+    # warm-up
+    sim.run_steps(ts, args.warmup)
+    sim.sync()
+
+    # timed region
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    sim.sync()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = sim.kernel_launches()
+    e0.record(stream)
+    sim.run_steps(ts, args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    launches = sim.kernel_launches() - launches0
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    ms_max = allmax(ms)
+    np3, ng3 = NP ** 3, NG ** 3
+    value = world * np3 * args.steps / (ms_max * 1e-3)
+
+    # per-kernel timing (separate pass, events around every kernel)
+    sim.enable_timing(True)
+    sim.phase_times()
+    sim.run_steps(ts, args.steps)
+    ph_ms, ph_n = sim.phase_times()
+    sim.enable_timing(False)
+    peak, peak_kind = measured_peak()
+    ab = alg_bytes(np3, ng3)
+    phases = {}
+    for k, b in ab.items():
+        n = int(ph_n.get(k, 0))
+        if n == 0:
+            continue
+        avg = ph_ms[k] / n
+        phases[k] = {"ms_per_launch": avg, "launches": n, "alg_bytes": b,
+                     "alg_gbs": b / (avg * 1e-3) / 1e9 if b else 0.0}
+    dom = max(phases, key=lambda k: phases[k]["ms_per_launch"])
+    d = phases[dom]
+    roofline = {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "phase": dom, "achieved": d["alg_gbs"], "peak": peak,
+                "unit": "GB/s", "frac": d["alg_gbs"] / peak, "peak_kind": peak_kind, "traffic": None,
+                "alg_bytes_per_launch": d["alg_bytes"], "ms_per_launch": d["ms_per_launch"]}
+    step_ms = ms_max / args.steps
+    b_step = 72 * np3 + 64 * ng3
+    step_roof = {"alg_bytes_per_step": b_step, "achieved_gbs": b_step / (step_ms * 1e-3) / 1e9,
+                 "frac": b_step / (step_ms * 1e-3) / 1e9 / peak, "peak": peak}
+    tp = os.path.join(ROOT, "profiles", "traffic_512.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traf = json.load(f)
+        if dom in traf:
+            roofline["traffic"] = traf[dom]
+
+    # end to end through the C-ABI with pinned host buffers, every step:
+    # H2D state -> one step -> D2H state
+    e2e = None
+    if not args.no_e2e:
+        x_h, v_h = sim.store_state()
+        xp = torch.from_numpy(x_h).pin_memory()
+        vp = torch.from_numpy(v_h).pin_memory()
+        xn, vn = xp.numpy(), vp.numpy()
+        sim.step_host(ts, xn, vn)  # warm-up
+        barrier()
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(args.e2e_steps):
+            sim.step_host(ts, xn, vn)
+        t1.record(stream)
+        t1.synchronize()
+        barrier()
+        ems = allmax(t0.elapsed_time(t1))
+        e2e = {"value": world * np3 * args.e2e_steps / (ems * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": 24 * np3, "d2h_bytes_per_step": 24 * np3, "steps": args.e2e_steps,
+               "path": "hgpm_step_host (C-ABI, pinned float3 x,v in and out every step)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        r = cpu_baseline(steps=1, warmup=0)
+        cpu = {"value": np3 / r["sec_per_step"], "unit": UNIT, "cores": r["threads"], "kind": "port",
+               "sample": "1 full 512^3 step of the OpenMP C++ transcription of the reference's serial step "
+                         "(float3 layout, float atomics, C2C FFTs) on %d host threads" % r["threads"]}
+
+    sim.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded EH no-wiggle Zel'dovich ICs (Philox white noise), random per rank",
+        "config": {"workload": "PM step (deposit, R2C FFT, Poisson+gradient, 3 C2R FFTs, gather+kick+drift), "
+                               "512^3 particles on a 512^3 grid, L=512 Mpc/h, flat LCDM, ICs at z=50, 100-step run",
+                   "np": NP, "ng": NG, "rl": RL, "parallelism": "replicas (one independent box per GPU)",
+                   "l2": "inputs larger than L2 (3.8 GB particle state, 5 GB grids)"},
+        "roofline": roofline, "step_roofline": step_roof, "phases": phases, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": int(launches), "clocks": clk,
+    }
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

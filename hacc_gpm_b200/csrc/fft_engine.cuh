@@ -1,0 +1,174 @@
+// fft_engine.cuh — shared-memory tile FFT for the PM step.
+//
+// A tile is C independent complex lines of length N held in shared memory as
+//   buf[e * ES + c]      e in [0, N) element, c in [0, C) line, ES >= C
+// i.e. lines are columns with unit stride between lines.  Every pass kernel
+// (z R2C/C2R lines, y and x strided lines) stages its data into this layout
+// and calls fft_tile<>.  The transform is a Stockham autosort mixed-radix
+// FFT (radices 2, 3, 4, 8): each stage reads R values per butterfly into
+// registers, synchronises, twiddles, does the radix-R DFT in registers and
+// writes back in place in Stockham order.  Threads are mapped line-fastest
+// so a half-warp touches 16 consecutive lines of one element (conflict-free
+// 64-bit shared accesses).
+//
+// Twiddles come from a per-length table tw[m] = exp(-2 pi i m / L) computed
+// on the host in double precision (no device transcendental functions);
+// a transform of length N may use a table of length N*TWS (stride TWS).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace hgpm {
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+// multiply by -i (forward) or +i (inverse)
+template <bool INV>
+__device__ __forceinline__ float2 rot90(float2 a) {
+    return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// ---- radix-R DFTs in registers (forward: exp(-2 pi i r m / R)) ----------
+template <int R, bool INV> struct Dft;
+
+template <bool INV> struct Dft<2, INV> {
+    static __device__ __forceinline__ void run(float2* v) {
+        float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    }
+};
+
+template <bool INV> struct Dft<3, INV> {
+    static __device__ __forceinline__ void run(float2* v) {
+        const float s3 = 0.86602540378443864676f;  // sqrt(3)/2
+        float2 t1 = cadd(v[1], v[2]);
+        float2 t2 = make_float2(v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y);
+        float2 d = csub(v[1], v[2]);
+        float2 t3 = make_float2(s3 * d.x, s3 * d.y);
+        float2 rt3 = rot90<INV>(t3);  // -i*t3 forward, +i*t3 inverse
+        v[0] = cadd(v[0], t1);
+        v[1] = cadd(t2, rt3);
+        v[2] = csub(t2, rt3);
+    }
+};
+
+template <bool INV> struct Dft<4, INV> {
+    static __device__ __forceinline__ void run(float2* v) {
+        float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+        float2 b0 = cadd(v[1], v[3]), b1 = rot90<INV>(csub(v[1], v[3]));
+        v[0] = cadd(a0, b0);
+        v[2] = csub(a0, b0);
+        v[1] = cadd(a1, b1);
+        v[3] = csub(a1, b1);
+    }
+};
+
+template <bool INV> struct Dft<8, INV> {
+    static __device__ __forceinline__ void run(float2* v) {
+        const float h = 0.70710678118654752440f;  // 1/sqrt(2)
+        float2 e[4] = {v[0], v[2], v[4], v[6]};
+        float2 o[4] = {v[1], v[3], v[5], v[7]};
+        Dft<4, INV>::run(e);
+        Dft<4, INV>::run(o);
+        // o[m] *= w8^m, w8 = exp(-+ i pi/4)
+        float2 o1 = INV ? make_float2(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
+                        : make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+        float2 o2 = rot90<INV>(o[2]);
+        float2 o3 = INV ? make_float2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
+                        : make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+        v[0] = cadd(e[0], o[0]);
+        v[4] = csub(e[0], o[0]);
+        v[1] = cadd(e[1], o1);
+        v[5] = csub(e[1], o1);
+        v[2] = cadd(e[2], o2);
+        v[6] = csub(e[2], o2);
+        v[3] = cadd(e[3], o3);
+        v[7] = csub(e[3], o3);
+    }
+};
+
+// ---- one Stockham stage -------------------------------------------------
+// NS = product of the radices of the previous stages.
+template <int N, int C, int ES, int NS, int R, bool INV, int NT, int TWS>
+__device__ __forceinline__ void fft_stage(float2* __restrict__ buf, const float2* __restrict__ tw) {
+    constexpr int NB = N / R;        // butterflies per line
+    constexpr int TOT = NB * C;      // butterflies in the tile
+    constexpr int PER = (TOT + NT - 1) / NT;
+    float2 v[PER][R];
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int b = tid + t * NT;
+        if ((TOT % NT) == 0 || b < TOT) {
+            const int c = b % C, j = b / C;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[t][r] = buf[(j + r * NB) * ES + c];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int b = tid + t * NT;
+        if ((TOT % NT) == 0 || b < TOT) {
+            const int c = b % C, j = b / C;
+            const int k = j % NS;
+            if (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    const float2 w = __ldg(&tw[TWS * (r * k * (N / (NS * R)))]);
+                    v[t][r] = INV ? cmulc(v[t][r], w) : cmul(v[t][r], w);
+                }
+            }
+            Dft<R, INV>::run(v[t]);
+            const int base = (j / NS) * NS * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) buf[(base + r * NS) * ES + c] = v[t][r];
+        }
+    }
+    __syncthreads();
+}
+
+template <int... Rs> struct RSeq {};
+
+template <int N, int C, int ES, bool INV, int NT, int TWS, int NS>
+__device__ __forceinline__ void fft_stages(float2*, const float2*, RSeq<>) {}
+
+template <int N, int C, int ES, bool INV, int NT, int TWS, int NS, int R, int... Rs>
+__device__ __forceinline__ void fft_stages(float2* buf, const float2* tw, RSeq<R, Rs...>) {
+    fft_stage<N, C, ES, NS, R, INV, NT, TWS>(buf, tw);
+    fft_stages<N, C, ES, INV, NT, TWS, NS * R>(buf, tw, RSeq<Rs...>{});
+}
+
+// Radix plans for the supported lengths (2^a 3^b, 8..1024).
+template <int N> struct Plan;
+template <> struct Plan<8> { using type = RSeq<8>; };
+template <> struct Plan<12> { using type = RSeq<3, 4>; };
+template <> struct Plan<16> { using type = RSeq<4, 4>; };
+template <> struct Plan<24> { using type = RSeq<3, 8>; };
+template <> struct Plan<32> { using type = RSeq<8, 4>; };
+template <> struct Plan<48> { using type = RSeq<3, 4, 4>; };
+template <> struct Plan<64> { using type = RSeq<8, 8>; };
+template <> struct Plan<96> { using type = RSeq<3, 8, 4>; };
+template <> struct Plan<128> { using type = RSeq<8, 4, 4>; };
+template <> struct Plan<192> { using type = RSeq<3, 8, 8>; };
+template <> struct Plan<256> { using type = RSeq<8, 8, 4>; };
+template <> struct Plan<384> { using type = RSeq<3, 8, 4, 4>; };
+template <> struct Plan<512> { using type = RSeq<8, 8, 8>; };
+template <> struct Plan<768> { using type = RSeq<3, 8, 8, 4>; };
+template <> struct Plan<1024> { using type = RSeq<8, 8, 4, 4>; };
+
+// Transform all C lines of the tile (natural order in, natural order out).
+// Caller must __syncthreads() after filling the tile; returns synchronised.
+template <int N, int C, int ES, bool INV, int NT, int TWS = 1>
+__device__ __forceinline__ void fft_tile(float2* buf, const float2* __restrict__ tw) {
+    fft_stages<N, C, ES, INV, NT, TWS, 1>(buf, tw, typename Plan<N>::type{});
+}
+
+}  // namespace hgpm

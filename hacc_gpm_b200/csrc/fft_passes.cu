@@ -1,0 +1,596 @@
+// fft_passes.cu — the 3D R2C/C2R FFT passes of the PM step and the x pass
+// fused with k-space operators.
+//
+// Layouts (row-major, z fastest, as get_index in src/haccgpm.hpp:423-429):
+//   real grid      float  [ng][ng][ng]
+//   half spectrum  float2 [ng][ng][zs]   kz in [0, ng/2], zs = padded row
+// The forward 3D transform is: z pass (R2C along contiguous rows) ->
+// y pass (strided, in place) -> x pass (strided).  The inverse runs the
+// passes in reverse order with a C2R z pass.  The step never materialises
+// the forward x output: the x pass is fused with the Green's function and
+// gradient (Poisson), with the IC displacement operator, or with P(k)
+// binning, all of which act on one x-line tile while it is in shared memory.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+
+#include "fft_engine.cuh"
+#include "hgpm_device.cuh"
+#include "hgpm_internal.h"
+
+namespace hgpm {
+
+extern __shared__ float4 hgpm_smem[];
+
+// ---------------------------------------------------------------------------
+// per-size tile configuration
+// ---------------------------------------------------------------------------
+template <int NG> struct Cfg {
+    static constexpr int M = NG / 2;                       // complex length of z lines
+    static constexpr int L = M >= 512 ? 8 : (M >= 256 ? 16 : (M >= 96 ? 32 : 64));  // z lines per CTA
+    static constexpr int CS = NG >= 768 ? 8 : 16;          // strided-pass columns per CTA
+    static constexpr int CX = NG >= 768 ? 4 : (NG >= 384 ? 8 : 16);  // fused x-pass columns
+    static constexpr int ZSMEM = M * (L + 1) * 8;
+    static constexpr int SSMEM = NG * CS * 8;
+    static constexpr int XSMEM = 2 * NG * CX * 8;
+};
+
+// ---------------------------------------------------------------------------
+// tile load/store between global strided lines and shared [N][C]
+// ---------------------------------------------------------------------------
+// Rows e in [0, N) at g + e*rs; columns [0, nvalid) valid (nvalid may be < C).
+template <int N, int C>
+__device__ __forceinline__ void load_tile(float2* __restrict__ tile, const float2* __restrict__ g,
+                                          size_t rs, int nvalid) {
+    constexpr int TPR = C / 2;
+    for (int i = threadIdx.x; i < N * TPR; i += kThreads) {
+        const int e = i / TPR;
+        const int c = 2 * (i % TPR);
+        const float2* src = g + (size_t)e * rs + c;
+        float4 v;
+        if (c + 1 < nvalid) {
+            v = *reinterpret_cast<const float4*>(src);
+        } else if (c < nvalid) {
+            float2 t = src[0];
+            v = make_float4(t.x, t.y, 0.f, 0.f);
+        } else {
+            v = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        *reinterpret_cast<float4*>(&tile[e * C + c]) = v;
+    }
+}
+
+template <int N, int C>
+__device__ __forceinline__ void store_tile(const float2* __restrict__ tile, float2* __restrict__ g,
+                                           size_t rs, int nvalid) {
+    constexpr int TPR = C / 2;
+    for (int i = threadIdx.x; i < N * TPR; i += kThreads) {
+        const int e = i / TPR;
+        const int c = 2 * (i % TPR);
+        float2* dst = g + (size_t)e * rs + c;
+        const float4 v = *reinterpret_cast<const float4*>(&tile[e * C + c]);
+        if (c + 1 < nvalid) {
+            *reinterpret_cast<float4*>(dst) = v;
+        } else if (c < nvalid) {
+            dst[0] = make_float2(v.x, v.y);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// z pass, forward R2C.  FIX: input is the int64 fixed-point density
+// (value * 2^32); it is converted to float delta = rho - mean in FP64 and the
+// accumulator is zeroed for the next deposit.  Otherwise input is float.
+// ---------------------------------------------------------------------------
+template <int NG, bool FIX>
+__global__ void __launch_bounds__(kThreads) zpass_r2c_kernel(void* __restrict__ in_, float2* __restrict__ out,
+                                                             int nlines, int zs, double mean,
+                                                             const float2* __restrict__ tw) {
+    constexpr int M = NG / 2, L = Cfg<NG>::L, ES = L + 1;
+    float2* buf = reinterpret_cast<float2*>(hgpm_smem);
+    const int line0 = blockIdx.x * L;
+    for (int i = threadIdx.x; i < L * M; i += kThreads) {
+        const int l = i / M, m = i % M;
+        const int line = line0 + l;
+        float2 z = make_float2(0.f, 0.f);
+        if (line < nlines) {
+            if (FIX) {
+                ulonglong2* p = reinterpret_cast<ulonglong2*>(reinterpret_cast<unsigned long long*>(in_) +
+                                                              (size_t)line * NG) + m;
+                const ulonglong2 q = *p;
+                z.x = (float)((double)(long long)q.x * kFixInv - mean);
+                z.y = (float)((double)(long long)q.y * kFixInv - mean);
+                *p = make_ulonglong2(0ull, 0ull);
+            } else {
+                z = reinterpret_cast<const float2*>(reinterpret_cast<const float*>(in_) + (size_t)line * NG)[m];
+            }
+        }
+        buf[m * ES + l] = z;
+    }
+    __syncthreads();
+    fft_tile<M, L, ES, false, kThreads, 2>(buf, tw);
+    constexpr int H = M / 2 + 1;
+    for (int i = threadIdx.x; i < L * H; i += kThreads) {
+        const int l = i / H, k = i % H;
+        const int line = line0 + l;
+        if (line >= nlines) continue;
+        const float2 zk = buf[k * ES + l];
+        const float2 zm = buf[((M - k) % M) * ES + l];
+        const float2 w = __ldg(&tw[k]);
+        // E = (Zk + conj Zm)/2, O = -i (Zk - conj Zm)/2, X[k] = E + w O,
+        // X[M-k] = conj(E - w O)
+        const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        const float2 o = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+        const float2 wo = cmul(w, o);
+        float2* dst = out + (size_t)line * zs;
+        dst[k] = cadd(e, wo);
+        if (k != M - k) {
+            const float2 xm = csub(e, wo);
+            dst[M - k] = make_float2(xm.x, -xm.y);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// z pass, inverse C2R, ncomp components (blockIdx.y), unnormalised * scale.
+// X[0] and X[ng/2] are taken as real (Hermitian extension), which makes the
+// result equal to the real part of the reference's full C2C inverse.
+// ---------------------------------------------------------------------------
+template <int NG>
+__global__ void __launch_bounds__(kThreads) zpass_c2r_kernel(const float2* __restrict__ in, float* __restrict__ out,
+                                                             int nlines, int zs, size_t in_cs, size_t out_cs,
+                                                             float scale, const float2* __restrict__ tw) {
+    constexpr int M = NG / 2, L = Cfg<NG>::L, ES = L + 1;
+    float2* buf = reinterpret_cast<float2*>(hgpm_smem);
+    in += (size_t)blockIdx.y * in_cs;
+    out += (size_t)blockIdx.y * out_cs;
+    const int line0 = blockIdx.x * L;
+    constexpr int H = M / 2 + 1;
+    for (int i = threadIdx.x; i < L * H; i += kThreads) {
+        const int l = i / H, k = i % H;
+        const int line = line0 + l;
+        float2 xk = make_float2(0.f, 0.f), xm = make_float2(0.f, 0.f);
+        if (line < nlines) {
+            const float2* src = in + (size_t)line * zs;
+            xk = src[k];
+            xm = src[M - k];
+        }
+        if (k == 0) {
+            xk.y = 0.f;
+            xm.y = 0.f;
+        }
+        const float2 w = __ldg(&tw[k]);
+        // S = X[k] + conj X[M-k], D = X[k] - conj X[M-k], T = i conj(w) D
+        // Z[k] = S + T, Z[M-k] = conj(S - T)
+        const float2 s = make_float2(xk.x + xm.x, xk.y - xm.y);
+        const float2 d = make_float2(xk.x - xm.x, xk.y + xm.y);
+        const float2 cd = cmulc(d, w);                  // conj(w) * d
+        const float2 t = make_float2(-cd.y, cd.x);      // i * conj(w) * d
+        buf[k * ES + l] = cadd(s, t);
+        if (k != 0 && k != M - k) {
+            const float2 zm = csub(s, t);
+            buf[(M - k) * ES + l] = make_float2(zm.x, -zm.y);
+        }
+    }
+    __syncthreads();
+    fft_tile<M, L, ES, true, kThreads, 2>(buf, tw);
+    for (int i = threadIdx.x; i < L * M; i += kThreads) {
+        const int l = i / M, m = i % M;
+        const int line = line0 + l;
+        if (line >= nlines) continue;
+        const float2 z = buf[m * ES + l];
+        reinterpret_cast<float2*>(out + (size_t)line * NG)[m] = make_float2(z.x * scale, z.y * scale);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// strided pass (y or x lines), in place, blockIdx = (column chunk, plane, comp)
+// ---------------------------------------------------------------------------
+template <int NG, bool INV>
+__global__ void __launch_bounds__(kThreads) strided_kernel(float2* __restrict__ data, int ncols, size_t rs,
+                                                           size_t ps, size_t cs, const float2* __restrict__ tw) {
+    constexpr int C = Cfg<NG>::CS;
+    float2* tile = reinterpret_cast<float2*>(hgpm_smem);
+    const int col0 = blockIdx.x * C;
+    float2* g = data + (size_t)blockIdx.z * cs + (size_t)blockIdx.y * ps + col0;
+    const int nvalid = ncols - col0;
+    load_tile<NG, C>(tile, g, rs, nvalid);
+    __syncthreads();
+    fft_tile<NG, C, C, INV, kThreads>(tile, tw);
+    store_tile<NG, C>(tile, g, rs, nvalid);
+}
+
+// ---------------------------------------------------------------------------
+// x pass fused with a k-space operator producing 3 components:
+//   forward x FFT of the (z,y)-transformed tile -> t = op.pre(k, rho_k) ->
+//   for d in 0..2: op.comp(d, k, t) -> inverse x FFT -> out[d]
+// plane = ky index, rows = kx index, columns = kz index.
+// ---------------------------------------------------------------------------
+template <int NG, class Op>
+__global__ void __launch_bounds__(kThreads) xfused_kernel(const float2* __restrict__ in, float2* __restrict__ out,
+                                                          int ncols, size_t rs, size_t ps, size_t out_cs,
+                                                          const float2* __restrict__ tw, Op op) {
+    constexpr int C = Cfg<NG>::CX;
+    float2* tile = reinterpret_cast<float2*>(hgpm_smem);
+    float2* work = tile + NG * C;
+    const int col0 = blockIdx.x * C;
+    const int iy = blockIdx.y;
+    const size_t off = (size_t)iy * ps + col0;
+    const int nvalid = ncols - col0;
+    load_tile<NG, C>(tile, in + off, rs, nvalid);
+    __syncthreads();
+    fft_tile<NG, C, C, false, kThreads>(tile, tw);
+    for (int i = threadIdx.x; i < NG * C; i += kThreads) {
+        const int ix = i / C, c = i % C;
+        tile[i] = op.pre(ix, iy, col0 + c, tile[i]);
+    }
+    // (fft_tile ended with a barrier; pre() only touches the thread's own cells)
+#pragma unroll 1
+    for (int d = 0; d < 3; ++d) {
+        for (int i = threadIdx.x; i < NG * C; i += kThreads) {
+            const int ix = i / C, c = i % C;
+            work[i] = op.comp(d, ix, iy, col0 + c, tile[i]);
+        }
+        __syncthreads();
+        fft_tile<NG, C, C, true, kThreads>(work, tw);
+        store_tile<NG, C>(work, out + (size_t)d * out_cs + off, rs, nvalid);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// x pass fused with P(k): forward x FFT, |delta|^2 * scale * CIC window, and
+// deterministic per-warp FP64 shell sums.  Persistent CTAs take tiles
+// blockIdx.x, +gridDim.x, ... and write one partial histogram each.
+// ---------------------------------------------------------------------------
+template <int NG>
+__global__ void __launch_bounds__(kThreads) xpk_kernel(const float2* __restrict__ in, int ncols, size_t rs,
+                                                       size_t ps, int nchunks, const float2* __restrict__ tw,
+                                                       PkArgs a, double* __restrict__ part_sum,
+                                                       unsigned long long* __restrict__ part_cnt) {
+    constexpr int C = Cfg<NG>::CX;
+    constexpr int M = NG / 2;
+    constexpr int NW = kThreads / 32;
+    float2* tile = reinterpret_cast<float2*>(hgpm_smem);
+    double* hs = reinterpret_cast<double*>(tile + NG * C);
+    unsigned long long* hc = reinterpret_cast<unsigned long long*>(hs + NW * a.nbins);
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    for (int i = threadIdx.x; i < NW * a.nbins; i += kThreads) {
+        hs[i] = 0.0;
+        hc[i] = 0ull;
+    }
+    const int ntiles = nchunks * NG;
+    for (int tile_id = blockIdx.x; tile_id < ntiles; tile_id += gridDim.x) {
+        const int chunk = tile_id % nchunks, iy = tile_id / nchunks;
+        const int col0 = chunk * C;
+        const int nvalid = ncols - col0;
+        __syncthreads();
+        load_tile<NG, C>(tile, in + (size_t)iy * ps + col0, rs, nvalid);
+        __syncthreads();
+        fft_tile<NG, C, C, false, kThreads>(tile, tw);
+        // each warp walks its own cells in a fixed order
+        for (int base = warp * 32; base < NG * C; base += kThreads) {
+            const int i = base + lane;
+            int bin = -1;
+            double val = 0.0;
+            int wgt = 0;
+            if (i < NG * C) {
+                const int ix = i / C, c = i % C, iz = col0 + c;
+                const bool dc = (ix == 0 && iy == 0 && iz == 0);
+                const bool corner = (ix == M && iy == M && iz == M);
+                if (c < nvalid && !dc && !corner) {
+                    const float kx = __ldg(&a.kf[ix]), ky = __ldg(&a.kf[iy]), kz = __ldg(&a.kf[iz]);
+                    const float s2 = __fadd_rn(__fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky)), __fmul_rn(kz, kz));
+                    const float kmag = __fsqrt_rn(s2);
+                    double fb;
+                    if (a.log_bins) {
+                        fb = log((double)kmag / a.min_k) / a.bin_delta;
+                    } else {
+                        fb = ((double)kmag - a.min_k) / a.bin_delta;
+                    }
+                    const int b = (int)fb;
+                    if (fb >= 0.0 && b < a.nbins) {
+                        const float2 v = tile[i];
+                        wgt = (iz == 0 || iz == M) ? 1 : 2;
+                        const double p = ((double)v.x * v.x + (double)v.y * v.y) * a.scale *
+                                         __ldg(&a.filt[ix]) * __ldg(&a.filt[iy]) * __ldg(&a.filt[iz]);
+                        val = p * wgt;
+                        bin = b;
+                    }
+                }
+            }
+            const unsigned grp = __match_any_sync(0xffffffffu, bin);
+            const int leader = __ffs(grp) - 1;
+            double s = 0.0;
+            unsigned long long n = 0;
+            unsigned m = grp;
+            while (m) {
+                const int src = __ffs(m) - 1;
+                m &= m - 1;
+                const double vv = __shfl_sync(grp, val, src);
+                const int ww = __shfl_sync(grp, wgt, src);
+                s += vv;
+                n += (unsigned long long)ww;
+            }
+            if (lane == leader && bin >= 0) {
+                hs[warp * a.nbins + bin] += s;
+                hc[warp * a.nbins + bin] += n;
+            }
+        }
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < a.nbins; b += kThreads) {
+        double s = 0.0;
+        unsigned long long n = 0;
+        for (int w = 0; w < NW; ++w) {
+            s += hs[w * a.nbins + b];
+            n += hc[w * a.nbins + b];
+        }
+        part_sum[(size_t)blockIdx.x * a.nbins + b] = s;
+        part_cnt[(size_t)blockIdx.x * a.nbins + b] = n;
+    }
+}
+
+__global__ void pk_reduce_kernel(const double* __restrict__ part_sum, const unsigned long long* __restrict__ part_cnt,
+                                 int nparts, int nbins, double* __restrict__ sum, unsigned long long* __restrict__ cnt) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nbins) return;
+    double s = 0.0;
+    unsigned long long n = 0;
+    for (int p = 0; p < nparts; ++p) {
+        s += part_sum[(size_t)p * nbins + b];
+        n += part_cnt[(size_t)p * nbins + b];
+    }
+    sum[b] = s;
+    cnt[b] = n;
+}
+
+// ---------------------------------------------------------------------------
+// k-space operators
+// ---------------------------------------------------------------------------
+// Poisson + gradient, kspace_solve_gradient (kspace_solver.cu:55-90) with
+// calcGreens (calcGreens.hpp:11-25): t = G rho_k, F_d = -i sin(k_d) t.
+// cosq[i] = cos(k_i) - 1 (double) and sk[i] = sin(k_i) are tabulated once per
+// grid side; G is formed in double from the sum of the (non-positive) cosq
+// terms, so there is no cancellation near k = 0.
+struct PoissonOp {
+    const double* cosq;  // cos(k_i) - 1, one entry per grid index
+    const float* sk;     // sin(k_i)
+    double coeff;        // 0.5 / ng^3
+    __device__ __forceinline__ float2 pre(int ix, int iy, int iz, float2 v) const {
+        const double s = __ldg(&cosq[ix]) + __ldg(&cosq[iy]) + __ldg(&cosq[iz]);
+        const float g = (s == 0.0) ? 0.f : (float)(coeff / s);
+        return make_float2(v.x * g, v.y * g);
+    }
+    __device__ __forceinline__ float2 comp(int d, int ix, int iy, int iz, float2 t) const {
+        const float sd = __ldg(&sk[d == 0 ? ix : (d == 1 ? iy : iz)]);
+        return make_float2(sd * t.y, -sd * t.x);
+    }
+};
+
+// Zel'dovich displacement (initializer.cpp:10-117): ScaleAmplitudes by
+// sqrt(P(|k|) n^3/rl^3) from the .ipk table (interpolation_initializer.cu:3-30),
+// then transformDensityField (transform_density_field_initializer.cu:72-112):
+// s_d = (Im k_d, -Re k_d) / (k^2 delta).
+struct ICOp {
+    const double* table;
+    int nbins;
+    double k_delta;
+    double pkscale;    // n^3 / rl^3
+    double inv_delta;  // 1 / delta
+    const float* kf;   // float(signed(i) * 2 pi / rl)
+    int* err;          // set when |k| runs past the table
+    __device__ __forceinline__ float2 pre(int ix, int iy, int iz, float2 v) const {
+        const float kx = __ldg(&kf[ix]), ky = __ldg(&kf[iy]), kz = __ldg(&kf[iz]);
+        const float k2f = __fadd_rn(__fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky)), __fmul_rn(kz, kz));
+        double y = 0.0;
+        if (!(ix == 0 && iy == 0 && iz == 0)) {
+            const double my_k = (double)__fsqrt_rn(k2f);
+            const int left = (int)(my_k / k_delta);
+            const int right = left + 1;
+            if (right >= nbins) {
+                atomicExch(err, 1);
+            } else if (left == 0) {
+                y = __ldg(&table[right]) * pkscale;
+            } else {
+                const double ly1 = log(__ldg(&table[left]));
+                const double lx1 = log(k_delta * (double)left);
+                const double ly2 = log(__ldg(&table[right]));
+                const double lx2 = log(k_delta * (double)right);
+                const double lx = log(my_k);
+                y = exp(ly1 + ((ly2 - ly1) / (lx2 - lx1)) * (lx - lx1)) * pkscale;
+            }
+        }
+        const double sc = sqrt(y);
+        v.x = (float)((double)v.x * sc);
+        v.y = (float)((double)v.y * sc);
+        const double k2 = (double)k2f;
+        const double mul = inv_delta * (k2 == 0.0 ? 0.0 : 1.0 / k2);
+        v.x = (float)((double)v.x * mul);
+        v.y = (float)((double)v.y * mul);
+        return v;
+    }
+    __device__ __forceinline__ float2 comp(int d, int ix, int iy, int iz, float2 t) const {
+        const float kd = __ldg(&kf[d == 0 ? ix : (d == 1 ? iy : iz)]);
+        return make_float2(t.y * kd, -t.x * kd);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// host launchers (dispatch on the grid side)
+// ---------------------------------------------------------------------------
+template <class K>
+static cudaError_t ensure_smem(K kernel, int bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+static inline unsigned cdiv(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
+
+template <int NG>
+static cudaError_t zfwd_impl(void* in, bool fixed, float2* out, int nlines, int zs, double mean,
+                             const float2* tw, cudaStream_t s) {
+    using G = Cfg<NG>;
+    const unsigned grid = cdiv(nlines, G::L);
+    if (fixed) {
+        auto k = zpass_r2c_kernel<NG, true>;
+        cudaError_t e = ensure_smem(k, G::ZSMEM);
+        if (e != cudaSuccess) return e;
+        k<<<grid, kThreads, G::ZSMEM, s>>>(in, out, nlines, zs, mean, tw);
+    } else {
+        auto k = zpass_r2c_kernel<NG, false>;
+        cudaError_t e = ensure_smem(k, G::ZSMEM);
+        if (e != cudaSuccess) return e;
+        k<<<grid, kThreads, G::ZSMEM, s>>>(in, out, nlines, zs, mean, tw);
+    }
+    return cudaGetLastError();
+}
+
+template <int NG>
+static cudaError_t zinv_impl(const float2* in, float* out, int nlines, int zs, size_t in_cs, size_t out_cs,
+                             int ncomp, float scale, const float2* tw, cudaStream_t s) {
+    using G = Cfg<NG>;
+    auto k = zpass_c2r_kernel<NG>;
+    cudaError_t e = ensure_smem(k, G::ZSMEM);
+    if (e != cudaSuccess) return e;
+    dim3 grid(cdiv(nlines, G::L), ncomp);
+    k<<<grid, kThreads, G::ZSMEM, s>>>(in, out, nlines, zs, in_cs, out_cs, scale, tw);
+    return cudaGetLastError();
+}
+
+template <int NG>
+static cudaError_t strided_impl(bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
+                                int ncomp, const float2* tw, cudaStream_t s) {
+    using G = Cfg<NG>;
+    dim3 grid(cdiv(ncols, G::CS), nplanes, ncomp);
+    if (inv) {
+        auto k = strided_kernel<NG, true>;
+        cudaError_t e = ensure_smem(k, G::SSMEM);
+        if (e != cudaSuccess) return e;
+        k<<<grid, kThreads, G::SSMEM, s>>>(data, ncols, rs, ps, cs, tw);
+    } else {
+        auto k = strided_kernel<NG, false>;
+        cudaError_t e = ensure_smem(k, G::SSMEM);
+        if (e != cudaSuccess) return e;
+        k<<<grid, kThreads, G::SSMEM, s>>>(data, ncols, rs, ps, cs, tw);
+    }
+    return cudaGetLastError();
+}
+
+template <int NG, class Op>
+static cudaError_t xfused_impl(const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
+                               size_t out_cs, const float2* tw, const Op& op, cudaStream_t s) {
+    using G = Cfg<NG>;
+    auto k = xfused_kernel<NG, Op>;
+    cudaError_t e = ensure_smem(k, G::XSMEM);
+    if (e != cudaSuccess) return e;
+    dim3 grid(cdiv(ncols, G::CX), nplanes);
+    k<<<grid, kThreads, G::XSMEM, s>>>(in, out, ncols, rs, ps, out_cs, tw, op);
+    return cudaGetLastError();
+}
+
+template <int NG>
+static cudaError_t xpk_impl(const float2* in, int ncols, size_t rs, size_t ps, const float2* tw, const PkArgs& a,
+                            double* part_sum, unsigned long long* part_cnt, int nparts, double* sum,
+                            unsigned long long* cnt, cudaStream_t s) {
+    using G = Cfg<NG>;
+    constexpr int NW = kThreads / 32;
+    const int smem = NG * G::CX * 8 + NW * a.nbins * 16;
+    auto k = xpk_kernel<NG>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const int nchunks = cdiv(ncols, G::CX);
+    k<<<nparts, kThreads, smem, s>>>(in, ncols, rs, ps, nchunks, tw, a, part_sum, part_cnt);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    pk_reduce_kernel<<<cdiv(a.nbins, 128), 128, 0, s>>>(part_sum, part_cnt, nparts, a.nbins, sum, cnt);
+    return cudaGetLastError();
+}
+
+#define HGPM_SIZES(X) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
+
+bool fft_size_supported(int ng) {
+    switch (ng) {
+#define X(n) case n:
+        HGPM_SIZES(X)
+#undef X
+        return true;
+        default:
+            return false;
+    }
+}
+
+cudaError_t launch_zfwd(int ng, void* in, bool fixed, float2* out, int nlines, int zs, double mean,
+                        const float2* tw, cudaStream_t s) {
+    switch (ng) {
+#define X(n) \
+    case n: return zfwd_impl<n>(in, fixed, out, nlines, zs, mean, tw, s);
+        HGPM_SIZES(X)
+#undef X
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_zinv(int ng, const float2* in, float* out, int nlines, int zs, size_t in_cs, size_t out_cs,
+                        int ncomp, float scale, const float2* tw, cudaStream_t s) {
+    switch (ng) {
+#define X(n) \
+    case n: return zinv_impl<n>(in, out, nlines, zs, in_cs, out_cs, ncomp, scale, tw, s);
+        HGPM_SIZES(X)
+#undef X
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
+                           int ncomp, const float2* tw, cudaStream_t s) {
+    switch (ng) {
+#define X(n) \
+    case n: return strided_impl<n>(inv, data, ncols, rs, ps, nplanes, cs, ncomp, tw, s);
+        HGPM_SIZES(X)
+#undef X
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_xpoisson(int ng, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
+                            size_t out_cs, const float2* tw, const double* cosq, const float* sk, double coeff,
+                            cudaStream_t s) {
+    PoissonOp op{cosq, sk, coeff};
+    switch (ng) {
+#define X(n) \
+    case n: return xfused_impl<n, PoissonOp>(in, out, ncols, rs, ps, nplanes, out_cs, tw, op, s);
+        HGPM_SIZES(X)
+#undef X
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_xic(int n, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
+                       size_t out_cs, const float2* tw, const double* table, int nbins, double k_delta,
+                       double pkscale, double inv_delta, const float* kf, int* err, cudaStream_t s) {
+    ICOp op{table, nbins, k_delta, pkscale, inv_delta, kf, err};
+    switch (n) {
+#define X(m) \
+    case m: return xfused_impl<m, ICOp>(in, out, ncols, rs, ps, nplanes, out_cs, tw, op, s);
+        HGPM_SIZES(X)
+#undef X
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_xpk(int ng, const float2* in, int ncols, size_t rs, size_t ps, const float2* tw, const PkArgs& a,
+                       double* part_sum, unsigned long long* part_cnt, int nparts, double* sum,
+                       unsigned long long* cnt, cudaStream_t s) {
+    switch (ng) {
+#define X(n) \
+    case n: return xpk_impl<n>(in, ncols, rs, ps, tw, a, part_sum, part_cnt, nparts, sum, cnt, s);
+        HGPM_SIZES(X)
+#undef X
+    }
+    return cudaErrorInvalidValue;
+}
+
+int pk_max_bins() { return 1024; }
+
+}  // namespace hgpm

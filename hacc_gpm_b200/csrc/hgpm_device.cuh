@@ -1,0 +1,36 @@
+// hgpm_device.cuh — device-side shared definitions of the PM step.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hgpm {
+
+constexpr int kThreads = 256;            // threads per CTA for all pass kernels
+constexpr double kFixScale = 4294967296.0;      // 2^32: int64 fixed-point density
+constexpr double kFixInv = 1.0 / 4294967296.0;
+constexpr float kFixScaleF = 4294967296.0f;
+
+// Particle positions are a packed cell (10 bits per axis, ng <= 1024) plus
+// an FP32 offset in [0, 1) per axis.
+__host__ __device__ __forceinline__ uint32_t pack_cell(int ix, int iy, int iz) {
+    return ((uint32_t)ix << 20) | ((uint32_t)iy << 10) | (uint32_t)iz;
+}
+__host__ __device__ __forceinline__ int cell_x(uint32_t c) { return (int)(c >> 20); }
+__host__ __device__ __forceinline__ int cell_y(uint32_t c) { return (int)((c >> 10) & 1023u); }
+__host__ __device__ __forceinline__ int cell_z(uint32_t c) { return (int)(c & 1023u); }
+
+// Particle state, structure of arrays (coalesced 4-byte streams).
+struct ParticleSoA {
+    uint32_t* cell;
+    float* ox;
+    float* oy;
+    float* oz;
+    float* vx;
+    float* vy;
+    float* vz;
+};
+
+// Signed mode index as get_kmodes maps it (src/haccgpm.hpp:255-274).
+__host__ __device__ __forceinline__ int signed_mode(int i, int n) { return i > n / 2 - 1 ? i - n : i; }
+
+}  // namespace hgpm

@@ -1,0 +1,57 @@
+// hgpm_internal.h — declarations shared by the CUDA translation units and
+// the host runtime of the PM step.  Not part of the public C-ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "hgpm_device.cuh"
+
+namespace hgpm {
+
+// Arguments of the fused x pass that bins P(k).
+struct PkArgs {
+    const float* kf;     // float(signed(i) * 2 pi / rl), one per grid index
+    const float* filt;   // per-axis CIC window factor
+    int nbins;
+    int log_bins;
+    double min_k;
+    double bin_delta;    // linear: width; log: width in ln k
+    double scale;        // (1/ng^3) * (rl/ng), scale_power.cu:8
+};
+
+bool fft_size_supported(int ng);
+int pk_max_bins();
+
+cudaError_t launch_zfwd(int ng, void* in, bool fixed, float2* out, int nlines, int zs, double mean,
+                        const float2* tw, cudaStream_t s);
+cudaError_t launch_zinv(int ng, const float2* in, float* out, int nlines, int zs, size_t in_cs, size_t out_cs,
+                        int ncomp, float scale, const float2* tw, cudaStream_t s);
+cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
+                           int ncomp, const float2* tw, cudaStream_t s);
+cudaError_t launch_xpoisson(int ng, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
+                            size_t out_cs, const float2* tw, const double* cosq, const float* sk, double coeff,
+                            cudaStream_t s);
+cudaError_t launch_xic(int n, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
+                       size_t out_cs, const float2* tw, const double* table, int nbins, double k_delta,
+                       double pkscale, double inv_delta, const float* kf, int* err, cudaStream_t s);
+cudaError_t launch_xpk(int ng, const float2* in, int ncols, size_t rs, size_t ps, const float2* tw, const PkArgs& a,
+                       double* part_sum, unsigned long long* part_cnt, int nparts, double* sum,
+                       unsigned long long* cnt, cudaStream_t s);
+
+cudaError_t launch_load_state(const float* x, const float* v, const ParticleSoA& p, size_t n, int ng, cudaStream_t s);
+cudaError_t launch_store_state(const ParticleSoA& p, float* x, float* v, size_t n, cudaStream_t s);
+cudaError_t launch_cells(const ParticleSoA& p, int32_t* out, size_t n, int ng, cudaStream_t s);
+cudaError_t launch_drift(const ParticleSoA& p, size_t n, int ng, float pf, cudaStream_t s);
+cudaError_t launch_deposit(const ParticleSoA& p, size_t n, int ng, float mass, unsigned long long* rho,
+                           cudaStream_t s);
+cudaError_t launch_kick_drift(const ParticleSoA& p, size_t n, int ng, const float* fx, const float* fy,
+                              const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift,
+                              cudaStream_t s);
+cudaError_t launch_density(const unsigned long long* rho64, float* rho, size_t n, cudaStream_t s);
+cudaError_t launch_ktables(int ng, double* cosq, float* sk, float* pkw, cudaStream_t s);
+cudaError_t launch_noise(float* out, size_t n, uint32_t seed, cudaStream_t s);
+cudaError_t launch_place(const float* sgrid, size_t scomp, const ParticleSoA& p, int np_side, int ng, float delta_f,
+                         float velmul, cudaStream_t s);
+
+}  // namespace hgpm

@@ -1,0 +1,972 @@
+// runtime.cu — host runtime of the PM step behind the C-ABI (include/hgpm_c.h):
+// params parser, FP64 time stepper and growth factors, device memory of a
+// context, and the phase sequencing that launches the kernels of
+// particles.cu and fft_passes.cu on the context's stream.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hgpm_c.h"
+#include "hgpm_internal.h"
+
+using namespace hgpm;
+
+// ===========================================================================
+// params (src/simulation/params.cpp)
+// ===========================================================================
+static void set_err(char* err, size_t errlen, const char* fmt, ...) {
+    if (!err || errlen == 0) return;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(err, errlen, fmt, ap);
+    va_end(ap);
+}
+
+static void params_defaults(hgpm_params* p) {
+    memset(p, 0, sizeof(*p));
+    p->block_size = 64;
+    p->w_de = -1.0;
+    p->t_cmb = 2.726;
+    p->neff_massless = 3.04;
+    p->z_ini = 200.0;
+    p->ol = 1.0;
+    p->pk_bins = 221;  // params.cpp:91
+    p->last_step = -1;
+    p->ref_quirks = 1;
+}
+
+static double atof_f(const char* s) { return (double)(float)atof(s); }
+
+extern "C" void hgpm_params_derive(hgpm_params* p) {
+    // params.cpp:237-245
+    p->overload = p->rl != 0.0 ? (int)ceil(((double)p->ng) / (p->rl) * p->ol) : 0;
+    p->omega_baryon = p->deut / p->hubble / p->hubble;
+    p->omega_cb = p->omega_cdm + p->omega_baryon;
+    p->omega_matter = p->omega_cb + p->omega_nu;
+    p->omega_radiation = 2.471e-5 * pow(p->t_cmb / 2.725f, 4.0f) / pow(p->hubble, 2.0f);
+    p->f_nu_massless = p->neff_massless * 7.0 / 8.0 * pow(4.0 / 11.0, 4.0 / 3.0);
+    p->f_nu_massive = p->neff_massive * 7.0 / 8.0 * pow(4.0 / 11.0, 4.0 / 3.0);
+}
+
+static int mark_steps(unsigned char* arr, const char* value, char* err, size_t errlen, const char* key) {
+    if (strcmp(value, "all") == 0) {
+        for (int i = 0; i < HGPM_MAX_STEPS; ++i) arr[i] = 1;
+        return HGPM_OK;
+    }
+    std::string v(value);
+    size_t pos = 0;
+    while (pos <= v.size()) {
+        size_t c = v.find(',', pos);
+        std::string tok = v.substr(pos, c == std::string::npos ? std::string::npos : c - pos);
+        if (!tok.empty()) {
+            int s = atoi(tok.c_str());
+            if (s < 0 || s >= HGPM_MAX_STEPS) {
+                set_err(err, errlen, "%s step %d outside [0, %d)", key, s, HGPM_MAX_STEPS);
+                return HGPM_ERR_ARG;
+            }
+            arr[s] = 1;
+        }
+        if (c == std::string::npos) break;
+        pos = c + 1;
+    }
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_params_parse(const char* text, hgpm_params* out, char* err, size_t errlen) {
+    if (!text || !out) return HGPM_ERR_ARG;
+    hgpm_params p;
+    params_defaults(&p);
+    const char* cur = text;
+    while (*cur) {
+        const char* nl = strchr(cur, '\n');
+        size_t len = nl ? (size_t)(nl - cur) : strlen(cur);
+        std::string line(cur, len);
+        cur = nl ? nl + 1 : cur + len;
+        char key[200] = {0}, value[200] = {0};
+        int got = sscanf(line.c_str(), "%199s %199s", key, value);
+        if (got < 1) continue;
+        if (!strcmp(key, "OMEGA_CDM")) p.omega_cdm = atof_f(value);
+        else if (!strcmp(key, "DEUT")) p.deut = atof_f(value);
+        else if (!strcmp(key, "OMEGA_NU")) p.omega_nu = atof_f(value);
+        else if (!strcmp(key, "HUBBLE")) p.hubble = atof_f(value);
+        else if (!strcmp(key, "SS8")) p.ss8 = atof_f(value);
+        else if (!strcmp(key, "NS")) p.ns = atof_f(value);
+        else if (!strcmp(key, "W_DE")) p.w_de = atof_f(value);
+        else if (!strcmp(key, "WA_DE")) p.wa_de = atof_f(value);
+        else if (!strcmp(key, "T_CMB")) p.t_cmb = atof_f(value);
+        else if (!strcmp(key, "N_EFF_MASSLESS")) p.neff_massless = atof_f(value);
+        else if (!strcmp(key, "N_EFF_MASSIVE")) p.neff_massive = atof_f(value);
+        else if (!strcmp(key, "OUTPUT_BASE_NAME")) snprintf(p.prefix, sizeof(p.prefix), "%s", value);
+        else if (!strcmp(key, "Z_IN")) p.z_ini = atof_f(value);
+        else if (!strcmp(key, "Z_FIN")) p.z_fin = atof_f(value);
+        else if (!strcmp(key, "N_STEPS")) p.nsteps = atoi(value);
+        else if (!strcmp(key, "NG")) p.ng = atoi(value);
+        else if (!strcmp(key, "NP")) p.np = atoi(value);
+        else if (!strcmp(key, "RL")) p.rl = atof_f(value);
+        else if (!strcmp(key, "SEED")) p.seed = atoi(value);
+        else if (!strcmp(key, "BLOCK_SIZE")) p.block_size = atoi(value);
+        else if (!strcmp(key, "LAST_STEP")) p.last_step = atoi(value);
+        else if (!strcmp(key, "PK_FOLDS")) p.pk_folds = atoi(value);
+        else if (!strcmp(key, "PK_BINS")) p.pk_bins = atoi(value);
+        else if (!strcmp(key, "PK_LOG")) p.pk_log = atoi(value);
+        else if (!strcmp(key, "REF_QUIRKS")) p.ref_quirks = atoi(value);
+        else if (!strcmp(key, "PK_DUMP")) {
+            int rc = mark_steps(p.pks, value, err, errlen, key);
+            if (rc) return rc;
+        } else if (!strcmp(key, "PARTICLE_DUMP")) {
+            int rc = mark_steps(p.dumps, value, err, errlen, key);
+            if (rc) return rc;
+        } else if (!strcmp(key, "DUMP_INIT")) p.dump_init = 1;
+        else if (!strcmp(key, "DUMP_FINAL")) p.dump_final = 1;
+        else if (!strcmp(key, "IPK")) snprintf(p.ipk, sizeof(p.ipk), "%s", value);
+        else if (!strcmp(key, "OL")) p.ol = atof(value);
+        // unknown keys are ignored, as in the reference
+    }
+    if (p.np == 0) {
+        set_err(err, errlen, "NP missing or zero (params.cpp:228 asserts np != 0)");
+        return HGPM_ERR_ARG;
+    }
+    if (p.last_step == -1) p.last_step = p.nsteps;
+    hgpm_params_derive(&p);
+    *out = p;
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_params_read(const char* path, hgpm_params* out, char* err, size_t errlen) {
+    FILE* f = fopen(path, "rb");
+    if (!f) {
+        set_err(err, errlen, "file %s not found", path);
+        return HGPM_ERR_IO;
+    }
+    std::string text;
+    char buf[4096];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof(buf), f)) > 0) text.append(buf, n);
+    fclose(f);
+    int rc = hgpm_params_parse(text.c_str(), out, err, errlen);
+    if (rc == HGPM_OK) snprintf(out->fname, sizeof(out->fname), "%s", path);
+    return rc;
+}
+
+extern "C" int hgpm_params_save(const hgpm_params* p) {
+    char fname2[400];
+    snprintf(fname2, sizeof(fname2), "%s.params", p->prefix);
+    FILE* fp = fopen(fname2, "w+");
+    if (!fp) return HGPM_ERR_IO;
+    fprintf(fp, "OMEGA_CDM %g\n", p->omega_cdm);
+    fprintf(fp, "DEUT %g\n", p->deut);
+    fprintf(fp, "OMEGA_NU %g\n", p->omega_nu);
+    fprintf(fp, "HUBBLE %g\n", p->hubble);
+    fprintf(fp, "SS8 %g\n", p->ss8);
+    fprintf(fp, "NS %g\n", p->ns);
+    fprintf(fp, "W_DE %g\n", p->w_de);
+    fprintf(fp, "WA_DE %g\n", p->wa_de);
+    fprintf(fp, "T_CMB %g\n", p->t_cmb);
+    fprintf(fp, "N_EFF_MASSLESS %g\n", p->neff_massless);
+    fprintf(fp, "N_EFF_MASSIVE %g\n", p->neff_massive);
+    fprintf(fp, "OMEGA_BARYON %g\n", p->omega_baryon);
+    fprintf(fp, "OMEGA_CB %g\n", p->omega_cb);
+    fprintf(fp, "OMEGA_MATTER %g\n", p->omega_matter);
+    fprintf(fp, "OMEGA_RADIATION %g\n", p->omega_radiation);
+    fprintf(fp, "M_F_NU_MASSLESS %g\n", p->f_nu_massless);
+    fprintf(fp, "M_F_NU_MASSIVE %g\n", p->f_nu_massive);
+    fprintf(fp, "OUTPUT_BASE_NAME %s\n", p->prefix);
+    fprintf(fp, "Z_IN %g\n", p->z_ini);
+    fprintf(fp, "Z_FIN %g\n", p->z_fin);
+    fprintf(fp, "N_STEPS %d\n", p->nsteps);
+    fprintf(fp, "NG %d\n", p->ng);
+    fprintf(fp, "NP %d\n", p->np);
+    fprintf(fp, "RL %g\n", p->rl);
+    fprintf(fp, "SEED %d\n", p->seed);
+    fprintf(fp, "BLOCK_SIZE %d\n", p->block_size);
+    fprintf(fp, "PK_FOLDS %d\n", p->pk_folds);
+    fclose(fp);
+    return HGPM_OK;
+}
+
+// ===========================================================================
+// time stepper (src/simulation/timestepper.cpp:7-68)
+// ===========================================================================
+static double omega_nu_massive(double a, const hgpm_params* p) {
+    double mat = p->omega_nu / pow(a, 3.0);
+    double rad = p->f_nu_massive * p->omega_radiation / pow(a, 4.0);
+    return (mat >= rad) * mat + (rad > mat) * rad;
+}
+
+extern "C" double hgpm_get_adot(double aa, const hgpm_params* p) {
+    double pp1 = pow(aa, -3.0 * (p->w_de + p->wa_de)) * exp(-3.0 * p->wa_de * (1.0 - aa));
+    double tmp = p->omega_cb + (1.0 + p->f_nu_massless) * p->omega_radiation / aa +
+                 omega_nu_massive(aa, p) * pow(aa, 3.0) +
+                 (1.0 - p->omega_matter - (1.0 + p->f_nu_massless) * p->omega_radiation) * pp1;
+    tmp /= aa;
+    return sqrt(tmp);
+}
+
+extern "C" double hgpm_get_fscal(double aa, double adot, double omega_cb, int ref_quirks) {
+    double dtdy = aa / (aa * adot);
+    if (ref_quirks) dtdy = (double)(float)dtdy;  // timestepper.cpp:24 `float dtdy`
+    double phiscal = 1.5 * omega_cb;
+    return phiscal * dtdy * (1.0 / aa);
+}
+
+static void ts_update(hgpm_timestepper* ts) {
+    ts->z = (1.0f / ts->aa) - 1;
+    ts->adot = hgpm_get_adot(ts->aa, &ts->params);
+    ts->fscal = hgpm_get_fscal(ts->aa, ts->adot, ts->params.omega_cb, ts->params.ref_quirks);
+}
+
+extern "C" void hgpm_ts_init(hgpm_timestepper* ts, const hgpm_params* p) {
+    memset(ts, 0, sizeof(*ts));
+    ts->params = *p;
+    ts->deltaT = (((1 / (p->z_fin + 1)) - (1 / (p->z_ini + 1))) / (double)p->nsteps);
+}
+extern "C" void hgpm_ts_set_initial_z(hgpm_timestepper* ts, double z) {
+    ts->aa = 1.0 / (z + 1.0);
+    ts_update(ts);
+}
+extern "C" void hgpm_ts_advance_half(hgpm_timestepper* ts) {
+    ts->aa += ts->deltaT * 0.5;
+    ts_update(ts);
+}
+extern "C" void hgpm_ts_reverse_half(hgpm_timestepper* ts) {
+    ts->aa -= ts->deltaT * 0.5;
+    ts_update(ts);
+}
+extern "C" float hgpm_ts_drift_prefactor(const hgpm_timestepper* ts, float frac) {
+    return (float)(((ts->deltaT) / (ts->aa * ts->aa * ts->adot)) * frac);
+}
+
+// ===========================================================================
+// growth factor (src/initial_conditions/cosmo.cpp:81-139)
+// ===========================================================================
+template <class T>
+static T g_da_dtau(T a, T om, T ol) {
+    T d2 = (T)1 + om * (((T)1 / a) - (T)1) + ol * ((a * a) - (T)1);
+    return std::sqrt(d2);
+}
+template <class T>
+static T g_da_dtau3(T a, T om, T ol) {
+    T d1 = g_da_dtau(a, om, ol);
+    return (T)1 / (d1 * d1 * d1);
+}
+template <class T>
+static T g_int(T a, T om, T ol, int bins) {
+    T start = 0, end = a;
+    T delta = (end - start) / ((T)bins);
+    T sum = 0;
+    for (int k = 1; k < bins; ++k) sum += g_da_dtau3(start + ((T)k) * delta, om, ol);
+    sum += (g_da_dtau3(start, om, ol) + g_da_dtau3(end, om, ol)) / (T)2;
+    sum *= delta;
+    return sum;
+}
+template <class T>
+static T g_delta(T a, T om, T ol, int bins) {
+    T integral = g_int(a, om, ol, bins);
+    T diff = g_da_dtau(a, om, ol);
+    T mul = ((T)5 * om) / ((T)2 * a);
+    return mul * diff * integral;
+}
+
+extern "C" void hgpm_growth(const hgpm_params* p, double z, double z_vel, double* delta, double* dot_delta) {
+    if (p->ref_quirks) {
+        // the reference's CosmoClass: float arithmetic, 100-bin trapezoid,
+        // central difference with h = 1e-4 (cosmo.cpp:106-139)
+        float om = (float)p->omega_matter;
+        float ol = 1 - (om + (float)p->omega_nu);
+        float a0 = 1.0f / (1.0f + (float)z);
+        float a1 = 1.0f / (1.0f + (float)z_vel);
+        float h = 0.0001f;
+        *delta = g_delta<float>(a0, om, ol, 100);
+        *dot_delta = (g_delta<float>(a1 + h, om, ol, 100) - g_delta<float>(a1 - h, om, ol, 100)) / (2.0f * h);
+    } else {
+        // FP64: the same integral with 20000 trapezoid bins and h = 1e-6
+        double om = p->omega_matter;
+        double ol = 1 - (om + p->omega_nu);
+        double a0 = 1.0 / (1.0 + z), a1 = 1.0 / (1.0 + z_vel), h = 1e-6;
+        *delta = g_delta<double>(a0, om, ol, 20000);
+        *dot_delta = (g_delta<double>(a1 + h, om, ol, 20000) - g_delta<double>(a1 - h, om, ol, 20000)) / (2.0 * h);
+    }
+}
+
+// ===========================================================================
+// context
+// ===========================================================================
+struct PhaseRec {
+    int phase;
+    cudaEvent_t a, b;
+};
+
+struct hgpm_ctx {
+    hgpm_params p;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int ng = 0, np = 0, zs = 0, zs_np = 0;
+    size_t ncell = 0, npart = 0, nspec = 0;
+    ParticleSoA part{};
+    void* part_block = nullptr;
+    unsigned long long* rho64 = nullptr;
+    bool rho_dirty = false;
+    float2* spec = nullptr;
+    float2* fspec = nullptr;
+    float* force = nullptr;
+    float2* tw_ng = nullptr;
+    float2* tw_np = nullptr;
+    double* cosq = nullptr;
+    float* sk = nullptr;
+    float* pkw = nullptr;
+    float* kf_pk = nullptr;
+    float* kf_ic = nullptr;
+    int* d_err = nullptr;
+    float* stage = nullptr;     // AoS float3 x, v staging (lazy)
+    double* pk_part = nullptr;  // P(k) partial sums (lazy)
+    unsigned long long* pk_pcnt = nullptr;
+    double* pk_sum = nullptr;
+    unsigned long long* pk_cnt = nullptr;
+    int pk_nparts = 0;
+    bool have_state = false;
+    bool timing = false;
+    std::vector<PhaseRec> recs;
+    std::vector<cudaEvent_t> free_events;
+    double phase_ms[HGPM_NPHASE] = {0};
+    int64_t phase_launch[HGPM_NPHASE] = {0};
+    int64_t launches = 0;
+    std::string err;
+};
+
+static int fail(hgpm_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return fail(c, e_ == cudaErrorMemoryAllocation ? HGPM_ERR_OOM : HGPM_ERR_CUDA,        \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+static cudaEvent_t take_event(hgpm_ctx* c) {
+    if (!c->free_events.empty()) {
+        cudaEvent_t e = c->free_events.back();
+        c->free_events.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+struct PhaseScope {
+    hgpm_ctx* c;
+    int phase;
+    cudaEvent_t a = nullptr;
+    PhaseScope(hgpm_ctx* c_, int ph) : c(c_), phase(ph) {
+        if (c->timing) {
+            a = take_event(c);
+            cudaEventRecord(a, c->stream);
+        }
+    }
+    ~PhaseScope() {
+        if (c->timing) {
+            cudaEvent_t b = take_event(c);
+            cudaEventRecord(b, c->stream);
+            c->recs.push_back({phase, a, b});
+        }
+    }
+};
+
+static void count(hgpm_ctx* c, int phase, int n) {
+    c->launches += n;
+    c->phase_launch[phase] += n;
+}
+
+enum { PH_DRIFT = 0, PH_DEPOSIT, PH_ZFWD, PH_YFWD, PH_POISSON, PH_YINV, PH_ZINV, PH_KICK, PH_PK };
+static_assert(PH_PK + 1 == HGPM_NPHASE, "phase ids");
+
+static std::vector<float2> twiddles(int n) {
+    std::vector<float2> t(n);
+    for (int m = 0; m < n; ++m) {
+        double ang = -2.0 * M_PI * (double)m / (double)n;
+        t[m] = make_float2((float)cos(ang), (float)sin(ang));
+    }
+    return t;
+}
+
+static int even_pad(int v) { return (v + 15) / 16 * 16; }
+
+extern "C" size_t hgpm_footprint_bytes(int ng, int np) {
+    size_t ncell = (size_t)ng * ng * ng, npart = (size_t)np * np * np;
+    size_t zs = even_pad(ng / 2 + 1);
+    size_t nspec = (size_t)ng * ng * zs;
+    size_t b = 0;
+    b += npart * 7 * 4;        // particle SoA
+    b += ncell * 8;            // int64 density
+    b += nspec * 8 * 4;        // spectrum + 3 force spectra
+    b += ncell * 4 * 3;        // force grids
+    b += (size_t)ng * 64;      // tables
+    return b;
+}
+
+extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
+    if (!p || !out) return HGPM_ERR_ARG;
+    *out = nullptr;
+    hgpm_ctx* c = new hgpm_ctx();
+    c->p = *p;
+    c->device = device;
+    c->ng = p->ng;
+    c->np = p->np;
+    auto bad = [&](int code, const char* msg) {
+        c->err = msg;
+        *out = c;  // return the context so the caller can read the message
+        return code;
+    };
+    if (!fft_size_supported(p->ng)) return bad(HGPM_ERR_ARG, "NG must be one of 16,24,32,48,64,96,128,192,256,384,512,768,1024");
+    if (!fft_size_supported(p->np)) return bad(HGPM_ERR_ARG, "NP must be one of 16,24,32,48,64,96,128,192,256,384,512,768,1024");
+    if (p->rl <= 0) return bad(HGPM_ERR_ARG, "RL must be positive");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return bad(HGPM_ERR_CUDA, cudaGetErrorString(e));
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bad(HGPM_ERR_CUDA, cudaGetErrorString(e));
+    c->ncell = (size_t)c->ng * c->ng * c->ng;
+    c->npart = (size_t)c->np * c->np * c->np;
+    c->zs = even_pad(c->ng / 2 + 1);
+    c->zs_np = even_pad(c->np / 2 + 1);
+    c->nspec = (size_t)c->ng * c->ng * c->zs;
+    size_t nspec_np = (size_t)c->np * c->np * c->zs_np;
+    size_t spec_elems = std::max(c->nspec, nspec_np);
+    size_t force_elems = 3 * std::max(c->ncell, c->npart);
+    int rc = HGPM_OK;
+    do {
+        // particles: one block, 7 arrays of npart 4-byte words (256-B aligned)
+        size_t stride = (c->npart * 4 + 255) / 256 * 256;
+        e = cudaMalloc(&c->part_block, stride * 7);
+        if (e != cudaSuccess) break;
+        char* b = (char*)c->part_block;
+        c->part.cell = (uint32_t*)(b);
+        c->part.ox = (float*)(b + stride);
+        c->part.oy = (float*)(b + 2 * stride);
+        c->part.oz = (float*)(b + 3 * stride);
+        c->part.vx = (float*)(b + 4 * stride);
+        c->part.vy = (float*)(b + 5 * stride);
+        c->part.vz = (float*)(b + 6 * stride);
+        if ((e = cudaMalloc(&c->rho64, c->ncell * 8)) != cudaSuccess) break;
+        if ((e = cudaMemsetAsync(c->rho64, 0, c->ncell * 8, c->stream)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&c->spec, spec_elems * 8)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&c->fspec, 3 * spec_elems * 8)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&c->force, force_elems * 4)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&c->tw_ng, c->ng * 8)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&c->tw_np, c->np * 8)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&c->cosq, c->ng * 8)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&c->sk, c->ng * 4)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&c->pkw, c->ng * 4)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&c->kf_pk, c->ng * 4)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&c->kf_ic, c->np * 4)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&c->d_err, 4)) != cudaSuccess) break;
+        std::vector<float2> t1 = twiddles(c->ng), t2 = twiddles(c->np);
+        if ((e = cudaMemcpy(c->tw_ng, t1.data(), c->ng * 8, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+        if ((e = cudaMemcpy(c->tw_np, t2.data(), c->np * 8, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+        if ((e = launch_ktables(c->ng, c->cosq, c->sk, c->pkw, c->stream)) != cudaSuccess) break;
+        if (!p->ref_quirks) {
+            std::vector<double> cq(c->ng);
+            for (int i = 0; i < c->ng; ++i) {
+                double s = sin(M_PI * (double)i / (double)c->ng);
+                cq[i] = -2.0 * s * s;  // cos(2 pi i/ng) - 1
+            }
+            if ((e = cudaMemcpyAsync(c->cosq, cq.data(), c->ng * 8, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess) break;
+        }
+        std::vector<float> kf(c->ng), kfi(c->np);
+        double dpk = 2.0 * M_PI / p->rl;
+        for (int i = 0; i < c->ng; ++i) kf[i] = (float)((double)signed_mode(i, c->ng) * dpk);
+        for (int i = 0; i < c->np; ++i) kfi[i] = (float)((double)signed_mode(i, c->np) * dpk);
+        if ((e = cudaMemcpy(c->kf_pk, kf.data(), c->ng * 4, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+        if ((e = cudaMemcpy(c->kf_ic, kfi.data(), c->np * 4, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+        if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) break;
+    } while (0);
+    if (e != cudaSuccess) {
+        rc = e == cudaErrorMemoryAllocation ? HGPM_ERR_OOM : HGPM_ERR_CUDA;
+        c->err = std::string("hgpm_create: ") + cudaGetErrorString(e);
+        cudaGetLastError();
+    }
+    c->launches += 1;
+    *out = c;
+    return rc;
+}
+
+extern "C" void hgpm_destroy(hgpm_ctx* c) {
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void* ptrs[] = {c->part_block, c->rho64, c->spec, c->fspec, c->force, c->tw_ng, c->tw_np, c->cosq, c->sk,
+                    c->pkw, c->kf_pk, c->kf_ic, c->d_err, c->stage, c->pk_part, c->pk_pcnt, c->pk_sum, c->pk_cnt};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    for (auto& r : c->recs) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : c->free_events) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+extern "C" const char* hgpm_last_error(const hgpm_ctx* c) { return c ? c->err.c_str() : "null context"; }
+extern "C" void* hgpm_stream(hgpm_ctx* c) { return c ? (void*)c->stream : nullptr; }
+extern "C" int hgpm_ng(const hgpm_ctx* c) { return c ? c->ng : 0; }
+extern "C" int hgpm_np(const hgpm_ctx* c) { return c ? c->np : 0; }
+
+extern "C" int hgpm_sync(hgpm_ctx* c) {
+    if (!c) return HGPM_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    return HGPM_OK;
+}
+
+// ===========================================================================
+// state I/O
+// ===========================================================================
+static int ensure_stage(hgpm_ctx* c) {
+    if (!c->stage) CK(cudaMalloc(&c->stage, c->npart * 6 * sizeof(float)));
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_load_state_device(hgpm_ctx* c, const float* x, const float* v) {
+    if (!c || !x || !v) return HGPM_ERR_ARG;
+    CK(launch_load_state(x, v, c->part, c->npart, c->ng, c->stream));
+    count(c, PH_DRIFT, 1);
+    c->have_state = true;
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_store_state_device(hgpm_ctx* c, float* x, float* v) {
+    if (!c || !x || !v) return HGPM_ERR_ARG;
+    if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
+    CK(launch_store_state(c->part, x, v, c->npart, c->stream));
+    count(c, PH_DRIFT, 1);
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_load_state(hgpm_ctx* c, const float* x, const float* v) {
+    if (!c || !x || !v) return HGPM_ERR_ARG;
+    int rc = ensure_stage(c);
+    if (rc) return rc;
+    size_t bytes = c->npart * 3 * sizeof(float);
+    CK(cudaMemcpyAsync(c->stage, x, bytes, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->stage + 3 * c->npart, v, bytes, cudaMemcpyHostToDevice, c->stream));
+    rc = hgpm_load_state_device(c, c->stage, c->stage + 3 * c->npart);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_store_state(hgpm_ctx* c, float* x, float* v) {
+    if (!c || !x || !v) return HGPM_ERR_ARG;
+    int rc = ensure_stage(c);
+    if (rc) return rc;
+    rc = hgpm_store_state_device(c, c->stage, c->stage + 3 * c->npart);
+    if (rc) return rc;
+    size_t bytes = c->npart * 3 * sizeof(float);
+    CK(cudaMemcpyAsync(x, c->stage, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(v, c->stage + 3 * c->npart, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_get_cells(hgpm_ctx* c, int32_t* cells) {
+    if (!c || !cells) return HGPM_ERR_ARG;
+    if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
+    std::vector<uint32_t> packed(c->npart);
+    CK(cudaMemcpyAsync(packed.data(), c->part.cell, c->npart * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < c->npart; ++i) {
+        uint32_t q = packed[i];
+        cells[i] = (cell_x(q) * c->ng + cell_y(q)) * c->ng + cell_z(q);
+    }
+    return HGPM_OK;
+}
+
+// ===========================================================================
+// phases
+// ===========================================================================
+extern "C" int hgpm_drift(hgpm_ctx* c, float prefactor) {
+    if (!c) return HGPM_ERR_ARG;
+    if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
+    PhaseScope ps(c, PH_DRIFT);
+    CK(launch_drift(c->part, c->npart, c->ng, prefactor, c->stream));
+    count(c, PH_DRIFT, 1);
+    return HGPM_OK;
+}
+
+static float cic_mass(int ng, int np) {
+    // pm_actions.cpp:229-230
+    float gpscale = (((float)ng / (float)np));
+    return gpscale * gpscale * gpscale;
+}
+
+static double mean_density(const hgpm_ctx* c) {
+    return (double)cic_mass(c->ng, c->np) * (double)c->npart / (double)c->ncell;
+}
+
+static int deposit_impl(hgpm_ctx* c) {
+    if (c->rho_dirty) CK(cudaMemsetAsync(c->rho64, 0, c->ncell * 8, c->stream));
+    CK(launch_deposit(c->part, c->npart, c->ng, cic_mass(c->ng, c->np), c->rho64, c->stream));
+    count(c, PH_DEPOSIT, 1);
+    c->rho_dirty = true;
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_deposit(hgpm_ctx* c) {
+    if (!c) return HGPM_ERR_ARG;
+    if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
+    PhaseScope ps(c, PH_DEPOSIT);
+    return deposit_impl(c);
+}
+
+extern "C" int hgpm_get_density(hgpm_ctx* c, float* rho) {
+    if (!c || !rho) return HGPM_ERR_ARG;
+    if (!c->rho_dirty) return fail(c, HGPM_ERR_STATE, "no deposited density (call hgpm_deposit first)");
+    std::vector<long long> h(c->ncell);
+    CK(cudaMemcpyAsync(h.data(), c->rho64, c->ncell * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < c->ncell; ++i) rho[i] = (float)((double)h[i] * kFixInv);
+    return HGPM_OK;
+}
+
+// forward z + y passes of the fixed-point density into c->spec (consumes and
+// zeroes the accumulator)
+static int forward_zy(hgpm_ctx* c) {
+    const int ng = c->ng, M = ng / 2;
+    {
+        PhaseScope ps(c, PH_ZFWD);
+        CK(launch_zfwd(ng, c->rho64, true, c->spec, ng * ng, c->zs, mean_density(c), c->tw_ng, c->stream));
+        c->rho_dirty = false;
+        count(c, PH_ZFWD, 1);
+    }
+    {
+        PhaseScope ps(c, PH_YFWD);
+        CK(launch_strided(ng, false, c->spec, M + 1, (size_t)c->zs, (size_t)ng * c->zs, ng, 0, 1, c->tw_ng, c->stream));
+        count(c, PH_YFWD, 1);
+    }
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_solve_gradient(hgpm_ctx* c) {
+    if (!c) return HGPM_ERR_ARG;
+    if (!c->rho_dirty) return fail(c, HGPM_ERR_STATE, "no deposited density (call hgpm_deposit first)");
+    const int ng = c->ng, M = ng / 2;
+    int rc = forward_zy(c);
+    if (rc) return rc;
+    const size_t cs = (size_t)ng * ng * c->zs;
+    {
+        PhaseScope ps(c, PH_POISSON);
+        CK(launch_xpoisson(ng, c->spec, c->fspec, M + 1, (size_t)ng * c->zs, (size_t)c->zs, ng, cs, c->tw_ng, c->cosq,
+                           c->sk, 0.5 / ((double)ng * ng * ng), c->stream));
+        count(c, PH_POISSON, 1);
+    }
+    {
+        PhaseScope ps(c, PH_YINV);
+        CK(launch_strided(ng, true, c->fspec, M + 1, (size_t)c->zs, (size_t)ng * c->zs, ng, cs, 3, c->tw_ng, c->stream));
+        count(c, PH_YINV, 1);
+    }
+    {
+        PhaseScope ps(c, PH_ZINV);
+        CK(launch_zinv(ng, c->fspec, c->force, ng * ng, c->zs, cs, c->ncell, 3, 1.0f, c->tw_ng, c->stream));
+        count(c, PH_ZINV, 1);
+    }
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_get_force(hgpm_ctx* c, float* f) {
+    if (!c || !f) return HGPM_ERR_ARG;
+    CK(cudaMemcpyAsync(f, c->force, c->ncell * 3 * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_kick_drift(hgpm_ctx* c, double deltaT, double fscal, float pf_a, float pf_b, int ndrift) {
+    if (!c || ndrift < 0 || ndrift > 2) return HGPM_ERR_ARG;
+    if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
+    PhaseScope ps(c, PH_KICK);
+    CK(launch_kick_drift(c->part, c->npart, c->ng, c->force, c->force + c->ncell, c->force + 2 * c->ncell, deltaT,
+                         fscal, pf_a, pf_b, ndrift, c->stream));
+    count(c, PH_KICK, 1);
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_kick(hgpm_ctx* c, double deltaT, double fscal) {
+    return hgpm_kick_drift(c, deltaT, fscal, 0.f, 0.f, 0);
+}
+
+extern "C" int hgpm_run_steps(hgpm_ctx* c, hgpm_timestepper* ts, int nsteps) {
+    if (!c || !ts || nsteps < 0) return HGPM_ERR_ARG;
+    if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
+    if (nsteps == 0) return HGPM_OK;
+    int rc = hgpm_drift(c, hgpm_ts_drift_prefactor(ts, 0.5f));  // driver_pm.cpp:114
+    if (rc) return rc;
+    for (int step = 0; step < nsteps; ++step) {
+        if ((rc = hgpm_deposit(c))) return rc;                   // :116
+        if ((rc = hgpm_solve_gradient(c))) return rc;            // :117
+        hgpm_ts_advance_half(ts);                                // :119
+        const double dt = ts->deltaT, fs = ts->fscal;
+        hgpm_ts_advance_half(ts);                                // :123
+        const float pf = hgpm_ts_drift_prefactor(ts, 0.5f);      // :125 and the next step's :114
+        if ((rc = hgpm_kick_drift(c, dt, fs, pf, pf, step + 1 < nsteps ? 2 : 1))) return rc;  // :121, :125
+    }
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_step_host(hgpm_ctx* c, hgpm_timestepper* ts, float* x, float* v) {
+    int rc = hgpm_load_state(c, x, v);
+    if (rc) return rc;
+    if ((rc = hgpm_run_steps(c, ts, 1))) return rc;
+    return hgpm_store_state(c, x, v);
+}
+
+// ===========================================================================
+// power spectrum
+// ===========================================================================
+static int pk_bins_setup(const hgpm_ctx* c, int nbins, int log_bins, double* min_k, double* bin_delta,
+                         std::vector<double>& centres) {
+    // power.cu:174-187 (fold 0): minK = 2pi/rl, maxK = sqrt(3 (ng/2)^2 d^2)
+    double d = (2 * M_PI) / c->p.rl;
+    double mk = d;
+    double maxk = sqrt(3 * ((c->ng / 2) * (c->ng / 2) * d * d));
+    centres.resize(nbins);
+    if (log_bins) {
+        double dl = log(maxk / mk) / (double)nbins;
+        for (int i = 0; i < nbins; ++i) centres[i] = mk * exp(dl * ((double)i + 0.5));
+        *bin_delta = dl;
+    } else {
+        double bd = (maxk - mk) / ((double)nbins);
+        for (int i = 0; i < nbins; ++i) centres[i] = mk + bd * (((float)i) + 0.5f);
+        *bin_delta = bd;
+    }
+    *min_k = mk;
+    return 0;
+}
+
+extern "C" int hgpm_power_spectrum(hgpm_ctx* c, int nbins, int log_bins, double* k_out, double* pk_out,
+                                   int64_t* n_out) {
+    if (!c || !k_out || !pk_out || !n_out || nbins <= 0) return HGPM_ERR_ARG;
+    if (nbins > pk_max_bins()) return fail(c, HGPM_ERR_ARG, "nbins %d above %d", nbins, pk_max_bins());
+    if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
+    const int ng = c->ng, M = ng / 2;
+    if (!c->pk_part) {
+        c->pk_nparts = 4 * 148;
+        CK(cudaMalloc(&c->pk_part, (size_t)c->pk_nparts * pk_max_bins() * 8));
+        CK(cudaMalloc(&c->pk_pcnt, (size_t)c->pk_nparts * pk_max_bins() * 8));
+        CK(cudaMalloc(&c->pk_sum, pk_max_bins() * 8));
+        CK(cudaMalloc(&c->pk_cnt, pk_max_bins() * 8));
+    }
+    PhaseScope ps(c, PH_PK);
+    int rc = deposit_impl(c);  // serial::CIC of the positions (power.cu:210)
+    if (rc) return rc;
+    rc = forward_zy(c);
+    if (rc) return rc;
+    PkArgs a;
+    std::vector<double> centres;
+    pk_bins_setup(c, nbins, log_bins, &a.min_k, &a.bin_delta, centres);
+    a.kf = c->kf_pk;
+    a.filt = c->pkw;
+    a.nbins = nbins;
+    a.log_bins = log_bins;
+    a.scale = (1.0f / ((double)ng * ng * ng)) * (c->p.rl / ng);
+    CK(launch_xpk(ng, c->spec, M + 1, (size_t)ng * c->zs, (size_t)c->zs, c->tw_ng, a, c->pk_part, c->pk_pcnt,
+                  c->pk_nparts, c->pk_sum, c->pk_cnt, c->stream));
+    count(c, PH_PK, 2);
+    std::vector<double> sum(nbins);
+    std::vector<unsigned long long> cnt(nbins);
+    CK(cudaMemcpyAsync(sum.data(), c->pk_sum, nbins * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(cnt.data(), c->pk_cnt, nbins * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < nbins; ++i) {
+        k_out[i] = centres[i];
+        n_out[i] = (int64_t)cnt[i];
+        pk_out[i] = cnt[i] ? sum[i] / (double)cnt[i] : 0.0;
+    }
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_write_pk(const char* fname, int nbins, const double* k, const double* pk, const int64_t* count) {
+    char fname2[400];
+    snprintf(fname2, sizeof(fname2), "%s.fold.%d", fname, 0);
+    FILE* fp = fopen(fname2, "w+");
+    if (!fp) return HGPM_ERR_IO;
+    for (int i = 0; i < nbins; ++i) {
+        double o = pk[i];
+        if ((o == o) && (count[i] != 0) && (o != 0)) fprintf(fp, "%g,%g,%d\n", k[i], o, (int)count[i]);
+    }
+    fclose(fp);
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_write_output(hgpm_ctx* c, const char* fname) {
+    if (!c || !fname) return HGPM_ERR_ARG;
+    std::vector<float> x(c->npart * 3), v(c->npart * 3);
+    int rc = hgpm_store_state(c, x.data(), v.data());
+    if (rc) return rc;
+    FILE* fp = fopen(fname, "w+");
+    if (!fp) return fail(c, HGPM_ERR_IO, "cannot open %s", fname);
+    fwrite(x.data(), sizeof(float) * 3, c->npart, fp);
+    fwrite(v.data(), sizeof(float) * 3, c->npart, fp);
+    fclose(fp);
+    return HGPM_OK;
+}
+
+// ===========================================================================
+// initial conditions (src/initial_conditions/initializer.cpp:65-166)
+// ===========================================================================
+extern "C" int hgpm_read_ipk(const char* path, double* header20, double* table, int max_bins, int* nbins) {
+    FILE* f = fopen(path, "rb");
+    if (!f) return HGPM_ERR_IO;
+    double header[20];
+    if (fread(header, sizeof(header), 1, f) != 1) {
+        fclose(f);
+        return HGPM_ERR_IO;
+    }
+    int nb = (int)header[2];
+    if (header20) memcpy(header20, header, sizeof(header));
+    if (nbins) *nbins = nb;
+    if (table) {
+        if (nb > max_bins) {
+            fclose(f);
+            return HGPM_ERR_ARG;
+        }
+        if (fread(table, sizeof(double), nb, f) != (size_t)nb) {
+            fclose(f);
+            return HGPM_ERR_IO;
+        }
+    }
+    fclose(f);
+    return HGPM_OK;
+}
+
+static int ic_common(hgpm_ctx* c, const float* noise_host, const double* table, int nbins, double k_delta) {
+    if (!c || !table || nbins < 2 || k_delta <= 0) return HGPM_ERR_ARG;
+    const int n = c->np, M = n / 2;
+    const size_t npart = c->npart;
+    // time stepper state at the IC epoch (driver_pm.cpp:63-65)
+    hgpm_timestepper ts;
+    hgpm_ts_init(&ts, &c->p);
+    hgpm_ts_set_initial_z(&ts, c->p.z_ini);
+    hgpm_ts_reverse_half(&ts);
+    // initializer.cpp:81-86
+    double this_a = (1 / (c->p.z_ini + 1)) - (ts.deltaT / 2.0f);
+    double velZ = (1.0f / this_a) - 1.0f;
+    double delta, dot_delta;
+    hgpm_growth(&c->p, c->p.z_ini, velZ, &delta, &dot_delta);
+    // table range: the largest |k| on the n^3 grid must sit inside the table
+    double kmax = sqrt(3.0) * (n / 2) * 2 * M_PI / c->p.rl;
+    if ((int)(kmax / k_delta) + 1 >= nbins)
+        return fail(c, HGPM_ERR_ARG, "input ipk only goes to k=%g, grid needs %g", k_delta * (nbins - 1), kmax);
+    double* d_table = nullptr;
+    CK(cudaMalloc(&d_table, (size_t)nbins * 8));
+    int rc = HGPM_OK;
+    do {
+        float* noise = c->force;  // scratch: the force grids are rebuilt every solve
+        cudaError_t e;
+        if (noise_host) {
+            e = cudaMemcpyAsync(noise, noise_host, npart * 4, cudaMemcpyHostToDevice, c->stream);
+        } else {
+            e = launch_noise(noise, npart, (uint32_t)c->p.seed, c->stream);
+            count(c, PH_PK, 1);
+        }
+        if (e != cudaSuccess) { rc = fail(c, HGPM_ERR_CUDA, "ic noise: %s", cudaGetErrorString(e)); break; }
+        if ((e = cudaMemcpyAsync(d_table, table, (size_t)nbins * 8, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess) {
+            rc = fail(c, HGPM_ERR_CUDA, "ic table: %s", cudaGetErrorString(e)); break;
+        }
+        if ((e = cudaMemsetAsync(c->d_err, 0, 4, c->stream)) != cudaSuccess) { rc = fail(c, HGPM_ERR_CUDA, "%s", cudaGetErrorString(e)); break; }
+        const size_t cs = (size_t)n * n * c->zs_np;
+        e = launch_zfwd(n, noise, false, c->spec, n * n, c->zs_np, 0.0, c->tw_np, c->stream);
+        if (e == cudaSuccess) e = launch_strided(n, false, c->spec, M + 1, (size_t)c->zs_np, (size_t)n * c->zs_np, n, 0, 1, c->tw_np, c->stream);
+        if (e == cudaSuccess)
+            e = launch_xic(n, c->spec, c->fspec, M + 1, (size_t)n * c->zs_np, (size_t)c->zs_np, n, cs, c->tw_np, d_table,
+                           nbins, k_delta, ((double)n * n * n) / (c->p.rl * c->p.rl * c->p.rl), 1.0 / delta, c->kf_ic,
+                           c->d_err, c->stream);
+        if (e == cudaSuccess) e = launch_strided(n, true, c->fspec, M + 1, (size_t)c->zs_np, (size_t)n * c->zs_np, n, cs, 3, c->tw_np, c->stream);
+        float scale = (float)(1.0f / ((double)npart));
+        if (e == cudaSuccess) e = launch_zinv(n, c->fspec, c->force, n * n, c->zs_np, cs, npart, 3, scale, c->tw_np, c->stream);
+        // placeParticles: velA = a - deltaT/2 (float), velMul in double then float
+        double a = 1.0 / (1.0 + c->p.z_ini);
+        float velA = a - (ts.deltaT * 0.5f);
+        float velmul = (float)((double)(velA * velA) * dot_delta * ts.fscal);
+        if (e == cudaSuccess) e = launch_place(c->force, npart, c->part, n, c->ng, (float)delta, velmul, c->stream);
+        count(c, PH_PK, 6);
+        if (e != cudaSuccess) { rc = fail(c, HGPM_ERR_CUDA, "ic kernels: %s", cudaGetErrorString(e)); break; }
+        int herr = 0;
+        if ((e = cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(c->stream)) != cudaSuccess) {
+            rc = fail(c, HGPM_ERR_CUDA, "ic sync: %s", cudaGetErrorString(e)); break;
+        }
+        if (herr) { rc = fail(c, HGPM_ERR_ARG, "ipk table too short for the grid's largest |k|"); break; }
+        c->have_state = true;
+    } while (0);
+    cudaFree(d_table);
+    return rc;
+}
+
+extern "C" int hgpm_ic_generate(hgpm_ctx* c, const double* table, int nbins, double k_delta) {
+    return ic_common(c, nullptr, table, nbins, k_delta);
+}
+
+extern "C" int hgpm_ic_from_noise(hgpm_ctx* c, const float* noise, const double* table, int nbins, double k_delta) {
+    if (!noise) return HGPM_ERR_ARG;
+    return ic_common(c, noise, table, nbins, k_delta);
+}
+
+extern "C" int hgpm_ic_noise(hgpm_ctx* c, float* out) {
+    if (!c || !out) return HGPM_ERR_ARG;
+    CK(launch_noise(c->force, c->npart, (uint32_t)c->p.seed, c->stream));
+    count(c, PH_PK, 1);
+    CK(cudaMemcpyAsync(out, c->force, c->npart * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return HGPM_OK;
+}
+
+// ===========================================================================
+// timing
+// ===========================================================================
+extern "C" int hgpm_enable_timing(hgpm_ctx* c, int on) {
+    if (!c) return HGPM_ERR_ARG;
+    c->timing = on != 0;
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_phase_times(hgpm_ctx* c, double* ms, int64_t* launches) {
+    if (!c) return HGPM_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    for (auto& r : c->recs) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, r.a, r.b);
+        c->phase_ms[r.phase] += t;
+        c->free_events.push_back(r.a);
+        c->free_events.push_back(r.b);
+    }
+    c->recs.clear();
+    for (int i = 0; i < HGPM_NPHASE; ++i) {
+        if (ms) ms[i] = c->phase_ms[i];
+        if (launches) launches[i] = c->phase_launch[i];
+        c->phase_ms[i] = 0.0;
+        c->phase_launch[i] = 0;
+    }
+    return HGPM_OK;
+}
+
+extern "C" int64_t hgpm_kernel_launches(hgpm_ctx* c, int reset) {
+    if (!c) return 0;
+    int64_t n = c->launches;
+    if (reset) c->launches = 0;
+    return n;
+}
+
+extern "C" size_t hgpm_sizeof_params(void) { return sizeof(hgpm_params); }
+extern "C" size_t hgpm_sizeof_timestepper(void) { return sizeof(hgpm_timestepper); }

@@ -1,0 +1,201 @@
+/*
+ * hgpm_c.h — C-ABI of the B200-native particle-mesh step (drop-in for the
+ * serial path of HACC_GPM).
+ *
+ * Plain C types only: opaque context handle, plain pointers and sizes, int
+ * status returns (HGPM_OK == 0), no exits.  Every call is stream-ordered on
+ * the context's CUDA stream; calls that take HOST pointers synchronise that
+ * stream before returning.  Error text for the last failure on a context is
+ * available from hgpm_last_error().
+ *
+ * Each entry point names the reference interface it replaces
+ * (file:line within the HACC_GPM project).
+ */
+#ifndef HGPM_C_H
+#define HGPM_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define HGPM_OK 0
+#define HGPM_ERR_ARG 1         /* invalid argument or unsupported size     */
+#define HGPM_ERR_CUDA 2        /* CUDA runtime error (message has details) */
+#define HGPM_ERR_IO 3          /* file missing / malformed                  */
+#define HGPM_ERR_OOM 4         /* device allocation failed                  */
+#define HGPM_ERR_STATE 5       /* call order violated (e.g. no particles)   */
+
+#define HGPM_MAX_STEPS 1000    /* src/haccgpm.hpp:106 */
+#define HGPM_MAX_NG 1024       /* largest grid side (10-bit packed cell)    */
+#define HGPM_PATH_MAX 300      /* char[300] fields of HACCGPM::Params       */
+
+/* ---- run parameters ----------------------------------------------------
+ * Mirror of HACCGPM::Params (src/haccgpm.hpp:118-174), serial fields only.
+ * Cosmology values are stored as double after float rounding, exactly as
+ * read_params does (params.cpp:109 `float val = atof(value)`).            */
+typedef struct hgpm_params {
+    char fname[HGPM_PATH_MAX];
+    char prefix[HGPM_PATH_MAX];     /* OUTPUT_BASE_NAME */
+    char ipk[HGPM_PATH_MAX];        /* IPK */
+    int ng, np;
+    double rl;
+    int block_size;
+    int seed;
+    double z_ini, z_fin;
+    int nsteps;
+    int last_step;                  /* LAST_STEP (defaults to nsteps) */
+    int pk_folds;
+    int pk_bins;                    /* PK_BINS (new key; reference fixes 221) */
+    int pk_log;                     /* PK_LOG (new key; 1 = log-spaced bins)  */
+    double ol;
+    int overload;
+    double hubble, omega_cdm, omega_nu, deut, ss8, ns, w_de, wa_de, t_cmb;
+    double neff_massless, neff_massive;
+    /* derived (params.cpp:237-245) */
+    double omega_baryon, omega_cb, omega_matter, omega_radiation;
+    double f_nu_massless, f_nu_massive;
+    unsigned char pks[HGPM_MAX_STEPS];
+    unsigned char dumps[HGPM_MAX_STEPS];
+    int dump_init, dump_final;
+    int ref_quirks;                 /* 1 (default): float dtdy / float growth
+                                       exactly as the reference; 0: FP64    */
+} hgpm_params;
+
+/* Replaces HACCGPM::read_params (src/simulation/params.cpp:72-250).
+ * Does not print or write the .params echo; see hgpm_params_save.        */
+int hgpm_params_read(const char* path, hgpm_params* out, char* err, size_t errlen);
+/* Parse params from a string (same grammar as hgpm_params_read).          */
+int hgpm_params_parse(const char* text, hgpm_params* out, char* err, size_t errlen);
+/* Recompute derived fields (params.cpp:237-245).                          */
+void hgpm_params_derive(hgpm_params* p);
+/* Replaces save_params (src/simulation/params.cpp:6-39): writes
+ * "<prefix>.params" byte-compatible with the reference.                   */
+int hgpm_params_save(const hgpm_params* p);
+
+/* ---- time stepper ------------------------------------------------------
+ * Replaces HACCGPM::Timestepper (src/simulation/timestepper.cpp:31-68),
+ * get_adot (:13-21) and get_fscal (:23-28).  Host-side FP64.              */
+typedef struct hgpm_timestepper {
+    double aa, z, deltaT, adot, fscal;
+    hgpm_params params;
+} hgpm_timestepper;
+
+void hgpm_ts_init(hgpm_timestepper* ts, const hgpm_params* p);
+void hgpm_ts_set_initial_z(hgpm_timestepper* ts, double z);
+void hgpm_ts_advance_half(hgpm_timestepper* ts);
+void hgpm_ts_reverse_half(hgpm_timestepper* ts);
+/* pm_actions.cpp:291: float prefactor = deltaT/(a*a*adot)*frac            */
+float hgpm_ts_drift_prefactor(const hgpm_timestepper* ts, float frac);
+double hgpm_get_adot(double aa, const hgpm_params* p);
+double hgpm_get_fscal(double aa, double adot, double omega_cb, int ref_quirks);
+
+/* Linear growth and its derivative at the IC epochs.
+ * Replaces CosmoClass::get_delta_and_dotDelta (cosmo.cpp:133-139).        */
+void hgpm_growth(const hgpm_params* p, double z, double z_vel, double* delta, double* dot_delta);
+
+/* ---- context (device memory + stream) ----------------------------------
+ * Replaces serial::MemoryManager (src/simulation/cuda/mmanager.cu:93-179)
+ * and serial::fft_cache_plan (src/fft_tools/cuda/ffts.cu:136).            */
+typedef struct hgpm_ctx hgpm_ctx;
+
+int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out);
+void hgpm_destroy(hgpm_ctx* ctx);
+const char* hgpm_last_error(const hgpm_ctx* ctx);
+/* Device bytes a context of this size holds (mem_calc.py:41-95 analogue). */
+size_t hgpm_footprint_bytes(int ng, int np);
+/* The CUDA stream (cudaStream_t) all work of this context is ordered on.   */
+void* hgpm_stream(hgpm_ctx* ctx);
+int hgpm_sync(hgpm_ctx* ctx);
+int hgpm_ng(const hgpm_ctx* ctx);
+int hgpm_np(const hgpm_ctx* ctx);
+
+/* ---- particle state ------------------------------------------------------
+ * Host buffers in the reference layout: float3 x[np^3], float3 v[np^3]
+ * (particle_t = float3, src/haccgpm.hpp:76-80), grid units, x in [0, ng).
+ * Inside the context positions are an int32 packed cell plus an FP32
+ * in-cell offset, so precision does not degrade with the box side.        */
+int hgpm_load_state(hgpm_ctx* ctx, const float* x_host, const float* v_host);
+int hgpm_store_state(hgpm_ctx* ctx, float* x_host, float* v_host);
+/* Same as above, but pointers are DEVICE pointers (stream-ordered).        */
+int hgpm_load_state_device(hgpm_ctx* ctx, const float* x_dev, const float* v_dev);
+int hgpm_store_state_device(hgpm_ctx* ctx, float* x_dev, float* v_dev);
+/* Linear cell index (ix*ng+iy)*ng+iz of every particle's CIC base cell
+ * (the reference's `int i = x` truncation, cic_pm.cu:52-54).              */
+int hgpm_get_cells(hgpm_ctx* ctx, int32_t* cells_host);
+
+/* ---- PM phases -----------------------------------------------------------*/
+/* serial::UpdatePositions (pm_actions.cpp:287-314, update_positions_pm.cu:3-20) */
+int hgpm_drift(hgpm_ctx* ctx, float prefactor);
+/* serial::CIC (pm_actions.cpp:221-258, cic_pm.cu:46-87): deterministic
+ * fixed-point int64 deposit; the density is bit-exact run to run.         */
+int hgpm_deposit(hgpm_ctx* ctx);
+/* Density after hgpm_deposit, float ng^3 (Re of the reference's d_grid).  */
+int hgpm_get_density(hgpm_ctx* ctx, float* rho_host);
+/* serial::SolveGradient (solver.cpp:144-170): R2C FFT, fused Green's
+ * function and -i sin(k) gradient, 3 C2R FFTs -> force grids.            */
+int hgpm_solve_gradient(hgpm_ctx* ctx);
+/* Force grids, float 3*ng^3 (x, y, z components; d_grad.xyz).             */
+int hgpm_get_force(hgpm_ctx* ctx, float* force_host);
+/* serial::UpdateVelocities (pm_actions.cpp:260-285, icic_pm.cu:72-127).    */
+int hgpm_kick(hgpm_ctx* ctx, double deltaT, double fscal);
+/* Fused CIC gather + kick + ndrift (0..2) drifts with prefactors pf_a, pf_b:
+ * the reference's UpdateVelocities followed by UpdatePositions calls.     */
+int hgpm_kick_drift(hgpm_ctx* ctx, double deltaT, double fscal, float pf_a, float pf_b, int ndrift);
+/* nsteps whole DKD steps (driver_pm.cpp:114-125), advancing *ts exactly as
+ * the reference's loop does; consecutive drifts are fused.                */
+int hgpm_run_steps(hgpm_ctx* ctx, hgpm_timestepper* ts, int nsteps);
+/* One step with the particle state in HOST buffers (reference layout):
+ * copies in, runs hgpm_run_steps(ctx, ts, 1), copies out.                 */
+int hgpm_step_host(hgpm_ctx* ctx, hgpm_timestepper* ts, float* x_host, float* v_host);
+
+/* ---- power spectrum ------------------------------------------------------
+ * serial::GetPowerSpectrum fold 0 (power.cu:152-246 with scale_power.cu,
+ * filter_power.cu, bin_power.cu): nbins bins (linear as the reference, or
+ * log-spaced when log_bins), FP64 shell sums, deterministic.  Outputs are
+ * host arrays of nbins: bin centre k, P(k) (0 where empty), mode count.  */
+int hgpm_power_spectrum(hgpm_ctx* ctx, int nbins, int log_bins, double* k_host,
+                        double* pk_host, int64_t* count_host);
+/* Writes "<fname>.fold.0" lines "%g,%g,%d" (power.cu:13-28).               */
+int hgpm_write_pk(const char* fname, int nbins, const double* k, const double* pk,
+                  const int64_t* count);
+/* serial::writeOutput (io.cu:12-44): raw float3 x then float3 v.           */
+int hgpm_write_output(hgpm_ctx* ctx, const char* fname);
+
+/* ---- initial conditions -------------------------------------------------
+ * serial::GenerateDisplacementIC (initializer.cpp:65-166).  The table is the
+ * .ipk P(k) body (read by hgpm_read_ipk), k_delta its spacing.
+ * hgpm_ic_generate draws the white noise with a counter-based Philox4x32-10
+ * generator keyed by params.seed; hgpm_ic_from_noise takes the noise grid
+ * (float np^3, host) instead, e.g. the reference's own cuRAND draw.        */
+int hgpm_read_ipk(const char* path, double* header20, double* table, int max_bins, int* nbins);
+int hgpm_ic_generate(hgpm_ctx* ctx, const double* table, int nbins, double k_delta);
+int hgpm_ic_from_noise(hgpm_ctx* ctx, const float* noise_host, const double* table,
+                       int nbins, double k_delta);
+/* The Philox white-noise grid hgpm_ic_generate would use (float np^3).     */
+int hgpm_ic_noise(hgpm_ctx* ctx, float* noise_host);
+
+/* ---- phase timing --------------------------------------------------------
+ * When enabled, phases record CUDA events; hgpm_phase_times returns the
+ * accumulated milliseconds per phase and launch counts since the last reset.
+ * One phase per kernel of the step: 0 drift, 1 deposit, 2 fft_z_fwd,
+ * 3 fft_y_fwd, 4 poisson_x (x pass fused with Green's function, gradient
+ * and inverse x), 5 fft_y_inv, 6 fft_z_inv, 7 kick_drift, 8 pk.           */
+#define HGPM_NPHASE 9
+int hgpm_enable_timing(hgpm_ctx* ctx, int on);
+int hgpm_phase_times(hgpm_ctx* ctx, double* ms, int64_t* launches);
+/* Number of kernels this context launched since creation / last reset.    */
+int64_t hgpm_kernel_launches(hgpm_ctx* ctx, int reset);
+
+/* ---- ABI checks ------------------------------------------------------------
+ * sizeof of the public structs, for bindings that mirror them.            */
+size_t hgpm_sizeof_params(void);
+size_t hgpm_sizeof_timestepper(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HGPM_C_H */
