@@ -56,11 +56,11 @@ def alg_bytes(np3, ng3):
 
 KERNEL_NAMES = {
     "deposit": "deposit_kernel",
-    "fft_z_fwd": "zpass_r2c_kernel<512,true>",
-    "fft_y_fwd": "strided_kernel<512,false>",
-    "poisson_x": "xfused_kernel<512,PoissonOp>",
-    "fft_y_inv": "strided_kernel<512,true>",
-    "fft_z_inv": "zpass_c2r_kernel<512>",
+    "fft_z_fwd": "zpass_r2c_kernel<NG,true>",
+    "fft_y_fwd": "strided_kernel<NG,false>",
+    "poisson_x": "xfused_kernel<NG,PoissonOp>",
+    "fft_y_inv": "strided_kernel<NG,true>",
+    "fft_z_inv": "zpass_c2r_kernel<NG>",
     "kick_drift": "kick_drift_kernel",
 }
 
@@ -162,7 +162,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--size", type=int, default=512, help="np = ng (profiling runs use a smaller box)")
     args = ap.parse_args()
+    global NG, NP, RL
+    NG = NP = args.size
+    RL = float(args.size)
     if args.impl == "reference":
         run_reference(args)
         return
@@ -250,14 +254,14 @@ def main():
                      "alg_gbs": b / (avg * 1e-3) / 1e9 if b else 0.0}
     dom = max(phases, key=lambda k: phases[k]["ms_per_launch"])
     d = phases[dom]
-    roofline = {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "phase": dom, "achieved": d["alg_gbs"], "peak": peak,
+    roofline = {"bound": "hbm", "kernel": KERNEL_NAMES[dom].replace("NG", str(NG)), "phase": dom, "achieved": d["alg_gbs"], "peak": peak,
                 "unit": "GB/s", "frac": d["alg_gbs"] / peak, "peak_kind": peak_kind, "traffic": None,
                 "alg_bytes_per_launch": d["alg_bytes"], "ms_per_launch": d["ms_per_launch"]}
     step_ms = ms_max / args.steps
     b_step = 72 * np3 + 64 * ng3
     step_roof = {"alg_bytes_per_step": b_step, "achieved_gbs": b_step / (step_ms * 1e-3) / 1e9,
                  "frac": b_step / (step_ms * 1e-3) / 1e9 / peak, "peak": peak}
-    tp = os.path.join(ROOT, "profiles", "traffic_512.json")
+    tp = os.path.join(ROOT, "profiles", "traffic_%d.json" % NG)
     if os.path.exists(tp):
         with open(tp) as f:
             traf = json.load(f)

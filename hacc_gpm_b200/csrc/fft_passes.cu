@@ -39,24 +39,48 @@ template <int NG> struct Cfg {
 // tile load/store between global strided lines and shared [N][C]
 // ---------------------------------------------------------------------------
 // Rows e in [0, N) at g + e*rs; columns [0, nvalid) valid (nvalid may be < C).
+// All of a thread's global loads are issued before any shared store
+// (register staging) so each CTA keeps its whole tile in flight.
 template <int N, int C>
 __device__ __forceinline__ void load_tile(float2* __restrict__ tile, const float2* __restrict__ g,
                                           size_t rs, int nvalid) {
-    constexpr int TPR = C / 2;
-    for (int i = threadIdx.x; i < N * TPR; i += kThreads) {
-        const int e = i / TPR;
-        const int c = 2 * (i % TPR);
-        const float2* src = g + (size_t)e * rs + c;
-        float4 v;
-        if (c + 1 < nvalid) {
-            v = *reinterpret_cast<const float4*>(src);
-        } else if (c < nvalid) {
-            float2 t = src[0];
-            v = make_float4(t.x, t.y, 0.f, 0.f);
-        } else {
-            v = make_float4(0.f, 0.f, 0.f, 0.f);
+    constexpr int TPR = C / 2;  // float4 (two complex) per row chunk
+    constexpr int TOT = N * TPR;
+    constexpr int PER = (TOT + kThreads - 1) / kThreads;
+    float4 v[PER];
+    if (nvalid >= C) {
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+            const int i = threadIdx.x + t * kThreads;
+            if ((TOT % kThreads) == 0 || i < TOT) {
+                const int e = i / TPR, c = 2 * (i % TPR);
+                v[t] = __ldcs(reinterpret_cast<const float4*>(g + (size_t)e * rs + c));
+            }
         }
-        *reinterpret_cast<float4*>(&tile[e * C + c]) = v;
+    } else {
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+            const int i = threadIdx.x + t * kThreads;
+            v[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if ((TOT % kThreads) == 0 || i < TOT) {
+                const int e = i / TPR, c = 2 * (i % TPR);
+                const float2* src = g + (size_t)e * rs + c;
+                if (c + 1 < nvalid) {
+                    v[t] = *reinterpret_cast<const float4*>(src);
+                } else if (c < nvalid) {
+                    const float2 s = src[0];
+                    v[t] = make_float4(s.x, s.y, 0.f, 0.f);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int i = threadIdx.x + t * kThreads;
+        if ((TOT % kThreads) == 0 || i < TOT) {
+            const int e = i / TPR, c = 2 * (i % TPR);
+            *reinterpret_cast<float4*>(&tile[e * C + c]) = v[t];
+        }
     }
 }
 
@@ -64,15 +88,20 @@ template <int N, int C>
 __device__ __forceinline__ void store_tile(const float2* __restrict__ tile, float2* __restrict__ g,
                                            size_t rs, int nvalid) {
     constexpr int TPR = C / 2;
-    for (int i = threadIdx.x; i < N * TPR; i += kThreads) {
-        const int e = i / TPR;
-        const int c = 2 * (i % TPR);
-        float2* dst = g + (size_t)e * rs + c;
-        const float4 v = *reinterpret_cast<const float4*>(&tile[e * C + c]);
-        if (c + 1 < nvalid) {
-            *reinterpret_cast<float4*>(dst) = v;
-        } else if (c < nvalid) {
-            dst[0] = make_float2(v.x, v.y);
+    constexpr int TOT = N * TPR;
+    constexpr int PER = (TOT + kThreads - 1) / kThreads;
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int i = threadIdx.x + t * kThreads;
+        if ((TOT % kThreads) == 0 || i < TOT) {
+            const int e = i / TPR, c = 2 * (i % TPR);
+            float2* dst = g + (size_t)e * rs + c;
+            const float4 v = *reinterpret_cast<const float4*>(&tile[e * C + c]);
+            if (c + 1 < nvalid) {
+                __stcs(reinterpret_cast<float4*>(dst), v);
+            } else if (c < nvalid) {
+                dst[0] = make_float2(v.x, v.y);
+            }
         }
     }
 }
@@ -89,23 +118,46 @@ __global__ void __launch_bounds__(kThreads) zpass_r2c_kernel(void* __restrict__ 
     constexpr int M = NG / 2, L = Cfg<NG>::L, ES = L + 1;
     float2* buf = reinterpret_cast<float2*>(hgpm_smem);
     const int line0 = blockIdx.x * L;
-    for (int i = threadIdx.x; i < L * M; i += kThreads) {
-        const int l = i / M, m = i % M;
-        const int line = line0 + l;
-        float2 z = make_float2(0.f, 0.f);
-        if (line < nlines) {
-            if (FIX) {
-                ulonglong2* p = reinterpret_cast<ulonglong2*>(reinterpret_cast<unsigned long long*>(in_) +
-                                                              (size_t)line * NG) + m;
-                const ulonglong2 q = *p;
-                z.x = (float)((double)(long long)q.x * kFixInv - mean);
-                z.y = (float)((double)(long long)q.y * kFixInv - mean);
-                *p = make_ulonglong2(0ull, 0ull);
-            } else {
-                z = reinterpret_cast<const float2*>(reinterpret_cast<const float*>(in_) + (size_t)line * NG)[m];
+    constexpr int TOT = L * M;
+    constexpr int PER = (TOT + kThreads - 1) / kThreads;
+    if (FIX) {
+        ulonglong2 q[PER];
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+            const int i = threadIdx.x + t * kThreads;
+            const int l = i / M, m = i % M;
+            q[t] = make_ulonglong2(0ull, 0ull);
+            if (((TOT % kThreads) == 0 || i < TOT) && line0 + l < nlines)
+                q[t] = __ldcs(reinterpret_cast<const ulonglong2*>(reinterpret_cast<unsigned long long*>(in_) +
+                                                                  (size_t)(line0 + l) * NG) + m);
+        }
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+            const int i = threadIdx.x + t * kThreads;
+            const int l = i / M, m = i % M;
+            if (((TOT % kThreads) == 0 || i < TOT)) {
+                if (line0 + l < nlines)
+                    __stcs(reinterpret_cast<ulonglong2*>(reinterpret_cast<unsigned long long*>(in_) +
+                                                         (size_t)(line0 + l) * NG) + m, make_ulonglong2(0ull, 0ull));
+                buf[m * ES + l] = make_float2((float)((double)(long long)q[t].x * kFixInv - mean),
+                                              (float)((double)(long long)q[t].y * kFixInv - mean));
             }
         }
-        buf[m * ES + l] = z;
+    } else {
+        float2 z[PER];
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+            const int i = threadIdx.x + t * kThreads;
+            const int l = i / M, m = i % M;
+            z[t] = make_float2(0.f, 0.f);
+            if (((TOT % kThreads) == 0 || i < TOT) && line0 + l < nlines)
+                z[t] = reinterpret_cast<const float2*>(reinterpret_cast<const float*>(in_) + (size_t)(line0 + l) * NG)[m];
+        }
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+            const int i = threadIdx.x + t * kThreads;
+            if ((TOT % kThreads) == 0 || i < TOT) buf[(i % M) * ES + i / M] = z[t];
+        }
     }
     __syncthreads();
     fft_tile<M, L, ES, false, kThreads, 2>(buf, tw);

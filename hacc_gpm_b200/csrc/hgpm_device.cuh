@@ -33,4 +33,21 @@ struct ParticleSoA {
 // Signed mode index as get_kmodes maps it (src/haccgpm.hpp:255-274).
 __host__ __device__ __forceinline__ int signed_mode(int i, int n) { return i > n / 2 - 1 ? i - n : i; }
 
+// Internal particle order: Lagrangian blocks of B^3 particles stored
+// contiguously (block-major, then x, y, z inside the block), so that one CTA
+// owns a compact patch of space.  The C-ABI exchanges particles in the
+// reference's lattice order q = (qx*np + qy)*np + qz (get_index).
+__host__ __device__ __forceinline__ int block_side(int np, int ng) {
+    return (np % 16 == 0 && ng <= np) ? 16 : 8;
+}
+__host__ __device__ __forceinline__ size_t lattice_of_internal(size_t p, int np, int B) {
+    const size_t B3 = (size_t)B * B * B;
+    const size_t blk = p / B3;
+    const int l = (int)(p % B3);
+    const int nb = np / B;
+    const int bz = (int)(blk % nb), by = (int)((blk / nb) % nb), bx = (int)(blk / ((size_t)nb * nb));
+    const int lz = l % B, ly = (l / B) % B, lx = l / (B * B);
+    return ((size_t)(bx * B + lx) * np + (by * B + ly)) * np + (bz * B + lz);
+}
+
 }  // namespace hgpm

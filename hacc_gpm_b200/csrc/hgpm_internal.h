@@ -39,11 +39,12 @@ cudaError_t launch_xpk(int ng, const float2* in, int ncols, size_t rs, size_t ps
                        double* part_sum, unsigned long long* part_cnt, int nparts, double* sum,
                        unsigned long long* cnt, cudaStream_t s);
 
-cudaError_t launch_load_state(const float* x, const float* v, const ParticleSoA& p, size_t n, int ng, cudaStream_t s);
-cudaError_t launch_store_state(const ParticleSoA& p, float* x, float* v, size_t n, cudaStream_t s);
-cudaError_t launch_cells(const ParticleSoA& p, int32_t* out, size_t n, int ng, cudaStream_t s);
+cudaError_t launch_load_state(const float* x, const float* v, const ParticleSoA& p, int np_side, int B, int ng,
+                              cudaStream_t s);
+cudaError_t launch_store_state(const ParticleSoA& p, float* x, float* v, int np_side, int B, cudaStream_t s);
 cudaError_t launch_drift(const ParticleSoA& p, size_t n, int ng, float pf, cudaStream_t s);
-cudaError_t launch_deposit(const ParticleSoA& p, size_t n, int ng, float mass, unsigned long long* rho,
+int deposit_cap_cells(int np_side, int ng);
+cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
                            cudaStream_t s);
 cudaError_t launch_kick_drift(const ParticleSoA& p, size_t n, int ng, const float* fx, const float* fy,
                               const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift,

@@ -46,41 +46,40 @@ __device__ __forceinline__ void split_axis(float x, int ng, int& i, float& o) {
     i = wrap_axis((int)fl, ng);
 }
 
+// State conversion between the reference layout (float3, lattice order) and
+// the internal SoA in Lagrangian-block order (hgpm_device.cuh).
 __global__ void load_state_kernel(const float* __restrict__ x, const float* __restrict__ v, ParticleSoA p,
-                                  size_t n, int ng) {
+                                  int np_side, int B, int ng) {
+    const size_t n = (size_t)np_side * np_side * np_side;
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const size_t q = lattice_of_internal(i, np_side, B);
     int ix, iy, iz;
     float ox, oy, oz;
-    split_axis(x[3 * i + 0], ng, ix, ox);
-    split_axis(x[3 * i + 1], ng, iy, oy);
-    split_axis(x[3 * i + 2], ng, iz, oz);
+    split_axis(x[3 * q + 0], ng, ix, ox);
+    split_axis(x[3 * q + 1], ng, iy, oy);
+    split_axis(x[3 * q + 2], ng, iz, oz);
     p.cell[i] = pack_cell(ix, iy, iz);
     p.ox[i] = ox;
     p.oy[i] = oy;
     p.oz[i] = oz;
-    p.vx[i] = v[3 * i + 0];
-    p.vy[i] = v[3 * i + 1];
-    p.vz[i] = v[3 * i + 2];
+    p.vx[i] = v[3 * q + 0];
+    p.vy[i] = v[3 * q + 1];
+    p.vz[i] = v[3 * q + 2];
 }
 
-__global__ void store_state_kernel(ParticleSoA p, float* __restrict__ x, float* __restrict__ v, size_t n) {
+__global__ void store_state_kernel(ParticleSoA p, float* __restrict__ x, float* __restrict__ v, int np_side, int B) {
+    const size_t n = (size_t)np_side * np_side * np_side;
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const size_t q = lattice_of_internal(i, np_side, B);
     const uint32_t c = p.cell[i];
-    x[3 * i + 0] = (float)cell_x(c) + p.ox[i];
-    x[3 * i + 1] = (float)cell_y(c) + p.oy[i];
-    x[3 * i + 2] = (float)cell_z(c) + p.oz[i];
-    v[3 * i + 0] = p.vx[i];
-    v[3 * i + 1] = p.vy[i];
-    v[3 * i + 2] = p.vz[i];
-}
-
-__global__ void cells_kernel(ParticleSoA p, int32_t* __restrict__ out, size_t n, int ng) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t c = p.cell[i];
-    out[i] = (cell_x(c) * ng + cell_y(c)) * ng + cell_z(c);
+    x[3 * q + 0] = (float)cell_x(c) + p.ox[i];
+    x[3 * q + 1] = (float)cell_y(c) + p.oy[i];
+    x[3 * q + 2] = (float)cell_z(c) + p.oz[i];
+    v[3 * q + 0] = p.vx[i];
+    v[3 * q + 1] = p.vy[i];
+    v[3 * q + 2] = p.vz[i];
 }
 
 __global__ void drift_kernel(ParticleSoA p, size_t n, int ng, float pf) {
@@ -100,19 +99,20 @@ __global__ void drift_kernel(ParticleSoA p, size_t n, int ng, float pf) {
 
 // CICKernel (cic_pm.cu:46-87) with float weights ((w_x*w_y)*w_z)*mass, each
 // rounded to a 2^-32 fixed-point int64 and added with integer atomics, so the
-// density is independent of particle and thread order.
-__global__ void deposit_kernel(ParticleSoA p, size_t n, int ng, float mass, unsigned long long* __restrict__ rho) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t c = __ldg(&p.cell[i]);
-    const float dx = __ldg(&p.ox[i]), dy = __ldg(&p.oy[i]), dz = __ldg(&p.oz[i]);
-    const int ix = cell_x(c), iy = cell_y(c), iz = cell_z(c);
-    const int ix1 = ix + 1 == ng ? 0 : ix + 1;
-    const int iy1 = iy + 1 == ng ? 0 : iy + 1;
-    const int iz1 = iz + 1 == ng ? 0 : iz + 1;
-    const uint32_t sx[2] = {(uint32_t)ix * ng * ng, (uint32_t)ix1 * ng * ng};
-    const uint32_t sy[2] = {(uint32_t)iy * ng, (uint32_t)iy1 * ng};
-    const uint32_t sz[2] = {(uint32_t)iz, (uint32_t)iz1};
+// density is independent of particle, thread and CTA order (bit-exact run to
+// run).  One CTA owns one Lagrangian block of B^3 particles: it finds the
+// bounding box of their cells, accumulates the block's CIC weights in a
+// shared-memory int64 window over that box, and flushes the window's non-zero
+// cells to the global accumulator with one coalesced red.add per cell.  A
+// block whose particles spread over more than cap_cells cells falls back to
+// per-corner global atomics.
+__device__ __forceinline__ int nearest_image(int d, int ng) {
+    if (d < -(ng >> 1)) d += ng;
+    else if (d >= (ng >> 1)) d -= ng;
+    return d;
+}
+
+__device__ __forceinline__ void cic_fixed(float dx, float dy, float dz, float mass, long long q[8]) {
     const float wx[2] = {1.f - dx, dx}, wy[2] = {1.f - dy, dy}, wz[2] = {1.f - dz, dz};
 #pragma unroll
     for (int a = 0; a < 2; ++a)
@@ -121,9 +121,105 @@ __global__ void deposit_kernel(ParticleSoA p, size_t n, int ng, float mass, unsi
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
                 const float mul = __fmul_rn(__fmul_rn(__fmul_rn(wx[a], wy[b]), wz[cc]), mass);
-                const long long q = __float2ll_rn(mul * kFixScaleF);
-                atomicAdd(&rho[sx[a] + sy[b] + sz[cc]], (unsigned long long)q);
+                q[(a * 2 + b) * 2 + cc] = __float2ll_rn(mul * kFixScaleF);
             }
+}
+
+template <int B>
+__global__ void __launch_bounds__(256) deposit_tiled_kernel(ParticleSoA p, int np_side, int ng, float mass,
+                                                            unsigned long long* __restrict__ rho, int cap_cells) {
+    constexpr int B3 = B * B * B;
+    constexpr int PPT = B3 / 256;
+    extern __shared__ unsigned long long win[];
+    __shared__ int bb[6];
+    const int tid = threadIdx.x;
+    const int nb = np_side / B;
+    const int blk = blockIdx.x;
+    const int bz = blk % nb, by = (blk / nb) % nb, bx = blk / (nb * nb);
+    const int ox = (int)((long long)bx * B * ng / np_side);
+    const int oy = (int)((long long)by * B * ng / np_side);
+    const int oz = (int)((long long)bz * B * ng / np_side);
+    if (tid < 3) bb[tid] = 0x7fffffff;
+    else if (tid < 6) bb[tid] = -0x7fffffff;
+    __syncthreads();
+    const size_t p0 = (size_t)blk * B3;
+    int rx[PPT], ry[PPT], rz[PPT];
+    int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        const uint32_t c = __ldg(&p.cell[p0 + tid + k * 256]);
+        rx[k] = nearest_image(cell_x(c) - ox, ng);
+        ry[k] = nearest_image(cell_y(c) - oy, ng);
+        rz[k] = nearest_image(cell_z(c) - oz, ng);
+        mn[0] = min(mn[0], rx[k]); mx[0] = max(mx[0], rx[k]);
+        mn[1] = min(mn[1], ry[k]); mx[1] = max(mx[1], ry[k]);
+        mn[2] = min(mn[2], rz[k]); mx[2] = max(mx[2], rz[k]);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        mn[a] = __reduce_min_sync(0xffffffffu, mn[a]);
+        mx[a] = __reduce_max_sync(0xffffffffu, mx[a]);
+    }
+    if ((tid & 31) == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(&bb[a], mn[a]);
+            atomicMax(&bb[3 + a], mx[a]);
+        }
+    }
+    __syncthreads();
+    const int lx0 = bb[0], ly0 = bb[1], lz0 = bb[2];
+    const int wx = bb[3] - lx0 + 2, wy = bb[4] - ly0 + 2, wz = bb[5] - lz0 + 2;
+    const long long vol = (long long)wx * wy * wz;
+    if (vol <= cap_cells) {
+        for (int i = tid; i < vol; i += 256) win[i] = 0ull;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            const size_t idx = p0 + tid + k * 256;
+            long long q[8];
+            cic_fixed(__ldg(&p.ox[idx]), __ldg(&p.oy[idx]), __ldg(&p.oz[idx]), mass, q);
+            const int a0 = rx[k] - lx0, b0 = ry[k] - ly0, c0 = rz[k] - lz0;
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b)
+#pragma unroll
+                    for (int cc = 0; cc < 2; ++cc)
+                        atomicAdd(&win[((a0 + a) * wy + (b0 + b)) * wz + (c0 + cc)],
+                                  (unsigned long long)q[(a * 2 + b) * 2 + cc]);
+        }
+        __syncthreads();
+        const int gx0 = ox + lx0, gy0 = oy + ly0, gz0 = oz + lz0;
+        for (int i = tid; i < vol; i += 256) {
+            const unsigned long long v = win[i];
+            if (v == 0ull) continue;
+            const int cz = i % wz, cy = (i / wz) % wy, cx = i / (wz * wy);
+            const int gx = wrap_axis(gx0 + cx, ng), gy = wrap_axis(gy0 + cy, ng), gz = wrap_axis(gz0 + cz, ng);
+            atomicAdd(&rho[((size_t)gx * ng + gy) * ng + gz], v);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            const size_t idx = p0 + tid + k * 256;
+            long long q[8];
+            cic_fixed(__ldg(&p.ox[idx]), __ldg(&p.oy[idx]), __ldg(&p.oz[idx]), mass, q);
+            const int ix = wrap_axis(ox + rx[k], ng), iy = wrap_axis(oy + ry[k], ng), iz = wrap_axis(oz + rz[k], ng);
+            const int ix1 = ix + 1 == ng ? 0 : ix + 1;
+            const int iy1 = iy + 1 == ng ? 0 : iy + 1;
+            const int iz1 = iz + 1 == ng ? 0 : iz + 1;
+            const size_t sx[2] = {(size_t)ix * ng * ng, (size_t)ix1 * ng * ng};
+            const size_t sy[2] = {(size_t)iy * ng, (size_t)iy1 * ng};
+            const size_t sz[2] = {(size_t)iz, (size_t)iz1};
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b)
+#pragma unroll
+                    for (int cc = 0; cc < 2; ++cc)
+                        atomicAdd(&rho[sx[a] + sy[b] + sz[cc]], (unsigned long long)q[(a * 2 + b) * 2 + cc]);
+        }
+    }
 }
 
 // ICICKernel (icic_pm.cu:72-127) fused with up to two UpdatePosKernel drifts:
@@ -243,16 +339,17 @@ __global__ void noise_kernel(float* __restrict__ out, size_t n, uint32_t seed) {
 // placeParticles (place_particles_initializer.cu:23-65): lattice point q of
 // particle idx (get_index with np), x = q*(ng/np) + delta*s (wrapped),
 // v = velmul * s.  The position is formed in FP64 and split into cell + offset.
-__global__ void place_kernel(const float* __restrict__ s, size_t scomp, ParticleSoA p, int np_side, int ng,
+__global__ void place_kernel(const float* __restrict__ s, size_t scomp, ParticleSoA p, int np_side, int B, int ng,
                              float delta_f, float velmul) {
     const size_t n = (size_t)np_side * np_side * np_side;
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const int qx = (int)(i / ((size_t)np_side * np_side));
-    const int qy = (int)((i / np_side) % np_side);
-    const int qz = (int)(i % np_side);
+    const size_t q = lattice_of_internal(i, np_side, B);
+    const int qx = (int)(q / ((size_t)np_side * np_side));
+    const int qy = (int)((q / np_side) % np_side);
+    const int qz = (int)(q % np_side);
     const float r = (float)ng / (float)np_side;
-    const float sxv = s[i], syv = s[scomp + i], szv = s[2 * scomp + i];
+    const float sxv = s[q], syv = s[scomp + q], szv = s[2 * scomp + q];
     const float dsx = delta_f * sxv, dsy = delta_f * syv, dsz = delta_f * szv;
     int ix, iy, iz;
     float ox, oy, oz;
@@ -289,25 +386,47 @@ __global__ void place_kernel(const float* __restrict__ s, size_t scomp, Particle
 // ---------------------------------------------------------------------------
 static inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
-cudaError_t launch_load_state(const float* x, const float* v, const ParticleSoA& p, size_t n, int ng, cudaStream_t s) {
-    load_state_kernel<<<nblk(n, 256), 256, 0, s>>>(x, v, p, n, ng);
+cudaError_t launch_load_state(const float* x, const float* v, const ParticleSoA& p, int np_side, int B, int ng,
+                              cudaStream_t s) {
+    const size_t n = (size_t)np_side * np_side * np_side;
+    load_state_kernel<<<nblk(n, 256), 256, 0, s>>>(x, v, p, np_side, B, ng);
     return cudaGetLastError();
 }
-cudaError_t launch_store_state(const ParticleSoA& p, float* x, float* v, size_t n, cudaStream_t s) {
-    store_state_kernel<<<nblk(n, 256), 256, 0, s>>>(p, x, v, n);
-    return cudaGetLastError();
-}
-cudaError_t launch_cells(const ParticleSoA& p, int32_t* out, size_t n, int ng, cudaStream_t s) {
-    cells_kernel<<<nblk(n, 256), 256, 0, s>>>(p, out, n, ng);
+cudaError_t launch_store_state(const ParticleSoA& p, float* x, float* v, int np_side, int B, cudaStream_t s) {
+    const size_t n = (size_t)np_side * np_side * np_side;
+    store_state_kernel<<<nblk(n, 256), 256, 0, s>>>(p, x, v, np_side, B);
     return cudaGetLastError();
 }
 cudaError_t launch_drift(const ParticleSoA& p, size_t n, int ng, float pf, cudaStream_t s) {
     drift_kernel<<<nblk(n, 256), 256, 0, s>>>(p, n, ng, pf);
     return cudaGetLastError();
 }
-cudaError_t launch_deposit(const ParticleSoA& p, size_t n, int ng, float mass, unsigned long long* rho,
+int deposit_cap_cells(int np_side, int ng) {
+    const int B = block_side(np_side, ng);
+    const int r = (B * ng + np_side - 1) / np_side + 6;  // block region + margin
+    int cap = r * r * r;
+    if (cap < 4096) cap = 4096;
+    if (cap > 12288) cap = 12288;  // 96 KB of int64: two CTAs per SM
+    return cap;
+}
+
+cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
                            cudaStream_t s) {
-    deposit_kernel<<<nblk(n, 256), 256, 0, s>>>(p, n, ng, mass, rho);
+    const int B = block_side(np_side, ng);
+    const int cap = deposit_cap_cells(np_side, ng);
+    const int nblocks = (np_side / B) * (np_side / B) * (np_side / B);
+    const int smem = cap * 8;
+    if (B == 16) {
+        auto k = deposit_tiled_kernel<16>;
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        k<<<nblocks, 256, smem, s>>>(p, np_side, ng, mass, rho, cap);
+    } else {
+        auto k = deposit_tiled_kernel<8>;
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        k<<<nblocks, 256, smem, s>>>(p, np_side, ng, mass, rho, cap);
+    }
     return cudaGetLastError();
 }
 cudaError_t launch_kick_drift(const ParticleSoA& p, size_t n, int ng, const float* fx, const float* fy,
@@ -331,7 +450,7 @@ cudaError_t launch_noise(float* out, size_t n, uint32_t seed, cudaStream_t s) {
 cudaError_t launch_place(const float* sgrid, size_t scomp, const ParticleSoA& p, int np_side, int ng, float delta_f,
                          float velmul, cudaStream_t s) {
     const size_t n = (size_t)np_side * np_side * np_side;
-    place_kernel<<<nblk(n, 256), 256, 0, s>>>(sgrid, scomp, p, np_side, ng, delta_f, velmul);
+    place_kernel<<<nblk(n, 256), 256, 0, s>>>(sgrid, scomp, p, np_side, block_side(np_side, ng), ng, delta_f, velmul);
     return cudaGetLastError();
 }
 

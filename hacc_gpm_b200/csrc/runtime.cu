@@ -306,7 +306,7 @@ struct hgpm_ctx {
     hgpm_params p;
     int device = 0;
     cudaStream_t stream = nullptr;
-    int ng = 0, np = 0, zs = 0, zs_np = 0;
+    int ng = 0, np = 0, zs = 0, zs_np = 0, blk = 8;
     size_t ncell = 0, npart = 0, nspec = 0;
     ParticleSoA part{};
     void* part_block = nullptr;
@@ -440,6 +440,7 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bad(HGPM_ERR_CUDA, cudaGetErrorString(e));
     c->ncell = (size_t)c->ng * c->ng * c->ng;
+    c->blk = block_side(c->np, c->ng);
     c->npart = (size_t)c->np * c->np * c->np;
     c->zs = even_pad(c->ng / 2 + 1);
     c->zs_np = even_pad(c->np / 2 + 1);
@@ -541,7 +542,7 @@ static int ensure_stage(hgpm_ctx* c) {
 
 extern "C" int hgpm_load_state_device(hgpm_ctx* c, const float* x, const float* v) {
     if (!c || !x || !v) return HGPM_ERR_ARG;
-    CK(launch_load_state(x, v, c->part, c->npart, c->ng, c->stream));
+    CK(launch_load_state(x, v, c->part, c->np, c->blk, c->ng, c->stream));
     count(c, PH_DRIFT, 1);
     c->have_state = true;
     return HGPM_OK;
@@ -550,7 +551,7 @@ extern "C" int hgpm_load_state_device(hgpm_ctx* c, const float* x, const float* 
 extern "C" int hgpm_store_state_device(hgpm_ctx* c, float* x, float* v) {
     if (!c || !x || !v) return HGPM_ERR_ARG;
     if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
-    CK(launch_store_state(c->part, x, v, c->npart, c->stream));
+    CK(launch_store_state(c->part, x, v, c->np, c->blk, c->stream));
     count(c, PH_DRIFT, 1);
     return HGPM_OK;
 }
@@ -589,7 +590,7 @@ extern "C" int hgpm_get_cells(hgpm_ctx* c, int32_t* cells) {
     CK(cudaStreamSynchronize(c->stream));
     for (size_t i = 0; i < c->npart; ++i) {
         uint32_t q = packed[i];
-        cells[i] = (cell_x(q) * c->ng + cell_y(q)) * c->ng + cell_z(q);
+        cells[lattice_of_internal(i, c->np, c->blk)] = (cell_x(q) * c->ng + cell_y(q)) * c->ng + cell_z(q);
     }
     return HGPM_OK;
 }
@@ -618,7 +619,7 @@ static double mean_density(const hgpm_ctx* c) {
 
 static int deposit_impl(hgpm_ctx* c) {
     if (c->rho_dirty) CK(cudaMemsetAsync(c->rho64, 0, c->ncell * 8, c->stream));
-    CK(launch_deposit(c->part, c->npart, c->ng, cic_mass(c->ng, c->np), c->rho64, c->stream));
+    CK(launch_deposit(c->part, c->np, c->ng, cic_mass(c->ng, c->np), c->rho64, c->stream));
     count(c, PH_DEPOSIT, 1);
     c->rho_dirty = true;
     return HGPM_OK;

@@ -15,7 +15,8 @@ from tests.helpers import PK_RTOL, POS_BOX_TOL, box_pos_err, oracle_ics, params_
 pytestmark = pytest.mark.gpu
 
 
-def _pair(ng, np_side=None, rl=None, z_ini=50.0, nsteps=10, extra=""):
+def _pair(ng, np_side=None, rl=None, z_ini=50.0, nsteps=100, extra=""):
+    # N_STEPS sets the step size (a run of nsteps from z_ini to 0); tests run fewer
     txt = params_text(ng, np_side, rl, z_ini=z_ini, nsteps=nsteps, extra=extra)
     return H.parse_params(txt), O.parse_params_text(txt)
 
@@ -23,7 +24,7 @@ def _pair(ng, np_side=None, rl=None, z_ini=50.0, nsteps=10, extra=""):
 @pytest.mark.parametrize("ng,np_side,rl,z,n", [(32, 32, 32.0, 50.0, 10), (48, 48, 96.0, 100.0, 8),
                                                (64, 32, 64.0, 50.0, 5)])
 def test_run_steps_match_oracle(ng, np_side, rl, z, n):
-    hp, op = _pair(ng, np_side, rl, z_ini=z, nsteps=n)
+    hp, op = _pair(ng, np_side, rl, z_ini=z)
     x0, v0, *_ = oracle_ics(op)
     with H.Simulation(hp) as s:
         s.load_state(x0, v0)
@@ -42,7 +43,7 @@ def test_run_steps_match_oracle(ng, np_side, rl, z, n):
 def test_run_steps_equals_unfused_phase_calls():
     """hgpm_run_steps (fused kick + two drifts) against the reference's call
     sequence driver_pm.cpp:114-125 issued phase by phase."""
-    hp, op = _pair(32, nsteps=6)
+    hp, op = _pair(32)
     x0, v0, *_ = oracle_ics(op)
     with H.Simulation(hp) as a, H.Simulation(hp) as b:
         ta, tb = H.Timestepper(hp), H.Timestepper(hp)
@@ -66,7 +67,7 @@ def test_run_steps_equals_unfused_phase_calls():
 
 
 def test_whole_step_deterministic():
-    hp, op = _pair(48, nsteps=4)
+    hp, op = _pair(48)
     x0, v0, *_ = oracle_ics(op)
     outs = []
     for _ in range(2):
@@ -169,7 +170,7 @@ def test_ic_table_too_short_is_an_error():
 
 
 def test_step_host_roundtrip_equals_device_resident():
-    hp, op = _pair(32, nsteps=3)
+    hp, op = _pair(32)
     x0, v0, *_ = oracle_ics(op)
     with H.Simulation(hp) as a, H.Simulation(hp) as b:
         ta, tb = H.Timestepper(hp), H.Timestepper(hp)
