@@ -33,6 +33,10 @@ template <int NG> struct Cfg {
     static constexpr int ZSMEM = M * (L + 1) * 8;
     static constexpr int SSMEM = NG * CS * 8;
     static constexpr int XSMEM = 2 * NG * CX * 8;
+    // threads per CTA of the strided and fused x passes: 512 halves the
+    // per-thread register staging so two CTAs (32 warps) fit per SM
+    static constexpr int NTS = NG >= 128 ? 512 : 256;
+    static constexpr int NTX = NG >= 128 ? 512 : 256;
 };
 
 // ---------------------------------------------------------------------------
@@ -41,18 +45,18 @@ template <int NG> struct Cfg {
 // Rows e in [0, N) at g + e*rs; columns [0, nvalid) valid (nvalid may be < C).
 // All of a thread's global loads are issued before any shared store
 // (register staging) so each CTA keeps its whole tile in flight.
-template <int N, int C>
+template <int N, int C, int NT = kThreads>
 __device__ __forceinline__ void load_tile(float2* __restrict__ tile, const float2* __restrict__ g,
                                           size_t rs, int nvalid) {
     constexpr int TPR = C / 2;  // float4 (two complex) per row chunk
     constexpr int TOT = N * TPR;
-    constexpr int PER = (TOT + kThreads - 1) / kThreads;
+    constexpr int PER = (TOT + NT - 1) / NT;
     float4 v[PER];
     if (nvalid >= C) {
 #pragma unroll
         for (int t = 0; t < PER; ++t) {
-            const int i = threadIdx.x + t * kThreads;
-            if ((TOT % kThreads) == 0 || i < TOT) {
+            const int i = threadIdx.x + t * NT;
+            if ((TOT % NT) == 0 || i < TOT) {
                 const int e = i / TPR, c = 2 * (i % TPR);
                 v[t] = __ldcs(reinterpret_cast<const float4*>(g + (size_t)e * rs + c));
             }
@@ -60,9 +64,9 @@ __device__ __forceinline__ void load_tile(float2* __restrict__ tile, const float
     } else {
 #pragma unroll
         for (int t = 0; t < PER; ++t) {
-            const int i = threadIdx.x + t * kThreads;
+            const int i = threadIdx.x + t * NT;
             v[t] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if ((TOT % kThreads) == 0 || i < TOT) {
+            if ((TOT % NT) == 0 || i < TOT) {
                 const int e = i / TPR, c = 2 * (i % TPR);
                 const float2* src = g + (size_t)e * rs + c;
                 if (c + 1 < nvalid) {
@@ -76,24 +80,24 @@ __device__ __forceinline__ void load_tile(float2* __restrict__ tile, const float
     }
 #pragma unroll
     for (int t = 0; t < PER; ++t) {
-        const int i = threadIdx.x + t * kThreads;
-        if ((TOT % kThreads) == 0 || i < TOT) {
+        const int i = threadIdx.x + t * NT;
+        if ((TOT % NT) == 0 || i < TOT) {
             const int e = i / TPR, c = 2 * (i % TPR);
             *reinterpret_cast<float4*>(&tile[e * C + c]) = v[t];
         }
     }
 }
 
-template <int N, int C>
+template <int N, int C, int NT = kThreads>
 __device__ __forceinline__ void store_tile(const float2* __restrict__ tile, float2* __restrict__ g,
                                            size_t rs, int nvalid) {
     constexpr int TPR = C / 2;
     constexpr int TOT = N * TPR;
-    constexpr int PER = (TOT + kThreads - 1) / kThreads;
+    constexpr int PER = (TOT + NT - 1) / NT;
 #pragma unroll
     for (int t = 0; t < PER; ++t) {
-        const int i = threadIdx.x + t * kThreads;
-        if ((TOT % kThreads) == 0 || i < TOT) {
+        const int i = threadIdx.x + t * NT;
+        if ((TOT % NT) == 0 || i < TOT) {
             const int e = i / TPR, c = 2 * (i % TPR);
             float2* dst = g + (size_t)e * rs + c;
             const float4 v = *reinterpret_cast<const float4*>(&tile[e * C + c]);
@@ -239,17 +243,17 @@ __global__ void __launch_bounds__(kThreads) zpass_c2r_kernel(const float2* __res
 // strided pass (y or x lines), in place, blockIdx = (column chunk, plane, comp)
 // ---------------------------------------------------------------------------
 template <int NG, bool INV>
-__global__ void __launch_bounds__(kThreads) strided_kernel(float2* __restrict__ data, int ncols, size_t rs,
-                                                           size_t ps, size_t cs, const float2* __restrict__ tw) {
-    constexpr int C = Cfg<NG>::CS;
+__global__ void __launch_bounds__(Cfg<NG>::NTS, 2) strided_kernel(float2* __restrict__ data, int ncols, size_t rs,
+                                                               size_t ps, size_t cs, const float2* __restrict__ tw) {
+    constexpr int C = Cfg<NG>::CS, NT = Cfg<NG>::NTS;
     float2* tile = reinterpret_cast<float2*>(hgpm_smem);
     const int col0 = blockIdx.x * C;
     float2* g = data + (size_t)blockIdx.z * cs + (size_t)blockIdx.y * ps + col0;
     const int nvalid = ncols - col0;
-    load_tile<NG, C>(tile, g, rs, nvalid);
+    load_tile<NG, C, NT>(tile, g, rs, nvalid);
     __syncthreads();
-    fft_tile<NG, C, C, INV, kThreads>(tile, tw);
-    store_tile<NG, C>(tile, g, rs, nvalid);
+    fft_tile<NG, C, C, INV, NT>(tile, tw);
+    store_tile<NG, C, NT>(tile, g, rs, nvalid);
 }
 
 // ---------------------------------------------------------------------------
@@ -259,33 +263,33 @@ __global__ void __launch_bounds__(kThreads) strided_kernel(float2* __restrict__ 
 // plane = ky index, rows = kx index, columns = kz index.
 // ---------------------------------------------------------------------------
 template <int NG, class Op>
-__global__ void __launch_bounds__(kThreads) xfused_kernel(const float2* __restrict__ in, float2* __restrict__ out,
-                                                          int ncols, size_t rs, size_t ps, size_t out_cs,
-                                                          const float2* __restrict__ tw, Op op) {
-    constexpr int C = Cfg<NG>::CX;
+__global__ void __launch_bounds__(Cfg<NG>::NTX) xfused_kernel(const float2* __restrict__ in, float2* __restrict__ out,
+                                                              int ncols, size_t rs, size_t ps, size_t out_cs,
+                                                              const float2* __restrict__ tw, Op op) {
+    constexpr int C = Cfg<NG>::CX, NT = Cfg<NG>::NTX;
     float2* tile = reinterpret_cast<float2*>(hgpm_smem);
     float2* work = tile + NG * C;
     const int col0 = blockIdx.x * C;
     const int iy = blockIdx.y;
     const size_t off = (size_t)iy * ps + col0;
     const int nvalid = ncols - col0;
-    load_tile<NG, C>(tile, in + off, rs, nvalid);
+    load_tile<NG, C, NT>(tile, in + off, rs, nvalid);
     __syncthreads();
-    fft_tile<NG, C, C, false, kThreads>(tile, tw);
-    for (int i = threadIdx.x; i < NG * C; i += kThreads) {
+    fft_tile<NG, C, C, false, NT>(tile, tw);
+    for (int i = threadIdx.x; i < NG * C; i += NT) {
         const int ix = i / C, c = i % C;
         tile[i] = op.pre(ix, iy, col0 + c, tile[i]);
     }
     // (fft_tile ended with a barrier; pre() only touches the thread's own cells)
 #pragma unroll 1
     for (int d = 0; d < 3; ++d) {
-        for (int i = threadIdx.x; i < NG * C; i += kThreads) {
+        for (int i = threadIdx.x; i < NG * C; i += NT) {
             const int ix = i / C, c = i % C;
             work[i] = op.comp(d, ix, iy, col0 + c, tile[i]);
         }
         __syncthreads();
-        fft_tile<NG, C, C, true, kThreads>(work, tw);
-        store_tile<NG, C>(work, out + (size_t)d * out_cs + off, rs, nvalid);
+        fft_tile<NG, C, C, true, NT>(work, tw);
+        store_tile<NG, C, NT>(work, out + (size_t)d * out_cs + off, rs, nvalid);
         __syncthreads();
     }
 }
@@ -405,17 +409,24 @@ __global__ void pk_reduce_kernel(const double* __restrict__ part_sum, const unsi
 // cosq[i] = cos(k_i) - 1 (double) and sk[i] = sin(k_i) are tabulated once per
 // grid side; G is formed in double from the sum of the (non-positive) cosq
 // terms, so there is no cancellation near k = 0.
+// A derivative along d at the Nyquist index of d is anti-Hermitian in the
+// reference's full C2C (both partners carry the same signed k = -n/2), so its
+// real part — all the reference keeps — is exactly zero; the half-spectrum
+// C2R would instead Hermitian-extend it.  comp() therefore returns 0 there.
 struct PoissonOp {
     const double* cosq;  // cos(k_i) - 1, one entry per grid index
     const float* sk;     // sin(k_i)
     double coeff;        // 0.5 / ng^3
+    int nyq;             // ng / 2
     __device__ __forceinline__ float2 pre(int ix, int iy, int iz, float2 v) const {
         const double s = __ldg(&cosq[ix]) + __ldg(&cosq[iy]) + __ldg(&cosq[iz]);
         const float g = (s == 0.0) ? 0.f : (float)(coeff / s);
         return make_float2(v.x * g, v.y * g);
     }
     __device__ __forceinline__ float2 comp(int d, int ix, int iy, int iz, float2 t) const {
-        const float sd = __ldg(&sk[d == 0 ? ix : (d == 1 ? iy : iz)]);
+        const int id = d == 0 ? ix : (d == 1 ? iy : iz);
+        if (id == nyq) return make_float2(0.f, 0.f);
+        const float sd = __ldg(&sk[id]);
         return make_float2(sd * t.y, -sd * t.x);
     }
 };
@@ -462,8 +473,11 @@ struct ICOp {
         v.y = (float)((double)v.y * mul);
         return v;
     }
+    int nyq;           // n / 2
     __device__ __forceinline__ float2 comp(int d, int ix, int iy, int iz, float2 t) const {
-        const float kd = __ldg(&kf[d == 0 ? ix : (d == 1 ? iy : iz)]);
+        const int id = d == 0 ? ix : (d == 1 ? iy : iz);
+        if (id == nyq) return make_float2(0.f, 0.f);
+        const float kd = __ldg(&kf[id]);
         return make_float2(t.y * kd, -t.x * kd);
     }
 };
@@ -519,12 +533,12 @@ static cudaError_t strided_impl(bool inv, float2* data, int ncols, size_t rs, si
         auto k = strided_kernel<NG, true>;
         cudaError_t e = ensure_smem(k, G::SSMEM);
         if (e != cudaSuccess) return e;
-        k<<<grid, kThreads, G::SSMEM, s>>>(data, ncols, rs, ps, cs, tw);
+        k<<<grid, G::NTS, G::SSMEM, s>>>(data, ncols, rs, ps, cs, tw);
     } else {
         auto k = strided_kernel<NG, false>;
         cudaError_t e = ensure_smem(k, G::SSMEM);
         if (e != cudaSuccess) return e;
-        k<<<grid, kThreads, G::SSMEM, s>>>(data, ncols, rs, ps, cs, tw);
+        k<<<grid, G::NTS, G::SSMEM, s>>>(data, ncols, rs, ps, cs, tw);
     }
     return cudaGetLastError();
 }
@@ -537,7 +551,7 @@ static cudaError_t xfused_impl(const float2* in, float2* out, int ncols, size_t 
     cudaError_t e = ensure_smem(k, G::XSMEM);
     if (e != cudaSuccess) return e;
     dim3 grid(cdiv(ncols, G::CX), nplanes);
-    k<<<grid, kThreads, G::XSMEM, s>>>(in, out, ncols, rs, ps, out_cs, tw, op);
+    k<<<grid, G::NTX, G::XSMEM, s>>>(in, out, ncols, rs, ps, out_cs, tw, op);
     return cudaGetLastError();
 }
 
@@ -608,7 +622,7 @@ cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs,
 cudaError_t launch_xpoisson(int ng, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
                             size_t out_cs, const float2* tw, const double* cosq, const float* sk, double coeff,
                             cudaStream_t s) {
-    PoissonOp op{cosq, sk, coeff};
+    PoissonOp op{cosq, sk, coeff, ng / 2};
     switch (ng) {
 #define X(n) \
     case n: return xfused_impl<n, PoissonOp>(in, out, ncols, rs, ps, nplanes, out_cs, tw, op, s);
@@ -621,7 +635,7 @@ cudaError_t launch_xpoisson(int ng, const float2* in, float2* out, int ncols, si
 cudaError_t launch_xic(int n, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
                        size_t out_cs, const float2* tw, const double* table, int nbins, double k_delta,
                        double pkscale, double inv_delta, const float* kf, int* err, cudaStream_t s) {
-    ICOp op{table, nbins, k_delta, pkscale, inv_delta, kf, err};
+    ICOp op{table, nbins, k_delta, pkscale, inv_delta, kf, err, n / 2};
     switch (n) {
 #define X(m) \
     case m: return xfused_impl<m, ICOp>(in, out, ncols, rs, ps, nplanes, out_cs, tw, op, s);

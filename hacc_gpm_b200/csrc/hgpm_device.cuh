@@ -6,9 +6,10 @@
 namespace hgpm {
 
 constexpr int kThreads = 256;            // threads per CTA for all pass kernels
-constexpr double kFixScale = 4294967296.0;      // 2^32: int64 fixed-point density
-constexpr double kFixInv = 1.0 / 4294967296.0;
-constexpr float kFixScaleF = 4294967296.0f;
+// int64 fixed-point density: value * 2^31 (a unit-mass CIC weight fits a u32)
+constexpr double kFixScale = 2147483648.0;
+constexpr double kFixInv = 1.0 / 2147483648.0;
+constexpr float kFixScaleF = 2147483648.0f;
 
 // Particle positions are a packed cell (10 bits per axis, ng <= 1024) plus
 // an FP32 offset in [0, 1) per axis.

@@ -46,7 +46,7 @@ cudaError_t launch_drift(const ParticleSoA& p, size_t n, int ng, float pf, cudaS
 int deposit_cap_cells(int np_side, int ng);
 cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
                            cudaStream_t s);
-cudaError_t launch_kick_drift(const ParticleSoA& p, size_t n, int ng, const float* fx, const float* fy,
+cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float* fx, const float* fy,
                               const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift,
                               cudaStream_t s);
 cudaError_t launch_density(const unsigned long long* rho64, float* rho, size_t n, cudaStream_t s);

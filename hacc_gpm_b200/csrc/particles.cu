@@ -98,13 +98,18 @@ __global__ void drift_kernel(ParticleSoA p, size_t n, int ng, float pf) {
 }
 
 // CICKernel (cic_pm.cu:46-87) with float weights ((w_x*w_y)*w_z)*mass, each
-// rounded to a 2^-32 fixed-point int64 and added with integer atomics, so the
-// density is independent of particle, thread and CTA order (bit-exact run to
-// run).  One CTA owns one Lagrangian block of B^3 particles: it finds the
-// bounding box of their cells, accumulates the block's CIC weights in a
-// shared-memory int64 window over that box, and flushes the window's non-zero
-// cells to the global accumulator with one coalesced red.add per cell.  A
-// block whose particles spread over more than cap_cells cells falls back to
+// rounded to a 2^-31 fixed-point integer and added with integer atomics, so
+// the density is independent of particle, thread and CTA order (bit-exact
+// run to run).  One CTA owns one Lagrangian block of B^3 particles: it finds
+// the bounding box of their cells, accumulates the block's CIC weights in a
+// shared-memory window over that box, and flushes the window's non-zero cells
+// to the global int64 accumulator with one coalesced red.add per cell.
+// Inside the window each cell is a (hi, lo) pair of 32-bit words updated with
+// native 32-bit shared atomics and an explicit carry.  A thread walks its
+// particles along Lagrangian x (B = 16), so particle k's upper-x corners are
+// merged in registers with particle k+1's lower-x corners whenever their
+// cells line up (about 4 instead of 8 shared atomics per particle).  A block
+// whose particles spread over more than cap_cells cells falls back to
 // per-corner global atomics.
 __device__ __forceinline__ int nearest_image(int d, int ng) {
     if (d < -(ng >> 1)) d += ng;
@@ -112,7 +117,35 @@ __device__ __forceinline__ int nearest_image(int d, int ng) {
     return d;
 }
 
-__device__ __forceinline__ void cic_fixed(float dx, float dy, float dz, float mass, long long q[8]) {
+// n / d for n, d < 2^16 with m = floor((2^32 - 1) / d) + 1 (exact in that range)
+__device__ __forceinline__ unsigned div_magic(unsigned d) { return 0xffffffffu / d + 1u; }
+__device__ __forceinline__ unsigned div_by(unsigned n, unsigned m) { return __umulhi(n, m); }
+
+// Window cell i (z fastest, then y, then x) -> global linear cell index.
+struct WinMap {
+    int wy, wz, gx0, gy0, gz0, ng;
+    unsigned mz, my;
+    __device__ __forceinline__ WinMap(int wy_, int wz_, int gx0_, int gy0_, int gz0_, int ng_)
+        : wy(wy_), wz(wz_), gx0(gx0_), gy0(gy0_), gz0(gz0_), ng(ng_) {
+        mz = div_magic((unsigned)wz_);
+        my = div_magic((unsigned)wy_);
+    }
+    __device__ __forceinline__ size_t global(int i) const {
+        const int row = (int)div_by((unsigned)i, mz);
+        const int cz = i - row * wz;
+        const int cx = (int)div_by((unsigned)row, my);
+        const int cy = row - cx * wy;
+        int gx = gx0 + cx, gy = gy0 + cy, gz = gz0 + cz;
+        gx = gx >= ng ? gx - ng : (gx < 0 ? gx + ng : gx);
+        gy = gy >= ng ? gy - ng : (gy < 0 ? gy + ng : gy);
+        gz = gz >= ng ? gz - ng : (gz < 0 ? gz + ng : gz);
+        return ((size_t)gx * ng + gy) * ng + gz;
+    }
+};
+
+// 8 fixed-point corner weights, index (a*2+b)*2+c for corner (+a, +b, +c)
+template <bool SMALL>
+__device__ __forceinline__ void cic_fixed(float dx, float dy, float dz, float mass, unsigned long long q[8]) {
     const float wx[2] = {1.f - dx, dx}, wy[2] = {1.f - dy, dy}, wz[2] = {1.f - dz, dz};
 #pragma unroll
     for (int a = 0; a < 2; ++a)
@@ -121,13 +154,40 @@ __device__ __forceinline__ void cic_fixed(float dx, float dy, float dz, float ma
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
                 const float mul = __fmul_rn(__fmul_rn(__fmul_rn(wx[a], wy[b]), wz[cc]), mass);
-                q[(a * 2 + b) * 2 + cc] = __float2ll_rn(mul * kFixScaleF);
+                // SMALL: mass <= 1, so mul * 2^31 < 2^32 fits an unsigned int
+                q[(a * 2 + b) * 2 + cc] = SMALL ? (unsigned long long)__float2uint_rn(mul * kFixScaleF)
+                                                : (unsigned long long)__float2ull_rn(mul * kFixScaleF);
             }
 }
 
-template <int B>
-__global__ void __launch_bounds__(256) deposit_tiled_kernel(ParticleSoA p, int np_side, int ng, float mass,
-                                                            unsigned long long* __restrict__ rho, int cap_cells) {
+// Window cell update.  SMALL (every contribution < 2^32): the low and high
+// 16-bit halves go to two u32 accumulators with return-free atomics; a CTA
+// makes at most B^3*8 <= 32768 contributions to a cell, so neither half can
+// overflow and hi*2^16 + lo is the exact 64-bit sum.  Otherwise: (hi, lo)
+// 32-bit words with an explicit carry from the returned old value.
+template <bool SMALL>
+__device__ __forceinline__ void win_add(unsigned* __restrict__ w0, unsigned* __restrict__ w1, int w,
+                                        unsigned long long v) {
+    if (SMALL) {
+        atomicAdd(&w0[w], (unsigned)v & 0xffffu);
+        atomicAdd(&w1[w], (unsigned)v >> 16);
+    } else {
+        const unsigned lo = (unsigned)v;
+        const unsigned old = atomicAdd(&w0[w], lo);
+        const unsigned hi = (unsigned)(v >> 32) + ((old + lo < old) ? 1u : 0u);
+        if (hi) atomicAdd(&w1[w], hi);
+    }
+}
+
+template <bool SMALL>
+__device__ __forceinline__ unsigned long long win_value(const unsigned* __restrict__ w0, const unsigned* __restrict__ w1,
+                                                        int i) {
+    return SMALL ? ((unsigned long long)w1[i] << 16) + w0[i] : ((unsigned long long)w1[i] << 32) | w0[i];
+}
+
+template <int B, bool SMALL>
+__global__ void __launch_bounds__(256, 3) deposit_tiled_kernel(ParticleSoA p, int np_side, int ng, float mass,
+                                                               unsigned long long* __restrict__ rho, int cap_cells) {
     constexpr int B3 = B * B * B;
     constexpr int PPT = B3 / 256;
     extern __shared__ unsigned long long win[];
@@ -143,17 +203,16 @@ __global__ void __launch_bounds__(256) deposit_tiled_kernel(ParticleSoA p, int n
     else if (tid < 6) bb[tid] = -0x7fffffff;
     __syncthreads();
     const size_t p0 = (size_t)blk * B3;
-    int rx[PPT], ry[PPT], rz[PPT];
     int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
-#pragma unroll
+#pragma unroll 4
     for (int k = 0; k < PPT; ++k) {
         const uint32_t c = __ldg(&p.cell[p0 + tid + k * 256]);
-        rx[k] = nearest_image(cell_x(c) - ox, ng);
-        ry[k] = nearest_image(cell_y(c) - oy, ng);
-        rz[k] = nearest_image(cell_z(c) - oz, ng);
-        mn[0] = min(mn[0], rx[k]); mx[0] = max(mx[0], rx[k]);
-        mn[1] = min(mn[1], ry[k]); mx[1] = max(mx[1], ry[k]);
-        mn[2] = min(mn[2], rz[k]); mx[2] = max(mx[2], rz[k]);
+        const int rx = nearest_image(cell_x(c) - ox, ng);
+        const int ry = nearest_image(cell_y(c) - oy, ng);
+        const int rz = nearest_image(cell_z(c) - oz, ng);
+        mn[0] = min(mn[0], rx); mx[0] = max(mx[0], rx);
+        mn[1] = min(mn[1], ry); mx[1] = max(mx[1], ry);
+        mn[2] = min(mn[2], rz); mx[2] = max(mx[2], rz);
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -172,39 +231,53 @@ __global__ void __launch_bounds__(256) deposit_tiled_kernel(ParticleSoA p, int n
     const int wx = bb[3] - lx0 + 2, wy = bb[4] - ly0 + 2, wz = bb[5] - lz0 + 2;
     const long long vol = (long long)wx * wy * wz;
     if (vol <= cap_cells) {
-        for (int i = tid; i < vol; i += 256) win[i] = 0ull;
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < PPT; ++k) {
-            const size_t idx = p0 + tid + k * 256;
-            long long q[8];
-            cic_fixed(__ldg(&p.ox[idx]), __ldg(&p.oy[idx]), __ldg(&p.oz[idx]), mass, q);
-            const int a0 = rx[k] - lx0, b0 = ry[k] - ly0, c0 = rz[k] - lz0;
-#pragma unroll
-            for (int a = 0; a < 2; ++a)
-#pragma unroll
-                for (int b = 0; b < 2; ++b)
-#pragma unroll
-                    for (int cc = 0; cc < 2; ++cc)
-                        atomicAdd(&win[((a0 + a) * wy + (b0 + b)) * wz + (c0 + cc)],
-                                  (unsigned long long)q[(a * 2 + b) * 2 + cc]);
+        unsigned* w0 = reinterpret_cast<unsigned*>(win);
+        unsigned* w1 = w0 + cap_cells;
+        for (int i = tid; i < vol; i += 256) {
+            w0[i] = 0u;
+            w1[i] = 0u;
         }
         __syncthreads();
-        const int gx0 = ox + lx0, gy0 = oy + ly0, gz0 = oz + lz0;
+        const int syz = wy * wz;
+        const int off[4] = {0, 1, wz, wz + 1};  // (b, c) corner offsets in the window
+        unsigned long long pend[4] = {0ull, 0ull, 0ull, 0ull};
+        int pw = -1;  // window index of the pending (upper-x) face; -1: none
+#pragma unroll 2
+        for (int k = 0; k < PPT; ++k) {
+            const size_t idx = p0 + tid + k * 256;
+            const uint32_t c = __ldg(&p.cell[idx]);
+            unsigned long long q[8];
+            cic_fixed<SMALL>(__ldg(&p.ox[idx]), __ldg(&p.oy[idx]), __ldg(&p.oz[idx]), mass, q);
+            const int cw = ((nearest_image(cell_x(c) - ox, ng) - lx0) * wy + (nearest_image(cell_y(c) - oy, ng) - ly0)) *
+                               wz + (nearest_image(cell_z(c) - oz, ng) - lz0);
+            if (pw == cw) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) q[j] += pend[j];
+            } else if (pw >= 0) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) win_add<SMALL>(w0, w1, pw + off[j], pend[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) win_add<SMALL>(w0, w1, cw + off[j], q[j]);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) pend[j] = q[4 + j];
+            pw = cw + syz;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) win_add<SMALL>(w0, w1, pw + off[j], pend[j]);
+        __syncthreads();
+        const WinMap map(wy, wz, ox + lx0, oy + ly0, oz + lz0, ng);
         for (int i = tid; i < vol; i += 256) {
-            const unsigned long long v = win[i];
-            if (v == 0ull) continue;
-            const int cz = i % wz, cy = (i / wz) % wy, cx = i / (wz * wy);
-            const int gx = wrap_axis(gx0 + cx, ng), gy = wrap_axis(gy0 + cy, ng), gz = wrap_axis(gz0 + cz, ng);
-            atomicAdd(&rho[((size_t)gx * ng + gy) * ng + gz], v);
+            const unsigned long long v = win_value<SMALL>(w0, w1, i);
+            if (v != 0ull) atomicAdd(&rho[map.global(i)], v);
         }
     } else {
-#pragma unroll
         for (int k = 0; k < PPT; ++k) {
             const size_t idx = p0 + tid + k * 256;
-            long long q[8];
-            cic_fixed(__ldg(&p.ox[idx]), __ldg(&p.oy[idx]), __ldg(&p.oz[idx]), mass, q);
-            const int ix = wrap_axis(ox + rx[k], ng), iy = wrap_axis(oy + ry[k], ng), iz = wrap_axis(oz + rz[k], ng);
+            const uint32_t c = __ldg(&p.cell[idx]);
+            unsigned long long q[8];
+            cic_fixed<SMALL>(__ldg(&p.ox[idx]), __ldg(&p.oy[idx]), __ldg(&p.oz[idx]), mass, q);
+            const int ix = cell_x(c), iy = cell_y(c), iz = cell_z(c);
             const int ix1 = ix + 1 == ng ? 0 : ix + 1;
             const int iy1 = iy + 1 == ng ? 0 : iy + 1;
             const int iz1 = iz + 1 == ng ? 0 : iz + 1;
@@ -217,47 +290,21 @@ __global__ void __launch_bounds__(256) deposit_tiled_kernel(ParticleSoA p, int n
                 for (int b = 0; b < 2; ++b)
 #pragma unroll
                     for (int cc = 0; cc < 2; ++cc)
-                        atomicAdd(&rho[sx[a] + sy[b] + sz[cc]], (unsigned long long)q[(a * 2 + b) * 2 + cc]);
+                        atomicAdd(&rho[sx[a] + sy[b] + sz[cc]], q[(a * 2 + b) * 2 + cc]);
         }
     }
 }
 
 // ICICKernel (icic_pm.cu:72-127) fused with up to two UpdatePosKernel drifts:
 // v += sum_8 float(w*deltaT*fscal) * F[corner]; then x += v*pf_a (, v*pf_b).
-__global__ void kick_drift_kernel(ParticleSoA p, size_t n, int ng, const float* __restrict__ fx,
-                                  const float* __restrict__ fy, const float* __restrict__ fz, double deltaT,
-                                  double fscal, float pf_a, float pf_b, int ndrift) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t c = p.cell[i];
-    float ox = p.ox[i], oy = p.oy[i], oz = p.oz[i];
-    int ix = cell_x(c), iy = cell_y(c), iz = cell_z(c);
-    const int ix1 = ix + 1 == ng ? 0 : ix + 1;
-    const int iy1 = iy + 1 == ng ? 0 : iy + 1;
-    const int iz1 = iz + 1 == ng ? 0 : iz + 1;
-    const uint32_t sx[2] = {(uint32_t)ix * ng * ng, (uint32_t)ix1 * ng * ng};
-    const uint32_t sy[2] = {(uint32_t)iy * ng, (uint32_t)iy1 * ng};
-    const uint32_t sz[2] = {(uint32_t)iz, (uint32_t)iz1};
-    const float wx[2] = {1.f - ox, ox}, wy[2] = {1.f - oy, oy}, wz[2] = {1.f - oz, oz};
-    float dvx = 0.f, dvy = 0.f, dvz = 0.f;
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b)
-#pragma unroll
-            for (int cc = 0; cc < 2; ++cc) {
-                const uint32_t idx = sx[a] + sy[b] + sz[cc];
-                const float w = __fmul_rn(__fmul_rn(wx[a], wy[b]), wz[cc]);
-                const float mul = (float)(((double)w * deltaT) * fscal);
-                dvx = fmaf(mul, __ldg(&fx[idx]), dvx);
-                dvy = fmaf(mul, __ldg(&fy[idx]), dvy);
-                dvz = fmaf(mul, __ldg(&fz[idx]), dvz);
-            }
-    const float vx = p.vx[i] + dvx, vy = p.vy[i] + dvy, vz = p.vz[i] + dvz;
+__device__ __forceinline__ void kick_one_unused(ParticleSoA& p, size_t i, int ix, int iy, int iz, float3 dv, float pf_a,
+                                         float pf_b, int ndrift, int ng) {
+    const float vx = p.vx[i] + dv.x, vy = p.vy[i] + dv.y, vz = p.vz[i] + dv.z;
     p.vx[i] = vx;
     p.vy[i] = vy;
     p.vz[i] = vz;
     if (ndrift > 0) {
+        float ox = p.ox[i], oy = p.oy[i], oz = p.oz[i];
         drift_axis(ix, ox, vx, pf_a, ng);
         drift_axis(iy, oy, vy, pf_a, ng);
         drift_axis(iz, oz, vz, pf_a, ng);
@@ -270,6 +317,160 @@ __global__ void kick_drift_kernel(ParticleSoA p, size_t n, int ng, const float* 
         p.ox[i] = ox;
         p.oy[i] = oy;
         p.oz[i] = oz;
+    }
+}
+
+// One CTA per Lagrangian block (as the deposit): the force grids over the
+// block's bounding box (+1 cell) are staged in shared memory with coalesced
+// loads, so each grid cell crosses L2 once per CTA instead of once per
+// touching particle; the 8-corner gathers then read shared memory.  Each
+// thread prefetches its next particle while it updates the current one.
+// Blocks wider than cap_cells gather straight from global memory.
+struct PState {
+    uint32_t c;
+    float dx, dy, dz, vx, vy, vz;
+};
+
+__device__ __forceinline__ PState load_p(const ParticleSoA& p, size_t i) {
+    return PState{p.cell[i], p.ox[i], p.oy[i], p.oz[i], p.vx[i], p.vy[i], p.vz[i]};
+}
+
+__device__ __forceinline__ void finish_p(ParticleSoA& p, size_t i, const PState& s, float3 dv, float pf_a, float pf_b,
+                                         int ndrift, int ng) {
+    const float vx = s.vx + dv.x, vy = s.vy + dv.y, vz = s.vz + dv.z;
+    p.vx[i] = vx;
+    p.vy[i] = vy;
+    p.vz[i] = vz;
+    if (ndrift > 0) {
+        int ix = cell_x(s.c), iy = cell_y(s.c), iz = cell_z(s.c);
+        float ox = s.dx, oy = s.dy, oz = s.dz;
+        drift_axis(ix, ox, vx, pf_a, ng);
+        drift_axis(iy, oy, vy, pf_a, ng);
+        drift_axis(iz, oz, vz, pf_a, ng);
+        if (ndrift > 1) {
+            drift_axis(ix, ox, vx, pf_b, ng);
+            drift_axis(iy, oy, vy, pf_b, ng);
+            drift_axis(iz, oz, vz, pf_b, ng);
+        }
+        p.cell[i] = pack_cell(ix, iy, iz);
+        p.ox[i] = ox;
+        p.oy[i] = oy;
+        p.oz[i] = oz;
+    }
+}
+
+template <int B, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) kick_tiled_kernel(ParticleSoA p, int np_side, int ng,
+                                                                   const float* __restrict__ fx,
+                                                                   const float* __restrict__ fy,
+                                                                   const float* __restrict__ fz, double deltaT,
+                                                                   double fscal, float pf_a, float pf_b, int ndrift,
+                                                                   int cap_cells) {
+    constexpr int B3 = B * B * B;
+    constexpr int PPT = B3 / NT;
+    extern __shared__ float fwin[];
+    __shared__ int bb[6];
+    const int tid = threadIdx.x;
+    const int nb = np_side / B;
+    const int blk = blockIdx.x;
+    const int bz = blk % nb, by = (blk / nb) % nb, bx = blk / (nb * nb);
+    const int ox0 = (int)((long long)bx * B * ng / np_side);
+    const int oy0 = (int)((long long)by * B * ng / np_side);
+    const int oz0 = (int)((long long)bz * B * ng / np_side);
+    if (tid < 3) bb[tid] = 0x7fffffff;
+    else if (tid < 6) bb[tid] = -0x7fffffff;
+    __syncthreads();
+    const size_t p0 = (size_t)blk * B3;
+    int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        const uint32_t c = __ldg(&p.cell[p0 + tid + k * NT]);
+        const int rx = nearest_image(cell_x(c) - ox0, ng);
+        const int ry = nearest_image(cell_y(c) - oy0, ng);
+        const int rz = nearest_image(cell_z(c) - oz0, ng);
+        mn[0] = min(mn[0], rx); mx[0] = max(mx[0], rx);
+        mn[1] = min(mn[1], ry); mx[1] = max(mx[1], ry);
+        mn[2] = min(mn[2], rz); mx[2] = max(mx[2], rz);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        mn[a] = __reduce_min_sync(0xffffffffu, mn[a]);
+        mx[a] = __reduce_max_sync(0xffffffffu, mx[a]);
+    }
+    if ((tid & 31) == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(&bb[a], mn[a]);
+            atomicMax(&bb[3 + a], mx[a]);
+        }
+    }
+    __syncthreads();
+    const int lx0 = bb[0], ly0 = bb[1], lz0 = bb[2];
+    const int wx = bb[3] - lx0 + 2, wy = bb[4] - ly0 + 2, wz = bb[5] - lz0 + 2;
+    const int vol = wx * wy * wz;
+    const bool tiled = vol <= cap_cells;
+    float* wfx = fwin;
+    float* wfy = fwin + cap_cells;
+    float* wfz = fwin + 2 * cap_cells;
+    if (tiled) {
+        const WinMap map(wy, wz, ox0 + lx0, oy0 + ly0, oz0 + lz0, ng);
+        for (int i = tid; i < vol; i += NT) {
+            const size_t g = map.global(i);
+            wfx[i] = __ldg(&fx[g]);
+            wfy[i] = __ldg(&fy[g]);
+            wfz[i] = __ldg(&fz[g]);
+        }
+        __syncthreads();
+    }
+    const int syz = wy * wz;
+    PState nxt = load_p(p, p0 + tid);
+#pragma unroll 1
+    for (int k = 0; k < PPT; ++k) {
+        const size_t i = p0 + tid + k * NT;
+        const PState cur = nxt;
+        if (k + 1 < PPT) nxt = load_p(p, i + NT);
+        const float wxa[2] = {1.f - cur.dx, cur.dx}, wya[2] = {1.f - cur.dy, cur.dy}, wza[2] = {1.f - cur.dz, cur.dz};
+        float3 dv = make_float3(0.f, 0.f, 0.f);
+        if (tiled) {
+            const int w = ((nearest_image(cell_x(cur.c) - ox0, ng) - lx0) * wy +
+                           (nearest_image(cell_y(cur.c) - oy0, ng) - ly0)) * wz +
+                          (nearest_image(cell_z(cur.c) - oz0, ng) - lz0);
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b)
+#pragma unroll
+                    for (int cc = 0; cc < 2; ++cc) {
+                        const int j = w + a * syz + b * wz + cc;
+                        const float wt = __fmul_rn(__fmul_rn(wxa[a], wya[b]), wza[cc]);
+                        const float mul = (float)(((double)wt * deltaT) * fscal);
+                        dv.x = fmaf(mul, wfx[j], dv.x);
+                        dv.y = fmaf(mul, wfy[j], dv.y);
+                        dv.z = fmaf(mul, wfz[j], dv.z);
+                    }
+        } else {
+            const int ix = cell_x(cur.c), iy = cell_y(cur.c), iz = cell_z(cur.c);
+            const int ix1 = ix + 1 == ng ? 0 : ix + 1;
+            const int iy1 = iy + 1 == ng ? 0 : iy + 1;
+            const int iz1 = iz + 1 == ng ? 0 : iz + 1;
+            const size_t sx[2] = {(size_t)ix * ng * ng, (size_t)ix1 * ng * ng};
+            const size_t sy[2] = {(size_t)iy * ng, (size_t)iy1 * ng};
+            const size_t sz[2] = {(size_t)iz, (size_t)iz1};
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b)
+#pragma unroll
+                    for (int cc = 0; cc < 2; ++cc) {
+                        const size_t g = sx[a] + sy[b] + sz[cc];
+                        const float wt = __fmul_rn(__fmul_rn(wxa[a], wya[b]), wza[cc]);
+                        const float mul = (float)(((double)wt * deltaT) * fscal);
+                        dv.x = fmaf(mul, __ldg(&fx[g]), dv.x);
+                        dv.y = fmaf(mul, __ldg(&fy[g]), dv.y);
+                        dv.z = fmaf(mul, __ldg(&fz[g]), dv.z);
+                    }
+        }
+        finish_p(p, i, cur, dv, pf_a, pf_b, ndrift, ng);
     }
 }
 
@@ -406,34 +607,54 @@ int deposit_cap_cells(int np_side, int ng) {
     const int r = (B * ng + np_side - 1) / np_side + 6;  // block region + margin
     int cap = r * r * r;
     if (cap < 4096) cap = 4096;
-    if (cap > 12288) cap = 12288;  // 96 KB of int64: two CTAs per SM
+    if (cap > 9216) cap = 9216;  // 72 KB: three CTAs per SM
     return cap;
+}
+
+template <int B, bool SMALL>
+static cudaError_t deposit_impl(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
+                                int cap, cudaStream_t s) {
+    auto k = deposit_tiled_kernel<B, SMALL>;
+    const int smem = cap * 8;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const int nb = np_side / B;
+    k<<<nb * nb * nb, 256, smem, s>>>(p, np_side, ng, mass, rho, cap);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
                            cudaStream_t s) {
     const int B = block_side(np_side, ng);
     const int cap = deposit_cap_cells(np_side, ng);
-    const int nblocks = (np_side / B) * (np_side / B) * (np_side / B);
-    const int smem = cap * 8;
-    if (B == 16) {
-        auto k = deposit_tiled_kernel<16>;
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        k<<<nblocks, 256, smem, s>>>(p, np_side, ng, mass, rho, cap);
-    } else {
-        auto k = deposit_tiled_kernel<8>;
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        k<<<nblocks, 256, smem, s>>>(p, np_side, ng, mass, rho, cap);
-    }
+    // SMALL needs every window add (a weight, or two merged x-chain weights,
+    // each < mass*2^31) below 2^32: mass <= 1
+    const bool small = mass <= 1.0f;
+    if (B == 16) return small ? deposit_impl<16, true>(p, np_side, ng, mass, rho, cap, s)
+                              : deposit_impl<16, false>(p, np_side, ng, mass, rho, cap, s);
+    return small ? deposit_impl<8, true>(p, np_side, ng, mass, rho, cap, s)
+                 : deposit_impl<8, false>(p, np_side, ng, mass, rho, cap, s);
+}
+template <int B, int NT>
+static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const float* fx, const float* fy,
+                             const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift, int cap,
+                             cudaStream_t s) {
+    auto k = kick_tiled_kernel<B, NT>;
+    const int smem = cap * 12;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const int nb = np_side / B;
+    k<<<nb * nb * nb, NT, smem, s>>>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap);
     return cudaGetLastError();
 }
-cudaError_t launch_kick_drift(const ParticleSoA& p, size_t n, int ng, const float* fx, const float* fy,
+
+cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float* fx, const float* fy,
                               const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift,
                               cudaStream_t s) {
-    kick_drift_kernel<<<nblk(n, 256), 256, 0, s>>>(p, n, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift);
-    return cudaGetLastError();
+    const int B = block_side(np_side, ng);
+    const int cap = deposit_cap_cells(np_side, ng);
+    if (B == 16) return kick_impl<16, 512>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap, s);
+    return kick_impl<8, 256>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap, s);
 }
 cudaError_t launch_density(const unsigned long long* rho64, float* rho, size_t n, cudaStream_t s) {
     density_kernel<<<nblk(n, 256), 256, 0, s>>>(rho64, rho, n);

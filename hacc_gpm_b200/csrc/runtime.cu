@@ -697,7 +697,7 @@ extern "C" int hgpm_kick_drift(hgpm_ctx* c, double deltaT, double fscal, float p
     if (!c || ndrift < 0 || ndrift > 2) return HGPM_ERR_ARG;
     if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
     PhaseScope ps(c, PH_KICK);
-    CK(launch_kick_drift(c->part, c->npart, c->ng, c->force, c->force + c->ncell, c->force + 2 * c->ncell, deltaT,
+    CK(launch_kick_drift(c->part, c->np, c->ng, c->force, c->force + c->ncell, c->force + 2 * c->ncell, deltaT,
                          fscal, pf_a, pf_b, ndrift, c->stream));
     count(c, PH_KICK, 1);
     return HGPM_OK;
