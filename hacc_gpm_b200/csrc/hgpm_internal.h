@@ -39,6 +39,11 @@ cudaError_t launch_xpk(int ng, const float2* in, int ncols, size_t rs, size_t ps
                        double* part_sum, unsigned long long* part_cnt, int nparts, double* sum,
                        unsigned long long* cnt, cudaStream_t s);
 
+// Persistent TMA-fed strided pass over a half-spectrum buffer (y lines, or x
+// lines when isx); err is set if a bounded mbarrier wait times out.
+cudaError_t launch_strided_tma(int ng, bool inv, bool isx, float2* data, int ncols, int zs, size_t cs, int ncomp,
+                               const float2* tw, int* err, cudaStream_t s);
+
 cudaError_t launch_load_state(const float* x, const float* v, const ParticleSoA& p, int np_side, int B, int ng,
                               cudaStream_t s);
 cudaError_t launch_store_state(const ParticleSoA& p, float* x, float* v, int np_side, int B, cudaStream_t s);

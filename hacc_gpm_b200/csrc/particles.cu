@@ -242,12 +242,22 @@ __global__ void __launch_bounds__(256, 3) deposit_tiled_kernel(ParticleSoA p, in
         const int off[4] = {0, 1, wz, wz + 1};  // (b, c) corner offsets in the window
         unsigned long long pend[4] = {0ull, 0ull, 0ull, 0ull};
         int pw = -1;  // window index of the pending (upper-x) face; -1: none
-#pragma unroll 2
+        // next particle's cell and offsets are loaded one iteration ahead
+        uint32_t nc = __ldg(&p.cell[p0 + tid]);
+        float nx = __ldg(&p.ox[p0 + tid]), ny = __ldg(&p.oy[p0 + tid]), nz = __ldg(&p.oz[p0 + tid]);
+#pragma unroll 1
         for (int k = 0; k < PPT; ++k) {
-            const size_t idx = p0 + tid + k * 256;
-            const uint32_t c = __ldg(&p.cell[idx]);
+            const uint32_t c = nc;
+            const float cx = nx, cy = ny, cz = nz;
+            if (k + 1 < PPT) {
+                const size_t nidx = p0 + tid + (k + 1) * 256;
+                nc = __ldg(&p.cell[nidx]);
+                nx = __ldg(&p.ox[nidx]);
+                ny = __ldg(&p.oy[nidx]);
+                nz = __ldg(&p.oz[nidx]);
+            }
             unsigned long long q[8];
-            cic_fixed<SMALL>(__ldg(&p.ox[idx]), __ldg(&p.oy[idx]), __ldg(&p.oz[idx]), mass, q);
+            cic_fixed<SMALL>(cx, cy, cz, mass, q);
             const int cw = ((nearest_image(cell_x(c) - ox, ng) - lx0) * wy + (nearest_image(cell_y(c) - oy, ng) - ly0)) *
                                wz + (nearest_image(cell_z(c) - oz, ng) - lz0);
             if (pw == cw) {
@@ -423,13 +433,17 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_tiled_kernel(ParticleSoA p
         __syncthreads();
     }
     const int syz = wy * wz;
+    // the kick factor deltaT*fscal is folded into the x weight (FP32; the
+    // reference forms float(w*deltaT*fscal) in double, a <=1 ulp difference)
+    const float dtf = (float)(deltaT * fscal);
     PState nxt = load_p(p, p0 + tid);
 #pragma unroll 1
     for (int k = 0; k < PPT; ++k) {
         const size_t i = p0 + tid + k * NT;
         const PState cur = nxt;
         if (k + 1 < PPT) nxt = load_p(p, i + NT);
-        const float wxa[2] = {1.f - cur.dx, cur.dx}, wya[2] = {1.f - cur.dy, cur.dy}, wza[2] = {1.f - cur.dz, cur.dz};
+        const float wxa[2] = {(1.f - cur.dx) * dtf, cur.dx * dtf}, wya[2] = {1.f - cur.dy, cur.dy},
+                    wza[2] = {1.f - cur.dz, cur.dz};
         float3 dv = make_float3(0.f, 0.f, 0.f);
         if (tiled) {
             const int w = ((nearest_image(cell_x(cur.c) - ox0, ng) - lx0) * wy +
@@ -442,8 +456,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_tiled_kernel(ParticleSoA p
 #pragma unroll
                     for (int cc = 0; cc < 2; ++cc) {
                         const int j = w + a * syz + b * wz + cc;
-                        const float wt = __fmul_rn(__fmul_rn(wxa[a], wya[b]), wza[cc]);
-                        const float mul = (float)(((double)wt * deltaT) * fscal);
+                        const float mul = __fmul_rn(__fmul_rn(wxa[a], wya[b]), wza[cc]);
                         dv.x = fmaf(mul, wfx[j], dv.x);
                         dv.y = fmaf(mul, wfy[j], dv.y);
                         dv.z = fmaf(mul, wfz[j], dv.z);
@@ -463,8 +476,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_tiled_kernel(ParticleSoA p
 #pragma unroll
                     for (int cc = 0; cc < 2; ++cc) {
                         const size_t g = sx[a] + sy[b] + sz[cc];
-                        const float wt = __fmul_rn(__fmul_rn(wxa[a], wya[b]), wza[cc]);
-                        const float mul = (float)(((double)wt * deltaT) * fscal);
+                        const float mul = __fmul_rn(__fmul_rn(wxa[a], wya[b]), wza[cc]);
                         dv.x = fmaf(mul, __ldg(&fx[g]), dv.x);
                         dv.y = fmaf(mul, __ldg(&fy[g]), dv.y);
                         dv.z = fmaf(mul, __ldg(&fz[g]), dv.z);

@@ -323,6 +323,7 @@ struct hgpm_ctx {
     float* kf_pk = nullptr;
     float* kf_ic = nullptr;
     int* d_err = nullptr;
+    bool tma = true;  // TMA-fed persistent y passes (HGPM_NO_TMA=1 selects the plain kernels)
     float* stage = nullptr;     // AoS float3 x, v staging (lazy)
     double* pk_part = nullptr;  // P(k) partial sums (lazy)
     unsigned long long* pk_pcnt = nullptr;
@@ -440,6 +441,10 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bad(HGPM_ERR_CUDA, cudaGetErrorString(e));
     c->ncell = (size_t)c->ng * c->ng * c->ng;
+    {
+        const char* nt = getenv("HGPM_NO_TMA");
+        c->tma = !(nt && nt[0] == '1');
+    }
     c->blk = block_side(c->np, c->ng);
     c->npart = (size_t)c->np * c->np * c->np;
     c->zs = even_pad(c->ng / 2 + 1);
@@ -474,7 +479,9 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
         if ((e = cudaMalloc(&c->pkw, c->ng * 4)) != cudaSuccess) break;
         if ((e = cudaMalloc(&c->kf_pk, c->ng * 4)) != cudaSuccess) break;
         if ((e = cudaMalloc(&c->kf_ic, c->np * 4)) != cudaSuccess) break;
-        if ((e = cudaMalloc(&c->d_err, 4)) != cudaSuccess) break;
+        // d_err[0]: IC table overrun; d_err[1]: a bounded TMA/mbarrier wait timed out
+        if ((e = cudaMalloc(&c->d_err, 8)) != cudaSuccess) break;
+        if ((e = cudaMemsetAsync(c->d_err, 0, 8, c->stream)) != cudaSuccess) break;
         std::vector<float2> t1 = twiddles(c->ng), t2 = twiddles(c->np);
         if ((e = cudaMemcpy(c->tw_ng, t1.data(), c->ng * 8, cudaMemcpyHostToDevice)) != cudaSuccess) break;
         if ((e = cudaMemcpy(c->tw_np, t2.data(), c->np * 8, cudaMemcpyHostToDevice)) != cudaSuccess) break;
@@ -526,10 +533,21 @@ extern "C" void* hgpm_stream(hgpm_ctx* c) { return c ? (void*)c->stream : nullpt
 extern "C" int hgpm_ng(const hgpm_ctx* c) { return c ? c->ng : 0; }
 extern "C" int hgpm_np(const hgpm_ctx* c) { return c ? c->np : 0; }
 
+// Synchronise and report a timed-out bounded wait of a TMA pass, if any.
+static int sync_check(hgpm_ctx* c) {
+    int herr[2] = {0, 0};
+    CK(cudaMemcpyAsync(herr, c->d_err, 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (herr[1]) {
+        cudaMemsetAsync(c->d_err + 1, 0, 4, c->stream);
+        return fail(c, HGPM_ERR_CUDA, "a TMA-fed FFT pass timed out waiting for its tile (results invalid)");
+    }
+    return HGPM_OK;
+}
+
 extern "C" int hgpm_sync(hgpm_ctx* c) {
     if (!c) return HGPM_ERR_ARG;
-    CK(cudaStreamSynchronize(c->stream));
-    return HGPM_OK;
+    return sync_check(c);
 }
 
 // ===========================================================================
@@ -578,8 +596,7 @@ extern "C" int hgpm_store_state(hgpm_ctx* c, float* x, float* v) {
     size_t bytes = c->npart * 3 * sizeof(float);
     CK(cudaMemcpyAsync(x, c->stage, bytes, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaMemcpyAsync(v, c->stage + 3 * c->npart, bytes, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    return HGPM_OK;
+    return sync_check(c);
 }
 
 extern "C" int hgpm_get_cells(hgpm_ctx* c, int32_t* cells) {
@@ -654,7 +671,11 @@ static int forward_zy(hgpm_ctx* c) {
     }
     {
         PhaseScope ps(c, PH_YFWD);
-        CK(launch_strided(ng, false, c->spec, M + 1, (size_t)c->zs, (size_t)ng * c->zs, ng, 0, 1, c->tw_ng, c->stream));
+        if (c->tma)
+            CK(launch_strided_tma(ng, false, false, c->spec, M + 1, c->zs, 0, 1, c->tw_ng, c->d_err + 1, c->stream));
+        else
+            CK(launch_strided(ng, false, c->spec, M + 1, (size_t)c->zs, (size_t)ng * c->zs, ng, 0, 1, c->tw_ng,
+                              c->stream));
         count(c, PH_YFWD, 1);
     }
     return HGPM_OK;
@@ -675,7 +696,11 @@ extern "C" int hgpm_solve_gradient(hgpm_ctx* c) {
     }
     {
         PhaseScope ps(c, PH_YINV);
-        CK(launch_strided(ng, true, c->fspec, M + 1, (size_t)c->zs, (size_t)ng * c->zs, ng, cs, 3, c->tw_ng, c->stream));
+        if (c->tma)
+            CK(launch_strided_tma(ng, true, false, c->fspec, M + 1, c->zs, cs, 3, c->tw_ng, c->d_err + 1, c->stream));
+        else
+            CK(launch_strided(ng, true, c->fspec, M + 1, (size_t)c->zs, (size_t)ng * c->zs, ng, cs, 3, c->tw_ng,
+                              c->stream));
         count(c, PH_YINV, 1);
     }
     {

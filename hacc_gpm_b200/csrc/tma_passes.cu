@@ -1,0 +1,252 @@
+// tma_passes.cu — strided FFT passes (y lines, and x lines for the plain
+// transforms) as persistent kernels fed by TMA.
+//
+// Each CTA walks tiles t = blockIdx.x, +gridDim.x, ...; a tile is NG rows
+// (the FFT axis) by CT contiguous complex columns of one plane of one
+// component.  Thread 0 issues cp.async.bulk.tensor loads of the NEXT tile
+// into the other shared-memory buffer (completion on an mbarrier with a
+// transaction count) while all threads transform the current tile; the
+// result goes back with a cp.async.bulk.tensor store.  The tensor map's
+// inner extent is the valid half-spectrum width (ng/2 + 1 complex), so the
+// ragged last column chunk is zero-filled on load and clipped on store.
+// No multicast is used anywhere.  Every mbarrier wait is bounded: on time-out
+// the CTA records an error, waits (bounded) for its own copies and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft_engine.cuh"
+#include "hgpm_device.cuh"
+#include "hgpm_internal.h"
+
+namespace hgpm {
+
+constexpr int kTmaThreads = 256;
+constexpr unsigned kMaxPolls = 1u << 22;
+
+template <int NG> struct TmaCfg {
+    static constexpr int CT = NG <= 256 ? 16 : (NG <= 512 ? 8 : 4);  // complex columns per tile
+    // rows per TMA box: a divisor of NG that is <= 256 (384 -> 2 x 192)
+    static constexpr int RB = NG <= 256 ? NG : (NG % 256 == 0 ? 256 : NG / 2);
+    static constexpr int NBOX = NG / RB;
+    static constexpr int TILE_BYTES = NG * CT * 8;
+    static constexpr int SMEM = 2 * TILE_BYTES + 1024;               // + alignment slack
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// bounded wait: false after kMaxPolls unsuccessful polls
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (unsigned i = 0; i < kMaxPolls; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap* tm, int c0, int c1, int c2, int c3, const void* src) {
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(
+                     reinterpret_cast<uint64_t>(tm)),
+                 "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(src))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// tile t -> (column chunk, plane, component)
+struct TileIdx {
+    int chunk, plane, comp;
+};
+__device__ __forceinline__ TileIdx tile_of(int t, int nchunks, int nplanes) {
+    TileIdx r;
+    r.chunk = t % nchunks;
+    const int rest = t / nchunks;
+    r.plane = rest % nplanes;
+    r.comp = rest / nplanes;
+    return r;
+}
+
+// ISX = false: lines along y (tensor dim 1), plane = x (dim 2).
+// ISX = true : lines along x (tensor dim 2), plane = y (dim 1).
+template <int NG, bool ISX>
+__device__ __forceinline__ void issue_tile_load(const CUtensorMap* tm, float2* buf, uint64_t* bar, const TileIdx& ti) {
+    using G = TmaCfg<NG>;
+    mbar_expect_tx(bar, G::TILE_BYTES);
+    const int c0 = 2 * G::CT * ti.chunk;
+#pragma unroll
+    for (int b = 0; b < G::NBOX; ++b) {
+        float2* dst = buf + (size_t)b * G::RB * G::CT;
+        if (ISX) tma_load_4d(dst, tm, c0, ti.plane, b * G::RB, ti.comp, bar);
+        else tma_load_4d(dst, tm, c0, b * G::RB, ti.plane, ti.comp, bar);
+    }
+}
+
+template <int NG, bool ISX>
+__device__ __forceinline__ void issue_tile_store(const CUtensorMap* tm, const float2* buf, const TileIdx& ti) {
+    using G = TmaCfg<NG>;
+    const int c0 = 2 * G::CT * ti.chunk;
+#pragma unroll
+    for (int b = 0; b < G::NBOX; ++b) {
+        const float2* src = buf + (size_t)b * G::RB * G::CT;
+        if (ISX) tma_store_4d(tm, c0, ti.plane, b * G::RB, ti.comp, src);
+        else tma_store_4d(tm, c0, b * G::RB, ti.plane, ti.comp, src);
+    }
+    bulk_commit();
+}
+
+template <int NG, bool INV, bool ISX>
+__global__ void __launch_bounds__(kTmaThreads, 2) strided_tma_kernel(const __grid_constant__ CUtensorMap tm, int nchunks,
+                                                                  int nplanes, int ncomp, const float2* __restrict__ tw,
+                                                                  int* __restrict__ err) {
+    using G = TmaCfg<NG>;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* base =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    float2* buf[2] = {reinterpret_cast<float2*>(base), reinterpret_cast<float2*>(base + G::TILE_BYTES)};
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int failed;
+    const int ntiles = nchunks * nplanes * ncomp;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        failed = 0;
+        fence_async_shared();
+    }
+    __syncthreads();
+    int t = blockIdx.x;
+    if (threadIdx.x == 0 && t < ntiles) issue_tile_load<NG, ISX>(&tm, buf[0], &bar[0], tile_of(t, nchunks, nplanes));
+    int j = 0;
+    bool next_in_flight = false;
+    for (; t < ntiles; t += gridDim.x, ++j) {
+        const int cur = j & 1;
+        const int tn = t + gridDim.x;
+        if (threadIdx.x == 0) {
+            next_in_flight = false;
+            if (tn < ntiles) {
+                // the other buffer was stored from in the previous iteration
+                bulk_wait_read_all();
+                issue_tile_load<NG, ISX>(&tm, buf[cur ^ 1], &bar[cur ^ 1], tile_of(tn, nchunks, nplanes));
+                next_in_flight = true;
+            }
+            if (!mbar_wait_bounded(&bar[cur], (j >> 1) & 1)) failed = 1;
+        }
+        __syncthreads();
+        if (failed) break;
+        fft_tile<NG, G::CT, G::CT, INV, kTmaThreads>(buf[cur], tw);
+        fence_async_shared();
+        __syncthreads();
+        if (threadIdx.x == 0) issue_tile_store<NG, ISX>(&tm, buf[cur], tile_of(t, nchunks, nplanes));
+    }
+    if (threadIdx.x == 0) {
+        if (failed) {
+            atomicExch(err, 1);
+            // the current load never completed; also drain the prefetched one
+            mbar_wait_bounded(&bar[j & 1], (j >> 1) & 1);
+            if (next_in_flight) mbar_wait_bounded(&bar[(j + 1) & 1], ((j + 1) >> 1) & 1);
+        }
+        bulk_wait_all();
+    }
+}
+
+// ---------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+static bool encode_fn() {
+    if (g_encode) return true;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+        return false;
+    g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    return true;
+}
+
+// Tensor map over a half-spectrum buffer: dims (2*ncols floats, ng, ng, ncomp),
+// row stride zs complex, component stride cs complex.
+static cudaError_t make_spec_map(CUtensorMap* tm, float2* data, int ng, int ncols, int zs, size_t cs, int ncomp,
+                                 int ct, int rb, bool isx) {
+    if (!encode_fn()) return cudaErrorNotSupported;
+    cuuint64_t dims[4] = {(cuuint64_t)(2 * ncols), (cuuint64_t)ng, (cuuint64_t)ng, (cuuint64_t)ncomp};
+    cuuint64_t strides[3] = {(cuuint64_t)zs * 8, (cuuint64_t)ng * zs * 8, (cuuint64_t)(cs ? cs : (size_t)ng * ng * zs) * 8};
+    cuuint32_t box[4] = {(cuuint32_t)(2 * ct), isx ? 1u : (cuuint32_t)rb, isx ? (cuuint32_t)rb : 1u, 1u};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = g_encode(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, data, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+static int g_num_sms = 0;
+
+template <int NG>
+static cudaError_t tma_impl(bool inv, bool isx, float2* data, int ncols, int zs, size_t cs, int ncomp,
+                            const float2* tw, int* err, cudaStream_t s) {
+    using G = TmaCfg<NG>;
+    CUtensorMap tm;
+    cudaError_t e = make_spec_map(&tm, data, NG, ncols, zs, cs, ncomp, G::CT, G::RB, isx);
+    if (e != cudaSuccess) return e;
+    if (!g_num_sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    const int nchunks = (ncols + G::CT - 1) / G::CT;
+    const int ntiles = nchunks * NG * ncomp;
+    // persistent grid: exactly the CTAs that are resident at once (no tail wave)
+#define HGPM_TMA_LAUNCH(I, X)                                                                       \
+    {                                                                                               \
+        auto k = strided_tma_kernel<NG, I, X>;                                                      \
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);          \
+        if (e != cudaSuccess) return e;                                                             \
+        int per_sm = 1;                                                                             \
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTmaThreads, G::SMEM);            \
+        int grid = g_num_sms * (per_sm < 1 ? 1 : per_sm);                                           \
+        if (grid > ntiles) grid = ntiles;                                                           \
+        k<<<grid, kTmaThreads, G::SMEM, s>>>(tm, nchunks, NG, ncomp, tw, err);                      \
+    }
+    if (inv) {
+        if (isx) HGPM_TMA_LAUNCH(true, true) else HGPM_TMA_LAUNCH(true, false)
+    } else {
+        if (isx) HGPM_TMA_LAUNCH(false, true) else HGPM_TMA_LAUNCH(false, false)
+    }
+#undef HGPM_TMA_LAUNCH
+    return cudaGetLastError();
+}
+
+cudaError_t launch_strided_tma(int ng, bool inv, bool isx, float2* data, int ncols, int zs, size_t cs, int ncomp,
+                               const float2* tw, int* err, cudaStream_t s) {
+    switch (ng) {
+#define X(n) \
+    case n: return tma_impl<n>(inv, isx, data, ncols, zs, cs, ncomp, tw, err, s);
+        X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
+#undef X
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace hgpm

@@ -88,6 +88,23 @@ def test_solve_gradient_matches_oracle(ng):
     assert rel_max_err(f, fo) < FIELD_RTOL
 
 
+@pytest.mark.parametrize("ng", [48, 64, 128])
+def test_tma_and_plain_strided_passes_bit_identical(ng, monkeypatch):
+    """The persistent TMA-fed y passes and the plain strided kernels run the
+    same per-line transform, so forces are bit-identical."""
+    x, v = lattice_state(ng, ng, disp=1.3, seed=ng + 7)
+    out = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("HGPM_NO_TMA", flag)
+        with make(ng) as s:
+            s.load_state(x, v)
+            s.cic()
+            s.solve_gradient()
+            out.append(s.get_force())
+            s.sync()
+    assert np.array_equal(out[0], out[1])
+
+
 def test_solve_gradient_plane_wave_analytic():
     """Particles arranged so that rho = 1 + A cos(2 pi x/ng) exactly on the
     grid is not reachable with CIC; instead place a sheet and compare with
