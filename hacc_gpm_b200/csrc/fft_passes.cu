@@ -17,6 +17,7 @@
 #include "fft_engine.cuh"
 #include "hgpm_device.cuh"
 #include "hgpm_internal.h"
+#include "kspace_ops.cuh"
 
 namespace hgpm {
 
@@ -202,15 +203,29 @@ __global__ void __launch_bounds__(kThreads) zpass_c2r_kernel(const float2* __res
     out += (size_t)blockIdx.y * out_cs;
     const int line0 = blockIdx.x * L;
     constexpr int H = M / 2 + 1;
-    for (int i = threadIdx.x; i < L * H; i += kThreads) {
+    constexpr int TOT = L * H;
+    constexpr int PER = (TOT + kThreads - 1) / kThreads;
+    // register-staged: every (X[k], X[M-k]) pair of the thread is in flight
+    // before the first use
+    float2 rk[PER], rm[PER];
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int i = threadIdx.x + t * kThreads;
         const int l = i / H, k = i % H;
-        const int line = line0 + l;
-        float2 xk = make_float2(0.f, 0.f), xm = make_float2(0.f, 0.f);
-        if (line < nlines) {
-            const float2* src = in + (size_t)line * zs;
-            xk = src[k];
-            xm = src[M - k];
+        rk[t] = make_float2(0.f, 0.f);
+        rm[t] = make_float2(0.f, 0.f);
+        if (i < TOT && line0 + l < nlines) {
+            const float2* src = in + (size_t)(line0 + l) * zs;
+            rk[t] = __ldcs(&src[k]);
+            rm[t] = __ldcs(&src[M - k]);
         }
+    }
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int i = threadIdx.x + t * kThreads;
+        if (i >= TOT) break;
+        const int l = i / H, k = i % H;
+        float2 xk = rk[t], xm = rm[t];
         if (k == 0) {
             xk.y = 0.f;
             xm.y = 0.f;
@@ -221,10 +236,10 @@ __global__ void __launch_bounds__(kThreads) zpass_c2r_kernel(const float2* __res
         const float2 s = make_float2(xk.x + xm.x, xk.y - xm.y);
         const float2 d = make_float2(xk.x - xm.x, xk.y + xm.y);
         const float2 cd = cmulc(d, w);                  // conj(w) * d
-        const float2 t = make_float2(-cd.y, cd.x);      // i * conj(w) * d
-        buf[k * ES + l] = cadd(s, t);
+        const float2 tt = make_float2(-cd.y, cd.x);     // i * conj(w) * d
+        buf[k * ES + l] = cadd(s, tt);
         if (k != 0 && k != M - k) {
-            const float2 zm = csub(s, t);
+            const float2 zm = csub(s, tt);
             buf[(M - k) * ES + l] = make_float2(zm.x, -zm.y);
         }
     }
@@ -400,87 +415,6 @@ __global__ void pk_reduce_kernel(const double* __restrict__ part_sum, const unsi
     sum[b] = s;
     cnt[b] = n;
 }
-
-// ---------------------------------------------------------------------------
-// k-space operators
-// ---------------------------------------------------------------------------
-// Poisson + gradient, kspace_solve_gradient (kspace_solver.cu:55-90) with
-// calcGreens (calcGreens.hpp:11-25): t = G rho_k, F_d = -i sin(k_d) t.
-// cosq[i] = cos(k_i) - 1 (double) and sk[i] = sin(k_i) are tabulated once per
-// grid side; G is formed in double from the sum of the (non-positive) cosq
-// terms, so there is no cancellation near k = 0.
-// A derivative along d at the Nyquist index of d is anti-Hermitian in the
-// reference's full C2C (both partners carry the same signed k = -n/2), so its
-// real part — all the reference keeps — is exactly zero; the half-spectrum
-// C2R would instead Hermitian-extend it.  comp() therefore returns 0 there.
-struct PoissonOp {
-    const double* cosq;  // cos(k_i) - 1, one entry per grid index
-    const float* sk;     // sin(k_i)
-    double coeff;        // 0.5 / ng^3
-    int nyq;             // ng / 2
-    __device__ __forceinline__ float2 pre(int ix, int iy, int iz, float2 v) const {
-        const double s = __ldg(&cosq[ix]) + __ldg(&cosq[iy]) + __ldg(&cosq[iz]);
-        const float g = (s == 0.0) ? 0.f : (float)(coeff / s);
-        return make_float2(v.x * g, v.y * g);
-    }
-    __device__ __forceinline__ float2 comp(int d, int ix, int iy, int iz, float2 t) const {
-        const int id = d == 0 ? ix : (d == 1 ? iy : iz);
-        if (id == nyq) return make_float2(0.f, 0.f);
-        const float sd = __ldg(&sk[id]);
-        return make_float2(sd * t.y, -sd * t.x);
-    }
-};
-
-// Zel'dovich displacement (initializer.cpp:10-117): ScaleAmplitudes by
-// sqrt(P(|k|) n^3/rl^3) from the .ipk table (interpolation_initializer.cu:3-30),
-// then transformDensityField (transform_density_field_initializer.cu:72-112):
-// s_d = (Im k_d, -Re k_d) / (k^2 delta).
-struct ICOp {
-    const double* table;
-    int nbins;
-    double k_delta;
-    double pkscale;    // n^3 / rl^3
-    double inv_delta;  // 1 / delta
-    const float* kf;   // float(signed(i) * 2 pi / rl)
-    int* err;          // set when |k| runs past the table
-    __device__ __forceinline__ float2 pre(int ix, int iy, int iz, float2 v) const {
-        const float kx = __ldg(&kf[ix]), ky = __ldg(&kf[iy]), kz = __ldg(&kf[iz]);
-        const float k2f = __fadd_rn(__fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky)), __fmul_rn(kz, kz));
-        double y = 0.0;
-        if (!(ix == 0 && iy == 0 && iz == 0)) {
-            const double my_k = (double)__fsqrt_rn(k2f);
-            const int left = (int)(my_k / k_delta);
-            const int right = left + 1;
-            if (right >= nbins) {
-                atomicExch(err, 1);
-            } else if (left == 0) {
-                y = __ldg(&table[right]) * pkscale;
-            } else {
-                const double ly1 = log(__ldg(&table[left]));
-                const double lx1 = log(k_delta * (double)left);
-                const double ly2 = log(__ldg(&table[right]));
-                const double lx2 = log(k_delta * (double)right);
-                const double lx = log(my_k);
-                y = exp(ly1 + ((ly2 - ly1) / (lx2 - lx1)) * (lx - lx1)) * pkscale;
-            }
-        }
-        const double sc = sqrt(y);
-        v.x = (float)((double)v.x * sc);
-        v.y = (float)((double)v.y * sc);
-        const double k2 = (double)k2f;
-        const double mul = inv_delta * (k2 == 0.0 ? 0.0 : 1.0 / k2);
-        v.x = (float)((double)v.x * mul);
-        v.y = (float)((double)v.y * mul);
-        return v;
-    }
-    int nyq;           // n / 2
-    __device__ __forceinline__ float2 comp(int d, int ix, int iy, int iz, float2 t) const {
-        const int id = d == 0 ? ix : (d == 1 ? iy : iz);
-        if (id == nyq) return make_float2(0.f, 0.f);
-        const float kd = __ldg(&kf[id]);
-        return make_float2(t.y * kd, -t.x * kd);
-    }
-};
 
 // ---------------------------------------------------------------------------
 // host launchers (dispatch on the grid side)

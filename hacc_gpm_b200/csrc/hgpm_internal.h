@@ -43,6 +43,9 @@ cudaError_t launch_xpk(int ng, const float2* in, int ncols, size_t rs, size_t ps
 // lines when isx); err is set if a bounded mbarrier wait times out.
 cudaError_t launch_strided_tma(int ng, bool inv, bool isx, float2* data, int ncols, int zs, size_t cs, int ncomp,
                                const float2* tw, int* err, cudaStream_t s);
+// Persistent TMA-fed x pass fused with the Green's function and gradient.
+cudaError_t launch_xpoisson_tma(int ng, float2* in, float2* out, int ncols, int zs, size_t out_cs, const float2* tw,
+                                const double* cosq, const float* sk, double coeff, int* err, cudaStream_t s);
 
 cudaError_t launch_load_state(const float* x, const float* v, const ParticleSoA& p, int np_side, int B, int ng,
                               cudaStream_t s);

@@ -424,11 +424,30 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_tiled_kernel(ParticleSoA p
     float* wfz = fwin + 2 * cap_cells;
     if (tiled) {
         const WinMap map(wy, wz, ox0 + lx0, oy0 + ly0, oz0 + lz0, ng);
-        for (int i = tid; i < vol; i += NT) {
-            const size_t g = map.global(i);
-            wfx[i] = __ldg(&fx[g]);
-            wfy[i] = __ldg(&fy[g]);
-            wfz[i] = __ldg(&fz[g]);
+        // batches of 8 cells per thread: all 24 loads of a batch are in flight
+        // before the first shared store
+        constexpr int KB = 8;
+        for (int i0 = tid; i0 < vol; i0 += KB * NT) {
+            float a[KB], b[KB], c[KB];
+#pragma unroll
+            for (int u = 0; u < KB; ++u) {
+                const int i = i0 + u * NT;
+                if (i < vol) {
+                    const size_t g = map.global(i);
+                    a[u] = __ldg(&fx[g]);
+                    b[u] = __ldg(&fy[g]);
+                    c[u] = __ldg(&fz[g]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < KB; ++u) {
+                const int i = i0 + u * NT;
+                if (i < vol) {
+                    wfx[i] = a[u];
+                    wfy[i] = b[u];
+                    wfz[i] = c[u];
+                }
+            }
         }
         __syncthreads();
     }
@@ -436,12 +455,15 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_tiled_kernel(ParticleSoA p
     // the kick factor deltaT*fscal is folded into the x weight (FP32; the
     // reference forms float(w*deltaT*fscal) in double, a <=1 ulp difference)
     const float dtf = (float)(deltaT * fscal);
-    PState nxt = load_p(p, p0 + tid);
+    // particles are loaded two iterations ahead
+    PState n1 = load_p(p, p0 + tid);
+    PState n2 = PPT > 1 ? load_p(p, p0 + tid + NT) : n1;
 #pragma unroll 1
     for (int k = 0; k < PPT; ++k) {
         const size_t i = p0 + tid + k * NT;
-        const PState cur = nxt;
-        if (k + 1 < PPT) nxt = load_p(p, i + NT);
+        const PState cur = n1;
+        n1 = n2;
+        if (k + 2 < PPT) n2 = load_p(p, i + 2 * NT);
         const float wxa[2] = {(1.f - cur.dx) * dtf, cur.dx * dtf}, wya[2] = {1.f - cur.dy, cur.dy},
                     wza[2] = {1.f - cur.dz, cur.dz};
         float3 dv = make_float3(0.f, 0.f, 0.f);

@@ -690,8 +690,12 @@ extern "C" int hgpm_solve_gradient(hgpm_ctx* c) {
     const size_t cs = (size_t)ng * ng * c->zs;
     {
         PhaseScope ps(c, PH_POISSON);
-        CK(launch_xpoisson(ng, c->spec, c->fspec, M + 1, (size_t)ng * c->zs, (size_t)c->zs, ng, cs, c->tw_ng, c->cosq,
-                           c->sk, 0.5 / ((double)ng * ng * ng), c->stream));
+        if (c->tma)
+            CK(launch_xpoisson_tma(ng, c->spec, c->fspec, M + 1, c->zs, cs, c->tw_ng, c->cosq, c->sk,
+                                   0.5 / ((double)ng * ng * ng), c->d_err + 1, c->stream));
+        else
+            CK(launch_xpoisson(ng, c->spec, c->fspec, M + 1, (size_t)ng * c->zs, (size_t)c->zs, ng, cs, c->tw_ng,
+                               c->cosq, c->sk, 0.5 / ((double)ng * ng * ng), c->stream));
         count(c, PH_POISSON, 1);
     }
     {

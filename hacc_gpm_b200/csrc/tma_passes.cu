@@ -19,76 +19,10 @@
 #include "fft_engine.cuh"
 #include "hgpm_device.cuh"
 #include "hgpm_internal.h"
+#include "kspace_ops.cuh"
+#include "tma_util.cuh"
 
 namespace hgpm {
-
-constexpr int kTmaThreads = 256;
-constexpr unsigned kMaxPolls = 1u << 22;
-
-template <int NG> struct TmaCfg {
-    static constexpr int CT = NG <= 256 ? 16 : (NG <= 512 ? 8 : 4);  // complex columns per tile
-    // rows per TMA box: a divisor of NG that is <= 256 (384 -> 2 x 192)
-    static constexpr int RB = NG <= 256 ? NG : (NG % 256 == 0 ? 256 : NG / 2);
-    static constexpr int NBOX = NG / RB;
-    static constexpr int TILE_BYTES = NG * CT * 8;
-    static constexpr int SMEM = 2 * TILE_BYTES + 1024;               // + alignment slack
-};
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return done != 0;
-}
-// bounded wait: false after kMaxPolls unsuccessful polls
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (unsigned i = 0; i < kMaxPolls; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3,
-                                            uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
-        "[%6];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
-        : "memory");
-}
-__device__ __forceinline__ void tma_store_4d(const CUtensorMap* tm, int c0, int c1, int c2, int c3, const void* src) {
-    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(
-                     reinterpret_cast<uint64_t>(tm)),
-                 "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(src))
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-
-// tile t -> (column chunk, plane, component)
-struct TileIdx {
-    int chunk, plane, comp;
-};
-__device__ __forceinline__ TileIdx tile_of(int t, int nchunks, int nplanes) {
-    TileIdx r;
-    r.chunk = t % nchunks;
-    const int rest = t / nchunks;
-    r.plane = rest % nplanes;
-    r.comp = rest / nplanes;
-    return r;
-}
 
 // ISX = false: lines along y (tensor dim 1), plane = x (dim 2).
 // ISX = true : lines along x (tensor dim 2), plane = y (dim 1).
@@ -173,6 +107,97 @@ __global__ void __launch_bounds__(kTmaThreads, 2) strided_tma_kernel(const __gri
 }
 
 // ---------------------------------------------------------------------------
+// x pass fused with a k-space operator (Poisson gradient), persistent and
+// TMA-fed: the next x-line tile (all kx of one ky, CT kz columns) streams in
+// while the current one is transformed forward, multiplied by the operator and
+// transformed back three times; the three results leave with coalesced
+// streaming stores.
+template <int NG, int CT, int NT>
+__device__ __forceinline__ void store_rows(const float2* __restrict__ tile, float2* __restrict__ g, size_t rs,
+                                           int nvalid) {
+    constexpr int TPR = CT / 2;
+    constexpr int TOT = NG * TPR;
+#pragma unroll 4
+    for (int i = threadIdx.x; i < TOT; i += NT) {
+        const int e = i / TPR, c = 2 * (i % TPR);
+        const float4 v = *reinterpret_cast<const float4*>(&tile[e * CT + c]);
+        float2* dst = g + (size_t)e * rs + c;
+        if (c + 1 < nvalid) __stcs(reinterpret_cast<float4*>(dst), v);
+        else if (c < nvalid) dst[0] = make_float2(v.x, v.y);
+    }
+}
+
+template <int NG, class Op>
+__global__ void __launch_bounds__(kTmaThreads, 2) xfused_tma_kernel(const __grid_constant__ CUtensorMap tm,
+                                                                    float2* __restrict__ out, size_t out_cs, int ncols,
+                                                                    int zs, int nchunks, const float2* __restrict__ tw,
+                                                                    Op op, int* __restrict__ err) {
+    using G = TmaCfg<NG>;
+    constexpr int CT = G::CT, NT = kTmaThreads;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* base =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    float2* in[2] = {reinterpret_cast<float2*>(base), reinterpret_cast<float2*>(base + G::TILE_BYTES)};
+    float2* work = reinterpret_cast<float2*>(base + 2 * G::TILE_BYTES);
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int failed;
+    const int ntiles = nchunks * NG;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        failed = 0;
+        fence_async_shared();
+    }
+    __syncthreads();
+    int t = blockIdx.x;
+    if (threadIdx.x == 0 && t < ntiles) issue_tile_load<NG, true>(&tm, in[0], &bar[0], tile_of(t, nchunks, NG));
+    int j = 0;
+    bool next_in_flight = false;
+    const size_t rs = (size_t)NG * zs;
+    for (; t < ntiles; t += gridDim.x, ++j) {
+        const int cur = j & 1;
+        const int tn = t + gridDim.x;
+        if (threadIdx.x == 0) {
+            next_in_flight = false;
+            if (tn < ntiles) {
+                issue_tile_load<NG, true>(&tm, in[cur ^ 1], &bar[cur ^ 1], tile_of(tn, nchunks, NG));
+                next_in_flight = true;
+            }
+            if (!mbar_wait_bounded(&bar[cur], (j >> 1) & 1)) failed = 1;
+        }
+        __syncthreads();
+        if (failed) break;
+        const TileIdx ti = tile_of(t, nchunks, NG);
+        const int iy = ti.plane, col0 = ti.chunk * CT;
+        float2* tile = in[cur];
+        fft_tile<NG, CT, CT, false, NT>(tile, tw);
+        for (int i = threadIdx.x; i < NG * CT; i += NT) {
+            const int iz = col0 + i % CT;
+            tile[i] = iz < ncols ? op.pre(i / CT, iy, iz, tile[i]) : make_float2(0.f, 0.f);
+        }
+        float2* gout = out + (size_t)iy * zs + col0;
+#pragma unroll 1
+        for (int d = 0; d < 3; ++d) {
+            for (int i = threadIdx.x; i < NG * CT; i += NT) {
+                const int iz = col0 + i % CT;
+                work[i] = iz < ncols ? op.comp(d, i / CT, iy, iz, tile[i]) : make_float2(0.f, 0.f);
+            }
+            __syncthreads();
+            fft_tile<NG, CT, CT, true, NT>(work, tw);
+            store_rows<NG, CT, NT>(work, gout + (size_t)d * out_cs, rs, ncols - col0);
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        if (failed) {
+            atomicExch(err, 1);
+            mbar_wait_bounded(&bar[j & 1], (j >> 1) & 1);
+            if (next_in_flight) mbar_wait_bounded(&bar[(j + 1) & 1], ((j + 1) >> 1) & 1);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
 static bool encode_fn() {
@@ -188,7 +213,7 @@ static bool encode_fn() {
 
 // Tensor map over a half-spectrum buffer: dims (2*ncols floats, ng, ng, ncomp),
 // row stride zs complex, component stride cs complex.
-static cudaError_t make_spec_map(CUtensorMap* tm, float2* data, int ng, int ncols, int zs, size_t cs, int ncomp,
+cudaError_t make_spec_map(CUtensorMap* tm, float2* data, int ng, int ncols, int zs, size_t cs, int ncomp,
                                  int ct, int rb, bool isx) {
     if (!encode_fn()) return cudaErrorNotSupported;
     cuuint64_t dims[4] = {(cuuint64_t)(2 * ncols), (cuuint64_t)ng, (cuuint64_t)ng, (cuuint64_t)ncomp};
@@ -236,6 +261,44 @@ static cudaError_t tma_impl(bool inv, bool isx, float2* data, int ncols, int zs,
     }
 #undef HGPM_TMA_LAUNCH
     return cudaGetLastError();
+}
+
+template <int NG>
+static cudaError_t xpoisson_tma_impl(float2* in, float2* out, int ncols, int zs, size_t out_cs, const float2* tw,
+                                     const PoissonOp& op, int* err, cudaStream_t s) {
+    using G = TmaCfg<NG>;
+    CUtensorMap tm;
+    cudaError_t e = make_spec_map(&tm, in, NG, ncols, zs, 0, 1, G::CT, G::RB, true);
+    if (e != cudaSuccess) return e;
+    if (!g_num_sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    constexpr int SMEM = 3 * G::TILE_BYTES + 1024;
+    const int nchunks = (ncols + G::CT - 1) / G::CT;
+    const int ntiles = nchunks * NG;
+    auto k = xfused_tma_kernel<NG, PoissonOp>;
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    if (e != cudaSuccess) return e;
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTmaThreads, SMEM);
+    int grid = g_num_sms * (per_sm < 1 ? 1 : per_sm);
+    if (grid > ntiles) grid = ntiles;
+    k<<<grid, kTmaThreads, SMEM, s>>>(tm, out, out_cs, ncols, zs, nchunks, tw, op, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_xpoisson_tma(int ng, float2* in, float2* out, int ncols, int zs, size_t out_cs, const float2* tw,
+                                const double* cosq, const float* sk, double coeff, int* err, cudaStream_t s) {
+    PoissonOp op{cosq, sk, coeff, ng / 2};
+    switch (ng) {
+#define X(n) \
+    case n: return xpoisson_tma_impl<n>(in, out, ncols, zs, out_cs, tw, op, err, s);
+        X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
+#undef X
+    }
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_strided_tma(int ng, bool inv, bool isx, float2* data, int ncols, int zs, size_t cs, int ncomp,
