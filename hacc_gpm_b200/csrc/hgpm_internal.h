@@ -56,7 +56,7 @@ cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass
                            cudaStream_t s);
 cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float* fx, const float* fy,
                               const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift,
-                              cudaStream_t s);
+                              int variant, cudaStream_t s);
 cudaError_t launch_density(const unsigned long long* rho64, float* rho, size_t n, cudaStream_t s);
 cudaError_t launch_ktables(int ng, double* cosq, float* sk, float* pkw, cudaStream_t s);
 cudaError_t launch_noise(float* out, size_t n, uint32_t seed, cudaStream_t s);

@@ -682,11 +682,52 @@ static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const fl
     return cudaGetLastError();
 }
 
+// Flat variant: one particle per thread, the 24 corner values gathered
+// straight from the (L2-resident) force grids; many warps per SM hide the
+// gather latency.
+__global__ void __launch_bounds__(256, 6) kick_flat_kernel(ParticleSoA p, size_t n, int ng,
+                                                           const float* __restrict__ fx, const float* __restrict__ fy,
+                                                           const float* __restrict__ fz, float dtf, float pf_a,
+                                                           float pf_b, int ndrift) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const PState cur = load_p(p, i);
+    const int ix = cell_x(cur.c), iy = cell_y(cur.c), iz = cell_z(cur.c);
+    const int ix1 = ix + 1 == ng ? 0 : ix + 1;
+    const int iy1 = iy + 1 == ng ? 0 : iy + 1;
+    const int iz1 = iz + 1 == ng ? 0 : iz + 1;
+    const uint32_t sx[2] = {(uint32_t)ix * ng * ng, (uint32_t)ix1 * ng * ng};
+    const uint32_t sy[2] = {(uint32_t)iy * ng, (uint32_t)iy1 * ng};
+    const uint32_t sz[2] = {(uint32_t)iz, (uint32_t)iz1};
+    const float wxa[2] = {(1.f - cur.dx) * dtf, cur.dx * dtf}, wya[2] = {1.f - cur.dy, cur.dy},
+                wza[2] = {1.f - cur.dz, cur.dz};
+    float3 dv = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const uint32_t g = sx[a] + sy[b] + sz[cc];
+                const float mul = __fmul_rn(__fmul_rn(wxa[a], wya[b]), wza[cc]);
+                dv.x = fmaf(mul, __ldg(&fx[g]), dv.x);
+                dv.y = fmaf(mul, __ldg(&fy[g]), dv.y);
+                dv.z = fmaf(mul, __ldg(&fz[g]), dv.z);
+            }
+    finish_p(p, i, cur, dv, pf_a, pf_b, ndrift, ng);
+}
+
 cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float* fx, const float* fy,
                               const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift,
-                              cudaStream_t s) {
+                              int variant, cudaStream_t s) {
     const int B = block_side(np_side, ng);
     const int cap = deposit_cap_cells(np_side, ng);
+    if (variant == 1) {
+        const size_t n = (size_t)np_side * np_side * np_side;
+        kick_flat_kernel<<<nblk(n, 256), 256, 0, s>>>(p, n, ng, fx, fy, fz, (float)(deltaT * fscal), pf_a, pf_b,
+                                                      ndrift);
+        return cudaGetLastError();
+    }
     if (B == 16) return kick_impl<16, 512>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap, s);
     return kick_impl<8, 256>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap, s);
 }

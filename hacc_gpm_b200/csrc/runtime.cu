@@ -323,7 +323,12 @@ struct hgpm_ctx {
     float* kf_pk = nullptr;
     float* kf_ic = nullptr;
     int* d_err = nullptr;
-    bool tma = true;  // TMA-fed persistent y passes (HGPM_NO_TMA=1 selects the plain kernels)
+    // kernel variants (environment, read at creation): HGPM_NO_TMA=1 selects the
+    // plain strided y passes, HGPM_XTMA=0|1 the plain/TMA-fed fused x pass,
+    // HGPM_KICK=0|1 the tiled/flat gather
+    bool tma = true;
+    bool xtma = false;
+    int kick_variant = 0;
     float* stage = nullptr;     // AoS float3 x, v staging (lazy)
     double* pk_part = nullptr;  // P(k) partial sums (lazy)
     unsigned long long* pk_pcnt = nullptr;
@@ -444,6 +449,10 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
     {
         const char* nt = getenv("HGPM_NO_TMA");
         c->tma = !(nt && nt[0] == '1');
+        const char* xt = getenv("HGPM_XTMA");
+        c->xtma = xt && xt[0] == '1';
+        const char* kv = getenv("HGPM_KICK");
+        if (kv && (kv[0] == '0' || kv[0] == '1')) c->kick_variant = kv[0] - '0';
     }
     c->blk = block_side(c->np, c->ng);
     c->npart = (size_t)c->np * c->np * c->np;
@@ -690,7 +699,7 @@ extern "C" int hgpm_solve_gradient(hgpm_ctx* c) {
     const size_t cs = (size_t)ng * ng * c->zs;
     {
         PhaseScope ps(c, PH_POISSON);
-        if (c->tma)
+        if (c->xtma)
             CK(launch_xpoisson_tma(ng, c->spec, c->fspec, M + 1, c->zs, cs, c->tw_ng, c->cosq, c->sk,
                                    0.5 / ((double)ng * ng * ng), c->d_err + 1, c->stream));
         else
@@ -727,7 +736,7 @@ extern "C" int hgpm_kick_drift(hgpm_ctx* c, double deltaT, double fscal, float p
     if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
     PhaseScope ps(c, PH_KICK);
     CK(launch_kick_drift(c->part, c->np, c->ng, c->force, c->force + c->ncell, c->force + 2 * c->ncell, deltaT,
-                         fscal, pf_a, pf_b, ndrift, c->stream));
+                         fscal, pf_a, pf_b, ndrift, c->kick_variant, c->stream));
     count(c, PH_KICK, 1);
     return HGPM_OK;
 }

@@ -127,21 +127,30 @@ __device__ __forceinline__ void store_rows(const float2* __restrict__ tile, floa
     }
 }
 
-template <int NG, class Op>
-__global__ void __launch_bounds__(kTmaThreads, 2) xfused_tma_kernel(const __grid_constant__ CUtensorMap tm,
-                                                                    float2* __restrict__ out, size_t out_cs, int ncols,
-                                                                    int zs, int nchunks, const float2* __restrict__ tw,
-                                                                    Op op, int* __restrict__ err) {
+template <int NG, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) xpoisson_tma_kernel(const __grid_constant__ CUtensorMap tm,
+                                                                     float2* __restrict__ out, size_t out_cs,
+                                                                     int ncols, int zs, int nchunks,
+                                                                     const float2* __restrict__ tw,
+                                                                     const double* __restrict__ cosq_g,
+                                                                     const float* __restrict__ sk_g, double coeff,
+                                                                     int* __restrict__ err) {
     using G = TmaCfg<NG>;
-    constexpr int CT = G::CT, NT = kTmaThreads;
+    constexpr int CT = G::CT;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* base =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     float2* in[2] = {reinterpret_cast<float2*>(base), reinterpret_cast<float2*>(base + G::TILE_BYTES)};
     float2* work = reinterpret_cast<float2*>(base + 2 * G::TILE_BYTES);
+    double* cosq = reinterpret_cast<double*>(base + 3 * G::TILE_BYTES);
+    float* sk = reinterpret_cast<float*>(cosq + NG);
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int failed;
     const int ntiles = nchunks * NG;
+    for (int i = threadIdx.x; i < NG; i += NT) {
+        cosq[i] = cosq_g[i];
+        sk[i] = sk_g[i];
+    }
     if (threadIdx.x == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
@@ -154,6 +163,7 @@ __global__ void __launch_bounds__(kTmaThreads, 2) xfused_tma_kernel(const __grid
     int j = 0;
     bool next_in_flight = false;
     const size_t rs = (size_t)NG * zs;
+    constexpr int nyq = NG / 2;
     for (; t < ntiles; t += gridDim.x, ++j) {
         const int cur = j & 1;
         const int tn = t + gridDim.x;
@@ -171,16 +181,29 @@ __global__ void __launch_bounds__(kTmaThreads, 2) xfused_tma_kernel(const __grid
         const int iy = ti.plane, col0 = ti.chunk * CT;
         float2* tile = in[cur];
         fft_tile<NG, CT, CT, false, NT>(tile, tw);
+        // t = G rho_k (PoissonOp::pre with the tables in shared memory)
+        const double cy = cosq[iy];
         for (int i = threadIdx.x; i < NG * CT; i += NT) {
-            const int iz = col0 + i % CT;
-            tile[i] = iz < ncols ? op.pre(i / CT, iy, iz, tile[i]) : make_float2(0.f, 0.f);
+            const int ix = i / CT, iz = col0 + i % CT;
+            float2 v = make_float2(0.f, 0.f);
+            if (iz < ncols) {
+                const double sum = cosq[ix] + cy + cosq[iz];
+                const float g = (sum == 0.0) ? 0.f : (float)(coeff / sum);
+                v = tile[i];
+                v = make_float2(v.x * g, v.y * g);
+            }
+            tile[i] = v;
         }
         float2* gout = out + (size_t)iy * zs + col0;
 #pragma unroll 1
         for (int d = 0; d < 3; ++d) {
+            // F_d = -i sin(k_d) t, zero at the Nyquist index of d (PoissonOp::comp)
             for (int i = threadIdx.x; i < NG * CT; i += NT) {
-                const int iz = col0 + i % CT;
-                work[i] = iz < ncols ? op.comp(d, i / CT, iy, iz, tile[i]) : make_float2(0.f, 0.f);
+                const int ix = i / CT, iz = col0 + i % CT;
+                const int id = d == 0 ? ix : (d == 1 ? iy : iz);
+                const float sd = (id == nyq || iz >= ncols) ? 0.f : sk[id];
+                const float2 tv = tile[i];
+                work[i] = make_float2(sd * tv.y, -sd * tv.x);
             }
             __syncthreads();
             fft_tile<NG, CT, CT, true, NT>(work, tw);
@@ -265,8 +288,9 @@ static cudaError_t tma_impl(bool inv, bool isx, float2* data, int ncols, int zs,
 
 template <int NG>
 static cudaError_t xpoisson_tma_impl(float2* in, float2* out, int ncols, int zs, size_t out_cs, const float2* tw,
-                                     const PoissonOp& op, int* err, cudaStream_t s) {
+                                     const double* cosq, const float* sk, double coeff, int* err, cudaStream_t s) {
     using G = TmaCfg<NG>;
+    constexpr int NT = NG >= 128 ? 512 : 256;
     CUtensorMap tm;
     cudaError_t e = make_spec_map(&tm, in, NG, ncols, zs, 0, 1, G::CT, G::RB, true);
     if (e != cudaSuccess) return e;
@@ -275,26 +299,25 @@ static cudaError_t xpoisson_tma_impl(float2* in, float2* out, int ncols, int zs,
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
     }
-    constexpr int SMEM = 3 * G::TILE_BYTES + 1024;
+    constexpr int SMEM = 3 * G::TILE_BYTES + NG * 12 + 1024;
     const int nchunks = (ncols + G::CT - 1) / G::CT;
     const int ntiles = nchunks * NG;
-    auto k = xfused_tma_kernel<NG, PoissonOp>;
+    auto k = xpoisson_tma_kernel<NG, NT>;
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
     if (e != cudaSuccess) return e;
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTmaThreads, SMEM);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, SMEM);
     int grid = g_num_sms * (per_sm < 1 ? 1 : per_sm);
     if (grid > ntiles) grid = ntiles;
-    k<<<grid, kTmaThreads, SMEM, s>>>(tm, out, out_cs, ncols, zs, nchunks, tw, op, err);
+    k<<<grid, NT, SMEM, s>>>(tm, out, out_cs, ncols, zs, nchunks, tw, cosq, sk, coeff, err);
     return cudaGetLastError();
 }
 
 cudaError_t launch_xpoisson_tma(int ng, float2* in, float2* out, int ncols, int zs, size_t out_cs, const float2* tw,
                                 const double* cosq, const float* sk, double coeff, int* err, cudaStream_t s) {
-    PoissonOp op{cosq, sk, coeff, ng / 2};
     switch (ng) {
 #define X(n) \
-    case n: return xpoisson_tma_impl<n>(in, out, ncols, zs, out_cs, tw, op, err, s);
+    case n: return xpoisson_tma_impl<n>(in, out, ncols, zs, out_cs, tw, cosq, sk, coeff, err, s);
         X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
 #undef X
     }

@@ -105,6 +105,40 @@ def test_tma_and_plain_strided_passes_bit_identical(ng, monkeypatch):
     assert np.array_equal(out[0], out[1])
 
 
+@pytest.mark.parametrize("ng", [32, 64, 128])
+def test_fused_x_pass_variants_bit_identical(ng, monkeypatch):
+    """The persistent TMA-fed Poisson x pass and the plain fused x pass give
+    bit-identical forces."""
+    x, v = lattice_state(ng, ng, disp=1.1, seed=ng + 3)
+    out = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("HGPM_XTMA", flag)
+        with make(ng) as s:
+            s.load_state(x, v)
+            s.cic()
+            s.solve_gradient()
+            out.append(s.get_force())
+            s.sync()
+    assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("ng,np_side", [(32, 32), (48, 48), (64, 32)])
+def test_kick_variants_bit_identical(ng, np_side, monkeypatch):
+    """Tiled (shared-memory force window) and flat (global gather) kicks run
+    the same FP32 arithmetic in the same order."""
+    x, v = lattice_state(np_side, ng, disp=1.0, vel=1.0, seed=17)
+    out = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("HGPM_KICK", flag)
+        with make(ng, np_side) as s:
+            s.load_state(x, v)
+            s.cic()
+            s.solve_gradient()
+            s.kick_drift(0.0123, 1.7, 0.3, 0.25, 2)
+            out.append(s.store_state())
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
 def test_solve_gradient_plane_wave_analytic():
     """Particles arranged so that rho = 1 + A cos(2 pi x/ng) exactly on the
     grid is not reachable with CIC; instead place a sheet and compare with
