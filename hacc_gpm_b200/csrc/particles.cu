@@ -751,3 +751,107 @@ cudaError_t launch_place(const float* sgrid, size_t scomp, const ParticleSoA& p,
 }
 
 }  // namespace hgpm
+
+// ===========================================================================
+// Allocation-free CIC density
+//
+// Some callers cannot allocate device memory at all: code that runs inside a
+// host framework which owns every device allocation (a memory pool with a
+// fixed budget, or a plugin host that forbids its plugins to call
+// cudaMalloc), and code that must not allocate after start-up so that a long
+// run cannot fail later on an out-of-memory error.  For them,
+// hgpm_cic_density_noalloc computes the same deterministic density as
+// hgpm_deposit + hgpm_get_density from device positions into a device
+// density, and takes its int64 accumulation grid from this file-scope
+// device array instead of from an allocation.
+// ===========================================================================
+#define HGPM_NOALLOC_MAX_NG 128
+static __device__ __align__(256) unsigned long long g_noalloc_acc[HGPM_NOALLOC_MAX_NG * HGPM_NOALLOC_MAX_NG *
+                                                                   HGPM_NOALLOC_MAX_NG];
+
+namespace hgpm {
+
+__global__ void noalloc_zero_kernel(unsigned long long* __restrict__ acc, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) acc[i] = 0ull;
+}
+
+// One thread per particle: the same cell/offset split as load_state_kernel and
+// the same fixed-point corner weights as the tiled deposit, added with
+// integer atomics (so the result is bit-identical to the tiled deposit).
+template <bool SMALL>
+__global__ void noalloc_deposit_kernel(const float* __restrict__ x, size_t n, int ng, float mass,
+                                       unsigned long long* __restrict__ acc) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int ix, iy, iz;
+    float dx, dy, dz;
+    split_axis(x[3 * i + 0], ng, ix, dx);
+    split_axis(x[3 * i + 1], ng, iy, dy);
+    split_axis(x[3 * i + 2], ng, iz, dz);
+    unsigned long long q[8];
+    cic_fixed<SMALL>(dx, dy, dz, mass, q);
+    const int ix1 = ix + 1 == ng ? 0 : ix + 1;
+    const int iy1 = iy + 1 == ng ? 0 : iy + 1;
+    const int iz1 = iz + 1 == ng ? 0 : iz + 1;
+    const size_t sx[2] = {(size_t)ix * ng * ng, (size_t)ix1 * ng * ng};
+    const size_t sy[2] = {(size_t)iy * ng, (size_t)iy1 * ng};
+    const size_t sz[2] = {(size_t)iz, (size_t)iz1};
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) atomicAdd(&acc[sx[a] + sy[b] + sz[cc]], q[(a * 2 + b) * 2 + cc]);
+}
+
+}  // namespace hgpm
+
+#include <cstdio>
+#include <mutex>
+
+#include "../../include/hgpm_c.h"
+
+// Device address of g_noalloc_acc, looked up once per device (with that device
+// current); in host code the array's name is only a host-side stand-in.
+static unsigned long long* g_noalloc_ptr[64];
+static std::mutex g_noalloc_mu;
+
+extern "C" int hgpm_cic_density_noalloc(const float* x_dev, int np_side, int ng, float* rho_dev, void* stream) {
+    if (!x_dev || !rho_dev || np_side <= 0 || ng <= 0) return HGPM_ERR_ARG;
+    if (ng > HGPM_NOALLOC_MAX_NG) {
+        fprintf(stderr,
+                "hgpm_cic_density_noalloc: ng = %d exceeds the %d^3-cell limit of the built-in accumulation "
+                "grid; use hgpm_deposit on a context instead\n",
+                ng, HGPM_NOALLOC_MAX_NG);
+        return HGPM_ERR_ARG;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return HGPM_ERR_CUDA;
+    unsigned long long* acc;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_acc);
+            if (e != cudaSuccess || !p) {
+                fprintf(stderr, "hgpm_cic_density_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+                return HGPM_ERR_CUDA;
+            }
+            g_noalloc_ptr[dev] = static_cast<unsigned long long*>(p);
+        }
+        acc = g_noalloc_ptr[dev];
+    }
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t ncell = (size_t)ng * ng * ng;
+    const size_t n = (size_t)np_side * np_side * np_side;
+    const float gp = (float)ng / (float)np_side;  // pm_actions.cpp:229-230
+    const float mass = gp * gp * gp;
+    hgpm::noalloc_zero_kernel<<<(unsigned)((ncell + 255) / 256), 256, 0, s>>>(acc, ncell);
+    if (mass <= 1.0f)
+        hgpm::noalloc_deposit_kernel<true><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x_dev, n, ng, mass, acc);
+    else
+        hgpm::noalloc_deposit_kernel<false><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x_dev, n, ng, mass, acc);
+    if (hgpm::launch_density(acc, rho_dev, ncell, s) != cudaSuccess) return HGPM_ERR_CUDA;
+    return cudaGetLastError() == cudaSuccess ? HGPM_OK : HGPM_ERR_CUDA;
+}

@@ -190,6 +190,23 @@ int hgpm_phase_times(hgpm_ctx* ctx, double* ms, int64_t* launches);
 /* Number of kernels this context launched since creation / last reset.    */
 int64_t hgpm_kernel_launches(hgpm_ctx* ctx, int reset);
 
+/* ---- allocation-free density ------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (a host framework that owns every device allocation, or a run that
+ * must never allocate after start-up): the CIC density of np_side^3 particles
+ * (device float3 positions, grid units, reference layout) on an ng^3 grid,
+ * written as float into rho_dev (device, ng^3), bit-identical to
+ * hgpm_deposit + hgpm_get_density.  It allocates nothing: the int64
+ * accumulation grid is a built-in device array of 128^3 cells (16 MiB, held
+ * by every GPU that loads the library until exit), so ng > 128 is rejected
+ * with HGPM_ERR_ARG.  The array is cleared at the start of every call and
+ * keeps the last call's contents; calls on one device share it, so calls
+ * whose work overlaps on the GPU (different streams, or different host
+ * threads) race.  The first call on each device looks up the array's device
+ * address (cudaGetSymbolAddress) and should be made before any stream
+ * capture.  Stream-ordered on `stream` (a cudaStream_t, NULL = legacy).     */
+int hgpm_cic_density_noalloc(const float* x_dev, int np_side, int ng, float* rho_dev, void* stream);
+
 /* ---- ABI checks ------------------------------------------------------------
  * sizeof of the public structs, for bindings that mirror them.            */
 size_t hgpm_sizeof_params(void);
