@@ -8,7 +8,7 @@ C-ABI (``binding.py``), the batched ensemble / serving front ends and the
 ``.ipk`` writer.
 """
 from .binding import (HgpmError, Params, Simulation, Timestepper, footprint_bytes, growth, lib, parse_params,
-                      read_ipk, read_params)
+                      read_ipk, read_params, write_pk)
 
 __all__ = ["HgpmError", "Params", "Simulation", "Timestepper", "footprint_bytes", "growth", "lib", "parse_params",
-           "read_ipk", "read_params"]
+           "read_ipk", "read_params", "write_pk"]

@@ -246,6 +246,14 @@ def footprint_bytes(ng: int, np_side: int) -> int:
     return lib().hgpm_footprint_bytes(ng, np_side)
 
 
+def write_pk(fname: str, k: np.ndarray, pk: np.ndarray, count: np.ndarray):
+    """``writePkOutput`` (power.cu:13-28): "<fname>.fold.0" lines "%g,%g,%d"."""
+    k = np.ascontiguousarray(k, np.float64)
+    pk = np.ascontiguousarray(pk, np.float64)
+    n = np.ascontiguousarray(count, np.int64)
+    _check(None, lib().hgpm_write_pk(fname.encode(), k.size, _d(k), _d(pk), n.ctypes.data_as(C.POINTER(C.c_int64))))
+
+
 class Simulation:
     """One box on one GPU: ``serial::MemoryManager`` plus the serial phase
     functions, all running on the context's CUDA stream."""

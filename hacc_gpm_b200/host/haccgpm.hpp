@@ -1,0 +1,129 @@
+// haccgpm.hpp — C++ drop-in for the serial path of HACC_GPM, over the C-ABI
+// of include/hgpm_c.h.
+//
+// The names, argument meanings and call order are those of the reference's
+// public header (src/haccgpm.hpp): HACCGPM::Params (:118-174),
+// HACCGPM::read_params, HACCGPM::Timestepper (:178-198),
+// HACCGPM::CosmoClass (:200-254) and namespace HACCGPM::serial (:385-506),
+// so a caller written against the reference's serial() loop
+// (src/driver_pm.cpp:32-163) compiles against this header unchanged in the
+// calls it makes.  Error behaviour is the reference's: a failing call prints
+// the message and exits the process (the reference's gpuErrchk/cudaCall).
+//
+// Differences a caller can see:
+//   * MemoryManager holds an opaque context instead of raw d_pos / d_vel /
+//     d_grid / d_grad pointers (the state lives in HBM as packed cell + FP32
+//     offset; hgpm_store_state_device gives the reference's float3 layout).
+//   * forward_fft / backward_fft on caller-owned cufftComplex grids have no
+//     counterpart: the FFTs are internal to SolveGradient, GetPowerSpectrum
+//     and GenerateDisplacementIC.
+//   * InitGreens and fft_cache_plan are no-ops (the Green's function is
+//     computed inside the fused Poisson pass; there are no plans).
+//   * GetPowerSpectrum writes fold 0 only (PK_FOLDS > 0 makes the
+//     reference's BinPower index out of bounds, bin_power.cu:20-27).
+#pragma once
+
+#include <cstdint>
+
+#include "hgpm_c.h"
+
+namespace HACCGPM {
+
+typedef int64_t CPUTimer_t;  // microseconds since an arbitrary origin (timers.cpp)
+CPUTimer_t CPUTimer();
+
+// src/haccgpm.hpp:118-174, the fields the serial path reads.  `c` holds the
+// same values in the C-ABI layout; every call re-derives it from the named
+// fields, so a caller may edit them between read_params and use.
+struct Params {
+    char fname[HGPM_PATH_MAX];
+    int ng, np;
+    double rl;
+    int blockSize;
+    int seed;
+    double z_ini, z_fin;
+    int nsteps;
+    char prefix[HGPM_PATH_MAX];
+    double m_hubble, m_omega_cdm, m_omega_nu, m_deut, m_ss8, m_ns, m_w_de, m_wa_de, m_Tcmb;
+    double m_neff_massless, m_neff_massive;
+    double m_omega_baryon, m_omega_cb, m_omega_matter, m_omega_radiation;
+    double m_f_nu_massless, m_f_nu_massive;
+    bool pks[HGPM_MAX_STEPS];
+    bool dumps[HGPM_MAX_STEPS];
+    char ipk[HGPM_PATH_MAX];
+    bool do_analysis;
+    int lastStep;
+    int pkFolds;
+    int world_rank, world_size;
+    bool dump_init, dump_final;
+    double ol;
+    int overload;
+    int pk_bins;
+    bool pk_log;
+    hgpm_params c;
+};
+
+// params.cpp:201-250: parse, print (print_params) and write the
+// "<prefix>.params" echo (save_params).
+Params read_params(const char* fname);
+hgpm_params to_c(const Params& p);
+
+// timestepper.cpp:31-68
+class Timestepper {
+   public:
+    Params params;
+    double aa, z, deltaT, adot, fscal;
+    int world_rank;
+    explicit Timestepper(Params iparams);
+    void setInitialA(double a);
+    void setInitialZ(double z);
+    void advanceHalfStep();
+    void reverseHalfStep();
+    hgpm_timestepper to_c() const;
+
+   private:
+    void from_c(const hgpm_timestepper& t);
+};
+
+// cosmo.cpp:11-79: the serial path uses it only to find and read the .ipk
+class CosmoClass {
+   public:
+    double Omega_m, Omega_cb, h;
+    char ipk[HGPM_PATH_MAX];
+    CosmoClass() {}
+    explicit CosmoClass(Params& params);
+    // cosmo.cpp:26-79; *out is new[]-allocated, the caller delete[]s it
+    void read_ipk(double** out, int* nbins, double* k_delta, double* k_max, double* k_min, int calls = 0);
+};
+
+namespace serial {
+
+// mmanager.cu:93-179: owns the device state of one box
+class MemoryManager {
+   public:
+    hgpm_ctx* ctx = nullptr;
+    explicit MemoryManager(Params params);
+    ~MemoryManager();
+    MemoryManager(const MemoryManager&) = delete;
+    MemoryManager& operator=(const MemoryManager&) = delete;
+};
+
+void fft_cache_plan(int ng);
+void InitGreens(Params& params, MemoryManager& mem, int calls = 0);
+void GenerateDisplacementIC(MemoryManager& mem, CosmoClass& cosmo, Params& params, Timestepper& ts, int calls = 0);
+void UpdatePositions(Params& params, MemoryManager& mem, Timestepper ts, float frac, int calls = 0);
+void CIC(Params& params, MemoryManager& mem, int calls = 0);
+void SolveGradient(Params& params, MemoryManager& mem, int calls = 0);
+void UpdateVelocities(Params& params, MemoryManager& mem, Timestepper ts, int calls = 0);
+void GetPowerSpectrum(Params& params, MemoryManager& mem, const char* fname, int calls = 0);
+void writeOutput(Params& params, MemoryManager& mem, char* fname, int calls = 0);
+double get_fscal(double m_aa, double m_adot, double m_omega_cb);
+void printTimers(CPUTimer_t init, CPUTimer_t total);
+
+// Not in the reference: nsteps whole steps with the drifts fused into the
+// kick (bit-identical to the UpdatePositions/CIC/SolveGradient/
+// UpdateVelocities/UpdatePositions sequence); ts advances as that loop does.
+void RunSteps(Params& params, MemoryManager& mem, Timestepper& ts, int nsteps);
+
+}  // namespace serial
+}  // namespace HACCGPM

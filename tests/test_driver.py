@@ -1,0 +1,102 @@
+"""The C++ drop-in (hacc_gpm_b200/host): the reference's serial() run over
+the HACCGPM::serial:: shim.  CPU: usage, the .params echo and the
+reference's exit-on-error behaviour.  GPU: the files it writes against the
+Python API on the same seeded run, and the --fused loop against the
+per-phase loop."""
+import filecmp
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import hacc_gpm_b200 as H
+from hacc_gpm_b200 import build as B
+from hacc_gpm_b200 import ipk as ipkmod
+from oracle import pm_oracle as O
+
+
+def _driver():
+    if not os.path.exists(B.DRIVER):
+        B.build()
+    return B.DRIVER
+
+
+def _case(tmp, name, ng=32, extra="LAST_STEP 6\nPK_DUMP 2\nPARTICLE_DUMP 3\nDUMP_INIT\nDUMP_FINAL\n"):
+    d = tmp / name
+    d.mkdir()
+    txt = ipkmod.lcdm_params_text(ng, ng, float(ng), 50.0, 100, prefix=str(d / "run"), ipk=str(tmp / "run.ipk"),
+                                  extra=extra)
+    if not (tmp / "run.ipk").exists():
+        op = O.parse_params_text(txt)
+        header, table = ipkmod.make_ipk(ipkmod.cosmo_from_params(op), op.z_ini, k_max=20.0)
+        np.concatenate([header, table]).astype("<f8").tofile(str(tmp / "run.ipk"))
+    (d / "input.params").write_text(txt)
+    return d, txt
+
+
+def test_usage():
+    r = subprocess.run([_driver()], capture_output=True, text=True)
+    assert r.returncode == 1 and "USAGE" in r.stdout
+
+
+def test_echo_and_exit_on_error(tmp_path):
+    # NG 20 is not a supported FFT size: read_params prints and echoes, then
+    # MemoryManager fails and the process exits 1 with the message
+    d, txt = _case(tmp_path, "bad", extra="")
+    (d / "input.params").write_text(txt.replace("NG 32", "NG 20"))
+    r = subprocess.run([_driver(), str(d / "input.params")], capture_output=True, text=True)
+    assert r.returncode == 1
+    assert "MemoryManager" in r.stderr and "NG must be one of" in r.stderr
+    assert "OUTPUT_BASE_NAME" in r.stdout
+    p = H.parse_params(txt.replace("NG 32", "NG 20"))
+    p.prefix = str(d / "py")
+    p.save()
+    assert (d / "run.params").read_text() == (d / "py.params").read_text().replace(str(d / "py"), str(d / "run"))
+
+
+@pytest.mark.gpu
+def test_driver_files_match_api(tmp_path):
+    d, txt = _case(tmp_path, "plain")
+    r = subprocess.run([_driver(), str(d / "input.params")], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    for f in ("run.params", "run.pk.ini.fold.0", "run.pk.2.fold.0", "run.pk.fin.fold.0", "run.particles.ini",
+              "run.particles.3", "run.particles.fin"):
+        assert (d / f).exists(), f
+    hp = H.parse_params(txt)
+    n3 = 32 ** 3
+    header, table = H.read_ipk(str(tmp_path / "run.ipk"))
+    with H.Simulation(hp) as s:
+        s.generate_ic(table, header[3])
+        k, P, n = s.power_spectrum(221)
+        H.write_pk(str(tmp_path / "api.pk.ini"), k, P, n)
+        ts = H.Timestepper(hp)
+        ts.set_initial_z(hp.z_ini)
+        ts.reverse_half_step()
+        ts.advance_half_step()
+        for _ in range(6):
+            s.update_positions(ts, 0.5)
+            s.cic()
+            s.solve_gradient()
+            ts.advance_half_step()
+            s.update_velocities(ts)
+            ts.advance_half_step()
+            s.update_positions(ts, 0.5)
+        x, v = s.store_state()
+    assert (d / "run.pk.ini.fold.0").read_text() == (tmp_path / "api.pk.ini.fold.0").read_text()
+    fin = np.fromfile(str(d / "run.particles.fin"), dtype="<f4")
+    assert fin.size == 6 * n3
+    assert np.array_equal(fin[:3 * n3].reshape(-1, 3), x) and np.array_equal(fin[3 * n3:].reshape(-1, 3), v)
+
+
+@pytest.mark.gpu
+def test_driver_fused_equals_plain(tmp_path):
+    runs = []
+    for name, flags in (("a", []), ("b", ["--fused"])):
+        d, _ = _case(tmp_path, name)
+        r = subprocess.run([_driver(), str(d / "input.params"), *flags], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        runs.append(d)
+    for f in ("run.pk.ini.fold.0", "run.pk.2.fold.0", "run.pk.fin.fold.0", "run.particles.ini", "run.particles.3",
+              "run.particles.fin"):
+        assert filecmp.cmp(str(runs[0] / f), str(runs[1] / f), shallow=False), f
