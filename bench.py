@@ -18,6 +18,16 @@ SM clocks sampled during the timed region.
 
 --impl reference times the reference's algorithm on the host cores (the
 reference has no CPU path; oracle/_bin/cpu_pm is its OpenMP transcription).
+
+--workload ensemble | serve (1 GPU) measure the batched forms instead:
+  ensemble  96 boxes, ng = np from {32, 48, 64, 96, 128}, L ~ U[64, 512],
+            sigma8 ~ U[0.7, 0.9], z 100, 64 steps each: sims/hour batched
+            (one launch per phase per size class, CUDA graph) against the
+            same boxes one at a time through the plain step;
+  serve     a Poisson request stream (20/s, ng log-uniform over 32..256,
+            steps U[20, 200], own cosmology and seed) through the
+            continuous-batching server and one at a time: p50/p99 latency
+            and sims/hour, plus the saturated (all queued) throughput.
 """
 from __future__ import annotations
 
@@ -153,6 +163,85 @@ def run_reference(args):
     }))
 
 
+def _check_same(a, b):
+    """Largest relative P(k) difference and whether the mode counts agree."""
+    worst, counts = 0.0, True
+    for ra, rb in zip(a, b):
+        ra = ra.result if hasattr(ra, "result") else ra
+        rb = rb.result if hasattr(rb, "result") else rb
+        counts &= bool((ra["n"] == rb["n"]).all())
+        ok = ra["n"] > 0
+        if ok.any():
+            worst = max(worst, float(abs(ra["P"][ok] / rb["P"][ok] - 1).max()))
+    return worst, counts
+
+
+def run_forms(args):
+    """The batched ensemble and the serving loop (1 GPU)."""
+    import torch
+
+    from hacc_gpm_b200 import ensemble as E
+    from hacc_gpm_b200 import serve as S
+    torch.cuda.set_device(0)
+    if args.workload == "ensemble":
+        boxes = E.prepare_tables(E.ensemble_boxes(96))
+        warm = E.prepare_tables(E.ensemble_boxes(10, master_seed=1))
+        for b in warm:
+            b.nsteps = 3
+        E.run_serial(warm)
+        E.run_batched(warm)
+        torch.cuda.synchronize()
+        serial, t_serial = E.timed(E.run_serial, boxes)
+        batched, t_batch = E.timed(E.run_batched, boxes)
+        st_serial, st_batch = {}, {}
+        E.run_serial(boxes, stages=st_serial)
+        E.run_batched(boxes, stages=st_batch)
+        worst, counts = _check_same(batched, serial)
+        classes, _ = E.class_layout(boxes)
+        print(json.dumps({
+            "metric": "ensemble sims/hour (96 mixed boxes, 64 steps each)", "value": 96 / t_batch * 3600.0,
+            "unit": "sims/hour", "higher_is_better": True, "n_gpus": 1,
+            "one_at_a_time": {"value": 96 / t_serial * 3600.0, "seconds": t_serial},
+            "batched_seconds": t_batch, "speedup_vs_one_at_a_time": t_serial / t_batch,
+            "stages_s": {"batched": st_batch, "one_at_a_time": st_serial},
+            "speedup_compute_only": (sum(v for k, v in st_serial.items() if k != "create") /
+                                     sum(v for k, v in st_batch.items() if k != "create")),
+            "pk_max_rel_diff_vs_one_at_a_time": worst, "pk_counts_equal": counts,
+            "config": {"workload": "96 boxes, ng = np uniform over {32,48,64,96,128}, L ~ U[64,512] Mpc/h, "
+                                   "sigma8 ~ U[0.7,0.9], seeds 1000+i, EH ICs at z=100, 64 steps, P(k) 32 bins",
+                       "classes": classes, "timed": "ICs + 64 steps + final P(k) of every box (host-side "
+                                                    ".ipk tables prepared beforehand for both)",
+                       "batched": "one launch per phase per size class, classes on parallel streams, "
+                                  "CUDA graph per step"},
+            "dtype": "f32", "data": "synthetic: seeded EH no-wiggle Zel'dovich ICs (Philox white noise)",
+        }))
+        return
+    reqs = S.request_stream(args.requests)
+    warm = S.request_stream(8, rate=1000.0, seed=3, steps=(2, 3))
+    S.serve(warm, realtime=False)
+    S.serve_one_at_a_time(S.request_stream(8, rate=1000.0, seed=3, steps=(2, 3)), realtime=False)
+    torch.cuda.synchronize()
+    got, mk, stats = S.serve(reqs)
+    one, mk1 = S.serve_one_at_a_time(S.request_stream(args.requests))
+    sat, mks, _ = S.serve(S.request_stream(args.requests), realtime=False)
+    sat1, mks1 = S.serve_one_at_a_time(S.request_stream(args.requests), realtime=False)
+    worst, counts = _check_same(sorted(got, key=lambda r: r.tag), sorted(one, key=lambda r: r.tag))
+    out = S.latency_summary(got, mk)
+    print(json.dumps({
+        "metric": "serving p99 completion latency (Poisson 20 req/s)", "value": out["p99_s"], "unit": "s",
+        "higher_is_better": False, "n_gpus": 1, "batched": out, "one_at_a_time": S.latency_summary(one, mk1),
+        "saturated": {"batched_sims_per_hour": len(sat) / mks * 3600.0,
+                      "one_at_a_time_sims_per_hour": len(sat1) / mks1 * 3600.0, "speedup": mks1 / mks},
+        "pk_max_rel_diff_vs_one_at_a_time": worst, "pk_counts_equal": counts,
+        "config": {"workload": "%d requests, Poisson arrivals 20/s (seed 7), ng = np log-uniform over "
+                               "{32,48,64,96,128,192,256}, L = ng Mpc/h, steps U[20,200], Om U[0.25,0.35], "
+                               "sigma8 U[0.7,0.9], EH ICs at z=50" % args.requests,
+                   "classes": stats["classes"], "admission": "slots per size class from a 40 GB HBM budget "
+                                                            "split evenly over classes (footprint per slot)"},
+        "dtype": "f32", "data": "synthetic",
+    }))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -163,7 +252,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--size", type=int, default=512, help="np = ng (profiling runs use a smaller box)")
+    ap.add_argument("--workload", default="step", choices=["step", "ensemble", "serve"])
+    ap.add_argument("--requests", type=int, default=160, help="serve: requests in the stream")
     args = ap.parse_args()
+    if args.workload != "step":
+        run_forms(args)
+        return
     global NG, NP, RL
     NG = NP = args.size
     RL = float(args.size)

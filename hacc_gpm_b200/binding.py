@@ -126,6 +126,19 @@ def lib() -> C.CDLL:
         "hgpm_enable_timing": (C.c_int, [vp, C.c_int]),
         "hgpm_phase_times": (C.c_int, [vp, P(C.c_double), P(C.c_int64)]),
         "hgpm_kernel_launches": (C.c_int64, [vp, C.c_int]),
+        "hgpm_ens_create": (C.c_int, [C.c_int, P(C.c_int), P(C.c_int), P(C.c_int), C.c_int, P(vp)]),
+        "hgpm_ens_destroy": (None, [vp]),
+        "hgpm_ens_last_error": (C.c_char_p, [vp]),
+        "hgpm_ens_footprint_bytes": (C.c_size_t, [C.c_int, C.c_int, C.c_int]),
+        "hgpm_ens_stream": (vp, [vp]),
+        "hgpm_ens_slot": (C.c_int, [vp, C.c_int, C.c_int, P(_Params), P(vp)]),
+        "hgpm_ens_start": (C.c_int, [vp, C.c_int, C.c_int, P(_Timestepper), C.c_int]),
+        "hgpm_ens_release": (C.c_int, [vp, C.c_int, C.c_int]),
+        "hgpm_ens_step": (C.c_int, [vp, C.c_int]),
+        "hgpm_ens_use_graph": (C.c_int, [vp, C.c_int]),
+        "hgpm_ens_sync": (C.c_int, [vp]),
+        "hgpm_ens_status": (C.c_int, [vp, C.c_int, C.c_int, P(C.c_int), P(C.c_int)]),
+        "hgpm_ens_kernel_launches": (C.c_int64, [vp, C.c_int]),
         "hgpm_sizeof_params": (C.c_size_t, []),
         "hgpm_sizeof_timestepper": (C.c_size_t, []),
     }
@@ -273,10 +286,23 @@ class Simulation:
         self.ng = params.ng
         self.np = params.np
         self.npart = params.np ** 3
+        self._owned = True
+
+    @classmethod
+    def _borrow(cls, handle: C.c_void_p, params: Params) -> "Simulation":
+        """A context owned elsewhere (an ensemble slot); close() leaves it."""
+        s = cls.__new__(cls)
+        s.params = params.copy()
+        s.L = lib()
+        s._h = handle
+        s.ng, s.np, s.npart = params.ng, params.np, params.np ** 3
+        s._owned = False
+        return s
 
     def close(self):
         if getattr(self, "_h", None):
-            self.L.hgpm_destroy(self._h)
+            if getattr(self, "_owned", True):
+                self.L.hgpm_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -119,9 +119,14 @@ __device__ __forceinline__ void store_tile(const float2* __restrict__ tile, floa
 template <int NG, bool FIX>
 __global__ void __launch_bounds__(kThreads) zpass_r2c_kernel(void* __restrict__ in_, float2* __restrict__ out,
                                                              int nlines, int zs, double mean,
-                                                             const float2* __restrict__ tw) {
+                                                             const float2* __restrict__ tw, Slots sl) {
     constexpr int M = NG / 2, L = Cfg<NG>::L, ES = L + 1;
     float2* buf = reinterpret_cast<float2*>(hgpm_smem);
+    if (slot_idle(sl, blockIdx.y)) return;
+    // slot stride s0 counts input elements (int64 when FIX, float otherwise)
+    in_ = FIX ? (void*)(reinterpret_cast<unsigned long long*>(in_) + (size_t)blockIdx.y * sl.s0)
+              : (void*)(reinterpret_cast<float*>(in_) + (size_t)blockIdx.y * sl.s0);
+    out += (size_t)blockIdx.y * sl.s1;
     const int line0 = blockIdx.x * L;
     constexpr int TOT = L * M;
     constexpr int PER = (TOT + kThreads - 1) / kThreads;
@@ -189,18 +194,22 @@ __global__ void __launch_bounds__(kThreads) zpass_r2c_kernel(void* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// z pass, inverse C2R, ncomp components (blockIdx.y), unnormalised * scale.
+// z pass, inverse C2R, ncomp components, unnormalised * scale;
+// blockIdx.y = slot * ncomp + component.
 // X[0] and X[ng/2] are taken as real (Hermitian extension), which makes the
 // result equal to the real part of the reference's full C2C inverse.
 // ---------------------------------------------------------------------------
 template <int NG>
 __global__ void __launch_bounds__(kThreads) zpass_c2r_kernel(const float2* __restrict__ in, float* __restrict__ out,
                                                              int nlines, int zs, size_t in_cs, size_t out_cs,
-                                                             float scale, const float2* __restrict__ tw) {
+                                                             float scale, const float2* __restrict__ tw, int ncomp,
+                                                             Slots sl) {
     constexpr int M = NG / 2, L = Cfg<NG>::L, ES = L + 1;
     float2* buf = reinterpret_cast<float2*>(hgpm_smem);
-    in += (size_t)blockIdx.y * in_cs;
-    out += (size_t)blockIdx.y * out_cs;
+    const int slot = blockIdx.y / ncomp, comp = blockIdx.y % ncomp;
+    if (slot_idle(sl, slot)) return;
+    in += (size_t)slot * sl.s0 + (size_t)comp * in_cs;
+    out += (size_t)slot * sl.s1 + (size_t)comp * out_cs;
     const int line0 = blockIdx.x * L;
     constexpr int H = M / 2 + 1;
     constexpr int TOT = L * H;
@@ -255,15 +264,19 @@ __global__ void __launch_bounds__(kThreads) zpass_c2r_kernel(const float2* __res
 }
 
 // ---------------------------------------------------------------------------
-// strided pass (y or x lines), in place, blockIdx = (column chunk, plane, comp)
+// strided pass (y or x lines), in place,
+// blockIdx = (column chunk, plane, slot * ncomp + comp)
 // ---------------------------------------------------------------------------
 template <int NG, bool INV>
 __global__ void __launch_bounds__(Cfg<NG>::NTS, 2) strided_kernel(float2* __restrict__ data, int ncols, size_t rs,
-                                                               size_t ps, size_t cs, const float2* __restrict__ tw) {
+                                                               size_t ps, size_t cs, const float2* __restrict__ tw,
+                                                               int ncomp, Slots sl) {
     constexpr int C = Cfg<NG>::CS, NT = Cfg<NG>::NTS;
     float2* tile = reinterpret_cast<float2*>(hgpm_smem);
+    const int slot = blockIdx.z / ncomp, comp = blockIdx.z % ncomp;
+    if (slot_idle(sl, slot)) return;
     const int col0 = blockIdx.x * C;
-    float2* g = data + (size_t)blockIdx.z * cs + (size_t)blockIdx.y * ps + col0;
+    float2* g = data + (size_t)slot * sl.s0 + (size_t)comp * cs + (size_t)blockIdx.y * ps + col0;
     const int nvalid = ncols - col0;
     load_tile<NG, C, NT>(tile, g, rs, nvalid);
     __syncthreads();
@@ -275,15 +288,18 @@ __global__ void __launch_bounds__(Cfg<NG>::NTS, 2) strided_kernel(float2* __rest
 // x pass fused with a k-space operator producing 3 components:
 //   forward x FFT of the (z,y)-transformed tile -> t = op.pre(k, rho_k) ->
 //   for d in 0..2: op.comp(d, k, t) -> inverse x FFT -> out[d]
-// plane = ky index, rows = kx index, columns = kz index.
+// plane = ky index, rows = kx index, columns = kz index; blockIdx.z = slot.
 // ---------------------------------------------------------------------------
 template <int NG, class Op>
 __global__ void __launch_bounds__(Cfg<NG>::NTX) xfused_kernel(const float2* __restrict__ in, float2* __restrict__ out,
                                                               int ncols, size_t rs, size_t ps, size_t out_cs,
-                                                              const float2* __restrict__ tw, Op op) {
+                                                              const float2* __restrict__ tw, Op op, Slots sl) {
     constexpr int C = Cfg<NG>::CX, NT = Cfg<NG>::NTX;
     float2* tile = reinterpret_cast<float2*>(hgpm_smem);
     float2* work = tile + NG * C;
+    if (slot_idle(sl, blockIdx.z)) return;
+    in += (size_t)blockIdx.z * sl.s0;
+    out += (size_t)blockIdx.z * sl.s1;
     const int col0 = blockIdx.x * C;
     const int iy = blockIdx.y;
     const size_t off = (size_t)iy * ps + col0;
@@ -429,63 +445,64 @@ static inline unsigned cdiv(size_t a, size_t b) { return (unsigned)((a + b - 1) 
 
 template <int NG>
 static cudaError_t zfwd_impl(void* in, bool fixed, float2* out, int nlines, int zs, double mean,
-                             const float2* tw, cudaStream_t s) {
+                             const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
     using G = Cfg<NG>;
-    const unsigned grid = cdiv(nlines, G::L);
+    const dim3 grid(cdiv(nlines, G::L), nslots);
     if (fixed) {
         auto k = zpass_r2c_kernel<NG, true>;
         cudaError_t e = ensure_smem(k, G::ZSMEM);
         if (e != cudaSuccess) return e;
-        k<<<grid, kThreads, G::ZSMEM, s>>>(in, out, nlines, zs, mean, tw);
+        k<<<grid, kThreads, G::ZSMEM, s>>>(in, out, nlines, zs, mean, tw, sl);
     } else {
         auto k = zpass_r2c_kernel<NG, false>;
         cudaError_t e = ensure_smem(k, G::ZSMEM);
         if (e != cudaSuccess) return e;
-        k<<<grid, kThreads, G::ZSMEM, s>>>(in, out, nlines, zs, mean, tw);
+        k<<<grid, kThreads, G::ZSMEM, s>>>(in, out, nlines, zs, mean, tw, sl);
     }
     return cudaGetLastError();
 }
 
 template <int NG>
 static cudaError_t zinv_impl(const float2* in, float* out, int nlines, int zs, size_t in_cs, size_t out_cs,
-                             int ncomp, float scale, const float2* tw, cudaStream_t s) {
+                             int ncomp, float scale, const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
     using G = Cfg<NG>;
     auto k = zpass_c2r_kernel<NG>;
     cudaError_t e = ensure_smem(k, G::ZSMEM);
     if (e != cudaSuccess) return e;
-    dim3 grid(cdiv(nlines, G::L), ncomp);
-    k<<<grid, kThreads, G::ZSMEM, s>>>(in, out, nlines, zs, in_cs, out_cs, scale, tw);
+    dim3 grid(cdiv(nlines, G::L), ncomp * nslots);
+    k<<<grid, kThreads, G::ZSMEM, s>>>(in, out, nlines, zs, in_cs, out_cs, scale, tw, ncomp, sl);
     return cudaGetLastError();
 }
 
 template <int NG>
 static cudaError_t strided_impl(bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
-                                int ncomp, const float2* tw, cudaStream_t s) {
+                                int ncomp, const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
     using G = Cfg<NG>;
-    dim3 grid(cdiv(ncols, G::CS), nplanes, ncomp);
+    dim3 grid(cdiv(ncols, G::CS), nplanes, ncomp * nslots);
     if (inv) {
         auto k = strided_kernel<NG, true>;
         cudaError_t e = ensure_smem(k, G::SSMEM);
         if (e != cudaSuccess) return e;
-        k<<<grid, G::NTS, G::SSMEM, s>>>(data, ncols, rs, ps, cs, tw);
+        k<<<grid, G::NTS, G::SSMEM, s>>>(data, ncols, rs, ps, cs, tw, ncomp, sl);
     } else {
         auto k = strided_kernel<NG, false>;
         cudaError_t e = ensure_smem(k, G::SSMEM);
         if (e != cudaSuccess) return e;
-        k<<<grid, G::NTS, G::SSMEM, s>>>(data, ncols, rs, ps, cs, tw);
+        k<<<grid, G::NTS, G::SSMEM, s>>>(data, ncols, rs, ps, cs, tw, ncomp, sl);
     }
     return cudaGetLastError();
 }
 
 template <int NG, class Op>
 static cudaError_t xfused_impl(const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
-                               size_t out_cs, const float2* tw, const Op& op, cudaStream_t s) {
+                               size_t out_cs, const float2* tw, const Op& op, cudaStream_t s, const Slots& sl = Slots{},
+                               int nslots = 1) {
     using G = Cfg<NG>;
     auto k = xfused_kernel<NG, Op>;
     cudaError_t e = ensure_smem(k, G::XSMEM);
     if (e != cudaSuccess) return e;
-    dim3 grid(cdiv(ncols, G::CX), nplanes);
-    k<<<grid, G::NTX, G::XSMEM, s>>>(in, out, ncols, rs, ps, out_cs, tw, op);
+    dim3 grid(cdiv(ncols, G::CX), nplanes, nslots);
+    k<<<grid, G::NTX, G::XSMEM, s>>>(in, out, ncols, rs, ps, out_cs, tw, op, sl);
     return cudaGetLastError();
 }
 
@@ -521,10 +538,10 @@ bool fft_size_supported(int ng) {
 }
 
 cudaError_t launch_zfwd(int ng, void* in, bool fixed, float2* out, int nlines, int zs, double mean,
-                        const float2* tw, cudaStream_t s) {
+                        const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
     switch (ng) {
 #define X(n) \
-    case n: return zfwd_impl<n>(in, fixed, out, nlines, zs, mean, tw, s);
+    case n: return zfwd_impl<n>(in, fixed, out, nlines, zs, mean, tw, s, sl, nslots);
         HGPM_SIZES(X)
 #undef X
     }
@@ -532,10 +549,10 @@ cudaError_t launch_zfwd(int ng, void* in, bool fixed, float2* out, int nlines, i
 }
 
 cudaError_t launch_zinv(int ng, const float2* in, float* out, int nlines, int zs, size_t in_cs, size_t out_cs,
-                        int ncomp, float scale, const float2* tw, cudaStream_t s) {
+                        int ncomp, float scale, const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
     switch (ng) {
 #define X(n) \
-    case n: return zinv_impl<n>(in, out, nlines, zs, in_cs, out_cs, ncomp, scale, tw, s);
+    case n: return zinv_impl<n>(in, out, nlines, zs, in_cs, out_cs, ncomp, scale, tw, s, sl, nslots);
         HGPM_SIZES(X)
 #undef X
     }
@@ -543,10 +560,10 @@ cudaError_t launch_zinv(int ng, const float2* in, float* out, int nlines, int zs
 }
 
 cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
-                           int ncomp, const float2* tw, cudaStream_t s) {
+                           int ncomp, const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
     switch (ng) {
 #define X(n) \
-    case n: return strided_impl<n>(inv, data, ncols, rs, ps, nplanes, cs, ncomp, tw, s);
+    case n: return strided_impl<n>(inv, data, ncols, rs, ps, nplanes, cs, ncomp, tw, s, sl, nslots);
         HGPM_SIZES(X)
 #undef X
     }
@@ -555,11 +572,11 @@ cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs,
 
 cudaError_t launch_xpoisson(int ng, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
                             size_t out_cs, const float2* tw, const double* cosq, const float* sk, double coeff,
-                            cudaStream_t s) {
+                            cudaStream_t s, const Slots& sl, int nslots) {
     PoissonOp op{cosq, sk, coeff, ng / 2};
     switch (ng) {
 #define X(n) \
-    case n: return xfused_impl<n, PoissonOp>(in, out, ncols, rs, ps, nplanes, out_cs, tw, op, s);
+    case n: return xfused_impl<n, PoissonOp>(in, out, ncols, rs, ps, nplanes, out_cs, tw, op, s, sl, nslots);
         HGPM_SIZES(X)
 #undef X
     }

@@ -31,6 +31,30 @@ struct ParticleSoA {
     float* vz;
 };
 
+__host__ __device__ __forceinline__ ParticleSoA offset_soa(ParticleSoA p, size_t off) {
+    return ParticleSoA{p.cell + off, p.ox + off, p.oy + off, p.oz + off, p.vx + off, p.vy + off, p.vz + off};
+}
+
+// Slots of a batched launch: the boxes of one size class live in slabs with a
+// fixed element stride per buffer, so slot s of a kernel's first buffer starts
+// s*s0 elements after slot 0 (second buffer: s*s1).  `active` (may be null:
+// every slot runs) lets idle slots' CTAs return at once.  A single-box launch
+// passes Slots{} and has one slot.
+struct Slots {
+    const int* active = nullptr;
+    size_t s0 = 0, s1 = 0;
+};
+__device__ __forceinline__ bool slot_idle(const Slots& b, int slot) { return b.active && !b.active[slot]; }
+
+// Per-slot kick parameters of a batched step: row `slot` of a table of
+// float4 (dtf = float(deltaT*fscal), pf_a, pf_b, ndrift) indexed by the
+// slot's step counter.  sched == null: the launch's own scalars apply.
+struct KickSched {
+    const float4* sched = nullptr;
+    const int* step = nullptr;
+    int pitch = 0;
+};
+
 // Signed mode index as get_kmodes maps it (src/haccgpm.hpp:255-274).
 __host__ __device__ __forceinline__ int signed_mode(int i, int n) { return i > n / 2 - 1 ? i - n : i; }
 

@@ -23,15 +23,19 @@ struct PkArgs {
 bool fft_size_supported(int ng);
 int pk_max_bins();
 
+// Launchers of the step's kernels.  `sl`/`nslots` batch the launch over
+// nslots boxes of one size class (Slots in hgpm_device.cuh); the defaults
+// launch one box.
 cudaError_t launch_zfwd(int ng, void* in, bool fixed, float2* out, int nlines, int zs, double mean,
-                        const float2* tw, cudaStream_t s);
+                        const float2* tw, cudaStream_t s, const Slots& sl = Slots{}, int nslots = 1);
 cudaError_t launch_zinv(int ng, const float2* in, float* out, int nlines, int zs, size_t in_cs, size_t out_cs,
-                        int ncomp, float scale, const float2* tw, cudaStream_t s);
+                        int ncomp, float scale, const float2* tw, cudaStream_t s, const Slots& sl = Slots{},
+                        int nslots = 1);
 cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
-                           int ncomp, const float2* tw, cudaStream_t s);
+                           int ncomp, const float2* tw, cudaStream_t s, const Slots& sl = Slots{}, int nslots = 1);
 cudaError_t launch_xpoisson(int ng, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
                             size_t out_cs, const float2* tw, const double* cosq, const float* sk, double coeff,
-                            cudaStream_t s);
+                            cudaStream_t s, const Slots& sl = Slots{}, int nslots = 1);
 cudaError_t launch_xic(int n, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
                        size_t out_cs, const float2* tw, const double* table, int nbins, double k_delta,
                        double pkscale, double inv_delta, const float* kf, int* err, cudaStream_t s);
@@ -53,10 +57,14 @@ cudaError_t launch_store_state(const ParticleSoA& p, float* x, float* v, int np_
 cudaError_t launch_drift(const ParticleSoA& p, size_t n, int ng, float pf, cudaStream_t s);
 int deposit_cap_cells(int np_side, int ng);
 cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
-                           cudaStream_t s);
+                           cudaStream_t s, const Slots& sl = Slots{}, int nslots = 1);
 cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float* fx, const float* fy,
                               const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift,
-                              int variant, cudaStream_t s);
+                              int variant, cudaStream_t s, const Slots& sl = Slots{},
+                              const KickSched& ks = KickSched{}, int nslots = 1);
+// Batched step bookkeeping: each active slot's step counter advances and a
+// slot that has run nsteps[slot] steps goes idle.
+cudaError_t launch_slots_advance(int* active, int* step, const int* nsteps, int nslots, cudaStream_t s);
 cudaError_t launch_density(const unsigned long long* rho64, float* rho, size_t n, cudaStream_t s);
 cudaError_t launch_ktables(int ng, double* cosq, float* sk, float* pkw, cudaStream_t s);
 cudaError_t launch_noise(float* out, size_t n, uint32_t seed, cudaStream_t s);

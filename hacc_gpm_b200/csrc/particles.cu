@@ -187,11 +187,15 @@ __device__ __forceinline__ unsigned long long win_value(const unsigned* __restri
 
 template <int B, bool SMALL>
 __global__ void __launch_bounds__(256, 3) deposit_tiled_kernel(ParticleSoA p, int np_side, int ng, float mass,
-                                                               unsigned long long* __restrict__ rho, int cap_cells) {
+                                                               unsigned long long* __restrict__ rho, int cap_cells,
+                                                               Slots sl) {
     constexpr int B3 = B * B * B;
     constexpr int PPT = B3 / 256;
     extern __shared__ unsigned long long win[];
     __shared__ int bb[6];
+    if (slot_idle(sl, blockIdx.y)) return;
+    p = offset_soa(p, (size_t)blockIdx.y * sl.s0);
+    rho += (size_t)blockIdx.y * sl.s1;
     const int tid = threadIdx.x;
     const int nb = np_side / B;
     const int blk = blockIdx.x;
@@ -375,11 +379,27 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_tiled_kernel(ParticleSoA p
                                                                    const float* __restrict__ fy,
                                                                    const float* __restrict__ fz, double deltaT,
                                                                    double fscal, float pf_a, float pf_b, int ndrift,
-                                                                   int cap_cells) {
+                                                                   int cap_cells, Slots sl, KickSched ks) {
     constexpr int B3 = B * B * B;
     constexpr int PPT = B3 / NT;
     extern __shared__ float fwin[];
     __shared__ int bb[6];
+    const int slot = blockIdx.y;
+    if (slot_idle(sl, slot)) return;
+    p = offset_soa(p, (size_t)slot * sl.s0);
+    fx += (size_t)slot * sl.s1;
+    fy += (size_t)slot * sl.s1;
+    fz += (size_t)slot * sl.s1;
+    // the kick factor deltaT*fscal is folded into the x weight (FP32; the
+    // reference forms float(w*deltaT*fscal) in double, a <=1 ulp difference)
+    float dtf = (float)(deltaT * fscal);
+    if (ks.sched) {
+        const float4 q = ks.sched[(size_t)slot * ks.pitch + ks.step[slot]];
+        dtf = q.x;
+        pf_a = q.y;
+        pf_b = q.z;
+        ndrift = (int)q.w;
+    }
     const int tid = threadIdx.x;
     const int nb = np_side / B;
     const int blk = blockIdx.x;
@@ -452,9 +472,6 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_tiled_kernel(ParticleSoA p
         __syncthreads();
     }
     const int syz = wy * wz;
-    // the kick factor deltaT*fscal is folded into the x weight (FP32; the
-    // reference forms float(w*deltaT*fscal) in double, a <=1 ulp difference)
-    const float dtf = (float)(deltaT * fscal);
     // particles are loaded two iterations ahead
     PState n1 = load_p(p, p0 + tid);
     PState n2 = PPT > 1 ? load_p(p, p0 + tid + NT) : n1;
@@ -647,38 +664,39 @@ int deposit_cap_cells(int np_side, int ng) {
 
 template <int B, bool SMALL>
 static cudaError_t deposit_impl(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
-                                int cap, cudaStream_t s) {
+                                int cap, const Slots& sl, int nslots, cudaStream_t s) {
     auto k = deposit_tiled_kernel<B, SMALL>;
     const int smem = cap * 8;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     const int nb = np_side / B;
-    k<<<nb * nb * nb, 256, smem, s>>>(p, np_side, ng, mass, rho, cap);
+    k<<<dim3(nb * nb * nb, nslots), 256, smem, s>>>(p, np_side, ng, mass, rho, cap, sl);
     return cudaGetLastError();
 }
 
 cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
-                           cudaStream_t s) {
+                           cudaStream_t s, const Slots& sl, int nslots) {
     const int B = block_side(np_side, ng);
     const int cap = deposit_cap_cells(np_side, ng);
     // SMALL needs every window add (a weight, or two merged x-chain weights,
     // each < mass*2^31) below 2^32: mass <= 1
     const bool small = mass <= 1.0f;
-    if (B == 16) return small ? deposit_impl<16, true>(p, np_side, ng, mass, rho, cap, s)
-                              : deposit_impl<16, false>(p, np_side, ng, mass, rho, cap, s);
-    return small ? deposit_impl<8, true>(p, np_side, ng, mass, rho, cap, s)
-                 : deposit_impl<8, false>(p, np_side, ng, mass, rho, cap, s);
+    if (B == 16) return small ? deposit_impl<16, true>(p, np_side, ng, mass, rho, cap, sl, nslots, s)
+                              : deposit_impl<16, false>(p, np_side, ng, mass, rho, cap, sl, nslots, s);
+    return small ? deposit_impl<8, true>(p, np_side, ng, mass, rho, cap, sl, nslots, s)
+                 : deposit_impl<8, false>(p, np_side, ng, mass, rho, cap, sl, nslots, s);
 }
 template <int B, int NT>
 static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const float* fx, const float* fy,
                              const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift, int cap,
-                             cudaStream_t s) {
+                             const Slots& sl, const KickSched& ks, int nslots, cudaStream_t s) {
     auto k = kick_tiled_kernel<B, NT>;
     const int smem = cap * 12;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     const int nb = np_side / B;
-    k<<<nb * nb * nb, NT, smem, s>>>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap);
+    k<<<dim3(nb * nb * nb, nslots), NT, smem, s>>>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap,
+                                                     sl, ks);
     return cudaGetLastError();
 }
 
@@ -688,9 +706,21 @@ static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const fl
 __global__ void __launch_bounds__(256, 6) kick_flat_kernel(ParticleSoA p, size_t n, int ng,
                                                            const float* __restrict__ fx, const float* __restrict__ fy,
                                                            const float* __restrict__ fz, float dtf, float pf_a,
-                                                           float pf_b, int ndrift) {
+                                                           float pf_b, int ndrift, Slots sl, KickSched ks) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const int slot = blockIdx.y;
+    if (i >= n || slot_idle(sl, slot)) return;
+    p = offset_soa(p, (size_t)slot * sl.s0);
+    fx += (size_t)slot * sl.s1;
+    fy += (size_t)slot * sl.s1;
+    fz += (size_t)slot * sl.s1;
+    if (ks.sched) {
+        const float4 q = ks.sched[(size_t)slot * ks.pitch + ks.step[slot]];
+        dtf = q.x;
+        pf_a = q.y;
+        pf_b = q.z;
+        ndrift = (int)q.w;
+    }
     const PState cur = load_p(p, i);
     const int ix = cell_x(cur.c), iy = cell_y(cur.c), iz = cell_z(cur.c);
     const int ix1 = ix + 1 == ng ? 0 : ix + 1;
@@ -719,17 +749,31 @@ __global__ void __launch_bounds__(256, 6) kick_flat_kernel(ParticleSoA p, size_t
 
 cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float* fx, const float* fy,
                               const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift,
-                              int variant, cudaStream_t s) {
+                              int variant, cudaStream_t s, const Slots& sl, const KickSched& ks, int nslots) {
     const int B = block_side(np_side, ng);
     const int cap = deposit_cap_cells(np_side, ng);
     if (variant == 1) {
         const size_t n = (size_t)np_side * np_side * np_side;
-        kick_flat_kernel<<<nblk(n, 256), 256, 0, s>>>(p, n, ng, fx, fy, fz, (float)(deltaT * fscal), pf_a, pf_b,
-                                                      ndrift);
+        kick_flat_kernel<<<dim3(nblk(n, 256), nslots), 256, 0, s>>>(p, n, ng, fx, fy, fz, (float)(deltaT * fscal),
+                                                                    pf_a, pf_b, ndrift, sl, ks);
         return cudaGetLastError();
     }
-    if (B == 16) return kick_impl<16, 512>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap, s);
-    return kick_impl<8, 256>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap, s);
+    if (B == 16)
+        return kick_impl<16, 512>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap, sl, ks, nslots, s);
+    return kick_impl<8, 256>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap, sl, ks, nslots, s);
+}
+__global__ void slots_advance_kernel(int* __restrict__ active, int* __restrict__ step,
+                                     const int* __restrict__ nsteps, int nslots) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nslots || !active[k]) return;
+    const int st = step[k] + 1;
+    step[k] = st;
+    if (st >= nsteps[k]) active[k] = 0;
+}
+
+cudaError_t launch_slots_advance(int* active, int* step, const int* nsteps, int nslots, cudaStream_t s) {
+    slots_advance_kernel<<<nblk(nslots, 128), 128, 0, s>>>(active, step, nsteps, nslots);
+    return cudaGetLastError();
 }
 cudaError_t launch_density(const unsigned long long* rho64, float* rho, size_t n, cudaStream_t s) {
     density_kernel<<<nblk(n, 256), 256, 0, s>>>(rho64, rho, n);

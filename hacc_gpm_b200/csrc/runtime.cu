@@ -13,9 +13,8 @@
 #include <vector>
 
 #include "../../include/hgpm_c.h"
+#include "hgpm_ctx.h"
 #include "hgpm_internal.h"
-
-using namespace hgpm;
 
 // ===========================================================================
 // params (src/simulation/params.cpp)
@@ -295,111 +294,8 @@ extern "C" void hgpm_growth(const hgpm_params* p, double z, double z_vel, double
 }
 
 // ===========================================================================
-// context
+// context (struct hgpm_ctx in hgpm_ctx.h)
 // ===========================================================================
-struct PhaseRec {
-    int phase;
-    cudaEvent_t a, b;
-};
-
-struct hgpm_ctx {
-    hgpm_params p;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    int ng = 0, np = 0, zs = 0, zs_np = 0, blk = 8;
-    size_t ncell = 0, npart = 0, nspec = 0;
-    ParticleSoA part{};
-    void* part_block = nullptr;
-    unsigned long long* rho64 = nullptr;
-    bool rho_dirty = false;
-    float2* spec = nullptr;
-    float2* fspec = nullptr;
-    float* force = nullptr;
-    float2* tw_ng = nullptr;
-    float2* tw_np = nullptr;
-    double* cosq = nullptr;
-    float* sk = nullptr;
-    float* pkw = nullptr;
-    float* kf_pk = nullptr;
-    float* kf_ic = nullptr;
-    int* d_err = nullptr;
-    // kernel variants (environment, read at creation): HGPM_NO_TMA=1 selects the
-    // plain strided y passes, HGPM_XTMA=0|1 the plain/TMA-fed fused x pass,
-    // HGPM_KICK=0|1 the tiled/flat gather
-    bool tma = true;
-    bool xtma = false;
-    int kick_variant = 0;
-    float* stage = nullptr;     // AoS float3 x, v staging (lazy)
-    double* pk_part = nullptr;  // P(k) partial sums (lazy)
-    unsigned long long* pk_pcnt = nullptr;
-    double* pk_sum = nullptr;
-    unsigned long long* pk_cnt = nullptr;
-    int pk_nparts = 0;
-    bool have_state = false;
-    bool timing = false;
-    std::vector<PhaseRec> recs;
-    std::vector<cudaEvent_t> free_events;
-    double phase_ms[HGPM_NPHASE] = {0};
-    int64_t phase_launch[HGPM_NPHASE] = {0};
-    int64_t launches = 0;
-    std::string err;
-};
-
-static int fail(hgpm_ctx* c, int code, const char* fmt, ...) {
-    char buf[512];
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(buf, sizeof(buf), fmt, ap);
-    va_end(ap);
-    if (c) c->err = buf;
-    return code;
-}
-
-#define CK(call)                                                                                  \
-    do {                                                                                          \
-        cudaError_t e_ = (call);                                                                  \
-        if (e_ != cudaSuccess)                                                                    \
-            return fail(c, e_ == cudaErrorMemoryAllocation ? HGPM_ERR_OOM : HGPM_ERR_CUDA,        \
-                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
-    } while (0)
-
-static cudaEvent_t take_event(hgpm_ctx* c) {
-    if (!c->free_events.empty()) {
-        cudaEvent_t e = c->free_events.back();
-        c->free_events.pop_back();
-        return e;
-    }
-    cudaEvent_t e;
-    cudaEventCreate(&e);
-    return e;
-}
-
-struct PhaseScope {
-    hgpm_ctx* c;
-    int phase;
-    cudaEvent_t a = nullptr;
-    PhaseScope(hgpm_ctx* c_, int ph) : c(c_), phase(ph) {
-        if (c->timing) {
-            a = take_event(c);
-            cudaEventRecord(a, c->stream);
-        }
-    }
-    ~PhaseScope() {
-        if (c->timing) {
-            cudaEvent_t b = take_event(c);
-            cudaEventRecord(b, c->stream);
-            c->recs.push_back({phase, a, b});
-        }
-    }
-};
-
-static void count(hgpm_ctx* c, int phase, int n) {
-    c->launches += n;
-    c->phase_launch[phase] += n;
-}
-
-enum { PH_DRIFT = 0, PH_DEPOSIT, PH_ZFWD, PH_YFWD, PH_POISSON, PH_YINV, PH_ZINV, PH_KICK, PH_PK };
-static_assert(PH_PK + 1 == HGPM_NPHASE, "phase ids");
 
 static std::vector<float2> twiddles(int n) {
     std::vector<float2> t(n);
@@ -486,8 +382,6 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
         if ((e = cudaMalloc(&c->cosq, c->ng * 8)) != cudaSuccess) break;
         if ((e = cudaMalloc(&c->sk, c->ng * 4)) != cudaSuccess) break;
         if ((e = cudaMalloc(&c->pkw, c->ng * 4)) != cudaSuccess) break;
-        if ((e = cudaMalloc(&c->kf_pk, c->ng * 4)) != cudaSuccess) break;
-        if ((e = cudaMalloc(&c->kf_ic, c->np * 4)) != cudaSuccess) break;
         // d_err[0]: IC table overrun; d_err[1]: a bounded TMA/mbarrier wait timed out
         if ((e = cudaMalloc(&c->d_err, 8)) != cudaSuccess) break;
         if ((e = cudaMemsetAsync(c->d_err, 0, 8, c->stream)) != cudaSuccess) break;
@@ -503,37 +397,52 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
             }
             if ((e = cudaMemcpyAsync(c->cosq, cq.data(), c->ng * 8, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess) break;
         }
-        std::vector<float> kf(c->ng), kfi(c->np);
-        double dpk = 2.0 * M_PI / p->rl;
-        for (int i = 0; i < c->ng; ++i) kf[i] = (float)((double)signed_mode(i, c->ng) * dpk);
-        for (int i = 0; i < c->np; ++i) kfi[i] = (float)((double)signed_mode(i, c->np) * dpk);
-        if ((e = cudaMemcpy(c->kf_pk, kf.data(), c->ng * 4, cudaMemcpyHostToDevice)) != cudaSuccess) break;
-        if ((e = cudaMemcpy(c->kf_ic, kfi.data(), c->np * 4, cudaMemcpyHostToDevice)) != cudaSuccess) break;
         if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) break;
     } while (0);
     if (e != cudaSuccess) {
         rc = e == cudaErrorMemoryAllocation ? HGPM_ERR_OOM : HGPM_ERR_CUDA;
         c->err = std::string("hgpm_create: ") + cudaGetErrorString(e);
         cudaGetLastError();
+    } else {
+        rc = ctx_set_rl_tables(c);
     }
     c->launches += 1;
     *out = c;
     return rc;
 }
 
+int ctx_set_rl_tables(hgpm_ctx* c) {
+    if (!c->kf_pk) CK(cudaMalloc(&c->kf_pk, c->ng * 4));
+    if (!c->kf_ic) CK(cudaMalloc(&c->kf_ic, c->np * 4));
+    std::vector<float> kf(c->ng), kfi(c->np);
+    const double dpk = 2.0 * M_PI / c->p.rl;
+    for (int i = 0; i < c->ng; ++i) kf[i] = (float)((double)signed_mode(i, c->ng) * dpk);
+    for (int i = 0; i < c->np; ++i) kfi[i] = (float)((double)signed_mode(i, c->np) * dpk);
+    CK(cudaMemcpyAsync(c->kf_pk, kf.data(), c->ng * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->kf_ic, kfi.data(), c->np * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return HGPM_OK;
+}
+
 extern "C" void hgpm_destroy(hgpm_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void* ptrs[] = {c->part_block, c->rho64, c->spec, c->fspec, c->force, c->tw_ng, c->tw_np, c->cosq, c->sk,
-                    c->pkw, c->kf_pk, c->kf_ic, c->d_err, c->stage, c->pk_part, c->pk_pcnt, c->pk_sum, c->pk_cnt};
-    for (void* q : ptrs)
+    // a view owns only its RL tables and its IC table
+    void* own[] = {c->kf_pk, c->kf_ic, c->ic_table};
+    for (void* q : own)
         if (q) cudaFree(q);
+    if (!c->view) {
+        void* ptrs[] = {c->part_block, c->rho64, c->spec, c->fspec, c->force, c->tw_ng, c->tw_np, c->cosq, c->sk,
+                        c->pkw, c->d_err, c->stage, c->pk_part, c->pk_pcnt, c->pk_sum, c->pk_cnt};
+        for (void* q : ptrs)
+            if (q) cudaFree(q);
+    }
     for (auto& r : c->recs) {
         cudaEventDestroy(r.a);
         cudaEventDestroy(r.b);
     }
     for (auto e : c->free_events) cudaEventDestroy(e);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream && !c->view) cudaStreamDestroy(c->stream);
     delete c;
 }
 
@@ -633,11 +542,12 @@ extern "C" int hgpm_drift(hgpm_ctx* c, float prefactor) {
     return HGPM_OK;
 }
 
-static float cic_mass(int ng, int np) {
+float ctx_cic_mass(int ng, int np) {
     // pm_actions.cpp:229-230
     float gpscale = (((float)ng / (float)np));
     return gpscale * gpscale * gpscale;
 }
+static float cic_mass(int ng, int np) { return ctx_cic_mass(ng, np); }
 
 static double mean_density(const hgpm_ctx* c) {
     return (double)cic_mass(c->ng, c->np) * (double)c->npart / (double)c->ncell;
@@ -907,8 +817,14 @@ static int ic_common(hgpm_ctx* c, const float* noise_host, const double* table, 
     double kmax = sqrt(3.0) * (n / 2) * 2 * M_PI / c->p.rl;
     if ((int)(kmax / k_delta) + 1 >= nbins)
         return fail(c, HGPM_ERR_ARG, "input ipk only goes to k=%g, grid needs %g", k_delta * (nbins - 1), kmax);
-    double* d_table = nullptr;
-    CK(cudaMalloc(&d_table, (size_t)nbins * 8));
+    if (nbins > c->ic_table_cap) {
+        if (c->ic_table) CK(cudaFree(c->ic_table));
+        c->ic_table = nullptr;
+        c->ic_table_cap = 0;
+        CK(cudaMalloc(&c->ic_table, (size_t)nbins * 8));
+        c->ic_table_cap = nbins;
+    }
+    double* d_table = c->ic_table;
     int rc = HGPM_OK;
     do {
         float* noise = c->force;  // scratch: the force grids are rebuilt every solve
@@ -949,7 +865,6 @@ static int ic_common(hgpm_ctx* c, const float* noise_host, const double* table, 
         if (herr) { rc = fail(c, HGPM_ERR_ARG, "ipk table too short for the grid's largest |k|"); break; }
         c->have_state = true;
     } while (0);
-    cudaFree(d_table);
     return rc;
 }
 

@@ -190,6 +190,42 @@ int hgpm_phase_times(hgpm_ctx* ctx, double* ms, int64_t* launches);
 /* Number of kernels this context launched since creation / last reset.    */
 int64_t hgpm_kernel_launches(hgpm_ctx* ctx, int reset);
 
+/* ---- batched ensembles ------------------------------------------------------
+ * No counterpart in the reference (its driver runs one box per process,
+ * driver_pm.cpp:32-163).  An ensemble holds size classes; class i is
+ * nslots[i] boxes of one (ng[i], np[i]).  hgpm_ens_step advances every
+ * running box by one PM step with ONE launch per phase per class (the slot
+ * is a grid dimension), classes on parallel streams, optionally replayed
+ * from one CUDA graph.  Per box the results are bit-identical to
+ * hgpm_run_steps on a single context.
+ *
+ * Life of a slot: hgpm_ens_slot binds params (NG/NP of the class, any RL,
+ * cosmology and seed) and returns the slot as a context ("view", owned by
+ * the ensemble, never passed to hgpm_destroy) for ICs, state I/O and P(k);
+ * hgpm_ens_start queues its nsteps-step run; hgpm_ens_step / hgpm_ens_sync /
+ * hgpm_ens_status advance and observe it; hgpm_ens_release frees the slot
+ * once it has finished.  All work is ordered on the ensemble's stream.   */
+typedef struct hgpm_ensemble hgpm_ensemble;
+
+int hgpm_ens_create(int nclass, const int* ng, const int* np, const int* nslots, int device,
+                    hgpm_ensemble** out);
+void hgpm_ens_destroy(hgpm_ensemble* ens);
+const char* hgpm_ens_last_error(const hgpm_ensemble* ens);
+/* Device bytes of one class of nslots boxes (admission by footprint).     */
+size_t hgpm_ens_footprint_bytes(int ng, int np, int nslots);
+void* hgpm_ens_stream(hgpm_ensemble* ens);
+int hgpm_ens_slot(hgpm_ensemble* ens, int cls, int slot, const hgpm_params* p, hgpm_ctx** view);
+/* *ts as hgpm_run_steps takes it; returns advanced through nsteps.        */
+int hgpm_ens_start(hgpm_ensemble* ens, int cls, int slot, hgpm_timestepper* ts, int nsteps);
+int hgpm_ens_release(hgpm_ensemble* ens, int cls, int slot);
+/* nsteps batched steps (slots that finish go idle on the device).         */
+int hgpm_ens_step(hgpm_ensemble* ens, int nsteps);
+int hgpm_ens_use_graph(hgpm_ensemble* ens, int on);
+/* Wait for queued work; refresh the host copy of every slot's status.     */
+int hgpm_ens_sync(hgpm_ensemble* ens);
+int hgpm_ens_status(hgpm_ensemble* ens, int cls, int slot, int* running, int* steps_done);
+int64_t hgpm_ens_kernel_launches(hgpm_ensemble* ens, int reset);
+
 /* ---- allocation-free density ------------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory (a host framework that owns every device allocation, or a run that

@@ -1,0 +1,56 @@
+"""Host logic of the batched ensemble and the serving loop (no kernels):
+slot layout, the request stream, capacity by footprint, argument checks."""
+import numpy as np
+import pytest
+
+import hacc_gpm_b200 as H
+from hacc_gpm_b200 import ensemble as E
+from hacc_gpm_b200 import serve as S
+
+
+def test_class_layout_covers_every_box_once():
+    boxes = E.ensemble_boxes(96)
+    classes, where = E.class_layout(boxes)
+    assert [c[0] for c in classes] == sorted({b.ng for b in boxes})
+    assert sum(c[2] for c in classes) == 96
+    assert len(set(where)) == 96
+    for b, (ci, si) in zip(boxes, where):
+        assert classes[ci][0] == b.ng and 0 <= si < classes[ci][2]
+
+
+def test_ensemble_workload_distribution():
+    boxes = E.ensemble_boxes(96)
+    assert all(b.ng in (32, 48, 64, 96, 128) and 64 <= b.rl <= 512 and 0.7 <= b.sigma8 <= 0.9 for b in boxes)
+    assert [b.seed for b in boxes] == list(range(1000, 1096))
+    assert all(b.nsteps == 64 and b.z_ini == 100.0 for b in boxes)
+    assert E.ensemble_boxes(96)[5].rl == boxes[5].rl  # seeded
+
+
+def test_tables_cover_grid():
+    b = E.ensemble_boxes(3)[0]
+    E.prepare_tables([b])
+    kmax_grid = np.sqrt(3.0) * (b.ng / 2) * 2 * np.pi / b.rl
+    assert b.k_delta * (len(b.table) - 1) > kmax_grid
+
+
+def test_request_stream():
+    reqs = S.request_stream(400, rate=20.0, seed=7)
+    t = np.array([r.arrival for r in reqs])
+    assert np.all(np.diff(t) > 0)
+    assert 15.0 < len(reqs) / t[-1] < 25.0  # mean rate 20/s
+    assert {r.ng for r in reqs} <= {32, 48, 64, 96, 128, 192, 256}
+    assert all(20 <= r.nsteps <= 200 and 0.25 <= r.omega_m <= 0.35 and 0.7 <= r.sigma8 <= 0.9 for r in reqs)
+    assert len({r.seed for r in reqs}) == 400
+
+
+def test_capacity_by_footprint():
+    caps = S.class_capacity([32, 64, 128, 256], 8e9, max_slots=64)
+    for ng, npp, n in caps:
+        assert n >= 1 and (n == 1 or n * H.ensemble.Ensemble.footprint_bytes(ng, npp, 1) <= 2e9 + 1)
+    assert [c[2] for c in caps] == sorted([c[2] for c in caps], reverse=True)
+    assert E.Ensemble.footprint_bytes(64, 64, 4) > 4 * H.footprint_bytes(64, 64) * 0.9
+
+
+def test_bad_class_rejected_without_gpu():
+    with pytest.raises(H.HgpmError, match="NG/NP must be one of"):
+        E.Ensemble([(20, 20, 2)])
