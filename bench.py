@@ -5,9 +5,14 @@
 
 One process per GPU (torchrun for N > 1).  Each rank advances its own
 independent box (replicas: the step itself has no collective), so scaling
-is weak.  The timed region is exactly K whole DKD steps on the device
-(CUDA events on the box's stream, barrier + synchronize on both sides, max
-over ranks).  value = particle updates of all ranks / that time.
+is weak.  The workload is a 100-step run from z = 50 to z = 0; the cost of
+a step grows as the particles cluster (about 7 ms early, 10.6 ms at z = 0 on
+one B200), and the middle of the run costs about the run's average.  So
+the run is advanced untimed to step 45 - W, then W warm-up steps, then
+exactly K timed steps (CUDA events on the box's stream, barrier +
+synchronize on both sides, max over ranks; per-kernel events inside the
+same region).  value = particle updates of all ranks / that time.  The
+whole 100-step run is also timed once ("full_run").
 
 Also reported (rank 0): per-kernel timings and the roofline of the dominant
 kernel against the measured HBM peak, the end-to-end number through the
@@ -49,6 +54,7 @@ NG = NP = 512
 RL = 512.0
 Z_INI = 50.0
 NSTEPS_RUN = 100  # step size of the run the timed steps belong to (z 50 -> 0 in 100 steps)
+MID_STEP = 45     # the timed steps start here (the mid-run cost is the run's average)
 
 # Algorithmic bytes per launch of each kernel (precision-form state:
 # x = 12 B offset + 4 B cell, v = 12 B; FP32 grids).  Sum = 72 Np + 64 Ng.
@@ -85,7 +91,7 @@ def measured_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks/throttle reasons sampled every 50 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -99,7 +105,7 @@ class ClockSampler:
     def start(self):
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
-                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                       "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.p = None
@@ -251,6 +257,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-full", action="store_true", help="skip the whole-run timing")
     ap.add_argument("--size", type=int, default=512, help="np = ng (profiling runs use a smaller box)")
     ap.add_argument("--workload", default="step", choices=["step", "ensemble", "serve"])
     ap.add_argument("--requests", type=int, default=160, help="serve: requests in the stream")
@@ -305,12 +312,16 @@ def main():
     ts.advance_half_step()
     stream = torch.cuda.ExternalStream(sim.stream)
 
-    # warm-up
+    # untimed advance to the middle of the run, then warm-up
+    start = max(0, min(MID_STEP, NSTEPS_RUN - args.steps) - args.warmup)
+    sim.run_steps(ts, start)
     sim.run_steps(ts, args.warmup)
     sim.sync()
 
-    # timed region
+    # timed region (per-kernel events on the same stream, inside the region)
     clocks = ClockSampler(local)
+    sim.enable_timing(True)
+    sim.phase_times()
     barrier()
     torch.cuda.synchronize()
     sim.sync()
@@ -325,17 +336,13 @@ def main():
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
+    ph_ms, ph_n = sim.phase_times()
+    sim.enable_timing(False)
     ms = e0.elapsed_time(e1)
     ms_max = allmax(ms)
     np3, ng3 = NP ** 3, NG ** 3
     value = world * np3 * args.steps / (ms_max * 1e-3)
-
-    # per-kernel timing (separate pass, events around every kernel)
-    sim.enable_timing(True)
-    sim.phase_times()
-    sim.run_steps(ts, args.steps)
-    ph_ms, ph_n = sim.phase_times()
-    sim.enable_timing(False)
+    run_state = {"first_timed_step": start + args.warmup, "a_after": ts.aa}
     peak, peak_kind = measured_peak()
     ab = alg_bytes(np3, ng3)
     phases = {}
@@ -386,6 +393,25 @@ def main():
                "h2d_bytes_per_step": 24 * np3, "d2h_bytes_per_step": 24 * np3, "steps": args.e2e_steps,
                "path": "hgpm_step_host (C-ABI, pinned float3 x,v in and out every step)"}
 
+    # the whole 100-step run once (fresh ICs), for the run-average cost
+    full = None
+    if not args.no_full:
+        sim.generate_ic(table, header[3])
+        tsf = H.Timestepper(params)
+        tsf.set_initial_z(params.z_ini)
+        tsf.reverse_half_step()
+        tsf.advance_half_step()
+        sim.sync()
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        sim.run_steps(tsf, NSTEPS_RUN)
+        f1.record(stream)
+        f1.synchronize()
+        fms = allmax(f0.elapsed_time(f1))
+        full = {"steps": NSTEPS_RUN, "ms_per_step": fms / NSTEPS_RUN,
+                "value": world * np3 * NSTEPS_RUN / (fms * 1e-3), "unit": UNIT, "z": "50 -> 0"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         r = cpu_baseline(steps=1, warmup=0)
@@ -405,9 +431,10 @@ def main():
         "config": {"workload": "PM step (deposit, R2C FFT, Poisson+gradient, 3 C2R FFTs, gather+kick+drift), "
                                "512^3 particles on a 512^3 grid, L=512 Mpc/h, flat LCDM, ICs at z=50, 100-step run",
                    "np": NP, "ng": NG, "rl": RL, "parallelism": "replicas (one independent box per GPU)",
-                   "l2": "inputs larger than L2 (3.8 GB particle state, 5 GB grids)"},
+                   "l2": "inputs larger than L2 (3.8 GB particle state, 5 GB grids)",
+                   "timed": "K steps from step 45 of the 100-step run (mid-run cost = run average)"},
         "roofline": roofline, "step_roofline": step_roof, "phases": phases, "cpu_baseline": cpu, "e2e": e2e,
-        "gpu_launches": int(launches), "clocks": clk,
+        "full_run": full, "timed_steps": run_state, "gpu_launches": int(launches), "clocks": clk,
     }
     print(json.dumps(out))
 

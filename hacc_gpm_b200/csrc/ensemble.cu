@@ -46,6 +46,10 @@ struct EnsClass {
     int* d_step = nullptr;     // [nslots] steps done
     int* d_nsteps = nullptr;   // [nslots]
     float4* d_sched = nullptr; // [nslots][HGPM_MAX_STEPS]
+    int* blkwin = nullptr;     // [nslots][window_records] per-block CIC windows
+    size_t win_stride = 0;
+    int* spill = nullptr;      // counters [4][nslots], then queues [2][nslots][nblocks]
+    SpillList dep_spill, kick_spill;
     int* h_mirror = nullptr;   // pinned: active[nslots], step[nslots], start staging
     float4* h_sched = nullptr; // pinned: one schedule row per slot
     // scratch the slot views share (their calls are ordered on one stream)
@@ -69,7 +73,7 @@ struct hgpm_ensemble {
     std::vector<EnsClass> cls;
     bool use_graph = false;
     cudaGraphExec_t exec = nullptr;
-    int kick_variant = 0;
+    int kick_variant = 2;
     int64_t launches = 0;
     std::string err;
 };
@@ -113,7 +117,8 @@ extern "C" size_t hgpm_ens_footprint_bytes(int ng, int np, int nslots) {
     k.ng = ng;
     k.np = np;
     class_geometry(k);
-    size_t per = k.part_stride * 7 * 4 + k.ncell * 8 + k.spec_elems * 8 * 4 + k.force_elems * 4;
+    size_t per = k.part_stride * 7 * 4 + k.ncell * 8 + k.spec_elems * 8 * 4 + k.force_elems * 4 +
+                 (size_t)window_records(np, ng) * 4;
     const size_t shared = k.npart * 6 * 4 + (size_t)(4 * 148 + 1) * 1024 * 16 + (size_t)ng * 64;
     return per * (size_t)nslots + (size_t)nslots * (HGPM_MAX_STEPS * 16 + 64) + shared;
 }
@@ -168,6 +173,17 @@ static int make_class(hgpm_ensemble* E, EnsClass& k) {
     ECK(cudaMemsetAsync(k.d_step, 0, 4 * S, E->stream));
     ECK(cudaMemsetAsync(k.d_nsteps, 0, 4 * S, E->stream));
     ECK(cudaMalloc(&k.d_sched, sizeof(float4) * HGPM_MAX_STEPS * S));
+    k.win_stride = (size_t)window_records(k.np, k.ng);
+    ECK(cudaMalloc(&k.blkwin, k.win_stride * 4 * S));
+    {
+        const int nblocks = (int)(k.win_stride / 8);
+        ECK(cudaMalloc(&k.spill, (4 * S + 2 * S * (size_t)nblocks) * 4));
+        // counters: deposit queues, kick queues, blocks over the kick's cap,
+        // the kick's work counters
+        k.dep_spill = SpillList{k.spill, k.spill + 4 * S, nblocks, k.spill + 2 * S, k.spill + 3 * S};
+        k.kick_spill = SpillList{k.spill + S, k.spill + 4 * S + S * (size_t)nblocks, nblocks, k.spill + 2 * S,
+                                 k.spill + 3 * S};
+    }
     ECK(cudaMallocHost(&k.h_mirror, sizeof(int) * (2 * S + 4 * S)));
     ECK(cudaMallocHost(&k.h_sched, sizeof(float4) * HGPM_MAX_STEPS * S));
     memset(k.h_mirror, 0, sizeof(int) * 6 * S);
@@ -186,7 +202,7 @@ static void free_class(EnsClass& k) {
     for (hgpm_ctx* v : k.views)
         if (v) hgpm_destroy(v);
     void* d[] = {k.slab, k.tw_ng, k.tw_np, k.cosq, k.sk, k.pkw, k.d_err, k.d_active, k.d_step, k.d_nsteps,
-                 k.d_sched, k.stage, k.pk_part, k.pk_pcnt, k.pk_sum, k.pk_cnt};
+                 k.d_sched, k.stage, k.pk_part, k.pk_pcnt, k.pk_sum, k.pk_cnt, k.blkwin, k.spill};
     for (void* q : d)
         if (q) cudaFree(q);
     if (k.h_mirror) cudaFreeHost(k.h_mirror);
@@ -217,7 +233,7 @@ extern "C" int hgpm_ens_create(int nclass, const int* ng, const int* np, const i
         if (nslots[i] <= 0 || nslots[i] > 65535 / 3) return efail(E, HGPM_ERR_ARG, "class %d: bad slot count", i);
     }
     const char* kv = getenv("HGPM_KICK");
-    if (kv && (kv[0] == '0' || kv[0] == '1')) E->kick_variant = kv[0] - '0';
+    if (kv && kv[0] >= '0' && kv[0] <= '2') E->kick_variant = kv[0] - '0';
     ECK(cudaSetDevice(device));
     ECK(cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking));
     ECK(cudaEventCreateWithFlags(&E->fork, cudaEventDisableTiming));
@@ -298,6 +314,11 @@ extern "C" int hgpm_ens_slot(hgpm_ensemble* E, int ci, int slot, const hgpm_para
         c->sk = k.sk;
         c->pkw = k.pkw;
         c->d_err = k.d_err;
+        c->blkwin = k.blkwin + k.win_stride * slot;
+        c->dep_spill = SpillList{k.dep_spill.cnt + slot, k.dep_spill.items + (size_t)slot * k.dep_spill.nblocks,
+                                 k.dep_spill.nblocks, k.dep_spill.over + slot, k.dep_spill.next + slot};
+        c->kick_spill = SpillList{k.kick_spill.cnt + slot, k.kick_spill.items + (size_t)slot * k.kick_spill.nblocks,
+                                  k.kick_spill.nblocks, k.kick_spill.over + slot, k.kick_spill.next + slot};
         c->stage = k.stage;
         c->pk_part = k.pk_part;
         c->pk_pcnt = k.pk_pcnt;
@@ -390,7 +411,8 @@ static int class_step(hgpm_ensemble* E, EnsClass& k, cudaStream_t s) {
     p.vy = (float*)(b + 5 * a);
     p.vz = (float*)(b + 6 * a);
     const int* act = k.d_active;
-    ECK(launch_deposit(p, k.np, ng, mass, k.rho64, s, Slots{act, k.part_stride, k.ncell}, S));
+    ECK(launch_deposit(p, k.np, ng, mass, k.rho64, k.blkwin, k.dep_spill, s,
+                       Slots{act, k.part_stride, k.ncell, k.win_stride}, S));
     ECK(launch_zfwd(ng, k.rho64, true, k.spec, ng * ng, k.zs, mean, k.tw_ng, s, Slots{act, k.ncell, k.spec_elems}, S));
     ECK(launch_strided(ng, false, k.spec, M + 1, (size_t)k.zs, (size_t)ng * k.zs, ng, 0, 1, k.tw_ng, s,
                        Slots{act, k.spec_elems, 0}, S));
@@ -401,10 +423,11 @@ static int class_step(hgpm_ensemble* E, EnsClass& k, cudaStream_t s) {
     ECK(launch_zinv(ng, k.fspec, k.force, ng * ng, k.zs, cs, k.ncell, 3, 1.0f, k.tw_ng, s,
                     Slots{act, 3 * k.spec_elems, k.force_elems}, S));
     ECK(launch_kick_drift(p, k.np, ng, k.force, k.force + k.ncell, k.force + 2 * k.ncell, 0.0, 0.0, 0.f, 0.f, 0,
-                          E->kick_variant, s, Slots{act, k.part_stride, k.force_elems},
+                          E->kick_variant, k.blkwin, true, k.kick_spill, s,
+                          Slots{act, k.part_stride, k.force_elems, k.win_stride},
                           KickSched{k.d_sched, k.d_step, HGPM_MAX_STEPS}, S));
     ECK(launch_slots_advance(k.d_active, k.d_step, k.d_nsteps, S, s));
-    E->launches += 8;
+    E->launches += 8 + kick_kernels(E->kick_variant, k.np, ng);  // deposit 2, FFT 5, advance 1
     return HGPM_OK;
 }
 
@@ -456,7 +479,8 @@ extern "C" int hgpm_ens_step(hgpm_ensemble* E, int nsteps) {
             cudaGraphDestroy(g);
             ECK(ie);
         }
-        const int per = 8 * (int)E->cls.size();
+        int per = 0;
+        for (auto& k : E->cls) per += 8 + kick_kernels(E->kick_variant, k.np, k.ng);
         for (int i = 0; i < nsteps; ++i) {
             ECK(cudaGraphLaunch(E->exec, E->stream));
             E->launches += per;

@@ -111,6 +111,33 @@ __device__ __forceinline__ void store_tile(const float2* __restrict__ tile, floa
     }
 }
 
+// store_tile with a per-column operator applied on the way out:
+// g[e][c] = op.comp(d, 0, iy, col0 + c, tile[e][c]) (components d >= 1 of the
+// fused x pass, whose factor depends on the plane and column only).
+template <int N, int C, int NT, class Op>
+__device__ __forceinline__ void store_tile_comp(const float2* __restrict__ tile, float2* __restrict__ g, size_t rs,
+                                                int nvalid, const Op& op, int d, int iy, int col0) {
+    constexpr int TPR = C / 2;
+    constexpr int TOT = N * TPR;
+    constexpr int PER = (TOT + NT - 1) / NT;
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int i = threadIdx.x + t * NT;
+        if ((TOT % NT) == 0 || i < TOT) {
+            const int e = i / TPR, c = 2 * (i % TPR);
+            float2* dst = g + (size_t)e * rs + c;
+            const float4 v = *reinterpret_cast<const float4*>(&tile[e * C + c]);
+            const float2 a = op.comp(d, 0, iy, col0 + c, make_float2(v.x, v.y));
+            const float2 b = op.comp(d, 0, iy, col0 + c + 1, make_float2(v.z, v.w));
+            if (c + 1 < nvalid) {
+                __stcs(reinterpret_cast<float4*>(dst), make_float4(a.x, a.y, b.x, b.y));
+            } else if (c < nvalid) {
+                dst[0] = a;
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // z pass, forward R2C.  FIX: input is the int64 fixed-point density
 // (value * 2^32); it is converted to float delta = rho - mean in FP64 and the
@@ -287,7 +314,11 @@ __global__ void __launch_bounds__(Cfg<NG>::NTS, 2) strided_kernel(float2* __rest
 // ---------------------------------------------------------------------------
 // x pass fused with a k-space operator producing 3 components:
 //   forward x FFT of the (z,y)-transformed tile -> t = op.pre(k, rho_k) ->
-//   for d in 0..2: op.comp(d, k, t) -> inverse x FFT -> out[d]
+//   out[0] = IFFT_x(op.comp(0, k, t));  T = IFFT_x(t) ->
+//   out[1] = op.comp(1, ky, kz, T), out[2] = op.comp(2, ky, kz, T).
+// The y and z components' operators (e.g. -i sin(k_y)) are constant along an
+// x line, so they commute with the inverse x transform: two inverse FFTs per
+// tile instead of three.
 // plane = ky index, rows = kx index, columns = kz index; blockIdx.z = slot.
 // ---------------------------------------------------------------------------
 template <int NG, class Op>
@@ -312,17 +343,17 @@ __global__ void __launch_bounds__(Cfg<NG>::NTX) xfused_kernel(const float2* __re
         tile[i] = op.pre(ix, iy, col0 + c, tile[i]);
     }
     // (fft_tile ended with a barrier; pre() only touches the thread's own cells)
-#pragma unroll 1
-    for (int d = 0; d < 3; ++d) {
-        for (int i = threadIdx.x; i < NG * C; i += NT) {
-            const int ix = i / C, c = i % C;
-            work[i] = op.comp(d, ix, iy, col0 + c, tile[i]);
-        }
-        __syncthreads();
-        fft_tile<NG, C, C, true, NT>(work, tw);
-        store_tile<NG, C, NT>(work, out + (size_t)d * out_cs + off, rs, nvalid);
-        __syncthreads();
+    for (int i = threadIdx.x; i < NG * C; i += NT) {
+        const int ix = i / C, c = i % C;
+        work[i] = op.comp(0, ix, iy, col0 + c, tile[i]);
     }
+    __syncthreads();
+    fft_tile<NG, C, C, true, NT>(work, tw);
+    store_tile<NG, C, NT>(work, out + off, rs, nvalid);
+    // (no thread writes tile between the barrier above and this transform)
+    fft_tile<NG, C, C, true, NT>(tile, tw);
+    store_tile_comp<NG, C, NT>(tile, out + out_cs + off, rs, nvalid, op, 1, iy, col0);
+    store_tile_comp<NG, C, NT>(tile, out + 2 * out_cs + off, rs, nvalid, op, 2, iy, col0);
 }
 
 // ---------------------------------------------------------------------------
@@ -437,8 +468,7 @@ __global__ void pk_reduce_kernel(const double* __restrict__ part_sum, const unsi
 // ---------------------------------------------------------------------------
 template <class K>
 static cudaError_t ensure_smem(K kernel, int bytes) {
-    if (bytes <= 48 * 1024) return cudaSuccess;
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return smem_attr_once((const void*)kernel, bytes);
 }
 
 static inline unsigned cdiv(size_t a, size_t b) { return (unsigned)((a + b - 1) / b); }
@@ -514,7 +544,7 @@ static cudaError_t xpk_impl(const float2* in, int ncols, size_t rs, size_t ps, c
     constexpr int NW = kThreads / 32;
     const int smem = NG * G::CX * 8 + NW * a.nbins * 16;
     auto k = xpk_kernel<NG>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = smem_attr_once((const void*)k, smem);
     if (e != cudaSuccess) return e;
     const int nchunks = cdiv(ncols, G::CX);
     k<<<nparts, kThreads, smem, s>>>(in, ncols, rs, ps, nchunks, tw, a, part_sum, part_cnt);

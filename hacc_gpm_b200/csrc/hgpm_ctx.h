@@ -40,12 +40,15 @@ struct hgpm_ctx {
     float* kf_pk = nullptr;
     float* kf_ic = nullptr;
     int* d_err = nullptr;
+    int* blkwin = nullptr;   // per-block CIC windows of the last deposit
+    SpillList dep_spill, kick_spill;  // blocks too wide for the windows
+    bool win_valid = false;  // blkwin describes the current positions
     // kernel variants (environment, read at creation): HGPM_NO_TMA=1 selects the
     // plain strided y passes, HGPM_XTMA=0|1 the plain/TMA-fed fused x pass,
-    // HGPM_KICK=0|1 the tiled/flat gather
+    // HGPM_KICK=0|1|2 the tiled / flat / float4-window gather (default 2)
     bool tma = true;
     bool xtma = false;
-    int kick_variant = 0;
+    int kick_variant = 2;
     float* stage = nullptr;     // AoS float3 x, v staging (lazy)
     double* pk_part = nullptr;  // P(k) partial sums (lazy)
     unsigned long long* pk_pcnt = nullptr;

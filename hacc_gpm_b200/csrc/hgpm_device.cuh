@@ -37,14 +37,29 @@ __host__ __device__ __forceinline__ ParticleSoA offset_soa(ParticleSoA p, size_t
 
 // Slots of a batched launch: the boxes of one size class live in slabs with a
 // fixed element stride per buffer, so slot s of a kernel's first buffer starts
-// s*s0 elements after slot 0 (second buffer: s*s1).  `active` (may be null:
-// every slot runs) lets idle slots' CTAs return at once.  A single-box launch
-// passes Slots{} and has one slot.
+// s*s0 elements after slot 0 (second buffer: s*s1; the per-block window
+// records of the deposit and kick: s*s2).  `active` (may be null: every slot
+// runs) lets idle slots' CTAs return at once.  A single-box launch passes
+// Slots{} and has one slot.
 struct Slots {
     const int* active = nullptr;
-    size_t s0 = 0, s1 = 0;
+    size_t s0 = 0, s1 = 0, s2 = 0;
 };
 __device__ __forceinline__ bool slot_idle(const Slots& b, int slot) { return b.active && !b.active[slot]; }
+
+// Blocks whose CIC window is wider than a kernel's shared-memory window:
+// the windowed kernel queues them (cnt[slot], items[slot * nblocks + i]) and
+// a one-particle-per-thread pass handles their particles.
+struct SpillList {
+    int* cnt = nullptr;
+    int* items = nullptr;
+    int nblocks = 0;
+    // blocks whose window exceeds the float4 kick's cap, counted by the
+    // deposit (over[slot]); the kick reads it to choose its path
+    int* over = nullptr;
+    // work counter of a persistent windowed kernel (next block to take)
+    int* next = nullptr;
+};
 
 // Per-slot kick parameters of a batched step: row `slot` of a table of
 // float4 (dtf = float(deltaT*fscal), pf_a, pf_b, ndrift) indexed by the

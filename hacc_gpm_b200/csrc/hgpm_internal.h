@@ -21,6 +21,12 @@ struct PkArgs {
 };
 
 bool fft_size_supported(int ng);
+// cudaFuncAttributeMaxDynamicSharedMemorySize for `func` on the current
+// device, set once per (device, kernel) rather than before every launch.
+cudaError_t smem_attr_once(const void* func, int bytes);
+// Resident CTAs per SM of `func` at this block size and shared memory
+// (occupancy query made once per (device, kernel)).
+int blocks_per_sm_once(const void* func, int threads, int smem);
 int pk_max_bins();
 
 // Launchers of the step's kernels.  `sl`/`nslots` batch the launch over
@@ -56,12 +62,24 @@ cudaError_t launch_load_state(const float* x, const float* v, const ParticleSoA&
 cudaError_t launch_store_state(const ParticleSoA& p, float* x, float* v, int np_side, int B, cudaStream_t s);
 cudaError_t launch_drift(const ParticleSoA& p, size_t n, int ng, float pf, cudaStream_t s);
 int deposit_cap_cells(int np_side, int ng);
+// The deposit writes every block's CIC window (kWinRec ints per block); the
+// kick reads it back when have_rec (positions unchanged since the deposit),
+// else measures and writes it.
+int window_records(int np_side, int ng);  // ints per box
+// Kernels one launch_kick_drift call launches for this variant and size.
+inline int kick_kernels(int variant, int np_side, int ng) {
+    return (variant == 2 && block_side(np_side, ng) == 16) ? 2 : 1;
+}
+// Blocks too wide for a kernel's window are queued in `spill` (the deposit's
+// and the kick's own lists) and run one particle per thread after the
+// windowed pass, inside the same launcher.
 cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
-                           cudaStream_t s, const Slots& sl = Slots{}, int nslots = 1);
+                           int* blkwin, const SpillList& spill, cudaStream_t s, const Slots& sl = Slots{},
+                           int nslots = 1);
 cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float* fx, const float* fy,
                               const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift,
-                              int variant, cudaStream_t s, const Slots& sl = Slots{},
-                              const KickSched& ks = KickSched{}, int nslots = 1);
+                              int variant, int* blkwin, bool have_rec, const SpillList& spill, cudaStream_t s,
+                              const Slots& sl = Slots{}, const KickSched& ks = KickSched{}, int nslots = 1);
 // Batched step bookkeeping: each active slot's step counter advances and a
 // slot that has run nsteps[slot] steps goes idle.
 cudaError_t launch_slots_advance(int* active, int* step, const int* nsteps, int nslots, cudaStream_t s);

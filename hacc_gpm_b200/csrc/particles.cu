@@ -9,6 +9,10 @@
 #include <stdint.h>
 #include <math.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "hgpm_device.cuh"
 #include "hgpm_internal.h"
 
@@ -143,6 +147,65 @@ struct WinMap {
     }
 };
 
+// Bounding box of a Lagrangian block's cells relative to the block's
+// lattice origin (o0x, o0y, o0z), plus one cell for the CIC upper corners:
+// window origin (l0) and extent (w) per axis.  Every thread of the CTA calls
+// it (two barriers); bb is 6 ints of shared memory.
+template <int NT, int PPT>
+__device__ __forceinline__ void block_window(const uint32_t* __restrict__ cell, size_t p0, int o0x, int o0y, int o0z,
+                                             int ng, int* bb, int l0[3], int w[3]) {
+    const int tid = threadIdx.x;
+    if (tid < 3) bb[tid] = 0x7fffffff;
+    else if (tid < 6) bb[tid] = -0x7fffffff;
+    __syncthreads();
+    int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
+#pragma unroll
+    for (int k = 0; k < PPT; ++k) {
+        const uint32_t c = __ldg(&cell[p0 + tid + k * NT]);
+        const int rx = nearest_image(cell_x(c) - o0x, ng);
+        const int ry = nearest_image(cell_y(c) - o0y, ng);
+        const int rz = nearest_image(cell_z(c) - o0z, ng);
+        mn[0] = min(mn[0], rx); mx[0] = max(mx[0], rx);
+        mn[1] = min(mn[1], ry); mx[1] = max(mx[1], ry);
+        mn[2] = min(mn[2], rz); mx[2] = max(mx[2], rz);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        mn[a] = __reduce_min_sync(0xffffffffu, mn[a]);
+        mx[a] = __reduce_max_sync(0xffffffffu, mx[a]);
+    }
+    if ((tid & 31) == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(&bb[a], mn[a]);
+            atomicMax(&bb[3 + a], mx[a]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        l0[a] = bb[a];
+        w[a] = bb[3 + a] - bb[a] + 2;
+    }
+}
+
+__device__ __forceinline__ int wrap_once(int g, int ng) { return g >= ng ? g - ng : (g < 0 ? g + ng : g); }
+
+// Window-relative coordinate of a cell along one axis: (g - origin) mod ng
+// for an origin already wrapped into [0, ng); exact for windows narrower
+// than the grid.
+__device__ __forceinline__ int win_rel(int g, int origin, int ng) {
+    const int d = g - origin;
+    return d < 0 ? d + ng : d;
+}
+
+// Per-block window record (origin l0 relative to the block's lattice corner,
+// extent w), written by the deposit for the kick of the same positions.
+constexpr int kWinRec = 8;
+// Window cap of the float4 kick (kick_win4_kernel): 110.6 KB, two 512-thread
+// CTAs per SM.  The deposit counts the blocks above it.
+constexpr int kWin4Cap = 6912;
+
 // 8 fixed-point corner weights, index (a*2+b)*2+c for corner (+a, +b, +c)
 template <bool SMALL>
 __device__ __forceinline__ void cic_fixed(float dx, float dy, float dz, float mass, unsigned long long q[8]) {
@@ -188,52 +251,30 @@ __device__ __forceinline__ unsigned long long win_value(const unsigned* __restri
 template <int B, bool SMALL>
 __global__ void __launch_bounds__(256, 3) deposit_tiled_kernel(ParticleSoA p, int np_side, int ng, float mass,
                                                                unsigned long long* __restrict__ rho, int cap_cells,
-                                                               Slots sl) {
+                                                               int* __restrict__ blkwin, SpillList spill, Slots sl) {
     constexpr int B3 = B * B * B;
     constexpr int PPT = B3 / 256;
     extern __shared__ unsigned long long win[];
     __shared__ int bb[6];
     if (slot_idle(sl, blockIdx.y)) return;
-    p = offset_soa(p, (size_t)blockIdx.y * sl.s0);
-    rho += (size_t)blockIdx.y * sl.s1;
     const int tid = threadIdx.x;
     const int nb = np_side / B;
     const int blk = blockIdx.x;
+    // this block's particles: 32-bit indices from here on
+    p = offset_soa(p, (size_t)blockIdx.y * sl.s0 + (size_t)blk * B3);
+    rho += (size_t)blockIdx.y * sl.s1;
     const int bz = blk % nb, by = (blk / nb) % nb, bx = blk / (nb * nb);
     const int ox = (int)((long long)bx * B * ng / np_side);
     const int oy = (int)((long long)by * B * ng / np_side);
     const int oz = (int)((long long)bz * B * ng / np_side);
-    if (tid < 3) bb[tid] = 0x7fffffff;
-    else if (tid < 6) bb[tid] = -0x7fffffff;
-    __syncthreads();
-    const size_t p0 = (size_t)blk * B3;
-    int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
-#pragma unroll 4
-    for (int k = 0; k < PPT; ++k) {
-        const uint32_t c = __ldg(&p.cell[p0 + tid + k * 256]);
-        const int rx = nearest_image(cell_x(c) - ox, ng);
-        const int ry = nearest_image(cell_y(c) - oy, ng);
-        const int rz = nearest_image(cell_z(c) - oz, ng);
-        mn[0] = min(mn[0], rx); mx[0] = max(mx[0], rx);
-        mn[1] = min(mn[1], ry); mx[1] = max(mx[1], ry);
-        mn[2] = min(mn[2], rz); mx[2] = max(mx[2], rz);
-    }
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        mn[a] = __reduce_min_sync(0xffffffffu, mn[a]);
-        mx[a] = __reduce_max_sync(0xffffffffu, mx[a]);
-    }
-    if ((tid & 31) == 0) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            atomicMin(&bb[a], mn[a]);
-            atomicMax(&bb[3 + a], mx[a]);
-        }
-    }
-    __syncthreads();
-    const int lx0 = bb[0], ly0 = bb[1], lz0 = bb[2];
-    const int wx = bb[3] - lx0 + 2, wy = bb[4] - ly0 + 2, wz = bb[5] - lz0 + 2;
+    int l0[3], w[3];
+    block_window<256, PPT>(p.cell, 0, ox, oy, oz, ng, bb, l0, w);
+    if (blkwin && tid < 6) blkwin[(size_t)blockIdx.y * sl.s2 + (size_t)blk * kWinRec + tid] = tid < 3 ? l0[tid] : w[tid - 3];
+    const int wx = w[0], wy = w[1], wz = w[2];
+    // window origin in grid coordinates, wrapped into [0, ng)
+    const int gx0 = wrap_once(ox + l0[0], ng), gy0 = wrap_once(oy + l0[1], ng), gz0 = wrap_once(oz + l0[2], ng);
     const long long vol = (long long)wx * wy * wz;
+    if (tid == 0 && spill.over && vol > kWin4Cap) atomicAdd(&spill.over[blockIdx.y], 1);
     if (vol <= cap_cells) {
         unsigned* w0 = reinterpret_cast<unsigned*>(win);
         unsigned* w1 = w0 + cap_cells;
@@ -247,14 +288,14 @@ __global__ void __launch_bounds__(256, 3) deposit_tiled_kernel(ParticleSoA p, in
         unsigned long long pend[4] = {0ull, 0ull, 0ull, 0ull};
         int pw = -1;  // window index of the pending (upper-x) face; -1: none
         // next particle's cell and offsets are loaded one iteration ahead
-        uint32_t nc = __ldg(&p.cell[p0 + tid]);
-        float nx = __ldg(&p.ox[p0 + tid]), ny = __ldg(&p.oy[p0 + tid]), nz = __ldg(&p.oz[p0 + tid]);
+        uint32_t nc = __ldg(&p.cell[tid]);
+        float nx = __ldg(&p.ox[tid]), ny = __ldg(&p.oy[tid]), nz = __ldg(&p.oz[tid]);
 #pragma unroll 1
         for (int k = 0; k < PPT; ++k) {
             const uint32_t c = nc;
             const float cx = nx, cy = ny, cz = nz;
             if (k + 1 < PPT) {
-                const size_t nidx = p0 + tid + (k + 1) * 256;
+                const int nidx = tid + (k + 1) * 256;
                 nc = __ldg(&p.cell[nidx]);
                 nx = __ldg(&p.ox[nidx]);
                 ny = __ldg(&p.oy[nidx]);
@@ -262,8 +303,8 @@ __global__ void __launch_bounds__(256, 3) deposit_tiled_kernel(ParticleSoA p, in
             }
             unsigned long long q[8];
             cic_fixed<SMALL>(cx, cy, cz, mass, q);
-            const int cw = ((nearest_image(cell_x(c) - ox, ng) - lx0) * wy + (nearest_image(cell_y(c) - oy, ng) - ly0)) *
-                               wz + (nearest_image(cell_z(c) - oz, ng) - lz0);
+            const int cw = (win_rel(cell_x(c), gx0, ng) * wy + win_rel(cell_y(c), gy0, ng)) * wz +
+                           win_rel(cell_z(c), gz0, ng);
             if (pw == cw) {
 #pragma unroll
                 for (int j = 0; j < 4; ++j) q[j] += pend[j];
@@ -280,31 +321,124 @@ __global__ void __launch_bounds__(256, 3) deposit_tiled_kernel(ParticleSoA p, in
 #pragma unroll
         for (int j = 0; j < 4; ++j) win_add<SMALL>(w0, w1, pw + off[j], pend[j]);
         __syncthreads();
-        const WinMap map(wy, wz, ox + lx0, oy + ly0, oz + lz0, ng);
+        const WinMap map(wy, wz, gx0, gy0, gz0, ng);
         for (int i = tid; i < vol; i += 256) {
             const unsigned long long v = win_value<SMALL>(w0, w1, i);
             if (v != 0ull) atomicAdd(&rho[map.global(i)], v);
         }
-    } else {
-        for (int k = 0; k < PPT; ++k) {
-            const size_t idx = p0 + tid + k * 256;
-            const uint32_t c = __ldg(&p.cell[idx]);
-            unsigned long long q[8];
-            cic_fixed<SMALL>(__ldg(&p.ox[idx]), __ldg(&p.oy[idx]), __ldg(&p.oz[idx]), mass, q);
-            const int ix = cell_x(c), iy = cell_y(c), iz = cell_z(c);
-            const int ix1 = ix + 1 == ng ? 0 : ix + 1;
-            const int iy1 = iy + 1 == ng ? 0 : iy + 1;
-            const int iz1 = iz + 1 == ng ? 0 : iz + 1;
-            const size_t sx[2] = {(size_t)ix * ng * ng, (size_t)ix1 * ng * ng};
-            const size_t sy[2] = {(size_t)iy * ng, (size_t)iy1 * ng};
-            const size_t sz[2] = {(size_t)iz, (size_t)iz1};
+    } else if (tid == 0) {
+        // too wide for the window: queued for deposit_spill_kernel
+        const int slot = blockIdx.y;
+        spill.items[(size_t)slot * spill.nblocks + atomicAdd(&spill.cnt[slot], 1)] = blk;
+    }
+}
+
+// The 8 fixed-point corner weights of one particle added straight to the
+// int64 grid (blocks too wide for a shared-memory window).
+template <bool SMALL>
+__device__ __forceinline__ void deposit_global(unsigned long long* __restrict__ rho, uint32_t c, float dx, float dy,
+                                               float dz, float mass, int ng) {
+    unsigned long long q[8];
+    cic_fixed<SMALL>(dx, dy, dz, mass, q);
+    const int ix = cell_x(c), iy = cell_y(c), iz = cell_z(c);
+    const int ix1 = ix + 1 == ng ? 0 : ix + 1;
+    const int iy1 = iy + 1 == ng ? 0 : iy + 1;
+    const int iz1 = iz + 1 == ng ? 0 : iz + 1;
+    const size_t sx[2] = {(size_t)ix * ng * ng, (size_t)ix1 * ng * ng};
+    const size_t sy[2] = {(size_t)iy * ng, (size_t)iy1 * ng};
+    const size_t sz[2] = {(size_t)iz, (size_t)iz1};
 #pragma unroll
-            for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < 2; ++a)
 #pragma unroll
-                for (int b = 0; b < 2; ++b)
+        for (int b = 0; b < 2; ++b)
 #pragma unroll
-                    for (int cc = 0; cc < 2; ++cc)
-                        atomicAdd(&rho[sx[a] + sy[b] + sz[cc]], q[(a * 2 + b) * 2 + cc]);
+            for (int cc = 0; cc < 2; ++cc) atomicAdd(&rho[sx[a] + sy[b] + sz[cc]], q[(a * 2 + b) * 2 + cc]);
+}
+
+// Blocks queued by deposit_tiled_kernel (window wider than its 72 KB): a
+// persistent grid of one CTA per SM with a kBigCap-cell window (216 KB) takes
+// them from the queue one at a time.  A thread walks PPT x-adjacent particles
+// (the x-chain of deposit_tiled_kernel).  Windows wider still add straight to
+// the global grid.
+constexpr int kBigCap = 27648;
+
+template <int B, bool SMALL, int NT>
+__global__ void __launch_bounds__(NT, 1) deposit_spill_kernel(ParticleSoA p, int np_side, int ng, float mass,
+                                                              unsigned long long* __restrict__ rho,
+                                                              const int* __restrict__ blkwin, SpillList spill,
+                                                              Slots sl) {
+    constexpr int B3 = B * B * B, PPT = B3 / NT, BB = B * B;
+    extern __shared__ unsigned long long win[];
+    const int slot = blockIdx.y;
+    if (slot_idle(sl, slot)) return;
+    const int cnt = __ldg(&spill.cnt[slot]);
+    if ((int)blockIdx.x >= cnt) return;
+    p = offset_soa(p, (size_t)slot * sl.s0);
+    rho += (size_t)slot * sl.s1;
+    const int* items = spill.items + (size_t)slot * spill.nblocks;
+    const int* recs = blkwin + (size_t)slot * sl.s2;
+    unsigned* w0 = reinterpret_cast<unsigned*>(win);
+    unsigned* w1 = w0 + kBigCap;
+    const int tid = threadIdx.x;
+    const int g = tid / BB, r = tid % BB;  // x group and (y, z) of the thread's chain
+    const int nb = np_side / B;
+    for (int t = blockIdx.x; t < cnt; t += gridDim.x) {
+        const int blk = __ldg(&items[t]);
+        const int* rec = recs + (size_t)blk * kWinRec;
+        const int wx = __ldg(&rec[3]), wy = __ldg(&rec[4]), wz = __ldg(&rec[5]);
+        const int bz = blk % nb, by = (blk / nb) % nb, bx = blk / (nb * nb);
+        const int gx0 = wrap_once((int)((long long)bx * B * ng / np_side) + __ldg(&rec[0]), ng);
+        const int gy0 = wrap_once((int)((long long)by * B * ng / np_side) + __ldg(&rec[1]), ng);
+        const int gz0 = wrap_once((int)((long long)bz * B * ng / np_side) + __ldg(&rec[2]), ng);
+        const long long vol = (long long)wx * wy * wz;
+        const ParticleSoA pb = offset_soa(p, (size_t)blk * B3);
+        if (vol <= kBigCap) {
+            for (int i = tid; i < vol; i += NT) {
+                w0[i] = 0u;
+                w1[i] = 0u;
+            }
+            __syncthreads();
+            const int syz = wy * wz;
+            const int off[4] = {0, 1, wz, wz + 1};
+            unsigned long long pend[4] = {0ull, 0ull, 0ull, 0ull};
+            int pw = -1;
+#pragma unroll
+            for (int k = 0; k < PPT; ++k) {
+                const int i = (g * PPT + k) * BB + r;
+                const uint32_t c = __ldg(&pb.cell[i]);
+                unsigned long long q[8];
+                cic_fixed<SMALL>(__ldg(&pb.ox[i]), __ldg(&pb.oy[i]), __ldg(&pb.oz[i]), mass, q);
+                const int cw = (win_rel(cell_x(c), gx0, ng) * wy + win_rel(cell_y(c), gy0, ng)) * wz +
+                               win_rel(cell_z(c), gz0, ng);
+                if (pw == cw) {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) q[j] += pend[j];
+                } else if (pw >= 0) {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) win_add<SMALL>(w0, w1, pw + off[j], pend[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) win_add<SMALL>(w0, w1, cw + off[j], q[j]);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) pend[j] = q[4 + j];
+                pw = cw + syz;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) win_add<SMALL>(w0, w1, pw + off[j], pend[j]);
+            __syncthreads();
+            const WinMap map(wy, wz, gx0, gy0, gz0, ng);
+            for (int i = tid; i < vol; i += NT) {
+                const unsigned long long v = win_value<SMALL>(w0, w1, i);
+                if (v != 0ull) atomicAdd(&rho[map.global(i)], v);
+            }
+            __syncthreads();
+        } else {
+#pragma unroll
+            for (int k = 0; k < PPT; ++k) {
+                const int i = (g * PPT + k) * BB + r;
+                deposit_global<SMALL>(rho, __ldg(&pb.cell[i]), __ldg(&pb.ox[i]), __ldg(&pb.oy[i]), __ldg(&pb.oz[i]),
+                                      mass, ng);
+            }
         }
     }
 }
@@ -525,6 +659,221 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_tiled_kernel(ParticleSoA p
     }
 }
 
+
+// Kick variant 2: the force window is staged as one float4 (fx, fy, fz, 0)
+// per cell, so each CIC corner is a single 16-byte shared load (8 per
+// particle instead of 24 4-byte loads), filled row by row.  The window
+// comes from the deposit's record when the positions are the ones it
+// deposited.  Windows above kWin4Cap cells gather from global memory.
+
+// Fill a float4 (fx, fy, fz, 0) window of wx*wy*wz cells whose origin is
+// (gx0, gy0, gz0) (wrapped into [0, ng)) row by row: a warp takes an (x, y)
+// row, lanes walk z, RU rows in flight per warp, the row start formed once.
+template <int NT, int RU>
+__device__ __forceinline__ void fill_win4(float4* __restrict__ win4, const float* __restrict__ fx,
+                                          const float* __restrict__ fy, const float* __restrict__ fz, int wx, int wy,
+                                          int wz, int gx0, int gy0, int gz0, int ng) {
+    constexpr int NW = NT / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nrows = wx * wy;
+    const unsigned my = div_magic((unsigned)wy);
+    for (int z0 = 0; z0 < wz; z0 += 32) {
+        const int z = z0 + lane;
+        const int gz = wrap_once(gz0 + z, ng);
+        for (int r0 = warp; r0 < nrows; r0 += RU * NW) {
+            float4 v[RU];
+#pragma unroll
+            for (int u = 0; u < RU; ++u) {
+                const int r = r0 + u * NW;
+                if (r < nrows && z < wz) {
+                    const int cx = (int)div_by((unsigned)r, my), cy = r - cx * wy;
+                    const size_t g = ((size_t)wrap_once(gx0 + cx, ng) * ng + wrap_once(gy0 + cy, ng)) * ng + gz;
+                    v[u] = make_float4(__ldg(&fx[g]), __ldg(&fy[g]), __ldg(&fz[g]), 0.f);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < RU; ++u) {
+                const int r = r0 + u * NW;
+                if (r < nrows && z < wz) win4[r * wz + z] = v[u];
+            }
+        }
+    }
+}
+
+// CIC gather of one particle from a float4 window (j0: its base cell).
+__device__ __forceinline__ float3 gather_win4(const float4* __restrict__ win4, int j0, int syz, int wz,
+                                              const PState& cur, float dtf) {
+    const float wxa[2] = {(1.f - cur.dx) * dtf, cur.dx * dtf}, wya[2] = {1.f - cur.dy, cur.dy},
+                wza[2] = {1.f - cur.dz, cur.dz};
+    float3 dv = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const float wab = __fmul_rn(wxa[a], wya[b]);
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const float4 f = win4[j0 + a * syz + b * wz + cc];
+                const float mul = __fmul_rn(wab, wza[cc]);
+                dv.x = fmaf(mul, f.x, dv.x);
+                dv.y = fmaf(mul, f.y, dv.y);
+                dv.z = fmaf(mul, f.z, dv.z);
+            }
+        }
+    return dv;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) kick_win4_kernel(ParticleSoA p, int np_side, int ng,
+                                                                  const float* __restrict__ fx,
+                                                                  const float* __restrict__ fy,
+                                                                  const float* __restrict__ fz, double deltaT,
+                                                                  double fscal, float pf_a, float pf_b, int ndrift,
+                                                                  int* __restrict__ blkwin, int have_rec,
+                                                                  SpillList spill, Slots sl, KickSched ks) {
+    constexpr int B = 16, B3 = B * B * B, PPT = B3 / NT;
+    // most blocks too wide for the window (counted by the deposit of these
+    // positions): kick_spill_kernel takes every particle instead
+    if (have_rec && spill.over && spill.over[blockIdx.y] * 2 > spill.nblocks) return;
+    extern __shared__ float4 win4[];
+    __shared__ int bb[6];
+    const int slot = blockIdx.y;
+    if (slot_idle(sl, slot)) return;
+    p = offset_soa(p, (size_t)slot * sl.s0);
+    fx += (size_t)slot * sl.s1;
+    fy += (size_t)slot * sl.s1;
+    fz += (size_t)slot * sl.s1;
+    float dtf = (float)(deltaT * fscal);
+    if (ks.sched) {
+        const float4 q = ks.sched[(size_t)slot * ks.pitch + ks.step[slot]];
+        dtf = q.x;
+        pf_a = q.y;
+        pf_b = q.z;
+        ndrift = (int)q.w;
+    }
+    const int tid = threadIdx.x;
+    const int nb = np_side / B;
+    __shared__ int next_blk;
+    for (;;) {
+        if (tid == 0) next_blk = atomicAdd(&spill.next[slot], 1);
+        __syncthreads();
+        const int blk = next_blk;
+        __syncthreads();  // everyone has read next_blk before thread 0 takes another
+        if (blk >= nb * nb * nb) break;
+        const int bz = blk % nb, by = (blk / nb) % nb, bx = blk / (nb * nb);
+        const int ox0 = (int)((long long)bx * B * ng / np_side);
+        const int oy0 = (int)((long long)by * B * ng / np_side);
+        const int oz0 = (int)((long long)bz * B * ng / np_side);
+        const size_t p0 = (size_t)blk * B3;
+        int* rec = blkwin + (size_t)slot * sl.s2 + (size_t)blk * kWinRec;
+        int l0[3], w[3];
+        if (have_rec) {
+            // the deposit of these same positions already measured the window
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                l0[a] = rec[a];
+                w[a] = rec[3 + a];
+            }
+        } else {
+            block_window<NT, PPT>(p.cell, p0, ox0, oy0, oz0, ng, bb, l0, w);
+            if (tid < 6) rec[tid] = tid < 3 ? l0[tid] : w[tid - 3];
+        }
+        const int wy = w[1], wz = w[2];
+        const int vol = w[0] * wy * wz;
+        if (vol > kWin4Cap) {
+            // too wide for the window: queued for kick_spill_kernel
+            if (tid == 0) spill.items[(size_t)slot * spill.nblocks + atomicAdd(&spill.cnt[slot], 1)] = blk;
+            continue;
+        }
+        const int gx0 = wrap_once(ox0 + l0[0], ng), gy0 = wrap_once(oy0 + l0[1], ng);
+        const int gz0 = wrap_once(oz0 + l0[2], ng);
+        fill_win4<NT, 4>(win4, fx, fy, fz, w[0], wy, wz, gx0, gy0, gz0, ng);
+        __syncthreads();
+        const int syz = wy * wz;
+        PState n1 = load_p(p, p0 + tid);
+        PState n2 = PPT > 1 ? load_p(p, p0 + tid + NT) : n1;
+#pragma unroll 1
+        for (int k = 0; k < PPT; ++k) {
+            const size_t i = p0 + tid + k * NT;
+            const PState cur = n1;
+            n1 = n2;
+            if (k + 2 < PPT) n2 = load_p(p, i + 2 * NT);
+            const int j0 = (win_rel(cell_x(cur.c), gx0, ng) * wy + win_rel(cell_y(cur.c), gy0, ng)) * wz +
+                           win_rel(cell_z(cur.c), gz0, ng);
+            finish_p(p, i, cur, gather_win4(win4, j0, syz, wz, cur, dtf), pf_a, pf_b, ndrift, ng);
+        }
+        __syncthreads();  // the window is refilled for the next block
+    }
+}
+
+// CIC gather of one particle straight from the global force grids (the
+// flat and spill kicks), in the windowed kernels' FP32 order.
+__device__ __forceinline__ float3 gather_global(const float* __restrict__ fx, const float* __restrict__ fy,
+                                                const float* __restrict__ fz, const PState& cur, float dtf, int ng) {
+    const int ix = cell_x(cur.c), iy = cell_y(cur.c), iz = cell_z(cur.c);
+    const int ix1 = ix + 1 == ng ? 0 : ix + 1;
+    const int iy1 = iy + 1 == ng ? 0 : iy + 1;
+    const int iz1 = iz + 1 == ng ? 0 : iz + 1;
+    const size_t sx[2] = {(size_t)ix * ng * ng, (size_t)ix1 * ng * ng};
+    const size_t sy[2] = {(size_t)iy * ng, (size_t)iy1 * ng};
+    const size_t sz[2] = {(size_t)iz, (size_t)iz1};
+    const float wxa[2] = {(1.f - cur.dx) * dtf, cur.dx * dtf}, wya[2] = {1.f - cur.dy, cur.dy},
+                wza[2] = {1.f - cur.dz, cur.dz};
+    float3 dv = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const size_t g = sx[a] + sy[b] + sz[cc];
+                const float mul = __fmul_rn(__fmul_rn(wxa[a], wya[b]), wza[cc]);
+                dv.x = fmaf(mul, __ldg(&fx[g]), dv.x);
+                dv.y = fmaf(mul, __ldg(&fy[g]), dv.y);
+                dv.z = fmaf(mul, __ldg(&fz[g]), dv.z);
+            }
+    return dv;
+}
+
+// Blocks queued by kick_win4_kernel (window above kWin4Cap cells), one
+// particle per thread over a persistent grid that walks the queue (block,
+// 256-particle part); the gathers read the global force grids.  (A larger
+// shared window per block, one CTA per SM, was slower here: at late times
+// the bounding boxes are mostly empty cells, so filling them costs more than
+// the gathers.)
+__global__ void __launch_bounds__(256) kick_spill_kernel(ParticleSoA p, int ng, const float* __restrict__ fx,
+                                                         const float* __restrict__ fy, const float* __restrict__ fz,
+                                                         double deltaT, double fscal, float pf_a, float pf_b,
+                                                         int ndrift, int have_rec, SpillList spill, Slots sl,
+                                                         KickSched ks) {
+    constexpr int SUB = 16 * 16 * 16 / 256;
+    const int slot = blockIdx.y;
+    if (slot_idle(sl, slot)) return;
+    // flat mode (kick_win4_kernel stood down): every block, in order
+    const bool all = have_rec && spill.over && spill.over[slot] * 2 > spill.nblocks;
+    const int n = (all ? spill.nblocks : __ldg(&spill.cnt[slot])) * SUB;
+    if ((int)blockIdx.x >= n) return;
+    p = offset_soa(p, (size_t)slot * sl.s0);
+    fx += (size_t)slot * sl.s1;
+    fy += (size_t)slot * sl.s1;
+    fz += (size_t)slot * sl.s1;
+    float dtf = (float)(deltaT * fscal);
+    if (ks.sched) {
+        const float4 q = ks.sched[(size_t)slot * ks.pitch + ks.step[slot]];
+        dtf = q.x;
+        pf_a = q.y;
+        pf_b = q.z;
+        ndrift = (int)q.w;
+    }
+    const int* items = spill.items + (size_t)slot * spill.nblocks;
+    for (int w = blockIdx.x; w < n; w += gridDim.x) {
+        const int blk = all ? w / SUB : __ldg(&items[w / SUB]);
+        const size_t i = (size_t)blk * (16 * 16 * 16) + (w % SUB) * 256 + threadIdx.x;
+        const PState cur = load_p(p, i);
+        finish_p(p, i, cur, gather_global(fx, fy, fz, cur, dtf, ng), pf_a, pf_b, ndrift, ng);
+    }
+}
+
 __global__ void density_kernel(const unsigned long long* __restrict__ rho64, float* __restrict__ rho, size_t n) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -638,6 +987,36 @@ __global__ void place_kernel(const float* __restrict__ s, size_t scomp, Particle
 // ---------------------------------------------------------------------------
 static inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
+cudaError_t smem_attr_once(const void* func, int bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, int> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> g(mu);
+    int& have = done[{dev, func}];
+    if (have >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) have = bytes;
+    return e;
+}
+
+int blocks_per_sm_once(const void* func, int threads, int smem) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, int> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> g(mu);
+    auto it = done.find({dev, func});
+    if (it != done.end()) return it->second;
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, threads, smem) != cudaSuccess) per_sm = 1;
+    if (per_sm < 1) per_sm = 1;
+    done[{dev, func}] = per_sm;
+    return per_sm;
+}
+
 cudaError_t launch_load_state(const float* x, const float* v, const ParticleSoA& p, int np_side, int B, int ng,
                               cudaStream_t s) {
     const size_t n = (size_t)np_side * np_side * np_side;
@@ -653,6 +1032,11 @@ cudaError_t launch_drift(const ParticleSoA& p, size_t n, int ng, float pf, cudaS
     drift_kernel<<<nblk(n, 256), 256, 0, s>>>(p, n, ng, pf);
     return cudaGetLastError();
 }
+int window_records(int np_side, int ng) {
+    const int nb = np_side / block_side(np_side, ng);
+    return nb * nb * nb * kWinRec;
+}
+
 int deposit_cap_cells(int np_side, int ng) {
     const int B = block_side(np_side, ng);
     const int r = (B * ng + np_side - 1) / np_side + 6;  // block region + margin
@@ -662,29 +1046,55 @@ int deposit_cap_cells(int np_side, int ng) {
     return cap;
 }
 
+static int num_sms() {
+    static int cached[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return 148;
+    if (!cached[dev]) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cached[dev] = n > 0 ? n : 148;
+    }
+    return cached[dev];
+}
+
 template <int B, bool SMALL>
 static cudaError_t deposit_impl(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
-                                int cap, const Slots& sl, int nslots, cudaStream_t s) {
+                                int cap, int* blkwin, const SpillList& spill, const Slots& sl, int nslots,
+                                cudaStream_t s) {
     auto k = deposit_tiled_kernel<B, SMALL>;
     const int smem = cap * 8;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = smem_attr_once((const void*)k, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(spill.cnt, 0, sizeof(int) * nslots, s);
+    if (e == cudaSuccess && spill.over) e = cudaMemsetAsync(spill.over, 0, sizeof(int) * nslots, s);
     if (e != cudaSuccess) return e;
     const int nb = np_side / B;
-    k<<<dim3(nb * nb * nb, nslots), 256, smem, s>>>(p, np_side, ng, mass, rho, cap, sl);
+    k<<<dim3(nb * nb * nb, nslots), 256, smem, s>>>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    constexpr int NTS = B * B * B >= 1024 ? 1024 : B * B * B;
+    auto ks = deposit_spill_kernel<B, SMALL, NTS>;
+    e = smem_attr_once((const void*)ks, kBigCap * 8);
+    if (e != cudaSuccess) return e;
+    const int per_slot = num_sms() / nslots > 1 ? num_sms() / nslots : 1;  // about one CTA per SM in all
+    ks<<<dim3(per_slot, nslots), NTS, kBigCap * 8, s>>>(p, np_side, ng, mass, rho, blkwin, spill, sl);
     return cudaGetLastError();
 }
 
 cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
-                           cudaStream_t s, const Slots& sl, int nslots) {
+                           int* blkwin, const SpillList& spill, cudaStream_t s, const Slots& sl, int nslots) {
+    if (!blkwin || !spill.cnt || !spill.items) return cudaErrorInvalidValue;
     const int B = block_side(np_side, ng);
     const int cap = deposit_cap_cells(np_side, ng);
     // SMALL needs every window add (a weight, or two merged x-chain weights,
     // each < mass*2^31) below 2^32: mass <= 1
     const bool small = mass <= 1.0f;
-    if (B == 16) return small ? deposit_impl<16, true>(p, np_side, ng, mass, rho, cap, sl, nslots, s)
-                              : deposit_impl<16, false>(p, np_side, ng, mass, rho, cap, sl, nslots, s);
-    return small ? deposit_impl<8, true>(p, np_side, ng, mass, rho, cap, sl, nslots, s)
-                 : deposit_impl<8, false>(p, np_side, ng, mass, rho, cap, sl, nslots, s);
+    if (B == 16) return small ? deposit_impl<16, true>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl, nslots, s)
+                              : deposit_impl<16, false>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl, nslots, s);
+    return small ? deposit_impl<8, true>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl, nslots, s)
+                 : deposit_impl<8, false>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl, nslots, s);
 }
 template <int B, int NT>
 static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const float* fx, const float* fy,
@@ -692,7 +1102,7 @@ static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const fl
                              const Slots& sl, const KickSched& ks, int nslots, cudaStream_t s) {
     auto k = kick_tiled_kernel<B, NT>;
     const int smem = cap * 12;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = smem_attr_once((const void*)k, smem);
     if (e != cudaSuccess) return e;
     const int nb = np_side / B;
     k<<<dim3(nb * nb * nb, nslots), NT, smem, s>>>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap,
@@ -749,9 +1159,36 @@ __global__ void __launch_bounds__(256, 6) kick_flat_kernel(ParticleSoA p, size_t
 
 cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float* fx, const float* fy,
                               const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift,
-                              int variant, cudaStream_t s, const Slots& sl, const KickSched& ks, int nslots) {
+                              int variant, int* blkwin, bool have_rec, const SpillList& spill, cudaStream_t s,
+                              const Slots& sl, const KickSched& ks, int nslots) {
     const int B = block_side(np_side, ng);
     const int cap = deposit_cap_cells(np_side, ng);
+    if (variant == 2 && B == 16) {
+        if (!spill.cnt || !spill.items || !spill.next || !blkwin) return cudaErrorInvalidValue;
+        auto k = kick_win4_kernel<512>;
+        const int smem = kWin4Cap * 16;
+        cudaError_t e = smem_attr_once((const void*)k, smem);
+        if (e != cudaSuccess) return e;
+        e = cudaMemsetAsync(spill.cnt, 0, sizeof(int) * nslots, s);
+        if (e != cudaSuccess) return e;
+        const int nb = np_side / 16;
+        // persistent: about two CTAs per SM over all slots, taking blocks in
+        // order from a per-slot counter (spill.next)
+        e = cudaMemsetAsync(spill.next, 0, sizeof(int) * nslots, s);
+        if (e != cudaSuccess) return e;
+        int per_slot = 2 * num_sms() / nslots;
+        if (per_slot < 1) per_slot = 1;
+        if (per_slot > nb * nb * nb) per_slot = nb * nb * nb;
+        k<<<dim3(per_slot, nslots), 512, smem, s>>>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift,
+                                                      blkwin, have_rec ? 1 : 0, spill, sl, ks);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        // persistent grid of exactly the resident CTAs (no second round)
+        const int sp_grid = num_sms() * blocks_per_sm_once((const void*)kick_spill_kernel, 256, 0);
+        kick_spill_kernel<<<dim3(sp_grid, nslots), 256, 0, s>>>(p, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b,
+                                                                       ndrift, have_rec ? 1 : 0, spill, sl, ks);
+        return cudaGetLastError();
+    }
     if (variant == 1) {
         const size_t n = (size_t)np_side * np_side * np_side;
         kick_flat_kernel<<<dim3(nblk(n, 256), nslots), 256, 0, s>>>(p, n, ng, fx, fy, fz, (float)(deltaT * fscal),

@@ -318,6 +318,7 @@ extern "C" size_t hgpm_footprint_bytes(int ng, int np) {
     b += nspec * 8 * 4;        // spectrum + 3 force spectra
     b += ncell * 4 * 3;        // force grids
     b += (size_t)ng * 64;      // tables
+    b += (size_t)window_records(np, ng) * 4;  // per-block CIC windows
     return b;
 }
 
@@ -348,7 +349,7 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
         const char* xt = getenv("HGPM_XTMA");
         c->xtma = xt && xt[0] == '1';
         const char* kv = getenv("HGPM_KICK");
-        if (kv && (kv[0] == '0' || kv[0] == '1')) c->kick_variant = kv[0] - '0';
+        if (kv && kv[0] >= '0' && kv[0] <= '2') c->kick_variant = kv[0] - '0';
     }
     c->blk = block_side(c->np, c->ng);
     c->npart = (size_t)c->np * c->np * c->np;
@@ -384,6 +385,16 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
         if ((e = cudaMalloc(&c->pkw, c->ng * 4)) != cudaSuccess) break;
         // d_err[0]: IC table overrun; d_err[1]: a bounded TMA/mbarrier wait timed out
         if ((e = cudaMalloc(&c->d_err, 8)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&c->blkwin, (size_t)window_records(c->np, c->ng) * 4)) != cudaSuccess) break;
+        {
+            const int nblocks = window_records(c->np, c->ng) / 8;
+            int* sp = nullptr;
+            if ((e = cudaMalloc(&sp, (size_t)(4 + 2 * nblocks) * 4)) != cudaSuccess) break;
+            // counters: deposit queue, kick queue, blocks over the kick's cap,
+            // the kick's work counter
+            c->dep_spill = SpillList{sp, sp + 4, nblocks, sp + 2, sp + 3};
+            c->kick_spill = SpillList{sp + 1, sp + 4 + nblocks, nblocks, sp + 2, sp + 3};
+        }
         if ((e = cudaMemsetAsync(c->d_err, 0, 8, c->stream)) != cudaSuccess) break;
         std::vector<float2> t1 = twiddles(c->ng), t2 = twiddles(c->np);
         if ((e = cudaMemcpy(c->tw_ng, t1.data(), c->ng * 8, cudaMemcpyHostToDevice)) != cudaSuccess) break;
@@ -433,7 +444,8 @@ extern "C" void hgpm_destroy(hgpm_ctx* c) {
         if (q) cudaFree(q);
     if (!c->view) {
         void* ptrs[] = {c->part_block, c->rho64, c->spec, c->fspec, c->force, c->tw_ng, c->tw_np, c->cosq, c->sk,
-                        c->pkw, c->d_err, c->stage, c->pk_part, c->pk_pcnt, c->pk_sum, c->pk_cnt};
+                        c->pkw, c->d_err, c->stage, c->pk_part, c->pk_pcnt, c->pk_sum, c->pk_cnt, c->blkwin,
+                        c->dep_spill.cnt};
         for (void* q : ptrs)
             if (q) cudaFree(q);
     }
@@ -481,6 +493,7 @@ extern "C" int hgpm_load_state_device(hgpm_ctx* c, const float* x, const float* 
     CK(launch_load_state(x, v, c->part, c->np, c->blk, c->ng, c->stream));
     count(c, PH_DRIFT, 1);
     c->have_state = true;
+    c->win_valid = false;
     return HGPM_OK;
 }
 
@@ -538,6 +551,7 @@ extern "C" int hgpm_drift(hgpm_ctx* c, float prefactor) {
     if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
     PhaseScope ps(c, PH_DRIFT);
     CK(launch_drift(c->part, c->npart, c->ng, prefactor, c->stream));
+    c->win_valid = false;
     count(c, PH_DRIFT, 1);
     return HGPM_OK;
 }
@@ -555,8 +569,9 @@ static double mean_density(const hgpm_ctx* c) {
 
 static int deposit_impl(hgpm_ctx* c) {
     if (c->rho_dirty) CK(cudaMemsetAsync(c->rho64, 0, c->ncell * 8, c->stream));
-    CK(launch_deposit(c->part, c->np, c->ng, cic_mass(c->ng, c->np), c->rho64, c->stream));
-    count(c, PH_DEPOSIT, 1);
+    CK(launch_deposit(c->part, c->np, c->ng, cic_mass(c->ng, c->np), c->rho64, c->blkwin, c->dep_spill, c->stream));
+    c->win_valid = true;
+    count(c, PH_DEPOSIT, 2);  // windowed pass + spill pass
     c->rho_dirty = true;
     return HGPM_OK;
 }
@@ -646,8 +661,10 @@ extern "C" int hgpm_kick_drift(hgpm_ctx* c, double deltaT, double fscal, float p
     if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
     PhaseScope ps(c, PH_KICK);
     CK(launch_kick_drift(c->part, c->np, c->ng, c->force, c->force + c->ncell, c->force + 2 * c->ncell, deltaT,
-                         fscal, pf_a, pf_b, ndrift, c->kick_variant, c->stream));
-    count(c, PH_KICK, 1);
+                         fscal, pf_a, pf_b, ndrift, c->kick_variant, c->blkwin, c->win_valid, c->kick_spill,
+                         c->stream));
+    if (ndrift > 0) c->win_valid = false;
+    count(c, PH_KICK, kick_kernels(c->kick_variant, c->np, c->ng));
     return HGPM_OK;
 }
 
@@ -864,6 +881,7 @@ static int ic_common(hgpm_ctx* c, const float* noise_host, const double* table, 
         }
         if (herr) { rc = fail(c, HGPM_ERR_ARG, "ipk table too short for the grid's largest |k|"); break; }
         c->have_state = true;
+        c->win_valid = false;
     } while (0);
     return rc;
 }

@@ -195,21 +195,43 @@ __global__ void __launch_bounds__(NT, 1024 / NT) xpoisson_tma_kernel(const __gri
             tile[i] = v;
         }
         float2* gout = out + (size_t)iy * zs + col0;
-#pragma unroll 1
-        for (int d = 0; d < 3; ++d) {
-            // F_d = -i sin(k_d) t, zero at the Nyquist index of d (PoissonOp::comp)
-            for (int i = threadIdx.x; i < NG * CT; i += NT) {
-                const int ix = i / CT, iz = col0 + i % CT;
-                const int id = d == 0 ? ix : (d == 1 ? iy : iz);
-                const float sd = (id == nyq || iz >= ncols) ? 0.f : sk[id];
-                const float2 tv = tile[i];
-                work[i] = make_float2(sd * tv.y, -sd * tv.x);
-            }
-            __syncthreads();
-            fft_tile<NG, CT, CT, true, NT>(work, tw);
-            store_rows<NG, CT, NT>(work, gout + (size_t)d * out_cs, rs, ncols - col0);
-            __syncthreads();
+        // F_x = -i sin(k_x) t, zero at the x Nyquist index (PoissonOp::comp)
+        for (int i = threadIdx.x; i < NG * CT; i += NT) {
+            const int ix = i / CT, iz = col0 + i % CT;
+            const float sd = (ix == nyq || iz >= ncols) ? 0.f : sk[ix];
+            const float2 tv = tile[i];
+            work[i] = make_float2(sd * tv.y, -sd * tv.x);
         }
+        __syncthreads();
+        fft_tile<NG, CT, CT, true, NT>(work, tw);
+        store_rows<NG, CT, NT>(work, gout, rs, ncols - col0);
+        // F_y, F_z: their factors are constant along x, applied after one
+        // inverse transform of t (as xfused_kernel)
+        fft_tile<NG, CT, CT, true, NT>(tile, tw);
+        const float sy = iy == nyq ? 0.f : sk[iy];
+        const int TPR = CT / 2;
+#pragma unroll 2
+        for (int i = threadIdx.x; i < NG * TPR; i += NT) {
+            const int e = i / TPR, c = 2 * (i % TPR);
+            const float4 v = *reinterpret_cast<const float4*>(&tile[e * CT + c]);
+            const int iz = col0 + c;
+            const float sz0 = (iz == nyq) ? 0.f : sk[iz < NG ? iz : 0];
+            const float sz1 = (iz + 1 == nyq) ? 0.f : sk[iz + 1 < NG ? iz + 1 : 0];
+            float2* dy = gout + out_cs + (size_t)e * rs + c;
+            float2* dz = gout + 2 * out_cs + (size_t)e * rs + c;
+            const float4 fy = make_float4(sy * v.y, -sy * v.x, sy * v.w, -sy * v.z);
+            const float4 fz = make_float4(sz0 * v.y, -sz0 * v.x, sz1 * v.w, -sz1 * v.z);
+            if (c + 1 < ncols - col0) {
+                __stcs(reinterpret_cast<float4*>(dy), fy);
+                __stcs(reinterpret_cast<float4*>(dz), fz);
+            } else if (c < ncols - col0) {
+                dy[0] = make_float2(fy.x, fy.y);
+                dz[0] = make_float2(fz.x, fz.y);
+            }
+        }
+        // the next TMA load into this buffer follows generic-proxy writes
+        fence_async_shared();
+        __syncthreads();
     }
     if (threadIdx.x == 0) {
         if (failed) {
@@ -269,11 +291,9 @@ static cudaError_t tma_impl(bool inv, bool isx, float2* data, int ncols, int zs,
 #define HGPM_TMA_LAUNCH(I, X)                                                                       \
     {                                                                                               \
         auto k = strided_tma_kernel<NG, I, X>;                                                      \
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);          \
+        e = smem_attr_once((const void*)k, G::SMEM);                                                \
         if (e != cudaSuccess) return e;                                                             \
-        int per_sm = 1;                                                                             \
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTmaThreads, G::SMEM);            \
-        int grid = g_num_sms * (per_sm < 1 ? 1 : per_sm);                                           \
+        int grid = g_num_sms * blocks_per_sm_once((const void*)k, kTmaThreads, G::SMEM);           \
         if (grid > ntiles) grid = ntiles;                                                           \
         k<<<grid, kTmaThreads, G::SMEM, s>>>(tm, nchunks, NG, ncomp, tw, err);                      \
     }
@@ -303,11 +323,9 @@ static cudaError_t xpoisson_tma_impl(float2* in, float2* out, int ncols, int zs,
     const int nchunks = (ncols + G::CT - 1) / G::CT;
     const int ntiles = nchunks * NG;
     auto k = xpoisson_tma_kernel<NG, NT>;
-    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    e = smem_attr_once((const void*)k, SMEM);
     if (e != cudaSuccess) return e;
-    int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, SMEM);
-    int grid = g_num_sms * (per_sm < 1 ? 1 : per_sm);
+    int grid = g_num_sms * blocks_per_sm_once((const void*)k, NT, SMEM);
     if (grid > ntiles) grid = ntiles;
     k<<<grid, NT, SMEM, s>>>(tm, out, out_cs, ncols, zs, nchunks, tw, cosq, sk, coeff, err);
     return cudaGetLastError();

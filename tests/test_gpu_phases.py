@@ -122,13 +122,15 @@ def test_fused_x_pass_variants_bit_identical(ng, monkeypatch):
     assert np.array_equal(out[0], out[1])
 
 
-@pytest.mark.parametrize("ng,np_side", [(32, 32), (48, 48), (64, 32)])
-def test_kick_variants_bit_identical(ng, np_side, monkeypatch):
-    """Tiled (shared-memory force window) and flat (global gather) kicks run
-    the same FP32 arithmetic in the same order."""
-    x, v = lattice_state(np_side, ng, disp=1.0, vel=1.0, seed=17)
+@pytest.mark.parametrize("ng,np_side,disp", [(32, 32, 1.0), (48, 48, 1.0), (64, 32, 1.0), (64, 64, 0.3),
+                                             (64, 64, 4.0)])
+def test_kick_variants_bit_identical(ng, np_side, disp, monkeypatch):
+    """Tiled (shared-memory force window), flat (global gather) and float4
+    window kicks run the same FP32 arithmetic in the same order; disp 4
+    spreads blocks past the window caps (global-gather fallback)."""
+    x, v = lattice_state(np_side, ng, disp=disp, vel=1.0, seed=17)
     out = []
-    for flag in ("0", "1"):
+    for flag in ("0", "1", "2"):
         monkeypatch.setenv("HGPM_KICK", flag)
         with make(ng, np_side) as s:
             s.load_state(x, v)
@@ -136,7 +138,8 @@ def test_kick_variants_bit_identical(ng, np_side, monkeypatch):
             s.solve_gradient()
             s.kick_drift(0.0123, 1.7, 0.3, 0.25, 2)
             out.append(s.store_state())
-    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0]) and np.array_equal(out[0][1], o[1])
 
 
 def test_solve_gradient_plane_wave_analytic():
