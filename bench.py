@@ -70,14 +70,15 @@ def alg_bytes(np3, ng3):
     }
 
 
+# The kernels of each phase (one launch each per step, unless noted).
 KERNEL_NAMES = {
-    "deposit": "deposit_kernel",
-    "fft_z_fwd": "zpass_r2c_kernel<NG,true>",
-    "fft_y_fwd": "strided_kernel<NG,false>",
+    "deposit": "deposit_tiled_kernel<16,1> + deposit_spill_kernel<16,1,1024> (queued wide blocks)",
+    "fft_z_fwd": "zpass_r2c_kernel<NG,1>",
+    "fft_y_fwd": "strided_tma_kernel<NG,0,0>",
     "poisson_x": "xfused_kernel<NG,PoissonOp>",
-    "fft_y_inv": "strided_kernel<NG,true>",
+    "fft_y_inv": "strided_tma_kernel<NG,1,0>",
     "fft_z_inv": "zpass_c2r_kernel<NG>",
-    "kick_drift": "kick_drift_kernel",
+    "kick_drift": "kick_win4_kernel<512> + kick_spill_kernel (queued wide blocks)",
 }
 
 
@@ -149,6 +150,39 @@ def cpu_baseline(steps=1, warmup=0, ng=NG, np_side=NP):
     return json.loads(out.stdout.strip().splitlines()[-1])
 
 
+def reference_gpu():
+    """The reference's own serial CUDA step (oracle/_ref/refpm, compiled from
+    the HACC_GPM sources when they were present at build time) on this GPU:
+    the same 512^3 run, steps 46-55 (mid-run) and the whole 100-step run.
+    Context for the GPU-to-GPU comparison; None when the harness is absent."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "refpm")
+    if not os.path.exists(exe):
+        return None
+    import numpy as np
+
+    from hacc_gpm_b200 import ipk as ipkmod
+    from oracle import pm_oracle as O
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        txt = ipkmod.lcdm_params_text(NG, NP, RL, Z_INI, NSTEPS_RUN, prefix=os.path.join(d, "r"),
+                                      ipk=os.path.join(d, "r.ipk"))
+        h, tab = ipkmod.make_ipk(ipkmod.cosmo_from_params(O.parse_params_text(txt)), Z_INI, k_max=20.0)
+        np.concatenate([h, tab]).astype("<f8").tofile(os.path.join(d, "r.ipk"))
+        pf = os.path.join(d, "r.in")
+        with open(pf, "w") as f:
+            f.write(txt)
+        for key, (w, k) in (("mid", (MID_STEP, 10)), ("full", (0, NSTEPS_RUN))):
+            r = subprocess.run([exe, "time", pf, str(w), str(k)], capture_output=True, text=True, timeout=900)
+            line = [l for l in r.stderr.splitlines() if l.startswith("REFPM_TIME")]
+            if r.returncode != 0 or not line:
+                return {"error": "refpm %s failed (rc %d)" % (key, r.returncode)}
+            ms = float(line[-1].split("ms_per_step=")[1])
+            out[key] = {"ms_per_step": ms, "value": NP ** 3 / (ms * 1e-3), "unit": UNIT}
+    out["what"] = ("the reference's serial CUDA path (HACCGPM::serial::UpdatePositions/CIC/SolveGradient/"
+                   "UpdateVelocities, cuFFT C2C, float atomics) compiled from its sources for sm_100a, CUDA events")
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -156,6 +190,13 @@ def run_reference(args):
     steps = max(1, min(args.steps, 3))
     r = cpu_baseline(steps=steps, warmup=1 if args.warmup > 0 else 0)
     v = NP ** 3 / r["sec_per_step"]
+    gpu = None
+    try:
+        import torch
+        if torch.cuda.is_available() and not args.no_full:
+            gpu = reference_gpu()
+    except Exception as e:  # the CPU arm stands on its own
+        gpu = {"error": str(e)[:200]}
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": r["steps"],
         "warmup": 1 if args.warmup > 0 else 0, "ms_per_step": r["sec_per_step"] * 1e3, "higher_is_better": True,
@@ -166,6 +207,7 @@ def run_reference(args):
                          "sample": "%d full 512^3 step(s) of the OpenMP C++ transcription of the reference's serial "
                                    "step (float3 layout, float atomics, C2C FFTs), after 1 warm-up" % r["steps"]},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": gpu,
     }))
 
 
@@ -350,14 +392,16 @@ def main():
         n = int(ph_n.get(k, 0))
         if n == 0:
             continue
-        avg = ph_ms[k] / n
-        phases[k] = {"ms_per_launch": avg, "launches": n, "alg_bytes": b,
+        # events bracket the phase (all its kernels) once per step
+        avg = ph_ms[k] / args.steps
+        phases[k] = {"ms_per_step": avg, "kernels": n, "alg_bytes": b,
                      "alg_gbs": b / (avg * 1e-3) / 1e9 if b else 0.0}
-    dom = max(phases, key=lambda k: phases[k]["ms_per_launch"])
+    dom = max(phases, key=lambda k: phases[k]["ms_per_step"])
     d = phases[dom]
-    roofline = {"bound": "hbm", "kernel": KERNEL_NAMES[dom].replace("NG", str(NG)), "phase": dom, "achieved": d["alg_gbs"], "peak": peak,
-                "unit": "GB/s", "frac": d["alg_gbs"] / peak, "peak_kind": peak_kind, "traffic": None,
-                "alg_bytes_per_launch": d["alg_bytes"], "ms_per_launch": d["ms_per_launch"]}
+    roofline = {"bound": "hbm", "kernel": KERNEL_NAMES[dom].replace("NG", str(NG)), "phase": dom,
+                "achieved": d["alg_gbs"], "peak": peak, "unit": "GB/s", "frac": d["alg_gbs"] / peak,
+                "peak_kind": peak_kind, "traffic": None, "alg_bytes_per_launch": d["alg_bytes"],
+                "ms_per_launch": d["ms_per_step"]}
     step_ms = ms_max / args.steps
     b_step = 72 * np3 + 64 * ng3
     step_roof = {"alg_bytes_per_step": b_step, "achieved_gbs": b_step / (step_ms * 1e-3) / 1e9,

@@ -73,7 +73,7 @@ struct hgpm_ensemble {
     std::vector<EnsClass> cls;
     bool use_graph = false;
     cudaGraphExec_t exec = nullptr;
-    int kick_variant = 2;
+    int kick_variant = 1;
     int64_t launches = 0;
     std::string err;
 };
@@ -108,7 +108,7 @@ static void class_geometry(EnsClass& k) {
     // strides rounded to 64 elements so every slot starts 256-byte aligned
     auto r64 = [](size_t v) { return (v + 63) / 64 * 64; };
     k.spec_elems = r64(std::max((size_t)k.ng * k.ng * k.zs, (size_t)k.np * k.np * k.zs_np));
-    k.force_elems = r64(3 * std::max(k.ncell, k.npart));
+    k.force_elems = r64(4 * std::max(k.ncell, k.npart));  // float4 grid; ICs use 3 planes of npart
     k.part_stride = r64(k.npart);
 }
 
@@ -420,11 +420,11 @@ static int class_step(hgpm_ensemble* E, EnsClass& k, cudaStream_t s) {
                         0.5 / ((double)ng * ng * ng), s, Slots{act, k.spec_elems, 3 * k.spec_elems}, S));
     ECK(launch_strided(ng, true, k.fspec, M + 1, (size_t)k.zs, (size_t)ng * k.zs, ng, cs, 3, k.tw_ng, s,
                        Slots{act, 3 * k.spec_elems, 0}, S));
-    ECK(launch_zinv(ng, k.fspec, k.force, ng * ng, k.zs, cs, k.ncell, 3, 1.0f, k.tw_ng, s,
-                    Slots{act, 3 * k.spec_elems, k.force_elems}, S));
-    ECK(launch_kick_drift(p, k.np, ng, k.force, k.force + k.ncell, k.force + 2 * k.ncell, 0.0, 0.0, 0.f, 0.f, 0,
-                          E->kick_variant, k.blkwin, true, k.kick_spill, s,
-                          Slots{act, k.part_stride, k.force_elems, k.win_stride},
+    float4* f4 = reinterpret_cast<float4*>(k.force);
+    ECK(launch_zinv3(ng, k.fspec, f4, ng * ng, k.zs, cs, 1.0f, k.tw_ng, s,
+                     Slots{act, 3 * k.spec_elems, k.force_elems / 4}, S));
+    ECK(launch_kick_drift(p, k.np, ng, f4, 0.0, 0.0, 0.f, 0.f, 0, E->kick_variant, k.blkwin, true, k.kick_spill, s,
+                          Slots{act, k.part_stride, k.force_elems / 4, k.win_stride},
                           KickSched{k.d_sched, k.d_step, HGPM_MAX_STEPS}, S));
     ECK(launch_slots_advance(k.d_active, k.d_step, k.d_nsteps, S, s));
     E->launches += 8 + kick_kernels(E->kick_variant, k.np, ng);  // deposit 2, FFT 5, advance 1

@@ -32,6 +32,9 @@ template <int NG> struct Cfg {
     static constexpr int CS = NG >= 768 ? 8 : 16;          // strided-pass columns per CTA
     static constexpr int CX = NG >= 768 ? 4 : (NG >= 384 ? 8 : 16);  // fused x-pass columns
     static constexpr int ZSMEM = M * (L + 1) * 8;
+    // the 3-component C2R pass: L3 lines of each component per CTA
+    static constexpr int L3 = L >= 2 ? L / 2 : 1;
+    static constexpr int Z3SMEM = M * (3 * L3 + 1) * 8;
     static constexpr int SSMEM = NG * CS * 8;
     static constexpr int XSMEM = 2 * NG * CX * 8;
     // threads per CTA of the strided and fused x passes: 512 halves the
@@ -291,6 +294,79 @@ __global__ void __launch_bounds__(kThreads) zpass_c2r_kernel(const float2* __res
 }
 
 // ---------------------------------------------------------------------------
+// z pass, inverse C2R of the three force components at once, written
+// interleaved as float4 (x, y, z, 0) per cell so the particle kick gathers
+// a corner with one 16-byte load.  Component c's spectrum is in + c * in_cs;
+// blockIdx.y = slot.
+// ---------------------------------------------------------------------------
+template <int NG>
+__global__ void __launch_bounds__(kThreads) zpass_c2r3_kernel(const float2* __restrict__ in, float4* __restrict__ out,
+                                                              int nlines, int zs, size_t in_cs, float scale,
+                                                              const float2* __restrict__ tw, Slots sl) {
+    // one tile of 3*L3 columns: component c's line l is column c*L3 + l, so
+    // a single set of FFT stages transforms all three components
+    constexpr int M = NG / 2, L3 = Cfg<NG>::L3, C3 = 3 * L3, ES = C3 + 1;
+    float2* buf = reinterpret_cast<float2*>(hgpm_smem);
+    const int slot = blockIdx.y;
+    if (slot_idle(sl, slot)) return;
+    in += (size_t)slot * sl.s0;
+    out += (size_t)slot * sl.s1;
+    const int line0 = blockIdx.x * L3;
+    constexpr int H = M / 2 + 1;
+    constexpr int TOT = L3 * H;
+    constexpr int PER = (TOT + kThreads - 1) / kThreads;
+#pragma unroll 1
+    for (int c = 0; c < 3; ++c) {
+        const float2* src0 = in + (size_t)c * in_cs;
+        float2 rk[PER], rm[PER];
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+            const int i = threadIdx.x + t * kThreads;
+            const int l = i / H, k = i % H;
+            rk[t] = make_float2(0.f, 0.f);
+            rm[t] = make_float2(0.f, 0.f);
+            if (i < TOT && line0 + l < nlines) {
+                const float2* src = src0 + (size_t)(line0 + l) * zs;
+                rk[t] = __ldcs(&src[k]);
+                rm[t] = __ldcs(&src[M - k]);
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+            const int i = threadIdx.x + t * kThreads;
+            if (i >= TOT) break;
+            const int l = c * L3 + i / H, k = i % H;
+            float2 xk = rk[t], xm = rm[t];
+            if (k == 0) {
+                xk.y = 0.f;
+                xm.y = 0.f;
+            }
+            const float2 w = __ldg(&tw[k]);
+            const float2 s = make_float2(xk.x + xm.x, xk.y - xm.y);
+            const float2 d = make_float2(xk.x - xm.x, xk.y + xm.y);
+            const float2 cd = cmulc(d, w);
+            const float2 tt = make_float2(-cd.y, cd.x);
+            buf[k * ES + l] = cadd(s, tt);
+            if (k != 0 && k != M - k) {
+                const float2 zm = csub(s, tt);
+                buf[(M - k) * ES + l] = make_float2(zm.x, -zm.y);
+            }
+        }
+    }
+    __syncthreads();
+    fft_tile<M, C3, ES, true, kThreads, 2>(buf, tw);
+    for (int i = threadIdx.x; i < L3 * M; i += kThreads) {
+        const int l = i / M, m = i % M;
+        const int line = line0 + l;
+        if (line >= nlines) continue;
+        const float2 a = buf[m * ES + l], b = buf[m * ES + L3 + l], c = buf[m * ES + 2 * L3 + l];
+        float4* dst = out + (size_t)line * NG + 2 * m;
+        __stcs(dst, make_float4(a.x * scale, b.x * scale, c.x * scale, 0.f));
+        __stcs(dst + 1, make_float4(a.y * scale, b.y * scale, c.y * scale, 0.f));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // strided pass (y or x lines), in place,
 // blockIdx = (column chunk, plane, slot * ncomp + comp)
 // ---------------------------------------------------------------------------
@@ -505,6 +581,18 @@ static cudaError_t zinv_impl(const float2* in, float* out, int nlines, int zs, s
 }
 
 template <int NG>
+static cudaError_t zinv3_impl(const float2* in, float4* out, int nlines, int zs, size_t in_cs, float scale,
+                              const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
+    using G = Cfg<NG>;
+    auto k = zpass_c2r3_kernel<NG>;
+    cudaError_t e = ensure_smem(k, G::Z3SMEM);
+    if (e != cudaSuccess) return e;
+    dim3 grid(cdiv(nlines, G::L3), nslots);
+    k<<<grid, kThreads, G::Z3SMEM, s>>>(in, out, nlines, zs, in_cs, scale, tw, sl);
+    return cudaGetLastError();
+}
+
+template <int NG>
 static cudaError_t strided_impl(bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
                                 int ncomp, const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
     using G = Cfg<NG>;
@@ -583,6 +671,17 @@ cudaError_t launch_zinv(int ng, const float2* in, float* out, int nlines, int zs
     switch (ng) {
 #define X(n) \
     case n: return zinv_impl<n>(in, out, nlines, zs, in_cs, out_cs, ncomp, scale, tw, s, sl, nslots);
+        HGPM_SIZES(X)
+#undef X
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_zinv3(int ng, const float2* in, float4* out, int nlines, int zs, size_t in_cs, float scale,
+                         const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
+    switch (ng) {
+#define X(n) \
+    case n: return zinv3_impl<n>(in, out, nlines, zs, in_cs, scale, tw, s, sl, nslots);
         HGPM_SIZES(X)
 #undef X
     }

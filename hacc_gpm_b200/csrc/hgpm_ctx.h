@@ -45,10 +45,11 @@ struct hgpm_ctx {
     bool win_valid = false;  // blkwin describes the current positions
     // kernel variants (environment, read at creation): HGPM_NO_TMA=1 selects the
     // plain strided y passes, HGPM_XTMA=0|1 the plain/TMA-fed fused x pass,
-    // HGPM_KICK=0|1|2 the tiled / flat / float4-window gather (default 2)
+    // HGPM_KICK=1|2: flat gathers from the float4 force grid (default) /
+    // float4 shared windows per Lagrangian block with a flat spill pass
     bool tma = true;
     bool xtma = false;
-    int kick_variant = 2;
+    int kick_variant = 1;
     float* stage = nullptr;     // AoS float3 x, v staging (lazy)
     double* pk_part = nullptr;  // P(k) partial sums (lazy)
     unsigned long long* pk_pcnt = nullptr;

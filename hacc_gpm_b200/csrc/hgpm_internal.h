@@ -37,6 +37,9 @@ cudaError_t launch_zfwd(int ng, void* in, bool fixed, float2* out, int nlines, i
 cudaError_t launch_zinv(int ng, const float2* in, float* out, int nlines, int zs, size_t in_cs, size_t out_cs,
                         int ncomp, float scale, const float2* tw, cudaStream_t s, const Slots& sl = Slots{},
                         int nslots = 1);
+// C2R of the 3 force components into one float4 (x, y, z, 0) grid.
+cudaError_t launch_zinv3(int ng, const float2* in, float4* out, int nlines, int zs, size_t in_cs, float scale,
+                         const float2* tw, cudaStream_t s, const Slots& sl = Slots{}, int nslots = 1);
 cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
                            int ncomp, const float2* tw, cudaStream_t s, const Slots& sl = Slots{}, int nslots = 1);
 cudaError_t launch_xpoisson(int ng, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
@@ -59,27 +62,29 @@ cudaError_t launch_xpoisson_tma(int ng, float2* in, float2* out, int ncols, int 
 
 cudaError_t launch_load_state(const float* x, const float* v, const ParticleSoA& p, int np_side, int B, int ng,
                               cudaStream_t s);
-cudaError_t launch_store_state(const ParticleSoA& p, float* x, float* v, int np_side, int B, cudaStream_t s);
+cudaError_t launch_store_state(const ParticleSoA& p, float* x, float* v, int np_side, int B, int ng,
+                               cudaStream_t s);
 cudaError_t launch_drift(const ParticleSoA& p, size_t n, int ng, float pf, cudaStream_t s);
 int deposit_cap_cells(int np_side, int ng);
 // The deposit writes every block's CIC window (kWinRec ints per block); the
 // kick reads it back when have_rec (positions unchanged since the deposit),
 // else measures and writes it.
 int window_records(int np_side, int ng);  // ints per box
-// Kernels one launch_kick_drift call launches for this variant and size.
-inline int kick_kernels(int variant, int np_side, int ng) {
-    return (variant == 2 && block_side(np_side, ng) == 16) ? 2 : 1;
-}
+// Kernels one launch_kick_drift call launches: flat (variant 1) one, the
+// windowed variants two (windowed + spill).
+inline int kick_kernels(int variant, int, int) { return variant == 1 ? 1 : 2; }
 // Blocks too wide for a kernel's window are queued in `spill` (the deposit's
 // and the kick's own lists) and run one particle per thread after the
 // windowed pass, inside the same launcher.
 cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
                            int* blkwin, const SpillList& spill, cudaStream_t s, const Slots& sl = Slots{},
                            int nslots = 1);
-cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float* fx, const float* fy,
-                              const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift,
-                              int variant, int* blkwin, bool have_rec, const SpillList& spill, cudaStream_t s,
-                              const Slots& sl = Slots{}, const KickSched& ks = KickSched{}, int nslots = 1);
+// f: the float4 (F_x, F_y, F_z, 0) force grid.  variant 1 forces the flat
+// (one particle per thread, global gathers) path for the whole box.
+cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float4* f, double deltaT,
+                              double fscal, float pf_a, float pf_b, int ndrift, int variant, int* blkwin,
+                              bool have_rec, const SpillList& spill, cudaStream_t s, const Slots& sl = Slots{},
+                              const KickSched& ks = KickSched{}, int nslots = 1);
 // Batched step bookkeeping: each active slot's step counter advances and a
 // slot that has run nsteps[slot] steps goes idle.
 cudaError_t launch_slots_advance(int* active, int* step, const int* nsteps, int nslots, cudaStream_t s);

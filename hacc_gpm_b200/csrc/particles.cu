@@ -72,15 +72,24 @@ __global__ void load_state_kernel(const float* __restrict__ x, const float* __re
     p.vz[i] = v[3 * q + 2];
 }
 
-__global__ void store_state_kernel(ParticleSoA p, float* __restrict__ x, float* __restrict__ v, int np_side, int B) {
+// x = cell + offset in float; a sum that rounds up to ng is stored as 0, so
+// positions stay in [0, ng) as the reference's fmod keeps them.
+__device__ __forceinline__ float join_axis(int cell, float o, float fng) {
+    const float x = (float)cell + o;
+    return x >= fng ? x - fng : x;
+}
+
+__global__ void store_state_kernel(ParticleSoA p, float* __restrict__ x, float* __restrict__ v, int np_side, int B,
+                                   int ng) {
     const size_t n = (size_t)np_side * np_side * np_side;
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const size_t q = lattice_of_internal(i, np_side, B);
     const uint32_t c = p.cell[i];
-    x[3 * q + 0] = (float)cell_x(c) + p.ox[i];
-    x[3 * q + 1] = (float)cell_y(c) + p.oy[i];
-    x[3 * q + 2] = (float)cell_z(c) + p.oz[i];
+    const float fng = (float)ng;
+    x[3 * q + 0] = join_axis(cell_x(c), p.ox[i], fng);
+    x[3 * q + 1] = join_axis(cell_y(c), p.oy[i], fng);
+    x[3 * q + 2] = join_axis(cell_z(c), p.oz[i], fng);
     v[3 * q + 0] = p.vx[i];
     v[3 * q + 1] = p.vy[i];
     v[3 * q + 2] = p.vz[i];
@@ -443,37 +452,10 @@ __global__ void __launch_bounds__(NT, 1) deposit_spill_kernel(ParticleSoA p, int
     }
 }
 
-// ICICKernel (icic_pm.cu:72-127) fused with up to two UpdatePosKernel drifts:
-// v += sum_8 float(w*deltaT*fscal) * F[corner]; then x += v*pf_a (, v*pf_b).
-__device__ __forceinline__ void kick_one_unused(ParticleSoA& p, size_t i, int ix, int iy, int iz, float3 dv, float pf_a,
-                                         float pf_b, int ndrift, int ng) {
-    const float vx = p.vx[i] + dv.x, vy = p.vy[i] + dv.y, vz = p.vz[i] + dv.z;
-    p.vx[i] = vx;
-    p.vy[i] = vy;
-    p.vz[i] = vz;
-    if (ndrift > 0) {
-        float ox = p.ox[i], oy = p.oy[i], oz = p.oz[i];
-        drift_axis(ix, ox, vx, pf_a, ng);
-        drift_axis(iy, oy, vy, pf_a, ng);
-        drift_axis(iz, oz, vz, pf_a, ng);
-        if (ndrift > 1) {
-            drift_axis(ix, ox, vx, pf_b, ng);
-            drift_axis(iy, oy, vy, pf_b, ng);
-            drift_axis(iz, oz, vz, pf_b, ng);
-        }
-        p.cell[i] = pack_cell(ix, iy, iz);
-        p.ox[i] = ox;
-        p.oy[i] = oy;
-        p.oz[i] = oz;
-    }
-}
-
-// One CTA per Lagrangian block (as the deposit): the force grids over the
-// block's bounding box (+1 cell) are staged in shared memory with coalesced
-// loads, so each grid cell crosses L2 once per CTA instead of once per
-// touching particle; the 8-corner gathers then read shared memory.  Each
-// thread prefetches its next particle while it updates the current one.
-// Blocks wider than cap_cells gather straight from global memory.
+// ICICKernel (icic_pm.cu:72-127) fused with up to two UpdatePosKernel drifts
+// (update_positions_pm.cu:3-20): v += sum_8 float(w*deltaT*fscal) F[corner],
+// then x += v*pf_a (, then x += v*pf_b).  The force grid is float4
+// (F_x, F_y, F_z, 0) per cell, so a corner is one 16-byte load.
 struct PState {
     uint32_t c;
     float dx, dy, dz, vx, vy, vz;
@@ -507,171 +489,26 @@ __device__ __forceinline__ void finish_p(ParticleSoA& p, size_t i, const PState&
     }
 }
 
-template <int B, int NT>
-__global__ void __launch_bounds__(NT, 1024 / NT) kick_tiled_kernel(ParticleSoA p, int np_side, int ng,
-                                                                   const float* __restrict__ fx,
-                                                                   const float* __restrict__ fy,
-                                                                   const float* __restrict__ fz, double deltaT,
-                                                                   double fscal, float pf_a, float pf_b, int ndrift,
-                                                                   int cap_cells, Slots sl, KickSched ks) {
-    constexpr int B3 = B * B * B;
-    constexpr int PPT = B3 / NT;
-    extern __shared__ float fwin[];
-    __shared__ int bb[6];
-    const int slot = blockIdx.y;
-    if (slot_idle(sl, slot)) return;
-    p = offset_soa(p, (size_t)slot * sl.s0);
-    fx += (size_t)slot * sl.s1;
-    fy += (size_t)slot * sl.s1;
-    fz += (size_t)slot * sl.s1;
-    // the kick factor deltaT*fscal is folded into the x weight (FP32; the
-    // reference forms float(w*deltaT*fscal) in double, a <=1 ulp difference)
-    float dtf = (float)(deltaT * fscal);
-    if (ks.sched) {
-        const float4 q = ks.sched[(size_t)slot * ks.pitch + ks.step[slot]];
-        dtf = q.x;
-        pf_a = q.y;
-        pf_b = q.z;
-        ndrift = (int)q.w;
+// The 8 CIC weights of a particle, the kick factor deltaT*fscal folded into
+// the x weight (FP32; the reference forms float(w*deltaT*fscal) in double, a
+// <= 1 ulp difference), in the reference's ((w_x w_y) w_z) order.
+struct KickWeights {
+    float wx[2], wy[2], wz[2];
+    __device__ __forceinline__ KickWeights(const PState& c, float dtf) {
+        wx[0] = (1.f - c.dx) * dtf;
+        wx[1] = c.dx * dtf;
+        wy[0] = 1.f - c.dy;
+        wy[1] = c.dy;
+        wz[0] = 1.f - c.dz;
+        wz[1] = c.dz;
     }
-    const int tid = threadIdx.x;
-    const int nb = np_side / B;
-    const int blk = blockIdx.x;
-    const int bz = blk % nb, by = (blk / nb) % nb, bx = blk / (nb * nb);
-    const int ox0 = (int)((long long)bx * B * ng / np_side);
-    const int oy0 = (int)((long long)by * B * ng / np_side);
-    const int oz0 = (int)((long long)bz * B * ng / np_side);
-    if (tid < 3) bb[tid] = 0x7fffffff;
-    else if (tid < 6) bb[tid] = -0x7fffffff;
-    __syncthreads();
-    const size_t p0 = (size_t)blk * B3;
-    int mn[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, mx[3] = {-0x7fffffff, -0x7fffffff, -0x7fffffff};
-#pragma unroll
-    for (int k = 0; k < PPT; ++k) {
-        const uint32_t c = __ldg(&p.cell[p0 + tid + k * NT]);
-        const int rx = nearest_image(cell_x(c) - ox0, ng);
-        const int ry = nearest_image(cell_y(c) - oy0, ng);
-        const int rz = nearest_image(cell_z(c) - oz0, ng);
-        mn[0] = min(mn[0], rx); mx[0] = max(mx[0], rx);
-        mn[1] = min(mn[1], ry); mx[1] = max(mx[1], ry);
-        mn[2] = min(mn[2], rz); mx[2] = max(mx[2], rz);
-    }
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        mn[a] = __reduce_min_sync(0xffffffffu, mn[a]);
-        mx[a] = __reduce_max_sync(0xffffffffu, mx[a]);
-    }
-    if ((tid & 31) == 0) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            atomicMin(&bb[a], mn[a]);
-            atomicMax(&bb[3 + a], mx[a]);
-        }
-    }
-    __syncthreads();
-    const int lx0 = bb[0], ly0 = bb[1], lz0 = bb[2];
-    const int wx = bb[3] - lx0 + 2, wy = bb[4] - ly0 + 2, wz = bb[5] - lz0 + 2;
-    const int vol = wx * wy * wz;
-    const bool tiled = vol <= cap_cells;
-    float* wfx = fwin;
-    float* wfy = fwin + cap_cells;
-    float* wfz = fwin + 2 * cap_cells;
-    if (tiled) {
-        const WinMap map(wy, wz, ox0 + lx0, oy0 + ly0, oz0 + lz0, ng);
-        // batches of 8 cells per thread: all 24 loads of a batch are in flight
-        // before the first shared store
-        constexpr int KB = 8;
-        for (int i0 = tid; i0 < vol; i0 += KB * NT) {
-            float a[KB], b[KB], c[KB];
-#pragma unroll
-            for (int u = 0; u < KB; ++u) {
-                const int i = i0 + u * NT;
-                if (i < vol) {
-                    const size_t g = map.global(i);
-                    a[u] = __ldg(&fx[g]);
-                    b[u] = __ldg(&fy[g]);
-                    c[u] = __ldg(&fz[g]);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < KB; ++u) {
-                const int i = i0 + u * NT;
-                if (i < vol) {
-                    wfx[i] = a[u];
-                    wfy[i] = b[u];
-                    wfz[i] = c[u];
-                }
-            }
-        }
-        __syncthreads();
-    }
-    const int syz = wy * wz;
-    // particles are loaded two iterations ahead
-    PState n1 = load_p(p, p0 + tid);
-    PState n2 = PPT > 1 ? load_p(p, p0 + tid + NT) : n1;
-#pragma unroll 1
-    for (int k = 0; k < PPT; ++k) {
-        const size_t i = p0 + tid + k * NT;
-        const PState cur = n1;
-        n1 = n2;
-        if (k + 2 < PPT) n2 = load_p(p, i + 2 * NT);
-        const float wxa[2] = {(1.f - cur.dx) * dtf, cur.dx * dtf}, wya[2] = {1.f - cur.dy, cur.dy},
-                    wza[2] = {1.f - cur.dz, cur.dz};
-        float3 dv = make_float3(0.f, 0.f, 0.f);
-        if (tiled) {
-            const int w = ((nearest_image(cell_x(cur.c) - ox0, ng) - lx0) * wy +
-                           (nearest_image(cell_y(cur.c) - oy0, ng) - ly0)) * wz +
-                          (nearest_image(cell_z(cur.c) - oz0, ng) - lz0);
-#pragma unroll
-            for (int a = 0; a < 2; ++a)
-#pragma unroll
-                for (int b = 0; b < 2; ++b)
-#pragma unroll
-                    for (int cc = 0; cc < 2; ++cc) {
-                        const int j = w + a * syz + b * wz + cc;
-                        const float mul = __fmul_rn(__fmul_rn(wxa[a], wya[b]), wza[cc]);
-                        dv.x = fmaf(mul, wfx[j], dv.x);
-                        dv.y = fmaf(mul, wfy[j], dv.y);
-                        dv.z = fmaf(mul, wfz[j], dv.z);
-                    }
-        } else {
-            const int ix = cell_x(cur.c), iy = cell_y(cur.c), iz = cell_z(cur.c);
-            const int ix1 = ix + 1 == ng ? 0 : ix + 1;
-            const int iy1 = iy + 1 == ng ? 0 : iy + 1;
-            const int iz1 = iz + 1 == ng ? 0 : iz + 1;
-            const size_t sx[2] = {(size_t)ix * ng * ng, (size_t)ix1 * ng * ng};
-            const size_t sy[2] = {(size_t)iy * ng, (size_t)iy1 * ng};
-            const size_t sz[2] = {(size_t)iz, (size_t)iz1};
-#pragma unroll
-            for (int a = 0; a < 2; ++a)
-#pragma unroll
-                for (int b = 0; b < 2; ++b)
-#pragma unroll
-                    for (int cc = 0; cc < 2; ++cc) {
-                        const size_t g = sx[a] + sy[b] + sz[cc];
-                        const float mul = __fmul_rn(__fmul_rn(wxa[a], wya[b]), wza[cc]);
-                        dv.x = fmaf(mul, __ldg(&fx[g]), dv.x);
-                        dv.y = fmaf(mul, __ldg(&fy[g]), dv.y);
-                        dv.z = fmaf(mul, __ldg(&fz[g]), dv.z);
-                    }
-        }
-        finish_p(p, i, cur, dv, pf_a, pf_b, ndrift, ng);
-    }
-}
+};
 
-
-// Kick variant 2: the force window is staged as one float4 (fx, fy, fz, 0)
-// per cell, so each CIC corner is a single 16-byte shared load (8 per
-// particle instead of 24 4-byte loads), filled row by row.  The window
-// comes from the deposit's record when the positions are the ones it
-// deposited.  Windows above kWin4Cap cells gather from global memory.
-
-// Fill a float4 (fx, fy, fz, 0) window of wx*wy*wz cells whose origin is
-// (gx0, gy0, gz0) (wrapped into [0, ng)) row by row: a warp takes an (x, y)
-// row, lanes walk z, RU rows in flight per warp, the row start formed once.
+// Fill a float4 window of wx*wy*wz cells whose origin (gx0, gy0, gz0) is
+// wrapped into [0, ng), row by row: a warp takes an (x, y) row, lanes walk z,
+// RU rows in flight per warp, the row start formed once.
 template <int NT, int RU>
-__device__ __forceinline__ void fill_win4(float4* __restrict__ win4, const float* __restrict__ fx,
-                                          const float* __restrict__ fy, const float* __restrict__ fz, int wx, int wy,
+__device__ __forceinline__ void fill_win4(float4* __restrict__ win4, const float4* __restrict__ f, int wx, int wy,
                                           int wz, int gx0, int gy0, int gz0, int ng) {
     constexpr int NW = NT / 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -687,8 +524,7 @@ __device__ __forceinline__ void fill_win4(float4* __restrict__ win4, const float
                 const int r = r0 + u * NW;
                 if (r < nrows && z < wz) {
                     const int cx = (int)div_by((unsigned)r, my), cy = r - cx * wy;
-                    const size_t g = ((size_t)wrap_once(gx0 + cx, ng) * ng + wrap_once(gy0 + cy, ng)) * ng + gz;
-                    v[u] = make_float4(__ldg(&fx[g]), __ldg(&fy[g]), __ldg(&fz[g]), 0.f);
+                    v[u] = __ldg(&f[((size_t)wrap_once(gx0 + cx, ng) * ng + wrap_once(gy0 + cy, ng)) * ng + gz]);
                 }
             }
 #pragma unroll
@@ -700,21 +536,18 @@ __device__ __forceinline__ void fill_win4(float4* __restrict__ win4, const float
     }
 }
 
-// CIC gather of one particle from a float4 window (j0: its base cell).
 __device__ __forceinline__ float3 gather_win4(const float4* __restrict__ win4, int j0, int syz, int wz,
-                                              const PState& cur, float dtf) {
-    const float wxa[2] = {(1.f - cur.dx) * dtf, cur.dx * dtf}, wya[2] = {1.f - cur.dy, cur.dy},
-                wza[2] = {1.f - cur.dz, cur.dz};
+                                              const KickWeights& w) {
     float3 dv = make_float3(0.f, 0.f, 0.f);
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
-            const float wab = __fmul_rn(wxa[a], wya[b]);
+            const float wab = __fmul_rn(w.wx[a], w.wy[b]);
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
                 const float4 f = win4[j0 + a * syz + b * wz + cc];
-                const float mul = __fmul_rn(wab, wza[cc]);
+                const float mul = __fmul_rn(wab, w.wz[cc]);
                 dv.x = fmaf(mul, f.x, dv.x);
                 dv.y = fmaf(mul, f.y, dv.y);
                 dv.z = fmaf(mul, f.z, dv.z);
@@ -723,27 +556,45 @@ __device__ __forceinline__ float3 gather_win4(const float4* __restrict__ win4, i
     return dv;
 }
 
-template <int NT>
-__global__ void __launch_bounds__(NT, 1024 / NT) kick_win4_kernel(ParticleSoA p, int np_side, int ng,
-                                                                  const float* __restrict__ fx,
-                                                                  const float* __restrict__ fy,
-                                                                  const float* __restrict__ fz, double deltaT,
-                                                                  double fscal, float pf_a, float pf_b, int ndrift,
-                                                                  int* __restrict__ blkwin, int have_rec,
-                                                                  SpillList spill, Slots sl, KickSched ks) {
-    constexpr int B = 16, B3 = B * B * B, PPT = B3 / NT;
-    // most blocks too wide for the window (counted by the deposit of these
-    // positions): kick_spill_kernel takes every particle instead
-    if (have_rec && spill.over && spill.over[blockIdx.y] * 2 > spill.nblocks) return;
-    extern __shared__ float4 win4[];
-    __shared__ int bb[6];
-    const int slot = blockIdx.y;
-    if (slot_idle(sl, slot)) return;
-    p = offset_soa(p, (size_t)slot * sl.s0);
-    fx += (size_t)slot * sl.s1;
-    fy += (size_t)slot * sl.s1;
-    fz += (size_t)slot * sl.s1;
-    float dtf = (float)(deltaT * fscal);
+__device__ __forceinline__ float3 gather_global(const float4* __restrict__ f, const PState& c, const KickWeights& w,
+                                                int ng) {
+    const int ix = cell_x(c.c), iy = cell_y(c.c), iz = cell_z(c.c);
+    const int ix1 = ix + 1 == ng ? 0 : ix + 1;
+    const int iy1 = iy + 1 == ng ? 0 : iy + 1;
+    const int iz1 = iz + 1 == ng ? 0 : iz + 1;
+    const size_t sx[2] = {(size_t)ix * ng * ng, (size_t)ix1 * ng * ng};
+    const size_t sy[2] = {(size_t)iy * ng, (size_t)iy1 * ng};
+    const size_t sz[2] = {(size_t)iz, (size_t)iz1};
+    float4 g[8];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) g[(a * 2 + b) * 2 + cc] = __ldg(&f[sx[a] + sy[b] + sz[cc]]);
+    float3 dv = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const float wab = __fmul_rn(w.wx[a], w.wy[b]);
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const float4 v = g[(a * 2 + b) * 2 + cc];
+                const float mul = __fmul_rn(wab, w.wz[cc]);
+                dv.x = fmaf(mul, v.x, dv.x);
+                dv.y = fmaf(mul, v.y, dv.y);
+                dv.z = fmaf(mul, v.z, dv.z);
+            }
+        }
+    return dv;
+}
+
+// Per-slot kick scalars: the launch's own, or the slot's row of a batched
+// step's schedule.
+__device__ __forceinline__ void kick_scalars(const KickSched& ks, int slot, double deltaT, double fscal, float& dtf,
+                                             float& pf_a, float& pf_b, int& ndrift) {
+    dtf = (float)(deltaT * fscal);
     if (ks.sched) {
         const float4 q = ks.sched[(size_t)slot * ks.pitch + ks.step[slot]];
         dtf = q.x;
@@ -751,9 +602,39 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_win4_kernel(ParticleSoA p,
         pf_b = q.z;
         ndrift = (int)q.w;
     }
+}
+
+// The whole box goes through kick_spill_kernel: forced (variant 1), or most
+// blocks' windows exceed kWin4Cap (counted by the deposit of these positions).
+__device__ __forceinline__ bool kick_flat_mode(int force_flat, int have_rec, const SpillList& spill, int slot) {
+    return force_flat || (have_rec && spill.over && spill.over[slot] * 2 > spill.nblocks);
+}
+
+// Windowed kick: persistent CTAs take Lagrangian blocks from a per-slot
+// counter; the block's force window (from the deposit's record when the
+// positions are the ones it deposited, else measured here and recorded) is
+// staged as float4, so each corner is one 16-byte shared load; the kick and
+// both drifts stay in registers.  Blocks whose window exceeds kWin4Cap cells
+// are queued for kick_spill_kernel.
+template <int B, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) kick_win4_kernel(ParticleSoA p, int np_side, int ng,
+                                                                  const float4* __restrict__ f, double deltaT,
+                                                                  double fscal, float pf_a, float pf_b, int ndrift,
+                                                                  int* __restrict__ blkwin, int have_rec,
+                                                                  int force_flat, SpillList spill, Slots sl,
+                                                                  KickSched ks) {
+    constexpr int B3 = B * B * B, PPT = B3 / NT;
+    extern __shared__ float4 win4[];
+    __shared__ int bb[6];
+    __shared__ int next_blk;
+    const int slot = blockIdx.y;
+    if (slot_idle(sl, slot) || kick_flat_mode(force_flat, have_rec, spill, slot)) return;
+    p = offset_soa(p, (size_t)slot * sl.s0);
+    f += (size_t)slot * sl.s1;
+    float dtf;
+    kick_scalars(ks, slot, deltaT, fscal, dtf, pf_a, pf_b, ndrift);
     const int tid = threadIdx.x;
     const int nb = np_side / B;
-    __shared__ int next_blk;
     for (;;) {
         if (tid == 0) next_blk = atomicAdd(&spill.next[slot], 1);
         __syncthreads();
@@ -768,7 +649,6 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_win4_kernel(ParticleSoA p,
         int* rec = blkwin + (size_t)slot * sl.s2 + (size_t)blk * kWinRec;
         int l0[3], w[3];
         if (have_rec) {
-            // the deposit of these same positions already measured the window
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
                 l0[a] = rec[a];
@@ -779,15 +659,13 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_win4_kernel(ParticleSoA p,
             if (tid < 6) rec[tid] = tid < 3 ? l0[tid] : w[tid - 3];
         }
         const int wy = w[1], wz = w[2];
-        const int vol = w[0] * wy * wz;
-        if (vol > kWin4Cap) {
-            // too wide for the window: queued for kick_spill_kernel
+        if (w[0] * wy * wz > kWin4Cap) {
             if (tid == 0) spill.items[(size_t)slot * spill.nblocks + atomicAdd(&spill.cnt[slot], 1)] = blk;
             continue;
         }
         const int gx0 = wrap_once(ox0 + l0[0], ng), gy0 = wrap_once(oy0 + l0[1], ng);
         const int gz0 = wrap_once(oz0 + l0[2], ng);
-        fill_win4<NT, 4>(win4, fx, fy, fz, w[0], wy, wz, gx0, gy0, gz0, ng);
+        fill_win4<NT, 4>(win4, f, w[0], wy, wz, gx0, gy0, gz0, ng);
         __syncthreads();
         const int syz = wy * wz;
         PState n1 = load_p(p, p0 + tid);
@@ -800,77 +678,39 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_win4_kernel(ParticleSoA p,
             if (k + 2 < PPT) n2 = load_p(p, i + 2 * NT);
             const int j0 = (win_rel(cell_x(cur.c), gx0, ng) * wy + win_rel(cell_y(cur.c), gy0, ng)) * wz +
                            win_rel(cell_z(cur.c), gz0, ng);
-            finish_p(p, i, cur, gather_win4(win4, j0, syz, wz, cur, dtf), pf_a, pf_b, ndrift, ng);
+            finish_p(p, i, cur, gather_win4(win4, j0, syz, wz, KickWeights(cur, dtf)), pf_a, pf_b, ndrift, ng);
         }
         __syncthreads();  // the window is refilled for the next block
     }
 }
 
-// CIC gather of one particle straight from the global force grids (the
-// flat and spill kicks), in the windowed kernels' FP32 order.
-__device__ __forceinline__ float3 gather_global(const float* __restrict__ fx, const float* __restrict__ fy,
-                                                const float* __restrict__ fz, const PState& cur, float dtf, int ng) {
-    const int ix = cell_x(cur.c), iy = cell_y(cur.c), iz = cell_z(cur.c);
-    const int ix1 = ix + 1 == ng ? 0 : ix + 1;
-    const int iy1 = iy + 1 == ng ? 0 : iy + 1;
-    const int iz1 = iz + 1 == ng ? 0 : iz + 1;
-    const size_t sx[2] = {(size_t)ix * ng * ng, (size_t)ix1 * ng * ng};
-    const size_t sy[2] = {(size_t)iy * ng, (size_t)iy1 * ng};
-    const size_t sz[2] = {(size_t)iz, (size_t)iz1};
-    const float wxa[2] = {(1.f - cur.dx) * dtf, cur.dx * dtf}, wya[2] = {1.f - cur.dy, cur.dy},
-                wza[2] = {1.f - cur.dz, cur.dz};
-    float3 dv = make_float3(0.f, 0.f, 0.f);
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b)
-#pragma unroll
-            for (int cc = 0; cc < 2; ++cc) {
-                const size_t g = sx[a] + sy[b] + sz[cc];
-                const float mul = __fmul_rn(__fmul_rn(wxa[a], wya[b]), wza[cc]);
-                dv.x = fmaf(mul, __ldg(&fx[g]), dv.x);
-                dv.y = fmaf(mul, __ldg(&fy[g]), dv.y);
-                dv.z = fmaf(mul, __ldg(&fz[g]), dv.z);
-            }
-    return dv;
-}
-
-// Blocks queued by kick_win4_kernel (window above kWin4Cap cells), one
-// particle per thread over a persistent grid that walks the queue (block,
-// 256-particle part); the gathers read the global force grids.  (A larger
-// shared window per block, one CTA per SM, was slower here: at late times
-// the bounding boxes are mostly empty cells, so filling them costs more than
-// the gathers.)
-__global__ void __launch_bounds__(256) kick_spill_kernel(ParticleSoA p, int ng, const float* __restrict__ fx,
-                                                         const float* __restrict__ fy, const float* __restrict__ fz,
+// Queued blocks (or, in flat mode, every block), one particle per thread over
+// a persistent grid that walks (block, 256-particle part) work items; the
+// corners are gathered from the global float4 force grid.  (A larger shared
+// window per block, one CTA per SM, was slower here: late in a run the
+// bounding boxes are mostly empty cells, so filling them costs more than the
+// gathers.)
+template <int B>
+__global__ void __launch_bounds__(256) kick_spill_kernel(ParticleSoA p, int ng, const float4* __restrict__ f,
                                                          double deltaT, double fscal, float pf_a, float pf_b,
-                                                         int ndrift, int have_rec, SpillList spill, Slots sl,
-                                                         KickSched ks) {
-    constexpr int SUB = 16 * 16 * 16 / 256;
+                                                         int ndrift, int have_rec, int force_flat, SpillList spill,
+                                                         Slots sl, KickSched ks) {
+    constexpr int B3 = B * B * B, SUB = B3 / 256;
     const int slot = blockIdx.y;
     if (slot_idle(sl, slot)) return;
-    // flat mode (kick_win4_kernel stood down): every block, in order
-    const bool all = have_rec && spill.over && spill.over[slot] * 2 > spill.nblocks;
+    const bool all = kick_flat_mode(force_flat, have_rec, spill, slot);
     const int n = (all ? spill.nblocks : __ldg(&spill.cnt[slot])) * SUB;
     if ((int)blockIdx.x >= n) return;
     p = offset_soa(p, (size_t)slot * sl.s0);
-    fx += (size_t)slot * sl.s1;
-    fy += (size_t)slot * sl.s1;
-    fz += (size_t)slot * sl.s1;
-    float dtf = (float)(deltaT * fscal);
-    if (ks.sched) {
-        const float4 q = ks.sched[(size_t)slot * ks.pitch + ks.step[slot]];
-        dtf = q.x;
-        pf_a = q.y;
-        pf_b = q.z;
-        ndrift = (int)q.w;
-    }
+    f += (size_t)slot * sl.s1;
+    float dtf;
+    kick_scalars(ks, slot, deltaT, fscal, dtf, pf_a, pf_b, ndrift);
     const int* items = spill.items + (size_t)slot * spill.nblocks;
     for (int w = blockIdx.x; w < n; w += gridDim.x) {
         const int blk = all ? w / SUB : __ldg(&items[w / SUB]);
-        const size_t i = (size_t)blk * (16 * 16 * 16) + (w % SUB) * 256 + threadIdx.x;
+        const size_t i = (size_t)blk * B3 + (w % SUB) * 256 + threadIdx.x;
         const PState cur = load_p(p, i);
-        finish_p(p, i, cur, gather_global(fx, fy, fz, cur, dtf, ng), pf_a, pf_b, ndrift, ng);
+        finish_p(p, i, cur, gather_global(f, cur, KickWeights(cur, dtf), ng), pf_a, pf_b, ndrift, ng);
     }
 }
 
@@ -1023,9 +863,10 @@ cudaError_t launch_load_state(const float* x, const float* v, const ParticleSoA&
     load_state_kernel<<<nblk(n, 256), 256, 0, s>>>(x, v, p, np_side, B, ng);
     return cudaGetLastError();
 }
-cudaError_t launch_store_state(const ParticleSoA& p, float* x, float* v, int np_side, int B, cudaStream_t s) {
+cudaError_t launch_store_state(const ParticleSoA& p, float* x, float* v, int np_side, int B, int ng,
+                               cudaStream_t s) {
     const size_t n = (size_t)np_side * np_side * np_side;
-    store_state_kernel<<<nblk(n, 256), 256, 0, s>>>(p, x, v, np_side, B);
+    store_state_kernel<<<nblk(n, 256), 256, 0, s>>>(p, x, v, np_side, B, ng);
     return cudaGetLastError();
 }
 cudaError_t launch_drift(const ParticleSoA& p, size_t n, int ng, float pf, cudaStream_t s) {
@@ -1096,108 +937,52 @@ cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass
     return small ? deposit_impl<8, true>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl, nslots, s)
                  : deposit_impl<8, false>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl, nslots, s);
 }
-template <int B, int NT>
-static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const float* fx, const float* fy,
-                             const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift, int cap,
-                             const Slots& sl, const KickSched& ks, int nslots, cudaStream_t s) {
-    auto k = kick_tiled_kernel<B, NT>;
-    const int smem = cap * 12;
+template <int B>
+static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const float4* f, double deltaT, double fscal,
+                             float pf_a, float pf_b, int ndrift, bool force_flat, int* blkwin, bool have_rec,
+                             const SpillList& spill, const Slots& sl, const KickSched& ks, int nslots,
+                             cudaStream_t s) {
+    constexpr int NT = 512;
+    auto ksp = kick_spill_kernel<B>;
+    // persistent grid of exactly the resident CTAs (no second round)
+    const int sp_grid = num_sms() * blocks_per_sm_once((const void*)ksp, 256, 0);
+    if (force_flat) {
+        ksp<<<dim3(sp_grid, nslots), 256, 0, s>>>(p, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, 0, 1, spill, sl, ks);
+        return cudaGetLastError();
+    }
+    auto k = kick_win4_kernel<B, NT>;
+    const int smem = kWin4Cap * 16;
     cudaError_t e = smem_attr_once((const void*)k, smem);
     if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(spill.cnt, 0, sizeof(int) * nslots, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(spill.next, 0, sizeof(int) * nslots, s);
+    if (e != cudaSuccess) return e;
     const int nb = np_side / B;
-    k<<<dim3(nb * nb * nb, nslots), NT, smem, s>>>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap,
-                                                     sl, ks);
+    // persistent: about two CTAs per SM over all slots, blocks taken in order
+    // from a per-slot counter
+    int per_slot = 2 * num_sms() / nslots;
+    if (per_slot < 1) per_slot = 1;
+    if (per_slot > nb * nb * nb) per_slot = nb * nb * nb;
+    k<<<dim3(per_slot, nslots), NT, smem, s>>>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, blkwin,
+                                                 have_rec ? 1 : 0, force_flat ? 1 : 0, spill, sl, ks);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    ksp<<<dim3(sp_grid, nslots), 256, 0, s>>>(p, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, have_rec ? 1 : 0,
+                                               force_flat ? 1 : 0, spill, sl, ks);
     return cudaGetLastError();
 }
 
-// Flat variant: one particle per thread, the 24 corner values gathered
-// straight from the (L2-resident) force grids; many warps per SM hide the
-// gather latency.
-__global__ void __launch_bounds__(256, 6) kick_flat_kernel(ParticleSoA p, size_t n, int ng,
-                                                           const float* __restrict__ fx, const float* __restrict__ fy,
-                                                           const float* __restrict__ fz, float dtf, float pf_a,
-                                                           float pf_b, int ndrift, Slots sl, KickSched ks) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int slot = blockIdx.y;
-    if (i >= n || slot_idle(sl, slot)) return;
-    p = offset_soa(p, (size_t)slot * sl.s0);
-    fx += (size_t)slot * sl.s1;
-    fy += (size_t)slot * sl.s1;
-    fz += (size_t)slot * sl.s1;
-    if (ks.sched) {
-        const float4 q = ks.sched[(size_t)slot * ks.pitch + ks.step[slot]];
-        dtf = q.x;
-        pf_a = q.y;
-        pf_b = q.z;
-        ndrift = (int)q.w;
-    }
-    const PState cur = load_p(p, i);
-    const int ix = cell_x(cur.c), iy = cell_y(cur.c), iz = cell_z(cur.c);
-    const int ix1 = ix + 1 == ng ? 0 : ix + 1;
-    const int iy1 = iy + 1 == ng ? 0 : iy + 1;
-    const int iz1 = iz + 1 == ng ? 0 : iz + 1;
-    const uint32_t sx[2] = {(uint32_t)ix * ng * ng, (uint32_t)ix1 * ng * ng};
-    const uint32_t sy[2] = {(uint32_t)iy * ng, (uint32_t)iy1 * ng};
-    const uint32_t sz[2] = {(uint32_t)iz, (uint32_t)iz1};
-    const float wxa[2] = {(1.f - cur.dx) * dtf, cur.dx * dtf}, wya[2] = {1.f - cur.dy, cur.dy},
-                wza[2] = {1.f - cur.dz, cur.dz};
-    float3 dv = make_float3(0.f, 0.f, 0.f);
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b)
-#pragma unroll
-            for (int cc = 0; cc < 2; ++cc) {
-                const uint32_t g = sx[a] + sy[b] + sz[cc];
-                const float mul = __fmul_rn(__fmul_rn(wxa[a], wya[b]), wza[cc]);
-                dv.x = fmaf(mul, __ldg(&fx[g]), dv.x);
-                dv.y = fmaf(mul, __ldg(&fy[g]), dv.y);
-                dv.z = fmaf(mul, __ldg(&fz[g]), dv.z);
-            }
-    finish_p(p, i, cur, dv, pf_a, pf_b, ndrift, ng);
-}
-
-cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float* fx, const float* fy,
-                              const float* fz, double deltaT, double fscal, float pf_a, float pf_b, int ndrift,
-                              int variant, int* blkwin, bool have_rec, const SpillList& spill, cudaStream_t s,
-                              const Slots& sl, const KickSched& ks, int nslots) {
-    const int B = block_side(np_side, ng);
-    const int cap = deposit_cap_cells(np_side, ng);
-    if (variant == 2 && B == 16) {
-        if (!spill.cnt || !spill.items || !spill.next || !blkwin) return cudaErrorInvalidValue;
-        auto k = kick_win4_kernel<512>;
-        const int smem = kWin4Cap * 16;
-        cudaError_t e = smem_attr_once((const void*)k, smem);
-        if (e != cudaSuccess) return e;
-        e = cudaMemsetAsync(spill.cnt, 0, sizeof(int) * nslots, s);
-        if (e != cudaSuccess) return e;
-        const int nb = np_side / 16;
-        // persistent: about two CTAs per SM over all slots, taking blocks in
-        // order from a per-slot counter (spill.next)
-        e = cudaMemsetAsync(spill.next, 0, sizeof(int) * nslots, s);
-        if (e != cudaSuccess) return e;
-        int per_slot = 2 * num_sms() / nslots;
-        if (per_slot < 1) per_slot = 1;
-        if (per_slot > nb * nb * nb) per_slot = nb * nb * nb;
-        k<<<dim3(per_slot, nslots), 512, smem, s>>>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift,
-                                                      blkwin, have_rec ? 1 : 0, spill, sl, ks);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-        // persistent grid of exactly the resident CTAs (no second round)
-        const int sp_grid = num_sms() * blocks_per_sm_once((const void*)kick_spill_kernel, 256, 0);
-        kick_spill_kernel<<<dim3(sp_grid, nslots), 256, 0, s>>>(p, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b,
-                                                                       ndrift, have_rec ? 1 : 0, spill, sl, ks);
-        return cudaGetLastError();
-    }
-    if (variant == 1) {
-        const size_t n = (size_t)np_side * np_side * np_side;
-        kick_flat_kernel<<<dim3(nblk(n, 256), nslots), 256, 0, s>>>(p, n, ng, fx, fy, fz, (float)(deltaT * fscal),
-                                                                    pf_a, pf_b, ndrift, sl, ks);
-        return cudaGetLastError();
-    }
-    if (B == 16)
-        return kick_impl<16, 512>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap, sl, ks, nslots, s);
-    return kick_impl<8, 256>(p, np_side, ng, fx, fy, fz, deltaT, fscal, pf_a, pf_b, ndrift, cap, sl, ks, nslots, s);
+cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float4* f, double deltaT,
+                              double fscal, float pf_a, float pf_b, int ndrift, int variant, int* blkwin,
+                              bool have_rec, const SpillList& spill, cudaStream_t s, const Slots& sl,
+                              const KickSched& ks, int nslots) {
+    if (!spill.cnt || !spill.items || !spill.next || !blkwin) return cudaErrorInvalidValue;
+    const bool flat = variant == 1;
+    if (block_side(np_side, ng) == 16)
+        return kick_impl<16>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, flat, blkwin, have_rec, spill, sl,
+                             ks, nslots, s);
+    return kick_impl<8>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, flat, blkwin, have_rec, spill, sl, ks,
+                        nslots, s);
 }
 __global__ void slots_advance_kernel(int* __restrict__ active, int* __restrict__ step,
                                      const int* __restrict__ nsteps, int nslots) {
@@ -1212,6 +997,7 @@ cudaError_t launch_slots_advance(int* active, int* step, const int* nsteps, int 
     slots_advance_kernel<<<nblk(nslots, 128), 128, 0, s>>>(active, step, nsteps, nslots);
     return cudaGetLastError();
 }
+
 cudaError_t launch_density(const unsigned long long* rho64, float* rho, size_t n, cudaStream_t s) {
     density_kernel<<<nblk(n, 256), 256, 0, s>>>(rho64, rho, n);
     return cudaGetLastError();

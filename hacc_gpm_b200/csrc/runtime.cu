@@ -316,7 +316,7 @@ extern "C" size_t hgpm_footprint_bytes(int ng, int np) {
     b += npart * 7 * 4;        // particle SoA
     b += ncell * 8;            // int64 density
     b += nspec * 8 * 4;        // spectrum + 3 force spectra
-    b += ncell * 4 * 3;        // force grids
+    b += ncell * 4 * 4;        // force grid (float4 per cell)
     b += (size_t)ng * 64;      // tables
     b += (size_t)window_records(np, ng) * 4;  // per-block CIC windows
     return b;
@@ -358,7 +358,8 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
     c->nspec = (size_t)c->ng * c->ng * c->zs;
     size_t nspec_np = (size_t)c->np * c->np * c->zs_np;
     size_t spec_elems = std::max(c->nspec, nspec_np);
-    size_t force_elems = 3 * std::max(c->ncell, c->npart);
+    // float4 force grid (4 floats per cell); ICs use it as 3 planes of npart
+    size_t force_elems = 4 * std::max(c->ncell, c->npart);
     int rc = HGPM_OK;
     do {
         // particles: one block, 7 arrays of npart 4-byte words (256-B aligned)
@@ -500,7 +501,7 @@ extern "C" int hgpm_load_state_device(hgpm_ctx* c, const float* x, const float* 
 extern "C" int hgpm_store_state_device(hgpm_ctx* c, float* x, float* v) {
     if (!c || !x || !v) return HGPM_ERR_ARG;
     if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
-    CK(launch_store_state(c->part, x, v, c->np, c->blk, c->stream));
+    CK(launch_store_state(c->part, x, v, c->np, c->blk, c->ng, c->stream));
     count(c, PH_DRIFT, 1);
     return HGPM_OK;
 }
@@ -643,7 +644,8 @@ extern "C" int hgpm_solve_gradient(hgpm_ctx* c) {
     }
     {
         PhaseScope ps(c, PH_ZINV);
-        CK(launch_zinv(ng, c->fspec, c->force, ng * ng, c->zs, cs, c->ncell, 3, 1.0f, c->tw_ng, c->stream));
+        CK(launch_zinv3(ng, c->fspec, reinterpret_cast<float4*>(c->force), ng * ng, c->zs, cs, 1.0f, c->tw_ng,
+                        c->stream));
         count(c, PH_ZINV, 1);
     }
     return HGPM_OK;
@@ -651,8 +653,16 @@ extern "C" int hgpm_solve_gradient(hgpm_ctx* c) {
 
 extern "C" int hgpm_get_force(hgpm_ctx* c, float* f) {
     if (!c || !f) return HGPM_ERR_ARG;
-    CK(cudaMemcpyAsync(f, c->force, c->ncell * 3 * 4, cudaMemcpyDeviceToHost, c->stream));
+    // the device grid is float4 (F_x, F_y, F_z, 0) per cell; the ABI returns
+    // three planes
+    std::vector<float4> g(c->ncell);
+    CK(cudaMemcpyAsync(g.data(), c->force, c->ncell * sizeof(float4), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < c->ncell; ++i) {
+        f[i] = g[i].x;
+        f[c->ncell + i] = g[i].y;
+        f[2 * c->ncell + i] = g[i].z;
+    }
     return HGPM_OK;
 }
 
@@ -660,9 +670,8 @@ extern "C" int hgpm_kick_drift(hgpm_ctx* c, double deltaT, double fscal, float p
     if (!c || ndrift < 0 || ndrift > 2) return HGPM_ERR_ARG;
     if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
     PhaseScope ps(c, PH_KICK);
-    CK(launch_kick_drift(c->part, c->np, c->ng, c->force, c->force + c->ncell, c->force + 2 * c->ncell, deltaT,
-                         fscal, pf_a, pf_b, ndrift, c->kick_variant, c->blkwin, c->win_valid, c->kick_spill,
-                         c->stream));
+    CK(launch_kick_drift(c->part, c->np, c->ng, reinterpret_cast<const float4*>(c->force), deltaT, fscal, pf_a, pf_b,
+                         ndrift, c->kick_variant, c->blkwin, c->win_valid, c->kick_spill, c->stream));
     if (ndrift > 0) c->win_valid = false;
     count(c, PH_KICK, kick_kernels(c->kick_variant, c->np, c->ng));
     return HGPM_OK;
