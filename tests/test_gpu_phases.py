@@ -122,6 +122,21 @@ def test_fused_x_pass_variants_bit_identical(ng, monkeypatch):
     assert np.array_equal(out[0], out[1])
 
 
+@pytest.mark.parametrize("ng,disp", [(32, 0.3), (64, 0.3), (64, 2.0), (64, 6.0)])
+def test_deposit_configurations_bit_identical(ng, disp, monkeypatch):
+    """The 256-thread / 72 KB and 512-thread / 110 KB windowed deposits (and
+    their spill passes, reached with disp 2 and 6) give the same int64 grid."""
+    x, v = lattice_state(ng, ng, disp=disp, vel=1.0, seed=23)
+    out = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("HGPM_DEPOSIT", flag)
+        with make(ng, ng) as s:
+            s.load_state(x, v)
+            s.cic()
+            out.append(s.get_density())
+    assert np.array_equal(out[0], out[1])
+
+
 @pytest.mark.parametrize("ng,np_side,disp", [(32, 32, 1.0), (48, 48, 1.0), (64, 32, 1.0), (64, 64, 0.3),
                                              (64, 64, 4.0)])
 def test_kick_variants_bit_identical(ng, np_side, disp, monkeypatch):
