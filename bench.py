@@ -72,13 +72,13 @@ def alg_bytes(np3, ng3):
 
 # The kernels of each phase (one launch each per step, unless noted).
 KERNEL_NAMES = {
-    "deposit": "deposit_tiled_kernel<16,1> + deposit_spill_kernel<16,1,1024> (queued wide blocks)",
+    "deposit": "deposit_tiled_kernel<16,1,512,2> + deposit_spill_kernel<16,1,1024> (queued wide blocks)",
     "fft_z_fwd": "zpass_r2c_kernel<NG,1>",
     "fft_y_fwd": "strided_tma_kernel<NG,0,0>",
     "poisson_x": "xfused_kernel<NG,PoissonOp>",
     "fft_y_inv": "strided_tma_kernel<NG,1,0>",
-    "fft_z_inv": "zpass_c2r_kernel<NG>",
-    "kick_drift": "kick_win4_kernel<512> + kick_spill_kernel (queued wide blocks)",
+    "fft_z_inv": "zpass_c2r3_kernel<NG>",
+    "kick_drift": "kick_spill_kernel<16> (flat: one particle per thread, float4 force gathers)",
 }
 
 

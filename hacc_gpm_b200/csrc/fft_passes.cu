@@ -147,7 +147,7 @@ __device__ __forceinline__ void store_tile_comp(const float2* __restrict__ tile,
 // accumulator is zeroed for the next deposit.  Otherwise input is float.
 // ---------------------------------------------------------------------------
 template <int NG, bool FIX>
-__global__ void __launch_bounds__(kThreads) zpass_r2c_kernel(void* __restrict__ in_, float2* __restrict__ out,
+__global__ void __launch_bounds__(kThreads, 4) zpass_r2c_kernel(void* __restrict__ in_, float2* __restrict__ out,
                                                              int nlines, int zs, double mean,
                                                              const float2* __restrict__ tw, Slots sl) {
     constexpr int M = NG / 2, L = Cfg<NG>::L, ES = L + 1;
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(kThreads) zpass_c2r_kernel(const float2* __res
 // blockIdx.y = slot.
 // ---------------------------------------------------------------------------
 template <int NG>
-__global__ void __launch_bounds__(kThreads) zpass_c2r3_kernel(const float2* __restrict__ in, float4* __restrict__ out,
+__global__ void __launch_bounds__(kThreads, 4) zpass_c2r3_kernel(const float2* __restrict__ in, float4* __restrict__ out,
                                                               int nlines, int zs, size_t in_cs, float scale,
                                                               const float2* __restrict__ tw, Slots sl) {
     // one tile of 3*L3 columns: component c's line l is column c*L3 + l, so

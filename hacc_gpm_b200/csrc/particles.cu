@@ -367,7 +367,7 @@ __device__ __forceinline__ void deposit_global(unsigned long long* __restrict__ 
             for (int cc = 0; cc < 2; ++cc) atomicAdd(&rho[sx[a] + sy[b] + sz[cc]], q[(a * 2 + b) * 2 + cc]);
 }
 
-// Blocks queued by deposit_tiled_kernel (window wider than its 72 KB): a
+// Blocks queued by deposit_tiled_kernel (window wider than its own): a
 // persistent grid of one CTA per SM with a kBigCap-cell window (216 KB) takes
 // them from the queue one at a time.  A thread walks PPT x-adjacent particles
 // (the x-chain of deposit_tiled_kernel).  Windows wider still add straight to
@@ -709,10 +709,20 @@ __global__ void __launch_bounds__(256) kick_spill_kernel(ParticleSoA p, int ng, 
     float dtf;
     kick_scalars(ks, slot, deltaT, fscal, dtf, pf_a, pf_b, ndrift);
     const int* items = spill.items + (size_t)slot * spill.nblocks;
-    for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    auto index = [&](int w) {
         const int blk = all ? w / SUB : __ldg(&items[w / SUB]);
-        const size_t i = (size_t)blk * B3 + (w % SUB) * 256 + threadIdx.x;
-        const PState cur = load_p(p, i);
+        return (size_t)blk * B3 + (w % SUB) * 256 + threadIdx.x;
+    };
+    // the next item's particle is loaded while this one's corners are gathered
+    size_t inext = index(blockIdx.x);
+    PState next = load_p(p, inext);
+    for (int w = blockIdx.x; w < n; w += gridDim.x) {
+        const size_t i = inext;
+        const PState cur = next;
+        if (w + (int)gridDim.x < n) {
+            inext = index(w + gridDim.x);
+            next = load_p(p, inext);
+        }
         finish_p(p, i, cur, gather_global(f, cur, KickWeights(cur, dtf), ng), pf_a, pf_b, ndrift, ng);
     }
 }
