@@ -317,28 +317,12 @@ def main():
     import numpy as np
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
+    from hacc_gpm_b200.replicas import Ranks
 
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def allmax(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rk = Ranks("nccl")  # replicas: NCCL only for the barrier and max-over-ranks timing
+    world, rank, local = rk.world, rk.rank, rk.local
+    barrier, allmax = rk.barrier, rk.allmax
 
     import hacc_gpm_b200 as H
     from hacc_gpm_b200 import ipk as ipkmod
@@ -464,8 +448,7 @@ def main():
                          "(float3 layout, float atomics, C2C FFTs) on %d host threads" % r["threads"]}
 
     sim.close()
-    if dist is not None:
-        dist.destroy_process_group()
+    rk.close()
     if rank != 0:
         return
     out = {
