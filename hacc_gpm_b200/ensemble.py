@@ -257,6 +257,15 @@ def run_batched(boxes, device: int = 0, graph: bool = True, keep_state: bool = F
             ens.close()
 
 
+def shard(boxes, rank: int, world: int):
+    """This rank's share of an ensemble on `world` GPUs (replicas: whole boxes
+    per GPU, split by predicted cost; no collective on the data path)."""
+    from .replicas import box_cost, partition
+
+    parts = partition([box_cost(b.ng, b.np_side or b.ng, b.nsteps) for b in boxes], world)
+    return [boxes[i] for i in parts[rank]]
+
+
 def ensemble_boxes(n: int = 96, master_seed: int = 20240601, sizes=(32, 48, 64, 96, 128), nsteps: int = 64,
                    z_ini: float = 100.0):
     """The batched-ensemble workload: n boxes, ng = np uniform over sizes,
