@@ -44,11 +44,12 @@ struct hgpm_ctx {
     SpillList dep_spill, kick_spill;  // blocks too wide for the windows
     bool win_valid = false;  // blkwin describes the current positions
     // kernel variants (environment, read at creation): HGPM_NO_TMA=1 selects the
-    // plain strided y passes, HGPM_XTMA=0|1 the plain/TMA-fed fused x pass,
+    // plain strided y passes, HGPM_XTMA=0|1 the plain/TMA-fed fused x pass
+    // (default 1, the TMA-fed one: 0.95 vs 0.99 ms at 512^3),
     // HGPM_KICK=1|2: flat gathers from the float4 force grid (default) /
     // float4 shared windows per Lagrangian block with a flat spill pass
     bool tma = true;
-    bool xtma = false;
+    bool xtma = true;
     int kick_variant = 1;
     float* stage = nullptr;     // AoS float3 x, v staging (lazy)
     double* pk_part = nullptr;  // P(k) partial sums (lazy)

@@ -347,7 +347,7 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
         const char* nt = getenv("HGPM_NO_TMA");
         c->tma = !(nt && nt[0] == '1');
         const char* xt = getenv("HGPM_XTMA");
-        c->xtma = xt && xt[0] == '1';
+        c->xtma = !(xt && xt[0] == '0');
         const char* kv = getenv("HGPM_KICK");
         if (kv && kv[0] >= '0' && kv[0] <= '2') c->kick_variant = kv[0] - '0';
     }
