@@ -118,12 +118,12 @@ __global__ void drift_kernel(ParticleSoA p, size_t n, int ng, float pf) {
 // shared-memory window over that box, and flushes the window's non-zero cells
 // to the global int64 accumulator with one coalesced red.add per cell.
 // Inside the window each cell is a (hi, lo) pair of 32-bit words updated with
-// native 32-bit shared atomics and an explicit carry.  A thread walks its
-// particles along Lagrangian x (B = 16), so particle k's upper-x corners are
-// merged in registers with particle k+1's lower-x corners whenever their
-// cells line up (about 4 instead of 8 shared atomics per particle).  A block
-// whose particles spread over more than cap_cells cells falls back to
-// per-corner global atomics.
+// native 32-bit shared atomics (win_add).  A thread walks its particles along
+// Lagrangian x, so particle k's upper-x corners are merged in registers with
+// particle k+1's lower-x corners whenever their cells line up (about 4
+// instead of 8 shared atomics per particle).  A block whose particles spread
+// over more than cap_cells cells is queued for deposit_spill_kernel (a wider
+// window, one CTA per SM; wider still, per-corner global atomics).
 __device__ __forceinline__ int nearest_image(int d, int ng) {
     if (d < -(ng >> 1)) d += ng;
     else if (d >= (ng >> 1)) d -= ng;
@@ -225,7 +225,8 @@ __device__ __forceinline__ void cic_fixed(float dx, float dy, float dz, float ma
         for (int b = 0; b < 2; ++b)
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
-                const float mul = __fmul_rn(__fmul_rn(__fmul_rn(wx[a], wy[b]), wz[cc]), mass);
+                float mul = __fmul_rn(__fmul_rn(wx[a], wy[b]), wz[cc]);
+                if (mass != 1.f) mul = __fmul_rn(mul, mass);  // exact when mass is 1 (ng = np)
                 // SMALL: mass <= 1, so mul * 2^31 < 2^32 fits an unsigned int
                 q[(a * 2 + b) * 2 + cc] = SMALL ? (unsigned long long)__float2uint_rn(mul * kFixScaleF)
                                                 : (unsigned long long)__float2ull_rn(mul * kFixScaleF);
@@ -897,7 +898,7 @@ int deposit_cap_cells(int np_side, int ng) {
     int cap = r * r * r;
     if (cap < 4096) cap = 4096;
     if (cap > 9216) cap = 9216;  // 72 KB: three CTAs per SM
-    return cap;
+    return cap & ~3;             // a multiple of 4: the windows are zeroed and read as uint4
 }
 
 static int num_sms() {
