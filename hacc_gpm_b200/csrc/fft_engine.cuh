@@ -95,8 +95,10 @@ template <bool INV> struct Dft<8, INV> {
 };
 
 // ---- one Stockham stage -------------------------------------------------
-// NS = product of the radices of the previous stages.
-template <int N, int C, int ES, int NS, int R, bool INV, int NT, int TWS>
+// NS = product of the radices of the previous stages.  TP: radix-4/8
+// twiddles beyond the loaded powers formed as products (fewer loads, more
+// registers; a pass whose registers are capped keeps TP false).
+template <int N, int C, int ES, int NS, int R, bool INV, int NT, int TWS, bool TP>
 __device__ __forceinline__ void fft_stage(float2* __restrict__ buf, const float2* __restrict__ tw) {
     constexpr int NB = N / R;        // butterflies per line
     constexpr int TOT = NB * C;      // butterflies in the tile
@@ -120,10 +122,28 @@ __device__ __forceinline__ void fft_stage(float2* __restrict__ buf, const float2
             const int c = b % C, j = b / C;
             const int k = j % NS;
             if (NS > 1) {
+                const int m = k * (N / (NS * R));  // twiddle r is tw[r * m]
+                if (TP && (R == 8 || R == 4)) {
+                    // powers 1, 2 (and 4) from the table, the rest as products
+                    // (one extra rounding each): fewer loads per butterfly
+                    float2 w[R];
+                    w[1] = __ldg(&tw[TWS * m]);
+                    w[2] = __ldg(&tw[TWS * 2 * m]);
+                    w[3] = cmul(w[1], w[2]);
+                    if (R == 8) {
+                        w[4] = __ldg(&tw[TWS * 4 * m]);
+                        w[5] = cmul(w[1], w[4]);
+                        w[6] = cmul(w[2], w[4]);
+                        w[7] = cmul(w[3], w[4]);
+                    }
 #pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    const float2 w = __ldg(&tw[TWS * (r * k * (N / (NS * R)))]);
-                    v[t][r] = INV ? cmulc(v[t][r], w) : cmul(v[t][r], w);
+                    for (int r = 1; r < R; ++r) v[t][r] = INV ? cmulc(v[t][r], w[r]) : cmul(v[t][r], w[r]);
+                } else {
+#pragma unroll
+                    for (int r = 1; r < R; ++r) {
+                        const float2 w = __ldg(&tw[TWS * (r * m)]);
+                        v[t][r] = INV ? cmulc(v[t][r], w) : cmul(v[t][r], w);
+                    }
                 }
             }
             Dft<R, INV>::run(v[t]);
@@ -137,13 +157,13 @@ __device__ __forceinline__ void fft_stage(float2* __restrict__ buf, const float2
 
 template <int... Rs> struct RSeq {};
 
-template <int N, int C, int ES, bool INV, int NT, int TWS, int NS>
+template <int N, int C, int ES, bool INV, int NT, int TWS, bool TP, int NS>
 __device__ __forceinline__ void fft_stages(float2*, const float2*, RSeq<>) {}
 
-template <int N, int C, int ES, bool INV, int NT, int TWS, int NS, int R, int... Rs>
+template <int N, int C, int ES, bool INV, int NT, int TWS, bool TP, int NS, int R, int... Rs>
 __device__ __forceinline__ void fft_stages(float2* buf, const float2* tw, RSeq<R, Rs...>) {
-    fft_stage<N, C, ES, NS, R, INV, NT, TWS>(buf, tw);
-    fft_stages<N, C, ES, INV, NT, TWS, NS * R>(buf, tw, RSeq<Rs...>{});
+    fft_stage<N, C, ES, NS, R, INV, NT, TWS, TP>(buf, tw);
+    fft_stages<N, C, ES, INV, NT, TWS, TP, NS * R>(buf, tw, RSeq<Rs...>{});
 }
 
 // Radix plans for the supported lengths (2^a 3^b, 8..1024).
@@ -166,9 +186,9 @@ template <> struct Plan<1024> { using type = RSeq<8, 8, 4, 4>; };
 
 // Transform all C lines of the tile (natural order in, natural order out).
 // Caller must __syncthreads() after filling the tile; returns synchronised.
-template <int N, int C, int ES, bool INV, int NT, int TWS = 1>
+template <int N, int C, int ES, bool INV, int NT, int TWS = 1, bool TP = true>
 __device__ __forceinline__ void fft_tile(float2* buf, const float2* __restrict__ tw) {
-    fft_stages<N, C, ES, INV, NT, TWS, 1>(buf, tw, typename Plan<N>::type{});
+    fft_stages<N, C, ES, INV, NT, TWS, TP, 1>(buf, tw, typename Plan<N>::type{});
 }
 
 }  // namespace hgpm

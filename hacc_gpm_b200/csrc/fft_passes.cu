@@ -413,7 +413,9 @@ __global__ void __launch_bounds__(Cfg<NG>::NTX) xfused_kernel(const float2* __re
     const int nvalid = ncols - col0;
     load_tile<NG, C, NT>(tile, in + off, rs, nvalid);
     __syncthreads();
-    fft_tile<NG, C, C, false, NT>(tile, tw);
+    // table twiddles throughout (as xpoisson_tma_kernel, whose register cap
+    // leaves no room for the product form): both x passes agree bit for bit
+    fft_tile<NG, C, C, false, NT, 1, false>(tile, tw);
     for (int i = threadIdx.x; i < NG * C; i += NT) {
         const int ix = i / C, c = i % C;
         tile[i] = op.pre(ix, iy, col0 + c, tile[i]);
@@ -424,10 +426,10 @@ __global__ void __launch_bounds__(Cfg<NG>::NTX) xfused_kernel(const float2* __re
         work[i] = op.comp(0, ix, iy, col0 + c, tile[i]);
     }
     __syncthreads();
-    fft_tile<NG, C, C, true, NT>(work, tw);
+    fft_tile<NG, C, C, true, NT, 1, false>(work, tw);
     store_tile<NG, C, NT>(work, out + off, rs, nvalid);
     // (no thread writes tile between the barrier above and this transform)
-    fft_tile<NG, C, C, true, NT>(tile, tw);
+    fft_tile<NG, C, C, true, NT, 1, false>(tile, tw);
     store_tile_comp<NG, C, NT>(tile, out + out_cs + off, rs, nvalid, op, 1, iy, col0);
     store_tile_comp<NG, C, NT>(tile, out + 2 * out_cs + off, rs, nvalid, op, 2, iy, col0);
 }

@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) xpoisson_tma_kernel(const __gri
         const TileIdx ti = tile_of(t, nchunks, NG);
         const int iy = ti.plane, col0 = ti.chunk * CT;
         float2* tile = in[cur];
-        fft_tile<NG, CT, CT, false, NT>(tile, tw);
+        fft_tile<NG, CT, CT, false, NT, 1, false>(tile, tw);
         // t = G rho_k (PoissonOp::pre with the tables in shared memory)
         const double cy = cosq[iy];
         for (int i = threadIdx.x; i < NG * CT; i += NT) {
@@ -203,11 +203,11 @@ __global__ void __launch_bounds__(NT, 1024 / NT) xpoisson_tma_kernel(const __gri
             work[i] = make_float2(sd * tv.y, -sd * tv.x);
         }
         __syncthreads();
-        fft_tile<NG, CT, CT, true, NT>(work, tw);
+        fft_tile<NG, CT, CT, true, NT, 1, false>(work, tw);
         store_rows<NG, CT, NT>(work, gout, rs, ncols - col0);
         // F_y, F_z: their factors are constant along x, applied after one
         // inverse transform of t (as xfused_kernel)
-        fft_tile<NG, CT, CT, true, NT>(tile, tw);
+        fft_tile<NG, CT, CT, true, NT, 1, false>(tile, tw);
         const float sy = iy == nyq ? 0.f : sk[iy];
         const int TPR = CT / 2;
 #pragma unroll 2
