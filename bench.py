@@ -140,7 +140,9 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(steps=1, warmup=0, ng=NG, np_side=NP):
+def cpu_baseline(steps=1, warmup=0, ng=None, np_side=None):
+    ng = NG if ng is None else ng  # the box size set by --size (read at call time)
+    np_side = NP if np_side is None else np_side
     exe = os.path.join(ROOT, "oracle", "_bin", "cpu_pm")
     if not os.path.exists(exe):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "cpu"], check=True)
@@ -153,7 +155,8 @@ def cpu_baseline(steps=1, warmup=0, ng=NG, np_side=NP):
 def reference_gpu():
     """The reference's own serial CUDA step (oracle/_ref/refpm, compiled from
     the HACC_GPM sources when they were present at build time) on this GPU:
-    the same 512^3 run, steps 46-55 (mid-run) and the whole 100-step run.
+    the same run (512^3 by default), steps 46-55 (mid-run) and the whole
+    100-step run.
     Context for the GPU-to-GPU comparison; None when the harness is absent."""
     exe = os.path.join(ROOT, "oracle", "_ref", "refpm")
     if not os.path.exists(exe):
@@ -198,17 +201,24 @@ def run_reference(args):
     except Exception as e:  # the CPU arm stands on its own
         gpu = {"error": str(e)[:200]}
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": r["steps"],
+        "impl": "reference", "metric": METRIC if NP == 512 else "particle-updates/s at %d^3" % NP, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": r["steps"],
         "warmup": 1 if args.warmup > 0 else 0, "ms_per_step": r["sec_per_step"] * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic: seeded perturbed lattice",
-        "config": {"workload": "PM step, 512^3 particles on a 512^3 grid, L=512 Mpc/h", "np": NP, "ng": NG,
-                   "rl": RL, "parallelism": "host cores (OpenMP)"},
+        "config": dict(step_config(), parallelism="host cores (OpenMP)"),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["threads"], "kind": "port",
-                         "sample": "%d full 512^3 step(s) of the OpenMP C++ transcription of the reference's serial "
-                                   "step (float3 layout, float atomics, C2C FFTs), after 1 warm-up" % r["steps"]},
+                         "sample": "%d full %d^3 step(s) of the OpenMP C++ transcription of the reference's serial "
+                                   "step (float3 layout, float atomics, C2C FFTs), after 1 warm-up" % (r["steps"], NP)},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_gpu": gpu,
     }))
+
+
+def step_config():
+    """The workload both arms report: one PM step of the box."""
+    return {"workload": "PM step (deposit, R2C FFT, Poisson+gradient, 3 C2R FFTs, gather+kick+drift), "
+                        "%d^3 particles on a %d^3 grid, L=%g Mpc/h, flat LCDM, ICs at z=50, %d-step run"
+                        % (NP, NG, RL, NSTEPS_RUN),
+            "np": NP, "ng": NG, "rl": RL}
 
 
 def _check_same(a, b):
@@ -444,22 +454,22 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         r = cpu_baseline(steps=1, warmup=0)
         cpu = {"value": np3 / r["sec_per_step"], "unit": UNIT, "cores": r["threads"], "kind": "port",
-               "sample": "1 full 512^3 step of the OpenMP C++ transcription of the reference's serial step "
-                         "(float3 layout, float atomics, C2C FFTs) on %d host threads" % r["threads"]}
+               "sample": "1 full %d^3 step of the OpenMP C++ transcription of the reference's serial step "
+                         "(float3 layout, float atomics, C2C FFTs) on %d host threads" % (NP, r["threads"])}
 
     sim.close()
     rk.close()
     if rank != 0:
         return
     out = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "metric": METRIC if NP == 512 else "particle-updates/s at %d^3" % NP, "value": value, "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: seeded EH no-wiggle Zel'dovich ICs (Philox white noise), random per rank",
-        "config": {"workload": "PM step (deposit, R2C FFT, Poisson+gradient, 3 C2R FFTs, gather+kick+drift), "
-                               "512^3 particles on a 512^3 grid, L=512 Mpc/h, flat LCDM, ICs at z=50, 100-step run",
-                   "np": NP, "ng": NG, "rl": RL, "parallelism": "replicas (one independent box per GPU)",
-                   "l2": "inputs larger than L2 (3.8 GB particle state, 5 GB grids)",
-                   "timed": "K steps from step 45 of the 100-step run (mid-run cost = run average)"},
+        "config": dict(step_config(), parallelism="replicas (one independent box per GPU)",
+                       l2="inputs larger than L2 (%.2g GB particle state, %.2g GB grids)"
+                          % (28 * NP ** 3 / 1e9, 40 * NG ** 3 / 1e9),
+                       timed="K steps from step 45 of the 100-step run (mid-run cost = run average)"),
         "roofline": roofline, "step_roofline": step_roof, "phases": phases, "cpu_baseline": cpu, "e2e": e2e,
         "full_run": full, "timed_steps": run_state, "gpu_launches": int(launches), "clocks": clk,
     }
