@@ -294,8 +294,11 @@ def run_forms(args):
         "config": {"workload": "%d requests, Poisson arrivals 20/s (seed 7), ng = np log-uniform over "
                                "{32,48,64,96,128,192,256}, L = ng Mpc/h, steps U[20,200], Om U[0.25,0.35], "
                                "sigma8 U[0.7,0.9], EH ICs at z=50" % args.requests,
-                   "classes": stats["classes"], "admission": "slots per size class from a 40 GB HBM budget "
-                                                            "split evenly over classes (footprint per slot)"},
+                   "classes": stats["classes"],
+                   "admission": "slots per size class from a 40 GB HBM budget split over the classes by footprint "
+                                "per slot, at most the slots whose batched step is ~2 ms of GPU time",
+                   "scheduling": "each class on its own stream at its own pace (batches of ~1 ms), stream "
+                                 "priority by box size (smaller first)"},
         "dtype": "f32", "data": "synthetic",
     }))
 

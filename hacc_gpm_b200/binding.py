@@ -139,6 +139,9 @@ def lib() -> C.CDLL:
         "hgpm_ens_sync": (C.c_int, [vp]),
         "hgpm_ens_status": (C.c_int, [vp, C.c_int, C.c_int, P(C.c_int), P(C.c_int)]),
         "hgpm_ens_kernel_launches": (C.c_int64, [vp, C.c_int]),
+        "hgpm_ens_step_class": (C.c_int, [vp, C.c_int, C.c_int]),
+        "hgpm_ens_class_done": (C.c_int, [vp, C.c_int, P(C.c_int)]),
+        "hgpm_ens_sync_class": (C.c_int, [vp, C.c_int]),
         "hgpm_sizeof_params": (C.c_size_t, []),
         "hgpm_sizeof_timestepper": (C.c_size_t, []),
     }

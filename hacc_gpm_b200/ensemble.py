@@ -140,6 +140,18 @@ class Ensemble:
     def sync(self):
         self._ck(self.L.hgpm_ens_sync(self._h))
 
+    def step_class(self, cls: int, n: int = 1):
+        """n steps of one class on its own stream (returns at once)."""
+        self._ck(self.L.hgpm_ens_step_class(self._h, cls, n))
+
+    def class_done(self, cls: int) -> bool:
+        d = C.c_int()
+        self._ck(self.L.hgpm_ens_class_done(self._h, cls, C.byref(d)))
+        return bool(d.value)
+
+    def sync_class(self, cls: int):
+        self._ck(self.L.hgpm_ens_sync_class(self._h, cls))
+
     def status(self, cls: int, slot: int):
         r, d = C.c_int(), C.c_int()
         self._ck(self.L.hgpm_ens_status(self._h, cls, slot, C.byref(r), C.byref(d)))

@@ -5,11 +5,12 @@ Requests (``ensemble.Box`` plus an arrival time) of mixed grid size, step
 count and cosmology are admitted into slots of a resident ``Ensemble``.
 Slot capacity per size class comes from an HBM budget and the per-slot
 footprint (``hgpm_ens_footprint_bytes``), so admission is by footprint: a
-request waits until a slot of its class is free.  Every tick advances all
-admitted requests by one PM step in one batched launch per phase per class;
-requests that arrive while others run are admitted at the next tick, their
-ICs generated in place, and a request that finishes frees its slot after its
-P(k) is taken.  Particle and grid state stay on the device throughout.
+request waits until a slot of its class is free.  Each class advances on its
+own stream at its own pace, all its admitted requests one PM step at a time
+in one batched launch per phase; requests that arrive while others run are
+admitted between their class's batches, their ICs generated in place, and a
+request that finishes frees its slot after its P(k) is taken.  Particle and
+grid state stay on the device throughout.
 
 ``serve_one_at_a_time`` is the comparison: the same requests, first come
 first served, each through its own context and the plain step.
@@ -45,58 +46,122 @@ def request_stream(n: int, rate: float = 20.0, seed: int = 7, sizes=(32, 48, 64,
     return out
 
 
-def class_capacity(sizes, hbm_budget: float, max_slots: int = 64):
-    """Slots per size class: the budget split evenly over the classes, each
-    share divided by the class's per-slot footprint."""
-    share = hbm_budget / len(sizes)
-    caps = []
-    for ng in sizes:
-        per = Ensemble.footprint_bytes(ng, ng, 1)
-        caps.append((ng, ng, int(max(1, min(max_slots, share // per)))))
-    return caps
+# GPU milliseconds of one PM step per particle + cell (7.6 ms for a 512^3 box
+# with a 512^3 grid on one B200), for the concurrency cap below
+STEP_MS_PER_UNIT = 7.6 / (2 * 512 ** 3)
+
+
+def class_capacity(sizes, hbm_budget: float, max_slots: int = 64, step_ms: float = None):
+    """Slots per size class by footprint: the budget is split evenly over the
+    classes, and what a class leaves unused (it stops at its cap) is split
+    again over the classes that can still take a slot, until no share buys
+    one.  Every class gets at least one slot.  The cap is max_slots and, with
+    step_ms, the slots whose batched step takes about step_ms of GPU time:
+    more large boxes at once would only share the GPU further and lengthen
+    every one of their runs (the serving p99)."""
+    per = {ng: Ensemble.footprint_bytes(ng, ng, 1) for ng in sizes}
+    cap = {ng: max_slots if step_ms is None else
+           int(max(1, min(max_slots, round(step_ms / (STEP_MS_PER_UNIT * 2 * ng ** 3))))) for ng in sizes}
+    n = {ng: 0 for ng in sizes}
+    left = float(hbm_budget)
+    open_ = list(sizes)
+    while open_:
+        share = left / len(open_)
+        gave = False
+        for ng in open_:
+            k = int(min(cap[ng] - n[ng], share // per[ng]))
+            if k > 0:
+                n[ng] += k
+                left -= k * per[ng]
+                gave = True
+        open_ = [ng for ng in open_ if n[ng] < cap[ng] and per[ng] <= left]
+        if not gave:
+            break
+    return [(ng, ng, int(max(1, n[ng]))) for ng in sizes]
 
 
 class Server:
-    def __init__(self, sizes, hbm_budget: float = 40e9, device: int = 0, graph: bool = True, max_slots: int = 64):
-        self.classes = class_capacity(sizes, hbm_budget, max_slots)
+    """Continuous batching over the size classes of one resident Ensemble.
+
+    Each class advances on its own stream at its own pace: when a class's
+    queued steps have run (a poll, no wait), its finished requests are
+    collected, waiting requests of that class are admitted into its free
+    slots, and its next batch of steps is queued.  A batch is sized to about
+    ``batch_ms`` of GPU time from the class's measured step time (at most
+    ``max_batch`` steps, and no more than the fewest steps a running request
+    still needs), so small boxes are not held to the pace of large ones and
+    the host loop keeps up with them."""
+
+    def __init__(self, sizes, hbm_budget: float = 40e9, device: int = 0, graph: bool = True, max_slots: int = 64,
+                 batch_ms: float = 1.0, max_batch: int = 8, step_ms: float = 2.0):
+        self.classes = class_capacity(sizes, hbm_budget, max_slots, step_ms)
         self.index = {c[0]: i for i, c in enumerate(self.classes)}
         self.ens = Ensemble(self.classes, device=device, graph=graph)
+        n = len(self.classes)
         self.free = {i: collections.deque(range(c[2])) for i, c in enumerate(self.classes)}
         self.running = {}  # (cls, slot) -> request
-        self.ticks = 0
+        self.busy = [False] * n      # steps queued on the class's stream
+        self.queued = [0] * n        # steps in the current batch
+        self.t_launch = [0.0] * n
+        self.step_ms = [None] * n    # measured seconds per step, per class (ms)
+        self.steps = [0] * n         # class steps run
+        self.batch_ms, self.max_batch = batch_ms, max_batch
 
     def close(self):
         self.ens.close()
 
     def admit(self, req: Box) -> bool:
         ci = self.index[req.ng]
-        if not self.free[ci]:
+        if self.busy[ci] or not self.free[ci]:
             return False
         si = self.free[ci].popleft()
         p = req.params()
         v = self.ens.slot(ci, si, p)
         v.generate_ic(req.table, req.k_delta)
         self.ens.start(ci, si, _ts_for(p), req.nsteps)
+        req.done_steps = 0
         self.running[(ci, si)] = req
         return True
 
-    def tick(self):
-        """One batched step of every running request; returns the finished
-        requests with their results."""
-        self.ens.step(1)
-        self.ens.sync()
-        self.ticks += 1
+    def poll(self):
+        """Finished requests (with results) of every class whose queued
+        steps have run."""
         done = []
-        for (ci, si), req in list(self.running.items()):
-            running, nd = self.ens.status(ci, si)
-            if not running:
-                v = self.ens.views[(ci, si)]
-                req.result = _result(v, req)
-                self.ens.release(ci, si)
-                self.free[ci].append(si)
-                del self.running[(ci, si)]
-                done.append(req)
+        for ci in range(len(self.classes)):
+            if not self.busy[ci] or not self.ens.class_done(ci):
+                continue
+            self.ens.sync_class(ci)
+            self.busy[ci] = False
+            ms = 1e3 * (time.perf_counter() - self.t_launch[ci]) / self.queued[ci]
+            self.step_ms[ci] = ms if self.step_ms[ci] is None else 0.5 * (self.step_ms[ci] + ms)
+            for (c, si), req in list(self.running.items()):
+                if c != ci:
+                    continue
+                running, req.done_steps = self.ens.status(ci, si)
+                if not running:
+                    v = self.ens.views[(ci, si)]
+                    req.result = _result(v, req)
+                    self.ens.release(ci, si)
+                    self.free[ci].append(si)
+                    del self.running[(ci, si)]
+                    done.append(req)
         return done
+
+    def launch(self):
+        """Queue the next batch of every idle class that has running requests."""
+        for ci in range(len(self.classes)):
+            if self.busy[ci]:
+                continue
+            rem = [r.nsteps - r.done_steps for (c, _), r in self.running.items() if c == ci]
+            if not rem:
+                continue
+            k = 1 if self.step_ms[ci] is None else int(self.batch_ms / max(self.step_ms[ci], 1e-3))
+            k = max(1, min(k, self.max_batch, min(rem)))
+            self.ens.step_class(ci, k)
+            self.busy[ci] = True
+            self.queued[ci] = k
+            self.t_launch[ci] = time.perf_counter()
+            self.steps[ci] += k
 
 
 def serve(requests, hbm_budget: float = 40e9, device: int = 0, graph: bool = True, realtime: bool = True,
@@ -117,23 +182,24 @@ def serve(requests, hbm_budget: float = 40e9, device: int = 0, graph: bool = Tru
             now = time.perf_counter() - t0
             while pending and (not realtime or pending[0].arrival <= now):
                 waiting.append(pending.popleft())
-            # first come first served within what fits
+            for r in srv.poll():
+                r.finish = time.perf_counter() - t0
+                r.latency = r.finish - (r.arrival if realtime else 0.0)
+                finished.append(r)
+            # first come first served within what fits (a class takes new
+            # requests between its batches)
             still = collections.deque()
             while waiting:
                 r = waiting.popleft()
                 if not srv.admit(r):
                     still.append(r)
             waiting = still
-            if srv.running:
-                for r in srv.tick():
-                    r.finish = time.perf_counter() - t0
-                    r.latency = r.finish - (r.arrival if realtime else 0.0)
-                    finished.append(r)
-            elif pending:
+            srv.launch()
+            if not srv.running and not waiting and pending:
                 time.sleep(max(0.0, min(pending[0].arrival - (time.perf_counter() - t0), 0.01)))
         makespan = time.perf_counter() - t0
-        return finished, makespan, {"ticks": srv.ticks, "classes": srv.classes,
-                                    "launches": srv.ens.kernel_launches()}
+        return finished, makespan, {"ticks": max(srv.steps), "steps_per_class": list(srv.steps),
+                                    "classes": srv.classes, "launches": srv.ens.kernel_launches()}
     finally:
         srv.close()
 

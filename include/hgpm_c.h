@@ -225,6 +225,19 @@ int hgpm_ens_use_graph(hgpm_ensemble* ens, int on);
 int hgpm_ens_sync(hgpm_ensemble* ens);
 int hgpm_ens_status(hgpm_ensemble* ens, int cls, int slot, int* running, int* steps_done);
 int64_t hgpm_ens_kernel_launches(hgpm_ensemble* ens, int reset);
+/* One class at a time, for a serving loop whose classes advance at their
+ * own pace (no counterpart in the reference either): hgpm_ens_step_class
+ * queues nsteps steps of class cls on the class's own stream, after the
+ * slot set-up queued so far, and returns; hgpm_ens_class_done sets *done to
+ * 1 once they have run (a poll, no wait); hgpm_ens_sync_class waits for
+ * them and refreshes that class's hgpm_ens_status.  While steps of a class
+ * are queued, make no slot call on that class (hgpm_ens_slot, _start,
+ * _release, or work on its views, whose deposit shares per-slot spill
+ * counters with the class step); the other classes are free meanwhile.   */
+/* Class streams carry stream priorities, smaller boxes higher.           */
+int hgpm_ens_step_class(hgpm_ensemble* ens, int cls, int nsteps);
+int hgpm_ens_class_done(hgpm_ensemble* ens, int cls, int* done);
+int hgpm_ens_sync_class(hgpm_ensemble* ens, int cls);
 
 /* ---- allocation-free density ------------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device

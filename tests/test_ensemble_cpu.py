@@ -45,9 +45,14 @@ def test_request_stream():
 
 def test_capacity_by_footprint():
     caps = S.class_capacity([32, 64, 128, 256], 8e9, max_slots=64)
-    for ng, npp, n in caps:
-        assert n >= 1 and (n == 1 or n * H.ensemble.Ensemble.footprint_bytes(ng, npp, 1) <= 2e9 + 1)
+    per = [E.Ensemble.footprint_bytes(ng, npp, 1) for ng, npp, _ in caps]
+    used = sum(n * f for (_, _, n), f in zip(caps, per))
+    assert all(1 <= n <= 64 for _, _, n in caps) and used <= 8e9
     assert [c[2] for c in caps] == sorted([c[2] for c in caps], reverse=True)
+    # what the small classes cannot use goes to the large ones: no class
+    # below its cap could still take a slot from what is left
+    assert all(n == 64 or f > 8e9 - used for (_, _, n), f in zip(caps, per))
+    assert caps[2][2] > 2e9 // per[2]
     assert E.Ensemble.footprint_bytes(64, 64, 4) > 4 * H.footprint_bytes(64, 64) * 0.9
 
 

@@ -34,6 +34,40 @@ def test_batched_equals_alone(graph):
         _same(a, b)
 
 
+@pytest.mark.parametrize("graph", [True, False])
+def test_per_class_stepping_equals_alone(graph):
+    """Classes advanced one at a time on their own streams, in batches of
+    different sizes and interleaved, give each box the state and P(k) of the
+    box run alone."""
+    boxes = _boxes()
+    alone = E.run_serial(boxes, keep_state=True)
+    classes, where = E.class_layout(boxes)
+    with E.Ensemble(classes, graph=graph) as ens:
+        for b, (ci, si) in zip(boxes, where):
+            p = b.params()
+            ens.slot(ci, si, p).generate_ic(b.table, b.k_delta)
+            ens.start(ci, si, E._ts_for(p), b.nsteps)
+        left = {ci: max(b.nsteps for b, (c, _) in zip(boxes, where) if c == ci) for ci in range(len(classes))}
+        batch = {ci: 1 + ci for ci in left}
+        while any(left.values()):
+            for ci in left:
+                if left[ci] and ens.class_done(ci):
+                    k = min(batch[ci], left[ci])
+                    ens.step_class(ci, k)
+                    left[ci] -= k
+        got = []
+        for ci in range(len(classes)):
+            ens.sync_class(ci)
+        for b, (ci, si) in zip(boxes, where):
+            assert ens.status(ci, si) == (False, b.nsteps)
+            v = ens.views[(ci, si)]
+            r = E._result(v, b)
+            r["x"], r["v"] = v.store_state()
+            got.append(r)
+    for a, b in zip(alone, got):
+        _same(a, b)
+
+
 def test_slot_reuse_and_errors():
     boxes = _boxes()[:2]
     classes, _ = E.class_layout(boxes)
