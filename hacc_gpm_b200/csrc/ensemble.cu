@@ -446,8 +446,8 @@ static int class_step(hgpm_ensemble* E, EnsClass& k, cudaStream_t s) {
                        Slots{act, k.spec_elems, 0}, S));
     ECK(launch_xpoisson(ng, k.spec, k.fspec, M + 1, (size_t)ng * k.zs, (size_t)k.zs, ng, cs, k.tw_ng, k.cosq, k.sk,
                         0.5 / ((double)ng * ng * ng), s, Slots{act, k.spec_elems, 3 * k.spec_elems}, S));
-    ECK(launch_strided(ng, true, k.fspec, M + 1, (size_t)k.zs, (size_t)ng * k.zs, ng, cs, 3, k.tw_ng, s,
-                       Slots{act, 3 * k.spec_elems, 0}, S));
+    ECK(launch_yinv2(ng, k.fspec, M + 1, (size_t)k.zs, (size_t)ng * k.zs, ng, cs, k.tw_ng, k.sk, s,
+                     Slots{act, 3 * k.spec_elems, 0}, S));
     float4* f4 = reinterpret_cast<float4*>(k.force);
     ECK(launch_zinv3(ng, k.fspec, f4, ng * ng, k.zs, cs, 1.0f, k.tw_ng, s,
                      Slots{act, 3 * k.spec_elems, k.force_elems / 4}, S));

@@ -430,8 +430,58 @@ __global__ void __launch_bounds__(Cfg<NG>::NTX) xfused_kernel(const float2* __re
     store_tile<NG, C, NT>(work, out + off, rs, nvalid);
     // (no thread writes tile between the barrier above and this transform)
     fft_tile<NG, C, C, true, NT, 1, false>(tile, tw);
-    store_tile_comp<NG, C, NT>(tile, out + out_cs + off, rs, nvalid, op, 1, iy, col0);
-    store_tile_comp<NG, C, NT>(tile, out + 2 * out_cs + off, rs, nvalid, op, 2, iy, col0);
+    if (Op::kTwoOut) {
+        // T itself; the inverse y pass applies the y and z factors
+        store_tile<NG, C, NT>(tile, out + out_cs + off, rs, nvalid);
+    } else {
+        store_tile_comp<NG, C, NT>(tile, out + out_cs + off, rs, nvalid, op, 1, iy, col0);
+        store_tile_comp<NG, C, NT>(tile, out + 2 * out_cs + off, rs, nvalid, op, 2, iy, col0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Inverse y pass of the Poisson force spectra.  Part 0 is F_x, transformed in
+// place.  Part 1 holds T = IFFT_x(G rho_k) as the fused x pass leaves it; the
+// pass forms F_y = -i sin(k_y) T and F_z = -i sin(k_z) T (PoissonOp::comp's
+// factors and arithmetic, zero at the Nyquist index), transforms both and
+// writes F_y over part 1 and F_z to component 2: the same values as the
+// three-component pass over x-pass outputs F_x, F_y, F_z, with one spectrum
+// fewer written by the x pass and read here.
+// blockIdx = (column chunk, plane, slot * 2 + part).
+// ---------------------------------------------------------------------------
+template <int NG>
+__global__ void __launch_bounds__(Cfg<NG>::NTS, 1) strided_inv2_kernel(float2* __restrict__ data, int ncols,
+                                                                    size_t rs, size_t ps, size_t cs,
+                                                                    const float2* __restrict__ tw,
+                                                                    const float* __restrict__ sk, Slots sl) {
+    constexpr int C = Cfg<NG>::CS, NT = Cfg<NG>::NTS, nyq = NG / 2;
+    float2* tile = reinterpret_cast<float2*>(hgpm_smem);
+    float2* work = tile + NG * C;
+    const int slot = blockIdx.z / 2, part = blockIdx.z % 2;
+    if (slot_idle(sl, slot)) return;
+    const int col0 = blockIdx.x * C;
+    float2* g = data + (size_t)slot * sl.s0 + (size_t)part * cs + (size_t)blockIdx.y * ps + col0;
+    const int nvalid = ncols - col0;
+    load_tile<NG, C, NT>(tile, g, rs, nvalid);
+    __syncthreads();
+    if (part == 0) {
+        fft_tile<NG, C, C, true, NT>(tile, tw);
+        store_tile<NG, C, NT>(tile, g, rs, nvalid);
+        return;
+    }
+    for (int i = threadIdx.x; i < NG * C; i += NT) {
+        const int e = i / C, iz = col0 + i % C;  // e: the y wavenumber index
+        const float2 v = tile[i];
+        const float sy = e == nyq ? 0.f : __ldg(&sk[e]);
+        const float sz = iz == nyq ? 0.f : __ldg(&sk[iz < NG ? iz : 0]);
+        work[i] = make_float2(sy * v.y, -sy * v.x);
+        tile[i] = make_float2(sz * v.y, -sz * v.x);
+    }
+    __syncthreads();
+    fft_tile<NG, C, C, true, NT>(work, tw);
+    store_tile<NG, C, NT>(work, g, rs, nvalid);
+    fft_tile<NG, C, C, true, NT>(tile, tw);
+    store_tile<NG, C, NT>(tile, g + cs, rs, nvalid);
 }
 
 // ---------------------------------------------------------------------------
@@ -613,6 +663,18 @@ static cudaError_t strided_impl(bool inv, float2* data, int ncols, size_t rs, si
     return cudaGetLastError();
 }
 
+template <int NG>
+static cudaError_t strided_inv2_impl(float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
+                                     const float2* tw, const float* sk, cudaStream_t s, const Slots& sl, int nslots) {
+    using G = Cfg<NG>;
+    auto k = strided_inv2_kernel<NG>;
+    cudaError_t e = ensure_smem(k, 2 * G::SSMEM);
+    if (e != cudaSuccess) return e;
+    dim3 grid(cdiv(ncols, G::CS), nplanes, 2 * nslots);
+    k<<<grid, G::NTS, 2 * G::SSMEM, s>>>(data, ncols, rs, ps, cs, tw, sk, sl);
+    return cudaGetLastError();
+}
+
 template <int NG, class Op>
 static cudaError_t xfused_impl(const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
                                size_t out_cs, const float2* tw, const Op& op, cudaStream_t s, const Slots& sl = Slots{},
@@ -695,6 +757,17 @@ cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs,
     switch (ng) {
 #define X(n) \
     case n: return strided_impl<n>(inv, data, ncols, rs, ps, nplanes, cs, ncomp, tw, s, sl, nslots);
+        HGPM_SIZES(X)
+#undef X
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_yinv2(int ng, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
+                         const float2* tw, const float* sk, cudaStream_t s, const Slots& sl, int nslots) {
+    switch (ng) {
+#define X(n) \
+    case n: return strided_inv2_impl<n>(data, ncols, rs, ps, nplanes, cs, tw, sk, s, sl, nslots);
         HGPM_SIZES(X)
 #undef X
     }

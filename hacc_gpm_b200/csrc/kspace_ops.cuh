@@ -20,6 +20,9 @@ namespace hgpm {
 // real part — all the reference keeps — is exactly zero; the half-spectrum
 // C2R would instead Hermitian-extend it.  comp() therefore returns 0 there.
 struct PoissonOp {
+    // the x pass stores F_x and T = IFFT_x(t) only; the inverse y pass forms
+    // F_y and F_z from T (comp(1), comp(2) factors are constant along x)
+    static constexpr bool kTwoOut = true;
     const double* cosq;  // cos(k_i) - 1, one entry per grid index
     const float* sk;     // sin(k_i)
     double coeff;        // 0.5 / ng^3
@@ -42,6 +45,7 @@ struct PoissonOp {
 // then transformDensityField (transform_density_field_initializer.cu:72-112):
 // s_d = (Im k_d, -Re k_d) / (k^2 delta).
 struct ICOp {
+    static constexpr bool kTwoOut = false;  // the x pass stores all three components
     const double* table;
     int nbins;
     double k_delta;

@@ -635,11 +635,12 @@ extern "C" int hgpm_solve_gradient(hgpm_ctx* c) {
     }
     {
         PhaseScope ps(c, PH_YINV);
+        // (F_x, T) from the x pass -> (F_x, F_y, F_z)
         if (c->tma)
-            CK(launch_strided_tma(ng, true, false, c->fspec, M + 1, c->zs, cs, 3, c->tw_ng, c->d_err + 1, c->stream));
+            CK(launch_yinv2_tma(ng, c->fspec, M + 1, c->zs, cs, c->tw_ng, c->sk, c->d_err + 1, c->stream));
         else
-            CK(launch_strided(ng, true, c->fspec, M + 1, (size_t)c->zs, (size_t)ng * c->zs, ng, cs, 3, c->tw_ng,
-                              c->stream));
+            CK(launch_yinv2(ng, c->fspec, M + 1, (size_t)c->zs, (size_t)ng * c->zs, ng, cs, c->tw_ng, c->sk,
+                            c->stream));
         count(c, PH_YINV, 1);
     }
     {
