@@ -59,11 +59,16 @@ MID_STEP = 45     # the timed steps start here (the mid-run cost is the run's av
 # Algorithmic bytes per launch of each kernel (precision-form state:
 # x = 12 B offset + 4 B cell, v = 12 B; FP32 grids).  Sum = 72 Np + 64 Ng.
 def alg_bytes(np3, ng3):
+    """Algorithmic bytes per phase: each input read once, each output
+    written once (FP32, 12 B per force vector).  The gradient is taken in
+    real space, so the x pass moves one spectrum in and one out (8 B/cell)
+    and the inverse z phase (C2R of the potential, 8 B/cell, then the
+    gradient, 4 + 12 B/cell) 24 B/cell: 72 Np + 56 Ng per step."""
     return {
         "deposit": 16 * np3 + 4 * ng3,
         "fft_z_fwd": 8 * ng3,
         "fft_y_fwd": 0,
-        "poisson_x": 16 * ng3,
+        "poisson_x": 8 * ng3,
         "fft_y_inv": 0,
         "fft_z_inv": 24 * ng3,
         "kick_drift": 56 * np3 + 12 * ng3,
@@ -75,9 +80,9 @@ KERNEL_NAMES = {
     "deposit": "deposit_tiled_kernel<16,1,512,2> + deposit_spill_kernel<16,1,1024> (queued wide blocks)",
     "fft_z_fwd": "zpass_r2c_kernel<NG,1>",
     "fft_y_fwd": "strided_tma_kernel<NG,0,0>",
-    "poisson_x": "xfused_kernel<NG,PoissonOp>",
+    "poisson_x": "xpotential_tma_kernel<NG,512> (forward x, Green's function, inverse x)",
     "fft_y_inv": "strided_tma_kernel<NG,1,0>",
-    "fft_z_inv": "zpass_c2r3_kernel<NG>",
+    "fft_z_inv": "zpass_c2r_kernel<NG> (the potential) + gradient_kernel (central differences, float4 force)",
     "kick_drift": "kick_spill_kernel<16> (flat: one particle per thread, float4 force gathers)",
 }
 
@@ -400,7 +405,7 @@ def main():
                 "peak_kind": peak_kind, "traffic": None, "alg_bytes_per_launch": d["alg_bytes"],
                 "ms_per_launch": d["ms_per_step"]}
     step_ms = ms_max / args.steps
-    b_step = 72 * np3 + 64 * ng3
+    b_step = sum(alg_bytes(np3, ng3).values())  # 72 Np + 56 Ng
     step_roof = {"alg_bytes_per_step": b_step, "achieved_gbs": b_step / (step_ms * 1e-3) / 1e9,
                  "frac": b_step / (step_ms * 1e-3) / 1e9 / peak, "peak": peak}
     tp = os.path.join(ROOT, "profiles", "traffic_%d.json" % NG)

@@ -422,10 +422,13 @@ extern "C" int hgpm_ens_release(hgpm_ensemble* E, int ci, int slot) {
     return HGPM_OK;
 }
 
+// Kernels of one class step besides the kick: deposit 2, z forward, y
+// forward, x potential, y inverse, z inverse, gradient, slot advance.
+constexpr int kStepKernels = 9;
+
 // All phases of one step for every slot of class k, on stream s.
 static int class_step(hgpm_ensemble* E, EnsClass& k, cudaStream_t s) {
     const int ng = k.ng, M = ng / 2, S = k.nslots;
-    const size_t cs = (size_t)ng * ng * k.zs;
     const float mass = ctx_cic_mass(ng, k.np);
     const double mean = (double)mass * (double)k.npart / (double)k.ncell;
     ParticleSoA p;
@@ -444,18 +447,20 @@ static int class_step(hgpm_ensemble* E, EnsClass& k, cudaStream_t s) {
     ECK(launch_zfwd(ng, k.rho64, true, k.spec, ng * ng, k.zs, mean, k.tw_ng, s, Slots{act, k.ncell, k.spec_elems}, S));
     ECK(launch_strided(ng, false, k.spec, M + 1, (size_t)k.zs, (size_t)ng * k.zs, ng, 0, 1, k.tw_ng, s,
                        Slots{act, k.spec_elems, 0}, S));
-    ECK(launch_xpoisson(ng, k.spec, k.fspec, M + 1, (size_t)ng * k.zs, (size_t)k.zs, ng, cs, k.tw_ng, k.cosq, k.sk,
-                        0.5 / ((double)ng * ng * ng), s, Slots{act, k.spec_elems, 3 * k.spec_elems}, S));
-    ECK(launch_yinv2(ng, k.fspec, M + 1, (size_t)k.zs, (size_t)ng * k.zs, ng, cs, k.tw_ng, k.sk, s,
-                     Slots{act, 3 * k.spec_elems, 0}, S));
+    ECK(launch_xpotential(ng, k.spec, k.fspec, M + 1, (size_t)ng * k.zs, (size_t)k.zs, ng, k.tw_ng, k.cosq,
+                          0.5 / ((double)ng * ng * ng), s, Slots{act, k.spec_elems, 3 * k.spec_elems}, S));
+    ECK(launch_strided(ng, true, k.fspec, M + 1, (size_t)k.zs, (size_t)ng * k.zs, ng, 0, 1, k.tw_ng, s,
+                       Slots{act, 3 * k.spec_elems, 0}, S));
     float4* f4 = reinterpret_cast<float4*>(k.force);
-    ECK(launch_zinv3(ng, k.fspec, f4, ng * ng, k.zs, cs, 1.0f, k.tw_ng, s,
-                     Slots{act, 3 * k.spec_elems, k.force_elems / 4}, S));
+    float* phi = reinterpret_cast<float*>(k.fspec + k.spec_elems);  // as a single context places it
+    ECK(launch_zinv(ng, k.fspec, phi, ng * ng, k.zs, 0, 0, 1, 1.0f, k.tw_ng, s,
+                    Slots{act, 3 * k.spec_elems, 6 * k.spec_elems}, S));
+    ECK(launch_gradient(ng, phi, f4, s, Slots{act, 6 * k.spec_elems, k.force_elems / 4}, S));
     ECK(launch_kick_drift(p, k.np, ng, f4, 0.0, 0.0, 0.f, 0.f, 0, E->kick_variant, k.blkwin, true, k.kick_spill, s,
                           Slots{act, k.part_stride, k.force_elems / 4, k.win_stride},
                           KickSched{k.d_sched, k.d_step, HGPM_MAX_STEPS}, S));
     ECK(launch_slots_advance(k.d_active, k.d_step, k.d_nsteps, S, s));
-    E->launches += 8 + kick_kernels(E->kick_variant, k.np, ng);  // deposit 2, FFT 5, advance 1
+    E->launches += kStepKernels + kick_kernels(E->kick_variant, k.np, ng);
     return HGPM_OK;
 }
 
@@ -512,7 +517,7 @@ extern "C" int hgpm_ens_step(hgpm_ensemble* E, int nsteps) {
             ECK(ie);
         }
         int per = 0;
-        for (auto& k : E->cls) per += 8 + kick_kernels(E->kick_variant, k.np, k.ng);
+        for (auto& k : E->cls) per += kStepKernels + kick_kernels(E->kick_variant, k.np, k.ng);
         for (int i = 0; i < nsteps; ++i) {
             ECK(cudaGraphLaunch(E->exec, E->stream));
             E->launches += per;
@@ -563,7 +568,7 @@ extern "C" int hgpm_ens_step_class(hgpm_ensemble* E, int ci, int nsteps) {
         }
         for (int i = 0; i < nsteps; ++i) {
             ECK(cudaGraphLaunch(k.exec, k.stream));
-            E->launches += 8 + kick_kernels(E->kick_variant, k.np, k.ng);
+            E->launches += kStepKernels + kick_kernels(E->kick_variant, k.np, k.ng);
         }
     } else {
         for (int i = 0; i < nsteps; ++i)

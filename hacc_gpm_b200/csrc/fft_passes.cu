@@ -32,9 +32,6 @@ template <int NG> struct Cfg {
     static constexpr int CS = NG >= 768 ? 8 : 16;          // strided-pass columns per CTA
     static constexpr int CX = NG >= 768 ? 4 : (NG >= 384 ? 8 : 16);  // fused x-pass columns
     static constexpr int ZSMEM = M * (L + 1) * 8;
-    // the 3-component C2R pass: L3 lines of each component per CTA
-    static constexpr int L3 = L >= 2 ? L / 2 : 1;
-    static constexpr int Z3SMEM = M * (3 * L3 + 1) * 8;
     static constexpr int SSMEM = NG * CS * 8;
     static constexpr int XSMEM = 2 * NG * CX * 8;
     // threads per CTA of the strided and fused x passes: 512 halves the
@@ -294,79 +291,6 @@ __global__ void __launch_bounds__(kThreads) zpass_c2r_kernel(const float2* __res
 }
 
 // ---------------------------------------------------------------------------
-// z pass, inverse C2R of the three force components at once, written
-// interleaved as float4 (x, y, z, 0) per cell so the particle kick gathers
-// a corner with one 16-byte load.  Component c's spectrum is in + c * in_cs;
-// blockIdx.y = slot.
-// ---------------------------------------------------------------------------
-template <int NG>
-__global__ void __launch_bounds__(kThreads, 4) zpass_c2r3_kernel(const float2* __restrict__ in, float4* __restrict__ out,
-                                                              int nlines, int zs, size_t in_cs, float scale,
-                                                              const float2* __restrict__ tw, Slots sl) {
-    // one tile of 3*L3 columns: component c's line l is column c*L3 + l, so
-    // a single set of FFT stages transforms all three components
-    constexpr int M = NG / 2, L3 = Cfg<NG>::L3, C3 = 3 * L3, ES = C3 + 1;
-    float2* buf = reinterpret_cast<float2*>(hgpm_smem);
-    const int slot = blockIdx.y;
-    if (slot_idle(sl, slot)) return;
-    in += (size_t)slot * sl.s0;
-    out += (size_t)slot * sl.s1;
-    const int line0 = blockIdx.x * L3;
-    constexpr int H = M / 2 + 1;
-    constexpr int TOT = L3 * H;
-    constexpr int PER = (TOT + kThreads - 1) / kThreads;
-#pragma unroll 1
-    for (int c = 0; c < 3; ++c) {
-        const float2* src0 = in + (size_t)c * in_cs;
-        float2 rk[PER], rm[PER];
-#pragma unroll
-        for (int t = 0; t < PER; ++t) {
-            const int i = threadIdx.x + t * kThreads;
-            const int l = i / H, k = i % H;
-            rk[t] = make_float2(0.f, 0.f);
-            rm[t] = make_float2(0.f, 0.f);
-            if (i < TOT && line0 + l < nlines) {
-                const float2* src = src0 + (size_t)(line0 + l) * zs;
-                rk[t] = __ldcs(&src[k]);
-                rm[t] = __ldcs(&src[M - k]);
-            }
-        }
-#pragma unroll
-        for (int t = 0; t < PER; ++t) {
-            const int i = threadIdx.x + t * kThreads;
-            if (i >= TOT) break;
-            const int l = c * L3 + i / H, k = i % H;
-            float2 xk = rk[t], xm = rm[t];
-            if (k == 0) {
-                xk.y = 0.f;
-                xm.y = 0.f;
-            }
-            const float2 w = __ldg(&tw[k]);
-            const float2 s = make_float2(xk.x + xm.x, xk.y - xm.y);
-            const float2 d = make_float2(xk.x - xm.x, xk.y + xm.y);
-            const float2 cd = cmulc(d, w);
-            const float2 tt = make_float2(-cd.y, cd.x);
-            buf[k * ES + l] = cadd(s, tt);
-            if (k != 0 && k != M - k) {
-                const float2 zm = csub(s, tt);
-                buf[(M - k) * ES + l] = make_float2(zm.x, -zm.y);
-            }
-        }
-    }
-    __syncthreads();
-    fft_tile<M, C3, ES, true, kThreads, 2>(buf, tw);
-    for (int i = threadIdx.x; i < L3 * M; i += kThreads) {
-        const int l = i / M, m = i % M;
-        const int line = line0 + l;
-        if (line >= nlines) continue;
-        const float2 a = buf[m * ES + l], b = buf[m * ES + L3 + l], c = buf[m * ES + 2 * L3 + l];
-        float4* dst = out + (size_t)line * NG + 2 * m;
-        __stcs(dst, make_float4(a.x * scale, b.x * scale, c.x * scale, 0.f));
-        __stcs(dst + 1, make_float4(a.y * scale, b.y * scale, c.y * scale, 0.f));
-    }
-}
-
-// ---------------------------------------------------------------------------
 // strided pass (y or x lines), in place,
 // blockIdx = (column chunk, plane, slot * ncomp + comp)
 // ---------------------------------------------------------------------------
@@ -413,12 +337,19 @@ __global__ void __launch_bounds__(Cfg<NG>::NTX) xfused_kernel(const float2* __re
     const int nvalid = ncols - col0;
     load_tile<NG, C, NT>(tile, in + off, rs, nvalid);
     __syncthreads();
-    // table twiddles throughout (as xpoisson_tma_kernel, whose register cap
+    // table twiddles throughout (as xpotential_tma_kernel, whose register cap
     // leaves no room for the product form): both x passes agree bit for bit
     fft_tile<NG, C, C, false, NT, 1, false>(tile, tw);
     for (int i = threadIdx.x; i < NG * C; i += NT) {
         const int ix = i / C, c = i % C;
         tile[i] = op.pre(ix, iy, col0 + c, tile[i]);
+    }
+    if (Op::kOut == 1) {
+        // one output: the inverse x transform of pre()'s result
+        __syncthreads();
+        fft_tile<NG, C, C, true, NT, 1, false>(tile, tw);
+        store_tile<NG, C, NT>(tile, out + off, rs, nvalid);
+        return;
     }
     // (fft_tile ended with a barrier; pre() only touches the thread's own cells)
     for (int i = threadIdx.x; i < NG * C; i += NT) {
@@ -430,58 +361,47 @@ __global__ void __launch_bounds__(Cfg<NG>::NTX) xfused_kernel(const float2* __re
     store_tile<NG, C, NT>(work, out + off, rs, nvalid);
     // (no thread writes tile between the barrier above and this transform)
     fft_tile<NG, C, C, true, NT, 1, false>(tile, tw);
-    if (Op::kTwoOut) {
-        // T itself; the inverse y pass applies the y and z factors
-        store_tile<NG, C, NT>(tile, out + out_cs + off, rs, nvalid);
-    } else {
-        store_tile_comp<NG, C, NT>(tile, out + out_cs + off, rs, nvalid, op, 1, iy, col0);
-        store_tile_comp<NG, C, NT>(tile, out + 2 * out_cs + off, rs, nvalid, op, 2, iy, col0);
-    }
+    store_tile_comp<NG, C, NT>(tile, out + out_cs + off, rs, nvalid, op, 1, iy, col0);
+    store_tile_comp<NG, C, NT>(tile, out + 2 * out_cs + off, rs, nvalid, op, 2, iy, col0);
 }
 
 // ---------------------------------------------------------------------------
-// Inverse y pass of the Poisson force spectra.  Part 0 is F_x, transformed in
-// place.  Part 1 holds T = IFFT_x(G rho_k) as the fused x pass leaves it; the
-// pass forms F_y = -i sin(k_y) T and F_z = -i sin(k_z) T (PoissonOp::comp's
-// factors and arithmetic, zero at the Nyquist index), transforms both and
-// writes F_y over part 1 and F_z to component 2: the same values as the
-// three-component pass over x-pass outputs F_x, F_y, F_z, with one spectrum
-// fewer written by the x pass and read here.
-// blockIdx = (column chunk, plane, slot * 2 + part).
+// Force grid from the potential phi (real, [ng][ng][ng], z fastest):
+// F_d(x) = (phi(x - e_d) - phi(x + e_d)) / 2, periodic, written as float4
+// (F_x, F_y, F_z, 0) per cell.  With the unnormalised transforms used here
+// this is exactly the reference's -i sin(k_d) G rho_k followed by the inverse
+// FFT (kspace_solver.cu:55-90, solver.cpp:144-170): the central difference
+// multiplies mode k by -i sin(2 pi k_d / ng), it is real, so it commutes with
+// taking the real part, and it annihilates the Nyquist mode of its own axis
+// as the reference's real part does.  A thread makes 4 z-consecutive cells
+// (one float4 of phi and its 6 neighbours, 4 float4 out); blockIdx.y = slot.
 // ---------------------------------------------------------------------------
-template <int NG>
-__global__ void __launch_bounds__(Cfg<NG>::NTS, 1) strided_inv2_kernel(float2* __restrict__ data, int ncols,
-                                                                    size_t rs, size_t ps, size_t cs,
-                                                                    const float2* __restrict__ tw,
-                                                                    const float* __restrict__ sk, Slots sl) {
-    constexpr int C = Cfg<NG>::CS, NT = Cfg<NG>::NTS, nyq = NG / 2;
-    float2* tile = reinterpret_cast<float2*>(hgpm_smem);
-    float2* work = tile + NG * C;
-    const int slot = blockIdx.z / 2, part = blockIdx.z % 2;
-    if (slot_idle(sl, slot)) return;
-    const int col0 = blockIdx.x * C;
-    float2* g = data + (size_t)slot * sl.s0 + (size_t)part * cs + (size_t)blockIdx.y * ps + col0;
-    const int nvalid = ncols - col0;
-    load_tile<NG, C, NT>(tile, g, rs, nvalid);
-    __syncthreads();
-    if (part == 0) {
-        fft_tile<NG, C, C, true, NT>(tile, tw);
-        store_tile<NG, C, NT>(tile, g, rs, nvalid);
-        return;
-    }
-    for (int i = threadIdx.x; i < NG * C; i += NT) {
-        const int e = i / C, iz = col0 + i % C;  // e: the y wavenumber index
-        const float2 v = tile[i];
-        const float sy = e == nyq ? 0.f : __ldg(&sk[e]);
-        const float sz = iz == nyq ? 0.f : __ldg(&sk[iz < NG ? iz : 0]);
-        work[i] = make_float2(sy * v.y, -sy * v.x);
-        tile[i] = make_float2(sz * v.y, -sz * v.x);
-    }
-    __syncthreads();
-    fft_tile<NG, C, C, true, NT>(work, tw);
-    store_tile<NG, C, NT>(work, g, rs, nvalid);
-    fft_tile<NG, C, C, true, NT>(tile, tw);
-    store_tile<NG, C, NT>(tile, g + cs, rs, nvalid);
+__global__ void __launch_bounds__(256) gradient_kernel(const float* __restrict__ phi, float4* __restrict__ f, int ng,
+                                                       Slots sl) {
+    if (slot_idle(sl, blockIdx.y)) return;
+    phi += (size_t)blockIdx.y * sl.s0;
+    f += (size_t)blockIdx.y * sl.s1;
+    const int nq = ng / 4;
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (size_t)ng * ng * nq) return;
+    const int z0 = (int)(q % nq) * 4;
+    const int row = (int)(q / nq);
+    const int y = row % ng, x = row / ng;
+    const int xm = x == 0 ? ng - 1 : x - 1, xp = x + 1 == ng ? 0 : x + 1;
+    const int ym = y == 0 ? ng - 1 : y - 1, yp = y + 1 == ng ? 0 : y + 1;
+    const size_t base = (size_t)row * ng;
+    const float4 c = __ldg(reinterpret_cast<const float4*>(phi + base + z0));
+    const float zm = __ldg(phi + base + (z0 == 0 ? ng - 1 : z0 - 1));
+    const float zp = __ldg(phi + base + (z0 + 4 == ng ? 0 : z0 + 4));
+    const float4 a = __ldg(reinterpret_cast<const float4*>(phi + ((size_t)xm * ng + y) * ng + z0));
+    const float4 b = __ldg(reinterpret_cast<const float4*>(phi + ((size_t)xp * ng + y) * ng + z0));
+    const float4 d = __ldg(reinterpret_cast<const float4*>(phi + ((size_t)x * ng + ym) * ng + z0));
+    const float4 e = __ldg(reinterpret_cast<const float4*>(phi + ((size_t)x * ng + yp) * ng + z0));
+    float4* o = f + base + z0;
+    __stcs(o + 0, make_float4(0.5f * (a.x - b.x), 0.5f * (d.x - e.x), 0.5f * (zm - c.y), 0.f));
+    __stcs(o + 1, make_float4(0.5f * (a.y - b.y), 0.5f * (d.y - e.y), 0.5f * (c.x - c.z), 0.f));
+    __stcs(o + 2, make_float4(0.5f * (a.z - b.z), 0.5f * (d.z - e.z), 0.5f * (c.y - c.w), 0.f));
+    __stcs(o + 3, make_float4(0.5f * (a.w - b.w), 0.5f * (d.w - e.w), 0.5f * (c.z - zp), 0.f));
 }
 
 // ---------------------------------------------------------------------------
@@ -633,18 +553,6 @@ static cudaError_t zinv_impl(const float2* in, float* out, int nlines, int zs, s
 }
 
 template <int NG>
-static cudaError_t zinv3_impl(const float2* in, float4* out, int nlines, int zs, size_t in_cs, float scale,
-                              const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
-    using G = Cfg<NG>;
-    auto k = zpass_c2r3_kernel<NG>;
-    cudaError_t e = ensure_smem(k, G::Z3SMEM);
-    if (e != cudaSuccess) return e;
-    dim3 grid(cdiv(nlines, G::L3), nslots);
-    k<<<grid, kThreads, G::Z3SMEM, s>>>(in, out, nlines, zs, in_cs, scale, tw, sl);
-    return cudaGetLastError();
-}
-
-template <int NG>
 static cudaError_t strided_impl(bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
                                 int ncomp, const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
     using G = Cfg<NG>;
@@ -660,18 +568,6 @@ static cudaError_t strided_impl(bool inv, float2* data, int ncols, size_t rs, si
         if (e != cudaSuccess) return e;
         k<<<grid, G::NTS, G::SSMEM, s>>>(data, ncols, rs, ps, cs, tw, ncomp, sl);
     }
-    return cudaGetLastError();
-}
-
-template <int NG>
-static cudaError_t strided_inv2_impl(float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
-                                     const float2* tw, const float* sk, cudaStream_t s, const Slots& sl, int nslots) {
-    using G = Cfg<NG>;
-    auto k = strided_inv2_kernel<NG>;
-    cudaError_t e = ensure_smem(k, 2 * G::SSMEM);
-    if (e != cudaSuccess) return e;
-    dim3 grid(cdiv(ncols, G::CS), nplanes, 2 * nslots);
-    k<<<grid, G::NTS, 2 * G::SSMEM, s>>>(data, ncols, rs, ps, cs, tw, sk, sl);
     return cudaGetLastError();
 }
 
@@ -741,17 +637,6 @@ cudaError_t launch_zinv(int ng, const float2* in, float* out, int nlines, int zs
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_zinv3(int ng, const float2* in, float4* out, int nlines, int zs, size_t in_cs, float scale,
-                         const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
-    switch (ng) {
-#define X(n) \
-    case n: return zinv3_impl<n>(in, out, nlines, zs, in_cs, scale, tw, s, sl, nslots);
-        HGPM_SIZES(X)
-#undef X
-    }
-    return cudaErrorInvalidValue;
-}
-
 cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
                            int ncomp, const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
     switch (ng) {
@@ -763,24 +648,20 @@ cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs,
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_yinv2(int ng, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
-                         const float2* tw, const float* sk, cudaStream_t s, const Slots& sl, int nslots) {
-    switch (ng) {
-#define X(n) \
-    case n: return strided_inv2_impl<n>(data, ncols, rs, ps, nplanes, cs, tw, sk, s, sl, nslots);
-        HGPM_SIZES(X)
-#undef X
-    }
-    return cudaErrorInvalidValue;
+cudaError_t launch_gradient(int ng, const float* phi, float4* f, cudaStream_t s, const Slots& sl, int nslots) {
+    if (!fft_size_supported(ng)) return cudaErrorInvalidValue;
+    const size_t nq = (size_t)ng * ng * (ng / 4);
+    gradient_kernel<<<dim3(cdiv(nq, 256), nslots), 256, 0, s>>>(phi, f, ng, sl);
+    return cudaGetLastError();
 }
 
-cudaError_t launch_xpoisson(int ng, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
-                            size_t out_cs, const float2* tw, const double* cosq, const float* sk, double coeff,
-                            cudaStream_t s, const Slots& sl, int nslots) {
-    PoissonOp op{cosq, sk, coeff, ng / 2};
+cudaError_t launch_xpotential(int ng, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
+                              const float2* tw, const double* cosq, double coeff, cudaStream_t s, const Slots& sl,
+                              int nslots) {
+    PotentialOp op{cosq, coeff};
     switch (ng) {
 #define X(n) \
-    case n: return xfused_impl<n, PoissonOp>(in, out, ncols, rs, ps, nplanes, out_cs, tw, op, s, sl, nslots);
+    case n: return xfused_impl<n, PotentialOp>(in, out, ncols, rs, ps, nplanes, 0, tw, op, s, sl, nslots);
         HGPM_SIZES(X)
 #undef X
     }

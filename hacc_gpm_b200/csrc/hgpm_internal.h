@@ -37,21 +37,17 @@ cudaError_t launch_zfwd(int ng, void* in, bool fixed, float2* out, int nlines, i
 cudaError_t launch_zinv(int ng, const float2* in, float* out, int nlines, int zs, size_t in_cs, size_t out_cs,
                         int ncomp, float scale, const float2* tw, cudaStream_t s, const Slots& sl = Slots{},
                         int nslots = 1);
-// C2R of the 3 force components into one float4 (x, y, z, 0) grid.
-cudaError_t launch_zinv3(int ng, const float2* in, float4* out, int nlines, int zs, size_t in_cs, float scale,
-                         const float2* tw, cudaStream_t s, const Slots& sl = Slots{}, int nslots = 1);
 cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
                            int ncomp, const float2* tw, cudaStream_t s, const Slots& sl = Slots{}, int nslots = 1);
-// x pass fused with the Green's function and gradient: writes F_x (component
-// 0) and T = IFFT_x(G rho_k) (component 1); launch_yinv2 completes F_y, F_z.
-cudaError_t launch_xpoisson(int ng, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
-                            size_t out_cs, const float2* tw, const double* cosq, const float* sk, double coeff,
-                            cudaStream_t s, const Slots& sl = Slots{}, int nslots = 1);
-// Inverse y pass of the force spectra from the x pass's (F_x, T) into
-// (F_x, F_y, F_z) (components at data + c * cs).
-cudaError_t launch_yinv2(int ng, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
-                         const float2* tw, const float* sk, cudaStream_t s, const Slots& sl = Slots{},
-                         int nslots = 1);
+// x pass fused with the Green's function: the potential's spectrum
+// G rho_k, transformed back along x, into out (one half-spectrum buffer).
+cudaError_t launch_xpotential(int ng, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
+                              const float2* tw, const double* cosq, double coeff, cudaStream_t s,
+                              const Slots& sl = Slots{}, int nslots = 1);
+// Force grid (F_x, F_y, F_z, 0) from the real potential by central
+// differences (the reference's -i sin(k) gradient, applied in real space).
+cudaError_t launch_gradient(int ng, const float* phi, float4* f, cudaStream_t s, const Slots& sl = Slots{},
+                            int nslots = 1);
 cudaError_t launch_xic(int n, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
                        size_t out_cs, const float2* tw, const double* table, int nbins, double k_delta,
                        double pkscale, double inv_delta, const float* kf, int* err, cudaStream_t s);
@@ -63,13 +59,9 @@ cudaError_t launch_xpk(int ng, const float2* in, int ncols, size_t rs, size_t ps
 // lines when isx); err is set if a bounded mbarrier wait times out.
 cudaError_t launch_strided_tma(int ng, bool inv, bool isx, float2* data, int ncols, int zs, size_t cs, int ncomp,
                                const float2* tw, int* err, cudaStream_t s);
-// TMA-fed launch_yinv2 (single box).
-cudaError_t launch_yinv2_tma(int ng, float2* data, int ncols, int zs, size_t cs, const float2* tw, const float* sk,
-                             int* err, cudaStream_t s);
-// Persistent TMA-fed x pass fused with the Green's function and gradient
-// (writes F_x and T, as launch_xpoisson).
-cudaError_t launch_xpoisson_tma(int ng, float2* in, float2* out, int ncols, int zs, size_t out_cs, const float2* tw,
-                                const double* cosq, const float* sk, double coeff, int* err, cudaStream_t s);
+// Persistent TMA-fed launch_xpotential (single box).
+cudaError_t launch_xpotential_tma(int ng, float2* in, float2* out, int ncols, int zs, const float2* tw,
+                                  const double* cosq, double coeff, int* err, cudaStream_t s);
 
 cudaError_t launch_load_state(const float* x, const float* v, const ParticleSoA& p, int np_side, int B, int ng,
                               cudaStream_t s);

@@ -10,34 +10,25 @@ namespace hgpm {
 // ---------------------------------------------------------------------------
 // k-space operators
 // ---------------------------------------------------------------------------
-// Poisson + gradient, kspace_solve_gradient (kspace_solver.cu:55-90) with
-// calcGreens (calcGreens.hpp:11-25): t = G rho_k, F_d = -i sin(k_d) t.
-// cosq[i] = cos(k_i) - 1 (double) and sk[i] = sin(k_i) are tabulated once per
-// grid side; G is formed in double from the sum of the (non-positive) cosq
-// terms, so there is no cancellation near k = 0.
-// A derivative along d at the Nyquist index of d is anti-Hermitian in the
-// reference's full C2C (both partners carry the same signed k = -n/2), so its
-// real part — all the reference keeps — is exactly zero; the half-spectrum
-// C2R would instead Hermitian-extend it.  comp() therefore returns 0 there.
-struct PoissonOp {
-    // the x pass stores F_x and T = IFFT_x(t) only; the inverse y pass forms
-    // F_y and F_z from T (comp(1), comp(2) factors are constant along x)
-    static constexpr bool kTwoOut = true;
+// Green's function of calcGreens (calcGreens.hpp:11-25): the x pass forms
+// the potential's spectrum t = G rho_k and transforms it back along x (one
+// output).  cosq[i] = cos(k_i) - 1 (double) is tabulated once per grid side;
+// G is formed in double from the sum of the (non-positive) cosq terms, so
+// there is no cancellation near k = 0.  The gradient of kspace_solve_gradient
+// (kspace_solver.cu:55-90), -i sin(k_d) t, is applied in real space after
+// the inverse transform (gradient_kernel: the central difference
+// (phi(x - e_d) - phi(x + e_d)) / 2 multiplies mode k by exactly
+// -i sin(2 pi k_d / ng)).
+struct PotentialOp {
+    static constexpr int kOut = 1;
     const double* cosq;  // cos(k_i) - 1, one entry per grid index
-    const float* sk;     // sin(k_i)
     double coeff;        // 0.5 / ng^3
-    int nyq;             // ng / 2
     __device__ __forceinline__ float2 pre(int ix, int iy, int iz, float2 v) const {
         const double s = __ldg(&cosq[ix]) + __ldg(&cosq[iy]) + __ldg(&cosq[iz]);
         const float g = (s == 0.0) ? 0.f : (float)(coeff / s);
         return make_float2(v.x * g, v.y * g);
     }
-    __device__ __forceinline__ float2 comp(int d, int ix, int iy, int iz, float2 t) const {
-        const int id = d == 0 ? ix : (d == 1 ? iy : iz);
-        if (id == nyq) return make_float2(0.f, 0.f);
-        const float sd = __ldg(&sk[id]);
-        return make_float2(sd * t.y, -sd * t.x);
-    }
+    __device__ __forceinline__ float2 comp(int, int, int, int, float2 t) const { return t; }
 };
 
 // Zel'dovich displacement (initializer.cpp:10-117): ScaleAmplitudes by
@@ -45,7 +36,7 @@ struct PoissonOp {
 // then transformDensityField (transform_density_field_initializer.cu:72-112):
 // s_d = (Im k_d, -Re k_d) / (k^2 delta).
 struct ICOp {
-    static constexpr bool kTwoOut = false;  // the x pass stores all three components
+    static constexpr int kOut = 3;  // the x pass stores all three components
     const double* table;
     int nbins;
     double k_delta;

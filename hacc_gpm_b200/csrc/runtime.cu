@@ -625,29 +625,32 @@ extern "C" int hgpm_solve_gradient(hgpm_ctx* c) {
     const size_t cs = (size_t)ng * ng * c->zs;
     {
         PhaseScope ps(c, PH_POISSON);
+        const double coeff = 0.5 / ((double)ng * ng * ng);
         if (c->xtma)
-            CK(launch_xpoisson_tma(ng, c->spec, c->fspec, M + 1, c->zs, cs, c->tw_ng, c->cosq, c->sk,
-                                   0.5 / ((double)ng * ng * ng), c->d_err + 1, c->stream));
+            CK(launch_xpotential_tma(ng, c->spec, c->fspec, M + 1, c->zs, c->tw_ng, c->cosq, coeff, c->d_err + 1,
+                                     c->stream));
         else
-            CK(launch_xpoisson(ng, c->spec, c->fspec, M + 1, (size_t)ng * c->zs, (size_t)c->zs, ng, cs, c->tw_ng,
-                               c->cosq, c->sk, 0.5 / ((double)ng * ng * ng), c->stream));
+            CK(launch_xpotential(ng, c->spec, c->fspec, M + 1, (size_t)ng * c->zs, (size_t)c->zs, ng, c->tw_ng,
+                                 c->cosq, coeff, c->stream));
         count(c, PH_POISSON, 1);
     }
     {
         PhaseScope ps(c, PH_YINV);
-        // (F_x, T) from the x pass -> (F_x, F_y, F_z)
         if (c->tma)
-            CK(launch_yinv2_tma(ng, c->fspec, M + 1, c->zs, cs, c->tw_ng, c->sk, c->d_err + 1, c->stream));
+            CK(launch_strided_tma(ng, true, false, c->fspec, M + 1, c->zs, 0, 1, c->tw_ng, c->d_err + 1, c->stream));
         else
-            CK(launch_yinv2(ng, c->fspec, M + 1, (size_t)c->zs, (size_t)ng * c->zs, ng, cs, c->tw_ng, c->sk,
-                            c->stream));
+            CK(launch_strided(ng, true, c->fspec, M + 1, (size_t)c->zs, (size_t)ng * c->zs, ng, 0, 1, c->tw_ng,
+                              c->stream));
         count(c, PH_YINV, 1);
     }
     {
+        // the real potential (in the space of the second force spectrum), then
+        // the force grid by central differences
         PhaseScope ps(c, PH_ZINV);
-        CK(launch_zinv3(ng, c->fspec, reinterpret_cast<float4*>(c->force), ng * ng, c->zs, cs, 1.0f, c->tw_ng,
-                        c->stream));
-        count(c, PH_ZINV, 1);
+        float* phi = reinterpret_cast<float*>(c->fspec + cs);
+        CK(launch_zinv(ng, c->fspec, phi, ng * ng, c->zs, 0, 0, 1, 1.0f, c->tw_ng, c->stream));
+        CK(launch_gradient(ng, phi, reinterpret_cast<float4*>(c->force), c->stream));
+        count(c, PH_ZINV, 2);
     }
     return HGPM_OK;
 }

@@ -107,11 +107,11 @@ __global__ void __launch_bounds__(kTmaThreads, 2) strided_tma_kernel(const __gri
 }
 
 // ---------------------------------------------------------------------------
-// x pass fused with a k-space operator (Poisson gradient), persistent and
-// TMA-fed: the next x-line tile (all kx of one ky, CT kz columns) streams in
-// while the current one is transformed forward, multiplied by the operator and
-// transformed back three times; the three results leave with coalesced
-// streaming stores.
+// x pass fused with the Green's function, persistent and TMA-fed: the next
+// x-line tile (all kx of one ky, CT kz columns) streams in while the current
+// one is transformed forward, multiplied by G (calcGreens.hpp:11-25, as
+// PotentialOp::pre) and transformed back; the potential's x-inverted spectrum
+// leaves with coalesced streaming stores.
 template <int NG, int CT, int NT>
 __device__ __forceinline__ void store_rows(const float2* __restrict__ tile, float2* __restrict__ g, size_t rs,
                                            int nvalid) {
@@ -128,29 +128,22 @@ __device__ __forceinline__ void store_rows(const float2* __restrict__ tile, floa
 }
 
 template <int NG, int NT>
-__global__ void __launch_bounds__(NT, 1024 / NT) xpoisson_tma_kernel(const __grid_constant__ CUtensorMap tm,
-                                                                     float2* __restrict__ out, size_t out_cs,
-                                                                     int ncols, int zs, int nchunks,
-                                                                     const float2* __restrict__ tw,
-                                                                     const double* __restrict__ cosq_g,
-                                                                     const float* __restrict__ sk_g, double coeff,
-                                                                     int* __restrict__ err) {
+__global__ void __launch_bounds__(NT, 1024 / NT) xpotential_tma_kernel(const __grid_constant__ CUtensorMap tm,
+                                                                       float2* __restrict__ out, int ncols, int zs,
+                                                                       int nchunks, const float2* __restrict__ tw,
+                                                                       const double* __restrict__ cosq_g,
+                                                                       double coeff, int* __restrict__ err) {
     using G = TmaCfg<NG>;
     constexpr int CT = G::CT;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* base =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     float2* in[2] = {reinterpret_cast<float2*>(base), reinterpret_cast<float2*>(base + G::TILE_BYTES)};
-    float2* work = reinterpret_cast<float2*>(base + 2 * G::TILE_BYTES);
-    double* cosq = reinterpret_cast<double*>(base + 3 * G::TILE_BYTES);
-    float* sk = reinterpret_cast<float*>(cosq + NG);
+    double* cosq = reinterpret_cast<double*>(base + 2 * G::TILE_BYTES);
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ int failed;
     const int ntiles = nchunks * NG;
-    for (int i = threadIdx.x; i < NG; i += NT) {
-        cosq[i] = cosq_g[i];
-        sk[i] = sk_g[i];
-    }
+    for (int i = threadIdx.x; i < NG; i += NT) cosq[i] = cosq_g[i];
     if (threadIdx.x == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
@@ -163,7 +156,6 @@ __global__ void __launch_bounds__(NT, 1024 / NT) xpoisson_tma_kernel(const __gri
     int j = 0;
     bool next_in_flight = false;
     const size_t rs = (size_t)NG * zs;
-    constexpr int nyq = NG / 2;
     for (; t < ntiles; t += gridDim.x, ++j) {
         const int cur = j & 1;
         const int tn = t + gridDim.x;
@@ -181,7 +173,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) xpoisson_tma_kernel(const __gri
         const int iy = ti.plane, col0 = ti.chunk * CT;
         float2* tile = in[cur];
         fft_tile<NG, CT, CT, false, NT, 1, false>(tile, tw);
-        // t = G rho_k (PoissonOp::pre with the tables in shared memory)
+        // t = G rho_k (PotentialOp::pre with the table in shared memory)
         const double cy = cosq[iy];
         for (int i = threadIdx.x; i < NG * CT; i += NT) {
             const int ix = i / CT, iz = col0 + i % CT;
@@ -194,21 +186,11 @@ __global__ void __launch_bounds__(NT, 1024 / NT) xpoisson_tma_kernel(const __gri
             }
             tile[i] = v;
         }
-        float2* gout = out + (size_t)iy * zs + col0;
-        // F_x = -i sin(k_x) t, zero at the x Nyquist index (PoissonOp::comp)
-        for (int i = threadIdx.x; i < NG * CT; i += NT) {
-            const int ix = i / CT, iz = col0 + i % CT;
-            const float sd = (ix == nyq || iz >= ncols) ? 0.f : sk[ix];
-            const float2 tv = tile[i];
-            work[i] = make_float2(sd * tv.y, -sd * tv.x);
-        }
         __syncthreads();
-        fft_tile<NG, CT, CT, true, NT, 1, false>(work, tw);
-        store_rows<NG, CT, NT>(work, gout, rs, ncols - col0);
-        // T = IFFT_x(t) to component 1: F_y and F_z are T times factors
-        // constant along x, applied by the inverse y pass (yinv2_tma_kernel)
+        // the potential's inverse x transform; the gradient is taken in real
+        // space (gradient_kernel)
         fft_tile<NG, CT, CT, true, NT, 1, false>(tile, tw);
-        store_rows<NG, CT, NT>(tile, gout + out_cs, rs, ncols - col0);
+        store_rows<NG, CT, NT>(tile, out + (size_t)iy * zs + col0, rs, ncols - col0);
         // the next TMA load into this buffer follows generic-proxy writes
         fence_async_shared();
         __syncthreads();
@@ -219,93 +201,6 @@ __global__ void __launch_bounds__(NT, 1024 / NT) xpoisson_tma_kernel(const __gri
             mbar_wait_bounded(&bar[j & 1], (j >> 1) & 1);
             if (next_in_flight) mbar_wait_bounded(&bar[(j + 1) & 1], ((j + 1) >> 1) & 1);
         }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Inverse y pass of the force spectra, persistent and TMA-fed (the TMA form
-// of strided_inv2_kernel): tiles t = (column chunk, x plane, part); part 0 is
-// F_x, transformed in place; part 1 is T, from which F_y = -i sin(k_y) T and
-// F_z = -i sin(k_z) T are formed in shared memory (PoissonOp::comp's factors,
-// zero at the Nyquist index), transformed, and stored to components 1 and 2.
-template <int NG>
-__global__ void __launch_bounds__(kTmaThreads, 2) yinv2_tma_kernel(const __grid_constant__ CUtensorMap tm, int nchunks,
-                                                                int nplanes, const float2* __restrict__ tw,
-                                                                const float* __restrict__ sk_g, int* __restrict__ err) {
-    using G = TmaCfg<NG>;
-    constexpr int CT = G::CT, nyq = NG / 2;
-    extern __shared__ unsigned char smem_raw[];
-    unsigned char* base =
-        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    float2* buf[2] = {reinterpret_cast<float2*>(base), reinterpret_cast<float2*>(base + G::TILE_BYTES)};
-    float2* work = reinterpret_cast<float2*>(base + 2 * G::TILE_BYTES);
-    float* sk = reinterpret_cast<float*>(base + 3 * G::TILE_BYTES);
-    __shared__ __align__(8) uint64_t bar[2];
-    __shared__ int failed;
-    const int ntiles = nchunks * nplanes * 2;
-    for (int i = threadIdx.x; i < NG; i += kTmaThreads) sk[i] = sk_g[i];
-    if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        failed = 0;
-        fence_async_shared();
-    }
-    __syncthreads();
-    int t = blockIdx.x;
-    if (threadIdx.x == 0 && t < ntiles) issue_tile_load<NG, false>(&tm, buf[0], &bar[0], tile_of(t, nchunks, nplanes));
-    int j = 0;
-    bool next_in_flight = false;
-    for (; t < ntiles; t += gridDim.x, ++j) {
-        const int cur = j & 1;
-        const int tn = t + gridDim.x;
-        if (threadIdx.x == 0) {
-            next_in_flight = false;
-            // every earlier store has finished reading its buffer (the other
-            // input buffer and the work tile)
-            bulk_wait_read_all();
-            if (tn < ntiles) {
-                issue_tile_load<NG, false>(&tm, buf[cur ^ 1], &bar[cur ^ 1], tile_of(tn, nchunks, nplanes));
-                next_in_flight = true;
-            }
-            if (!mbar_wait_bounded(&bar[cur], (j >> 1) & 1)) failed = 1;
-        }
-        __syncthreads();
-        if (failed) break;
-        const TileIdx ti = tile_of(t, nchunks, nplanes);
-        float2* tile = buf[cur];
-        if (ti.comp == 0) {
-            fft_tile<NG, CT, CT, true, kTmaThreads>(tile, tw);
-            fence_async_shared();
-            __syncthreads();
-            if (threadIdx.x == 0) issue_tile_store<NG, false>(&tm, tile, ti);
-            continue;
-        }
-        const int col0 = ti.chunk * CT;
-        for (int i = threadIdx.x; i < NG * CT; i += kTmaThreads) {
-            const int e = i / CT, iz = col0 + i % CT;  // e: the y wavenumber index
-            const float2 v = tile[i];
-            const float sy = e == nyq ? 0.f : sk[e];
-            const float sz = iz == nyq ? 0.f : sk[iz < NG ? iz : 0];
-            work[i] = make_float2(sy * v.y, -sy * v.x);
-            tile[i] = make_float2(sz * v.y, -sz * v.x);
-        }
-        __syncthreads();
-        fft_tile<NG, CT, CT, true, kTmaThreads>(work, tw);
-        fft_tile<NG, CT, CT, true, kTmaThreads>(tile, tw);
-        fence_async_shared();
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            issue_tile_store<NG, false>(&tm, work, TileIdx{ti.chunk, ti.plane, 1});
-            issue_tile_store<NG, false>(&tm, tile, TileIdx{ti.chunk, ti.plane, 2});
-        }
-    }
-    if (threadIdx.x == 0) {
-        if (failed) {
-            atomicExch(err, 1);
-            mbar_wait_bounded(&bar[j & 1], (j >> 1) & 1);
-            if (next_in_flight) mbar_wait_bounded(&bar[(j + 1) & 1], ((j + 1) >> 1) & 1);
-        }
-        bulk_wait_all();
     }
 }
 
@@ -374,8 +269,8 @@ static cudaError_t tma_impl(bool inv, bool isx, float2* data, int ncols, int zs,
 }
 
 template <int NG>
-static cudaError_t xpoisson_tma_impl(float2* in, float2* out, int ncols, int zs, size_t out_cs, const float2* tw,
-                                     const double* cosq, const float* sk, double coeff, int* err, cudaStream_t s) {
+static cudaError_t xpotential_tma_impl(float2* in, float2* out, int ncols, int zs, const float2* tw,
+                                       const double* cosq, double coeff, int* err, cudaStream_t s) {
     using G = TmaCfg<NG>;
     constexpr int NT = NG >= 128 ? 512 : 256;
     CUtensorMap tm;
@@ -386,58 +281,23 @@ static cudaError_t xpoisson_tma_impl(float2* in, float2* out, int ncols, int zs,
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
     }
-    constexpr int SMEM = 3 * G::TILE_BYTES + NG * 12 + 1024;
+    constexpr int SMEM = 2 * G::TILE_BYTES + NG * 8 + 1024;
     const int nchunks = (ncols + G::CT - 1) / G::CT;
     const int ntiles = nchunks * NG;
-    auto k = xpoisson_tma_kernel<NG, NT>;
+    auto k = xpotential_tma_kernel<NG, NT>;
     e = smem_attr_once((const void*)k, SMEM);
     if (e != cudaSuccess) return e;
     int grid = g_num_sms * blocks_per_sm_once((const void*)k, NT, SMEM);
     if (grid > ntiles) grid = ntiles;
-    k<<<grid, NT, SMEM, s>>>(tm, out, out_cs, ncols, zs, nchunks, tw, cosq, sk, coeff, err);
+    k<<<grid, NT, SMEM, s>>>(tm, out, ncols, zs, nchunks, tw, cosq, coeff, err);
     return cudaGetLastError();
 }
 
-template <int NG>
-static cudaError_t yinv2_tma_impl(float2* data, int ncols, int zs, size_t cs, const float2* tw, const float* sk,
-                                  int* err, cudaStream_t s) {
-    using G = TmaCfg<NG>;
-    CUtensorMap tm;
-    cudaError_t e = make_spec_map(&tm, data, NG, ncols, zs, cs, 3, G::CT, G::RB, false);
-    if (e != cudaSuccess) return e;
-    if (!g_num_sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    }
-    constexpr int SMEM = 3 * G::TILE_BYTES + NG * 4 + 1024;
-    const int nchunks = (ncols + G::CT - 1) / G::CT;
-    const int ntiles = nchunks * NG * 2;
-    auto k = yinv2_tma_kernel<NG>;
-    e = smem_attr_once((const void*)k, SMEM);
-    if (e != cudaSuccess) return e;
-    int grid = g_num_sms * blocks_per_sm_once((const void*)k, kTmaThreads, SMEM);
-    if (grid > ntiles) grid = ntiles;
-    k<<<grid, kTmaThreads, SMEM, s>>>(tm, nchunks, NG, tw, sk, err);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_yinv2_tma(int ng, float2* data, int ncols, int zs, size_t cs, const float2* tw, const float* sk,
-                             int* err, cudaStream_t s) {
+cudaError_t launch_xpotential_tma(int ng, float2* in, float2* out, int ncols, int zs, const float2* tw,
+                                  const double* cosq, double coeff, int* err, cudaStream_t s) {
     switch (ng) {
 #define X(n) \
-    case n: return yinv2_tma_impl<n>(data, ncols, zs, cs, tw, sk, err, s);
-        X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
-#undef X
-    }
-    return cudaErrorInvalidValue;
-}
-
-cudaError_t launch_xpoisson_tma(int ng, float2* in, float2* out, int ncols, int zs, size_t out_cs, const float2* tw,
-                                const double* cosq, const float* sk, double coeff, int* err, cudaStream_t s) {
-    switch (ng) {
-#define X(n) \
-    case n: return xpoisson_tma_impl<n>(in, out, ncols, zs, out_cs, tw, cosq, sk, coeff, err, s);
+    case n: return xpotential_tma_impl<n>(in, out, ncols, zs, tw, cosq, coeff, err, s);
         X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
 #undef X
     }
