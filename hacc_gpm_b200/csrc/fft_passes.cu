@@ -373,37 +373,61 @@ __global__ void __launch_bounds__(Cfg<NG>::NTX) xfused_kernel(const float2* __re
 // FFT (kspace_solver.cu:55-90, solver.cpp:144-170): the central difference
 // multiplies mode k by -i sin(2 pi k_d / ng), it is real, so it commutes with
 // taking the real part, and it annihilates the Nyquist mode of its own axis
-// as the reference's real part does.  A thread makes 4 z-consecutive cells
-// (one float4 of phi and its 6 neighbours, 4 float4 out); blockIdx.y = slot.
+// as the reference's real part does.  blockIdx.y = slot.
 // ---------------------------------------------------------------------------
+// 256-bit (8 x f32) global accesses, sm_100: 32-byte aligned addresses.
+struct F8 {
+    float v[8];
+};
+__device__ __forceinline__ F8 ldg8(const float* p) {
+    F8 r;
+    asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]), "=f"(r.v[5]), "=f"(r.v[6]),
+                   "=f"(r.v[7])
+                 : "l"(p));
+    return r;
+}
+// two float4 cells, streaming (evict-first)
+__device__ __forceinline__ void stcs8(float4* p, float4 a, float4 b) {
+    asm volatile("st.global.cs.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(a.x), "f"(a.y), "f"(a.z),
+                 "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w)
+                 : "memory");
+}
+
 __global__ void __launch_bounds__(256) gradient_kernel(const float* __restrict__ phi, float4* __restrict__ f, int ng,
                                                        Slots sl) {
     if (slot_idle(sl, blockIdx.y)) return;
     phi += (size_t)blockIdx.y * sl.s0;
     f += (size_t)blockIdx.y * sl.s1;
-    const int nq = ng / 4;
+    // a thread makes 8 z-consecutive cells: 256-bit loads of phi and of its
+    // x and y neighbours, 256-bit stores of two cells each (whole sectors)
+    const int n8 = ng / 8;
     const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= (size_t)ng * ng * nq) return;
-    const int z0 = (int)(q % nq) * 4;
-    const int row = (int)(q / nq);
+    if (q >= (size_t)ng * ng * n8) return;
+    const int z0 = (int)(q % n8) * 8;
+    const int row = (int)(q / n8);
     const int y = row % ng, x = row / ng;
     const int xm = x == 0 ? ng - 1 : x - 1, xp = x + 1 == ng ? 0 : x + 1;
     const int ym = y == 0 ? ng - 1 : y - 1, yp = y + 1 == ng ? 0 : y + 1;
     const size_t base = (size_t)row * ng;
-    const float4 c = __ldg(reinterpret_cast<const float4*>(phi + base + z0));
+    const F8 c = ldg8(phi + base + z0);
     const float zm = __ldg(phi + base + (z0 == 0 ? ng - 1 : z0 - 1));
-    const float zp = __ldg(phi + base + (z0 + 4 == ng ? 0 : z0 + 4));
-    const float4 a = __ldg(reinterpret_cast<const float4*>(phi + ((size_t)xm * ng + y) * ng + z0));
-    const float4 b = __ldg(reinterpret_cast<const float4*>(phi + ((size_t)xp * ng + y) * ng + z0));
-    const float4 d = __ldg(reinterpret_cast<const float4*>(phi + ((size_t)x * ng + ym) * ng + z0));
-    const float4 e = __ldg(reinterpret_cast<const float4*>(phi + ((size_t)x * ng + yp) * ng + z0));
-    float4* o = f + base + z0;
-    __stcs(o + 0, make_float4(0.5f * (a.x - b.x), 0.5f * (d.x - e.x), 0.5f * (zm - c.y), 0.f));
-    __stcs(o + 1, make_float4(0.5f * (a.y - b.y), 0.5f * (d.y - e.y), 0.5f * (c.x - c.z), 0.f));
-    __stcs(o + 2, make_float4(0.5f * (a.z - b.z), 0.5f * (d.z - e.z), 0.5f * (c.y - c.w), 0.f));
-    __stcs(o + 3, make_float4(0.5f * (a.w - b.w), 0.5f * (d.w - e.w), 0.5f * (c.z - zp), 0.f));
+    const float zp = __ldg(phi + base + (z0 + 8 == ng ? 0 : z0 + 8));
+    const F8 a = ldg8(phi + ((size_t)xm * ng + y) * ng + z0);
+    const F8 b = ldg8(phi + ((size_t)xp * ng + y) * ng + z0);
+    const F8 d = ldg8(phi + ((size_t)x * ng + ym) * ng + z0);
+    const F8 e = ldg8(phi + ((size_t)x * ng + yp) * ng + z0);
+    float4 o[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float lo = k == 0 ? zm : c.v[k - 1];
+        const float hi = k == 7 ? zp : c.v[k + 1];
+        o[k] = make_float4(0.5f * (a.v[k] - b.v[k]), 0.5f * (d.v[k] - e.v[k]), 0.5f * (lo - hi), 0.f);
+    }
+    float4* dst = f + base + z0;
+#pragma unroll
+    for (int k = 0; k < 8; k += 2) stcs8(dst + k, o[k], o[k + 1]);
 }
-
 // ---------------------------------------------------------------------------
 // x pass fused with P(k): forward x FFT, |delta|^2 * scale * CIC window, and
 // deterministic per-warp FP64 shell sums.  Persistent CTAs take tiles
@@ -650,7 +674,7 @@ cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs,
 
 cudaError_t launch_gradient(int ng, const float* phi, float4* f, cudaStream_t s, const Slots& sl, int nslots) {
     if (!fft_size_supported(ng)) return cudaErrorInvalidValue;
-    const size_t nq = (size_t)ng * ng * (ng / 4);
+    const size_t nq = (size_t)ng * ng * (ng / 8);
     gradient_kernel<<<dim3(cdiv(nq, 256), nslots), 256, 0, s>>>(phi, f, ng, sl);
     return cudaGetLastError();
 }
