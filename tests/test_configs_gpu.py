@@ -101,6 +101,8 @@ def test_config_b_vs_reference(tmp_path):
     m = (n > 0) & (P > 0)
     assert len(kr) == int(m.sum())
     assert np.abs(P[m] / Pr - 1).max() < 1e-3
+    print("config B vs reference: positions p50 %.3g p99.9 %.3g max %.3g of the box; P(k) max %.3g"
+          % (np.median(err), np.percentile(err, 99.9), err.max(), np.abs(P[m] / Pr - 1).max()))
 
 
 def test_config_c_precision_form_at_scale():
