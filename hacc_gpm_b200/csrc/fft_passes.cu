@@ -337,9 +337,10 @@ __global__ void __launch_bounds__(Cfg<NG>::NTX) xfused_kernel(const float2* __re
     const int nvalid = ncols - col0;
     load_tile<NG, C, NT>(tile, in + off, rs, nvalid);
     __syncthreads();
-    // table twiddles throughout (as xpotential_tma_kernel, whose register cap
-    // leaves no room for the product form): both x passes agree bit for bit
-    fft_tile<NG, C, C, false, NT, 1, false>(tile, tw);
+    // the potential pass forms twiddles as products (as xpotential_tma_kernel:
+    // both agree bit for bit); the three-output IC pass, whose registers are
+    // tighter, reads every twiddle from the table
+    fft_tile<NG, C, C, false, NT, 1, Op::kOut == 1>(tile, tw);
     for (int i = threadIdx.x; i < NG * C; i += NT) {
         const int ix = i / C, c = i % C;
         tile[i] = op.pre(ix, iy, col0 + c, tile[i]);
@@ -347,7 +348,7 @@ __global__ void __launch_bounds__(Cfg<NG>::NTX) xfused_kernel(const float2* __re
     if (Op::kOut == 1) {
         // one output: the inverse x transform of pre()'s result
         __syncthreads();
-        fft_tile<NG, C, C, true, NT, 1, false>(tile, tw);
+        fft_tile<NG, C, C, true, NT, 1, true>(tile, tw);
         store_tile<NG, C, NT>(tile, out + off, rs, nvalid);
         return;
     }
