@@ -118,6 +118,9 @@ def lib() -> C.CDLL:
         "hgpm_step_host": (C.c_int, [vp, P(_Timestepper), P(C.c_float), P(C.c_float)]),
         "hgpm_power_spectrum": (C.c_int, [vp, C.c_int, C.c_int, P(C.c_double), P(C.c_double), P(C.c_int64)]),
         "hgpm_write_pk": (C.c_int, [C.c_char_p, C.c_int, P(C.c_double), P(C.c_double), P(C.c_int64)]),
+        "hgpm_power_spectrum_fold": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, P(C.c_double), P(C.c_double),
+                                               P(C.c_int64)]),
+        "hgpm_write_pk_fold": (C.c_int, [C.c_char_p, C.c_int, C.c_int, P(C.c_double), P(C.c_double), P(C.c_int64)]),
         "hgpm_write_output": (C.c_int, [vp, C.c_char_p]),
         "hgpm_read_ipk": (C.c_int, [C.c_char_p, P(C.c_double), P(C.c_double), C.c_int, P(C.c_int)]),
         "hgpm_ic_generate": (C.c_int, [vp, P(C.c_double), C.c_int, C.c_double]),
@@ -262,12 +265,13 @@ def footprint_bytes(ng: int, np_side: int) -> int:
     return lib().hgpm_footprint_bytes(ng, np_side)
 
 
-def write_pk(fname: str, k: np.ndarray, pk: np.ndarray, count: np.ndarray):
-    """``writePkOutput`` (power.cu:13-28): "<fname>.fold.0" lines "%g,%g,%d"."""
+def write_pk(fname: str, k: np.ndarray, pk: np.ndarray, count: np.ndarray, fold: int = 0):
+    """``writePkOutput`` (power.cu:13-28): "<fname>.fold.<fold>" lines "%g,%g,%d"."""
     k = np.ascontiguousarray(k, np.float64)
     pk = np.ascontiguousarray(pk, np.float64)
     n = np.ascontiguousarray(count, np.int64)
-    _check(None, lib().hgpm_write_pk(fname.encode(), k.size, _d(k), _d(pk), n.ctypes.data_as(C.POINTER(C.c_int64))))
+    _check(None, lib().hgpm_write_pk_fold(fname.encode(), fold, k.size, _d(k), _d(pk),
+                                          n.ctypes.data_as(C.POINTER(C.c_int64))))
 
 
 class Simulation:
@@ -397,13 +401,14 @@ class Simulation:
         assert x.dtype == np.float32 and v.dtype == np.float32 and x.flags.c_contiguous and v.flags.c_contiguous
         self._ck(self.L.hgpm_step_host(self._h, C.byref(ts._raw), _f(x), _f(v)))
 
-    def power_spectrum(self, nbins: int = 221, log_bins: bool = False):
-        """``serial::GetPowerSpectrum`` fold 0: (k, P, counts)."""
+    def power_spectrum(self, nbins: int = 221, log_bins: bool = False, fold: int = 0):
+        """One fold of ``serial::GetPowerSpectrum`` (fold 0 by default):
+        (k, P, counts); see hgpm_power_spectrum_fold for folds > 0."""
         k = np.zeros(nbins)
         p = np.zeros(nbins)
         n = np.zeros(nbins, np.int64)
-        self._ck(self.L.hgpm_power_spectrum(self._h, nbins, int(log_bins), _d(k), _d(p),
-                                            n.ctypes.data_as(C.POINTER(C.c_int64))))
+        self._ck(self.L.hgpm_power_spectrum_fold(self._h, fold, nbins, int(log_bins), _d(k), _d(p),
+                                                 n.ctypes.data_as(C.POINTER(C.c_int64))))
         return k, p, n
 
     def write_output(self, fname: str):

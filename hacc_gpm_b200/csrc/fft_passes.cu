@@ -479,8 +479,11 @@ __global__ void __launch_bounds__(kThreads) xpk_kernel(const float2* __restrict_
                     } else {
                         fb = ((double)kmag - a.min_k) / a.bin_delta;
                     }
+                    // (int) truncates, as calc_power_bins does (bin_power.cu:12-13):
+                    // a mode just below minK lands in bin 0; further below
+                    // the reference indexes before the array, here it is dropped
                     const int b = (int)fb;
-                    if (fb >= 0.0 && b < a.nbins) {
+                    if (b >= 0 && b < a.nbins) {
                         const float2 v = tile[i];
                         wgt = (iz == 0 || iz == M) ? 1 : 2;
                         const double p = ((double)v.x * v.x + (double)v.y * v.y) * a.scale *

@@ -39,6 +39,7 @@ struct hgpm_ctx {
     float* pkw = nullptr;
     float* kf_pk = nullptr;
     float* kf_ic = nullptr;
+    float* kf_fold = nullptr;  // k table of the last folded P(k) (lazy)
     int* d_err = nullptr;
     int* blkwin = nullptr;   // per-block CIC windows of the last deposit
     SpillList dep_spill, kick_spill;  // blocks too wide for the windows

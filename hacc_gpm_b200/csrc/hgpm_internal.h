@@ -68,6 +68,10 @@ cudaError_t launch_load_state(const float* x, const float* v, const ParticleSoA&
 cudaError_t launch_store_state(const ParticleSoA& p, float* x, float* v, int np_side, int B, int ng,
                                cudaStream_t s);
 cudaError_t launch_drift(const ParticleSoA& p, size_t n, int ng, float pf, cudaStream_t s);
+// CIC (int64 fixed point, global atomics) of the positions folded `fold`
+// times (x -> 2x mod ng per axis, each time), for folded P(k).
+cudaError_t launch_deposit_folded(const ParticleSoA& p, size_t n, int ng, int fold, float mass,
+                                  unsigned long long* rho, cudaStream_t s);
 int deposit_cap_cells(int np_side, int ng);
 // The deposit writes every block's CIC window (kWinRec ints per block); the
 // kick reads it back when have_rec (positions unchanged since the deposit),

@@ -887,6 +887,48 @@ cudaError_t launch_drift(const ParticleSoA& p, size_t n, int ng, float pf, cudaS
     drift_kernel<<<nblk(n, 256), 256, 0, s>>>(p, n, ng, pf);
     return cudaGetLastError();
 }
+
+// CIC of the particles folded `fold` times for P(k): foldParticles
+// (fold_particles_power.cu:3-27) maps x to 2x mod ng per axis, applied fold
+// times to the power spectrum's copy of the positions (power.cu:194-199).
+// Done here exactly on the packed form (cell, offset): doubling a float is
+// exact and so is taking 1 off an offset in [1, 2).  The folded positions
+// spread a Lagrangian block over the whole grid, so the weights (the
+// deposit's fixed point) go straight to the int64 grid; P(k) only.
+template <bool SMALL>
+__global__ void deposit_folded_kernel(ParticleSoA p, size_t n, int ng, int fold, float mass,
+                                      unsigned long long* __restrict__ rho) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t c = __ldg(&p.cell[i]);
+    int cx = cell_x(c), cy = cell_y(c), cz = cell_z(c);
+    float ox = __ldg(&p.ox[i]), oy = __ldg(&p.oy[i]), oz = __ldg(&p.oz[i]);
+    for (int f = 0; f < fold; ++f) {
+        ox *= 2.f;
+        oy *= 2.f;
+        oz *= 2.f;
+        cx *= 2;
+        cy *= 2;
+        cz *= 2;
+        if (ox >= 1.f) { ox -= 1.f; ++cx; }
+        if (oy >= 1.f) { oy -= 1.f; ++cy; }
+        if (oz >= 1.f) { oz -= 1.f; ++cz; }
+        cx %= ng;
+        cy %= ng;
+        cz %= ng;
+    }
+    deposit_global<SMALL>(rho, pack_cell(cx, cy, cz), ox, oy, oz, mass, ng);
+}
+
+cudaError_t launch_deposit_folded(const ParticleSoA& p, size_t n, int ng, int fold, float mass,
+                                  unsigned long long* rho, cudaStream_t s) {
+    if (fold < 0) return cudaErrorInvalidValue;
+    if (mass <= 1.0f)
+        deposit_folded_kernel<true><<<nblk(n, 256), 256, 0, s>>>(p, n, ng, fold, mass, rho);
+    else
+        deposit_folded_kernel<false><<<nblk(n, 256), 256, 0, s>>>(p, n, ng, fold, mass, rho);
+    return cudaGetLastError();
+}
 int window_records(int np_side, int ng) {
     const int nb = np_side / block_side(np_side, ng);
     return nb * nb * nb * kWinRec;

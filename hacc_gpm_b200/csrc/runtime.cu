@@ -440,7 +440,7 @@ extern "C" void hgpm_destroy(hgpm_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
     // a view owns only its RL tables and its IC table
-    void* own[] = {c->kf_pk, c->kf_ic, c->ic_table};
+    void* own[] = {c->kf_pk, c->kf_ic, c->kf_fold, c->ic_table};
     for (void* q : own)
         if (q) cudaFree(q);
     if (!c->view) {
@@ -713,10 +713,12 @@ extern "C" int hgpm_step_host(hgpm_ctx* c, hgpm_timestepper* ts, float* x, float
 // ===========================================================================
 // power spectrum
 // ===========================================================================
-static int pk_bins_setup(const hgpm_ctx* c, int nbins, int log_bins, double* min_k, double* bin_delta,
-                         std::vector<double>& centres) {
-    // power.cu:174-187 (fold 0): minK = 2pi/rl, maxK = sqrt(3 (ng/2)^2 d^2)
-    double d = (2 * M_PI) / c->p.rl;
+// Bin edges of power.cu:174-187 for a box of side rl_bins: minK = 2pi/rl_bins,
+// maxK = sqrt(3 (ng/2)^2 d^2).  (The reference sets them once per call from
+// the most-folded box, rl / 2^PK_FOLDS, for every fold.)
+static int pk_bins_setup(const hgpm_ctx* c, double rl_bins, int nbins, int log_bins, double* min_k,
+                         double* bin_delta, std::vector<double>& centres) {
+    double d = (2 * M_PI) / rl_bins;
     double mk = d;
     double maxk = sqrt(3 * ((c->ng / 2) * (c->ng / 2) * d * d));
     centres.resize(nbins);
@@ -735,7 +737,14 @@ static int pk_bins_setup(const hgpm_ctx* c, int nbins, int log_bins, double* min
 
 extern "C" int hgpm_power_spectrum(hgpm_ctx* c, int nbins, int log_bins, double* k_out, double* pk_out,
                                    int64_t* n_out) {
-    if (!c || !k_out || !pk_out || !n_out || nbins <= 0) return HGPM_ERR_ARG;
+    return hgpm_power_spectrum_fold(c, 0, nbins, log_bins, k_out, pk_out, n_out);
+}
+
+// GetPowerSpectrum's fold loop body (power.cu:189-227) for one fold.
+extern "C" int hgpm_power_spectrum_fold(hgpm_ctx* c, int fold, int nbins, int log_bins, double* k_out,
+                                        double* pk_out, int64_t* n_out) {
+    if (!c || !k_out || !pk_out || !n_out || nbins <= 0 || fold < 0) return HGPM_ERR_ARG;
+    if (fold > 9) return fail(c, HGPM_ERR_ARG, "fold %d above 9", fold);
     if (nbins > pk_max_bins()) return fail(c, HGPM_ERR_ARG, "nbins %d above %d", nbins, pk_max_bins());
     if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
     const int ng = c->ng, M = ng / 2;
@@ -747,18 +756,40 @@ extern "C" int hgpm_power_spectrum(hgpm_ctx* c, int nbins, int log_bins, double*
         CK(cudaMalloc(&c->pk_cnt, pk_max_bins() * 8));
     }
     PhaseScope ps(c, PH_PK);
-    int rc = deposit_impl(c);  // serial::CIC of the positions (power.cu:210)
-    if (rc) return rc;
+    // the fold's box: rl / 2^fold (power.cu:193); with ref_quirks the bins come
+    // from rl / 2^max(PK_FOLDS, fold) and the power is scaled with the
+    // unfolded rl, as the reference does for every fold (power.cu:174-187,
+    // 215); without, both follow the fold's own box
+    const double rl_f = c->p.rl / pow(2.0, fold);
+    const int nf = c->p.pk_folds > fold ? c->p.pk_folds : fold;
+    const double rl_bins = c->p.ref_quirks ? c->p.rl / pow(2.0, nf) : rl_f;
+    const double rl_scale = c->p.ref_quirks ? c->p.rl : rl_f;
+    int rc;
+    if (fold == 0) {
+        rc = deposit_impl(c);  // serial::CIC of the positions (power.cu:210)
+        if (rc) return rc;
+    } else {
+        if (c->rho_dirty) CK(cudaMemsetAsync(c->rho64, 0, c->ncell * 8, c->stream));
+        CK(launch_deposit_folded(c->part, c->npart, c->ng, fold, cic_mass(c->ng, c->np), c->rho64, c->stream));
+        c->rho_dirty = true;
+        count(c, PH_PK, 1);
+        if (!c->kf_fold) CK(cudaMalloc(&c->kf_fold, c->ng * 4));
+        std::vector<float> kf(c->ng);
+        const double d = (2 * M_PI) / rl_f;
+        for (int i = 0; i < c->ng; ++i) kf[i] = (float)((double)signed_mode(i, c->ng) * d);
+        CK(cudaMemcpyAsync(c->kf_fold, kf.data(), c->ng * 4, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
     rc = forward_zy(c);
     if (rc) return rc;
     PkArgs a;
     std::vector<double> centres;
-    pk_bins_setup(c, nbins, log_bins, &a.min_k, &a.bin_delta, centres);
-    a.kf = c->kf_pk;
+    pk_bins_setup(c, rl_bins, nbins, log_bins, &a.min_k, &a.bin_delta, centres);
+    a.kf = fold == 0 ? c->kf_pk : c->kf_fold;
     a.filt = c->pkw;
     a.nbins = nbins;
     a.log_bins = log_bins;
-    a.scale = (1.0f / ((double)ng * ng * ng)) * (c->p.rl / ng);
+    a.scale = (1.0f / ((double)ng * ng * ng)) * (rl_scale / ng);
     CK(launch_xpk(ng, c->spec, M + 1, (size_t)ng * c->zs, (size_t)c->zs, c->tw_ng, a, c->pk_part, c->pk_pcnt,
                   c->pk_nparts, c->pk_sum, c->pk_cnt, c->stream));
     count(c, PH_PK, 2);
@@ -776,8 +807,13 @@ extern "C" int hgpm_power_spectrum(hgpm_ctx* c, int nbins, int log_bins, double*
 }
 
 extern "C" int hgpm_write_pk(const char* fname, int nbins, const double* k, const double* pk, const int64_t* count) {
+    return hgpm_write_pk_fold(fname, 0, nbins, k, pk, count);
+}
+
+extern "C" int hgpm_write_pk_fold(const char* fname, int fold, int nbins, const double* k, const double* pk,
+                                  const int64_t* count) {
     char fname2[400];
-    snprintf(fname2, sizeof(fname2), "%s.fold.%d", fname, 0);
+    snprintf(fname2, sizeof(fname2), "%s.fold.%d", fname, fold);
     FILE* fp = fopen(fname2, "w+");
     if (!fp) return HGPM_ERR_IO;
     for (int i = 0; i < nbins; ++i) {

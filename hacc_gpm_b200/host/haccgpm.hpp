@@ -19,8 +19,9 @@
 //     and GenerateDisplacementIC.
 //   * InitGreens and fft_cache_plan are no-ops (the Green's function is
 //     computed inside the fused Poisson pass; there are no plans).
-//   * GetPowerSpectrum writes fold 0 only (PK_FOLDS > 0 makes the
-//     reference's BinPower index out of bounds, bin_power.cu:20-27).
+//   * GetPowerSpectrum writes folds 0..PK_FOLDS; modes that the reference's
+//     BinPower would index before its bin arrays (bin_power.cu:12-16, folds
+//     > 0) are dropped (REF_QUIRKS 0: each fold binned in its own box).
 #pragma once
 
 #include <cstdint>

@@ -249,9 +249,14 @@ void GetPowerSpectrum(Params& params, MemoryManager& mem, const char* fname, int
     const int nb = params.pk_bins > 0 ? params.pk_bins : 221;
     std::vector<double> k(nb), pk(nb);
     std::vector<int64_t> n(nb);
-    check(mem.ctx, hgpm_power_spectrum(mem.ctx, nb, params.pk_log ? 1 : 0, k.data(), pk.data(), n.data()),
-          "GetPowerSpectrum");
-    if (hgpm_write_pk(fname, nb, k.data(), pk.data(), n.data()) != HGPM_OK) die("GetPowerSpectrum", fname);
+    // power.cu:189-227: one file per fold
+    for (int fold = 0; fold <= params.pkFolds; ++fold) {
+        check(mem.ctx,
+              hgpm_power_spectrum_fold(mem.ctx, fold, nb, params.pk_log ? 1 : 0, k.data(), pk.data(), n.data()),
+              "GetPowerSpectrum");
+        if (hgpm_write_pk_fold(fname, fold, nb, k.data(), pk.data(), n.data()) != HGPM_OK)
+            die("GetPowerSpectrum", fname);
+    }
 }
 
 void writeOutput(Params&, MemoryManager& mem, char* fname, int) {

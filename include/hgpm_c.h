@@ -162,6 +162,20 @@ int hgpm_power_spectrum(hgpm_ctx* ctx, int nbins, int log_bins, double* k_host,
 /* Writes "<fname>.fold.0" lines "%g,%g,%d" (power.cu:13-28).               */
 int hgpm_write_pk(const char* fname, int nbins, const double* k, const double* pk,
                   const int64_t* count);
+/* One fold of GetPowerSpectrum's PK_FOLDS loop (power.cu:189-227): the
+ * positions folded `fold` times (x -> 2x mod ng per axis each time,
+ * fold_particles_power.cu:3-27; exact on the packed positions) in a box of
+ * side rl / 2^fold.  ref_quirks = 1 (default) keeps the reference's choices:
+ * bin edges from rl / 2^max(PK_FOLDS, fold) for every fold and the power
+ * scaled with the unfolded rl; modes below the first edge by more than one
+ * bin, which the reference writes before its bin arrays (bin_power.cu:12-16),
+ * are dropped.  ref_quirks = 0: bins and scale from the fold's own box.
+ * fold 0 is hgpm_power_spectrum.  fold <= 9.                               */
+int hgpm_power_spectrum_fold(hgpm_ctx* ctx, int fold, int nbins, int log_bins, double* k_host,
+                             double* pk_host, int64_t* count_host);
+/* writePkOutput for any fold: "<fname>.fold.<fold>".                        */
+int hgpm_write_pk_fold(const char* fname, int fold, int nbins, const double* k, const double* pk,
+                       const int64_t* count);
 /* serial::writeOutput (io.cu:12-44): raw float3 x then float3 v.           */
 int hgpm_write_output(hgpm_ctx* ctx, const char* fname);
 

@@ -406,34 +406,56 @@ def pk_cic_filter(ng: int) -> np.ndarray:
 
 def pk_bin_index(ng: int, rl_fold: float, min_k: float, delta: float) -> np.ndarray:
     """calc_power_bins (bin_power.cu:3-17): float kmodes, sqrtf of the float
-    sum of squares, then (int)((|k| - minK)/delta) in double."""
+    sum of squares, then (int)((|k| - minK)/delta) in double (truncation:
+    a mode less than one bin below minK lands in bin 0; further below the
+    index is negative, which the reference writes before its arrays and
+    callers here drop)."""
     kf = kmodes_f32(ng, 2.0 * np.pi / rl_fold)
     kx = kf[:, None, None]
     ky = kf[None, :, None]
     kz = kf[None, None, :]
     s = (kx * kx + ky * ky).astype(np.float32) + kz * kz
     kmag = np.sqrt(s.astype(np.float32)).astype(np.float32)
-    return np.floor((kmag.astype(np.float64) - min_k) / delta).astype(np.int64)
+    return np.trunc((kmag.astype(np.float64) - min_k) / delta).astype(np.int64)
+
+
+def fold_positions(x: np.ndarray, ng: int, fold: int) -> np.ndarray:
+    """foldParticles (fold_particles_power.cu:3-27) applied `fold` times:
+    x -> 2x - ng [x >= ng/2], i.e. 2x mod ng, per axis (in float64)."""
+    y = np.array(x, dtype=np.float64)
+    for _ in range(fold):
+        y = 2.0 * y
+        y = np.where(y >= ng, y - ng, y)
+    return y
 
 
 def power_spectrum(x: np.ndarray, ng: int, np_side: int, rl: float, nbins: int = 221,
-                   folds: int = 0):
-    """serial::GetPowerSpectrum fold 0 (power.cu:152-246): CIC of the
-    particles, forward FFT, scalePower (|d|^2 (1/ng^3)(rl/ng),
-    scale_power.cu:3-12), PkCICFilter, BinPower skipping DC and the
-    (ng/2)^3 corner.  Sums in float64 (the reference sums in float).
-    Returns (k_centres, P, counts) for all bins (empty bins give P=nan)."""
-    if folds != 0:
-        raise NotImplementedError("fold > 0 writes out of bounds in the reference (bin_power.cu:12-16)")
-    rho = cic_deposit(x, ng, cic_mass(ng, np_side))
+                   folds: int = 0, fold: int = 0, ref_quirks: bool = True):
+    """One fold of serial::GetPowerSpectrum (power.cu:152-246): CIC of the
+    particles folded `fold` times, forward FFT, scalePower (|d|^2 (1/ng^3)
+    (rl/ng), scale_power.cu:3-12), PkCICFilter, BinPower (k in the fold's
+    box rl/2^fold) skipping DC and the (ng/2)^3 corner.  ref_quirks: bin
+    edges from rl/2^max(folds, fold) and the scale from the unfolded rl, as
+    the reference (power.cu:174-187, 215); otherwise both from the fold's
+    box.  Negative bin indices (reference: writes before its arrays) are
+    dropped.  Sums in float64 (the reference sums in float).  Returns
+    (k_centres, P, counts) for all bins (empty bins give P=nan)."""
+    rl_f = rl / (2.0 ** fold)
+    nf = max(folds, fold)
+    xf = fold_positions(x, ng, fold) if fold else x
+    rho = cic_deposit(xf, ng, cic_mass(ng, np_side))
     rk = np.fft.fftn(rho)
-    scale = (1.0 / float(ng * ng * ng)) * (rl / ng)
+    scale = (1.0 / float(ng * ng * ng)) * ((rl if ref_quirks else rl_f) / ng)
     pw = (rk.real ** 2 + rk.imag ** 2) * scale * pk_cic_filter(ng)
-    min_k, delta, centres = pk_bin_edges(ng, rl, nbins, folds)
-    idx = pk_bin_index(ng, rl, min_k, delta)
+    if ref_quirks:
+        min_k, delta, centres = pk_bin_edges(ng, rl, nbins, nf)
+    else:
+        min_k, delta, centres = pk_bin_edges(ng, rl_f, nbins, 0)
+    idx = pk_bin_index(ng, rl_f, min_k, delta)
     mask = np.ones((ng, ng, ng), dtype=bool)
     mask[0, 0, 0] = False
     mask[ng // 2, ng // 2, ng // 2] = False
+    mask &= idx >= 0
     ii = idx[mask]
     sums = np.bincount(ii, weights=pw[mask], minlength=nbins)[:nbins]
     counts = np.bincount(ii, minlength=nbins)[:nbins]

@@ -90,6 +90,26 @@ def test_driver_files_match_api(tmp_path):
 
 
 @pytest.mark.gpu
+def test_driver_writes_every_fold(tmp_path):
+    """PK_FOLDS 2: one pk file per fold (power.cu:189-227), each equal to the
+    API's fold through hgpm_write_pk_fold."""
+    d, txt = _case(tmp_path, "folds", extra="PK_FOLDS 2\n")
+    r = subprocess.run([_driver(), str(d / "input.params")], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    hp = H.parse_params(txt)
+    header, table = H.read_ipk(str(tmp_path / "run.ipk"))
+    with H.Simulation(hp) as s:
+        s.generate_ic(table, header[3])
+        for fold in range(3):
+            k, P, n = s.power_spectrum(221, fold=fold)
+            H.write_pk(str(tmp_path / "api.pk.ini"), k, P, n, fold=fold)
+    for fold in range(3):
+        name = "run.pk.ini.fold.%d" % fold
+        assert (d / name).exists(), name
+        assert (d / name).read_text() == (tmp_path / ("api.pk.ini.fold.%d" % fold)).read_text()
+
+
+@pytest.mark.gpu
 def test_driver_fused_equals_plain(tmp_path):
     runs = []
     for name, flags in (("a", []), ("b", ["--fused"])):

@@ -101,7 +101,7 @@ def test_power_spectrum_matches_oracle(ng, nbins, log_bins):
         maxk = np.sqrt(3 * ((ng // 2) ** 2 * d * d))
         dl = np.log(maxk / d) / nbins
         with np.errstate(divide="ignore"):
-            b = np.floor(np.log(kk / d) / dl)
+            b = np.trunc(np.log(kk / d) / dl)  # (int) truncation, as the kernel
         m = np.ones_like(kk, bool)
         m[0, 0, 0] = False
         m[ng // 2, ng // 2, ng // 2] = False
@@ -114,6 +114,25 @@ def test_power_spectrum_matches_oracle(ng, nbins, log_bins):
         ko, Po, no = O.power_spectrum(x0.astype(np.float64), ng, ng, op.rl, nbins)
         assert np.allclose(k, ko, rtol=1e-12)
     assert np.array_equal(n, no)
+    ok = no > 0
+    assert np.max(np.abs(P[ok] / Po[ok] - 1)) < PK_RTOL
+
+
+@pytest.mark.parametrize("ng,fold,quirks", [(32, 1, True), (32, 2, True), (48, 1, False), (32, 2, False)])
+def test_folded_power_spectrum_matches_oracle(ng, fold, quirks):
+    """One fold of GetPowerSpectrum's PK_FOLDS loop: positions folded `fold`
+    times (x -> 2x mod ng), binned with the reference's edges (from the most
+    folded box, unfolded scale) or the fold's own box."""
+    hp, op = _pair(ng, rl=2.0 * ng, z_ini=20.0, extra="PK_FOLDS 2\nREF_QUIRKS %d\n" % int(quirks))
+    x0, v0, *_ = oracle_ics(op)
+    with H.Simulation(hp) as s:
+        s.load_state(x0, v0)
+        k, P, n = s.power_spectrum(64, fold=fold)
+        x1, _ = s.store_state()
+    ko, Po, no = O.power_spectrum(x0.astype(np.float64), ng, ng, op.rl, 64, folds=2, fold=fold, ref_quirks=quirks)
+    assert np.array_equal(x1, x0)  # the state is not folded
+    assert np.allclose(k, ko, rtol=1e-12)
+    assert np.array_equal(n, no) and n.sum() > 0
     ok = no > 0
     assert np.max(np.abs(P[ok] / Po[ok] - 1)) < PK_RTOL
 

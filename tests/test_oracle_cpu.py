@@ -162,3 +162,38 @@ def test_ic_zeldovich_displacement_is_gradient_of_potential():
         mask[tuple(sl)] = False
     mask[0, 0, 0] = False
     assert np.allclose(div[mask], (dk / 2.0)[mask], rtol=1e-6, atol=1e-9 * np.abs(dk).max())
+
+
+@pytest.mark.parametrize("fold", [1, 2, 3])
+def test_fold_positions_is_doubling_mod_ng(fold):
+    """foldParticles (fold_particles_power.cu:3-27) applied `fold` times is
+    x -> 2^fold x mod ng; exact for dyadic positions."""
+    ng = 32
+    rng = np.random.default_rng(5)
+    x = np.floor(rng.uniform(0, ng, (500, 3)) * 256) / 256.0
+    y = O.fold_positions(x, ng, fold)
+    assert np.array_equal(y, np.mod(x * 2 ** fold, ng))
+    assert (y >= 0).all() and (y < ng).all()
+
+
+def test_folded_pk_quirk_bins_drop_modes_below_the_first_edge():
+    """With the reference's bins (edges from the most folded box) the low-k
+    modes of an unfolded P(k) fall before bin 0: those less than one bin
+    below land in bin 0 (truncation), the rest are dropped; with the fold's
+    own bins every mode but DC and the corner is binned."""
+    ng = 16
+    rng = np.random.default_rng(9)
+    x = rng.uniform(0, ng, (ng ** 3, 3))
+    _, _, nq = O.power_spectrum(x, ng, ng, 16.0, 32, folds=2, fold=0, ref_quirks=True)
+    _, _, nc = O.power_spectrum(x, ng, ng, 16.0, 32, folds=2, fold=0, ref_quirks=False)
+    assert nc.sum() == ng ** 3 - 2
+    assert 0 < nq.sum() < nc.sum()
+    d = 2 * np.pi / 16.0
+    min_k, delta, _ = O.pk_bin_edges(ng, 16.0, 32, 2)
+    assert min_k == pytest.approx(4 * d)
+    kf = O.kmodes_f32(ng, d).astype(np.float64)
+    kk = np.sqrt(kf[:, None, None] ** 2 + kf[None, :, None] ** 2 + kf[None, None, :] ** 2)
+    keep = (kk - min_k) / delta > -1.0
+    keep[0, 0, 0] = keep[ng // 2, ng // 2, ng // 2] = False
+    keep &= np.trunc((kk - min_k) / delta) < 32
+    assert nq.sum() == keep.sum()
