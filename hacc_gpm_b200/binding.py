@@ -118,6 +118,10 @@ def lib() -> C.CDLL:
         "hgpm_step_host": (C.c_int, [vp, P(_Timestepper), P(C.c_float), P(C.c_float)]),
         "hgpm_power_spectrum": (C.c_int, [vp, C.c_int, C.c_int, P(C.c_double), P(C.c_double), P(C.c_int64)]),
         "hgpm_write_pk": (C.c_int, [C.c_char_p, C.c_int, P(C.c_double), P(C.c_double), P(C.c_int64)]),
+        "hgpm_read_output": (C.c_int, [vp, C.c_char_p]),
+        "hgpm_checkpoint_bytes": (C.c_size_t, [vp]),
+        "hgpm_checkpoint_save": (C.c_int, [vp, P(_Timestepper), vp, C.c_size_t]),
+        "hgpm_checkpoint_load": (C.c_int, [vp, P(_Timestepper), vp, C.c_size_t]),
         "hgpm_power_spectrum_fold": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, P(C.c_double), P(C.c_double),
                                                P(C.c_int64)]),
         "hgpm_write_pk_fold": (C.c_int, [C.c_char_p, C.c_int, C.c_int, P(C.c_double), P(C.c_double), P(C.c_int64)]),
@@ -353,6 +357,25 @@ class Simulation:
 
     def store_state_device(self, x_ptr: int, v_ptr: int):
         self._ck(self.L.hgpm_store_state_device(self._h, C.c_void_p(x_ptr), C.c_void_p(v_ptr)))
+
+    def read_output(self, fname: str):
+        """Load the state from a ``serial::writeOutput`` dump (io.cu:12-44)."""
+        self._ck(self.L.hgpm_read_output(self._h, fname.encode()))
+
+    def checkpoint(self, ts: Timestepper) -> np.ndarray:
+        """The exact device state and ``ts`` as one byte array (resume with
+        ``restore``: bit-identical continuation)."""
+        buf = np.empty(self.L.hgpm_checkpoint_bytes(self._h), np.uint8)
+        self._ck(self.L.hgpm_checkpoint_save(self._h, C.byref(ts._raw), buf.ctypes.data_as(C.c_void_p), buf.size))
+        return buf
+
+    def restore(self, buf: np.ndarray) -> Timestepper:
+        """Load a ``checkpoint`` byte array; returns its time stepper."""
+        buf = np.ascontiguousarray(buf, np.uint8)
+        ts = Timestepper.__new__(Timestepper)
+        ts._raw = _Timestepper()
+        self._ck(self.L.hgpm_checkpoint_load(self._h, C.byref(ts._raw), buf.ctypes.data_as(C.c_void_p), buf.size))
+        return ts
 
     def get_cells(self) -> np.ndarray:
         out = np.empty(self.npart, np.int32)

@@ -531,6 +531,77 @@ extern "C" int hgpm_store_state(hgpm_ctx* c, float* x, float* v) {
     return sync_check(c);
 }
 
+// ---- checkpoints: the exact device state (packed cells, offsets,
+// velocities, in the context's internal order) plus the time stepper
+namespace {
+struct CkptHeader {
+    char magic[8];  // "HGPMCK01"
+    int32_t ng, np, blk, pad;
+    double rl;
+    int64_t npart;
+    hgpm_timestepper ts;
+};
+}  // namespace
+
+extern "C" size_t hgpm_checkpoint_bytes(const hgpm_ctx* c) {
+    return c ? sizeof(CkptHeader) + c->npart * 7 * 4 : 0;
+}
+
+extern "C" int hgpm_checkpoint_save(hgpm_ctx* c, const hgpm_timestepper* ts, void* buf, size_t bytes) {
+    if (!c || !ts || !buf) return HGPM_ERR_ARG;
+    if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
+    if (bytes < hgpm_checkpoint_bytes(c)) return fail(c, HGPM_ERR_ARG, "checkpoint buffer too small");
+    CkptHeader h;
+    memset(&h, 0, sizeof(h));
+    memcpy(h.magic, "HGPMCK01", 8);
+    h.ng = c->ng;
+    h.np = c->np;
+    h.blk = c->blk;
+    h.rl = c->p.rl;
+    h.npart = (int64_t)c->npart;
+    h.ts = *ts;
+    memcpy(buf, &h, sizeof(h));
+    char* d = (char*)buf + sizeof(h);
+    const void* src[7] = {c->part.cell, c->part.ox, c->part.oy, c->part.oz, c->part.vx, c->part.vy, c->part.vz};
+    for (int a = 0; a < 7; ++a)
+        CK(cudaMemcpyAsync(d + (size_t)a * c->npart * 4, src[a], c->npart * 4, cudaMemcpyDeviceToHost, c->stream));
+    return sync_check(c);
+}
+
+extern "C" int hgpm_checkpoint_load(hgpm_ctx* c, hgpm_timestepper* ts, const void* buf, size_t bytes) {
+    if (!c || !buf) return HGPM_ERR_ARG;
+    CkptHeader h;
+    if (bytes < sizeof(h)) return fail(c, HGPM_ERR_ARG, "checkpoint truncated");
+    memcpy(&h, buf, sizeof(h));
+    if (memcmp(h.magic, "HGPMCK01", 8) != 0) return fail(c, HGPM_ERR_ARG, "not a checkpoint");
+    if (h.ng != c->ng || h.np != c->np || h.blk != c->blk || h.npart != (int64_t)c->npart)
+        return fail(c, HGPM_ERR_ARG, "checkpoint of NG %d NP %d does not fit this context (NG %d NP %d)", h.ng, h.np,
+                    c->ng, c->np);
+    if (bytes < hgpm_checkpoint_bytes(c)) return fail(c, HGPM_ERR_ARG, "checkpoint truncated");
+    const char* s = (const char*)buf + sizeof(h);
+    void* dst[7] = {c->part.cell, c->part.ox, c->part.oy, c->part.oz, c->part.vx, c->part.vy, c->part.vz};
+    for (int a = 0; a < 7; ++a)
+        CK(cudaMemcpyAsync(dst[a], s + (size_t)a * c->npart * 4, c->npart * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_state = true;
+    c->win_valid = false;
+    if (ts) *ts = h.ts;
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_read_output(hgpm_ctx* c, const char* fname) {
+    if (!c || !fname) return HGPM_ERR_ARG;
+    FILE* fp = fopen(fname, "rb");
+    if (!fp) return fail(c, HGPM_ERR_IO, "cannot open %s", fname);
+    std::vector<float> x(c->npart * 3), v(c->npart * 3);
+    const size_t nx = fread(x.data(), sizeof(float) * 3, c->npart, fp);
+    const size_t nv = fread(v.data(), sizeof(float) * 3, c->npart, fp);
+    fclose(fp);
+    if (nx != c->npart || nv != c->npart)
+        return fail(c, HGPM_ERR_IO, "%s holds fewer than 2 x %zu float3", fname, c->npart);
+    return hgpm_load_state(c, x.data(), v.data());
+}
+
 extern "C" int hgpm_get_cells(hgpm_ctx* c, int32_t* cells) {
     if (!c || !cells) return HGPM_ERR_ARG;
     if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");

@@ -90,10 +90,16 @@ class Server:
     ``batch_ms`` of GPU time from the class's measured step time (at most
     ``max_batch`` steps, and no more than the fewest steps a running request
     still needs), so small boxes are not held to the pace of large ones and
-    the host loop keeps up with them."""
+    the host loop keeps up with them.
+
+    With ``segment_steps``, a request holds its slot for at most that many
+    steps at a time: at the end of a segment its exact state and time
+    stepper go to a host checkpoint (``Simulation.checkpoint``), the slot is
+    freed, and the request queues again to resume from the checkpoint
+    (pre-emption; the result is bit-identical to an uninterrupted run)."""
 
     def __init__(self, sizes, hbm_budget: float = 40e9, device: int = 0, graph: bool = True, max_slots: int = 64,
-                 batch_ms: float = 1.0, max_batch: int = 8, step_ms: float = 2.0):
+                 batch_ms: float = 1.0, max_batch: int = 8, step_ms: float = 2.0, segment_steps: int = None):
         self.classes = class_capacity(sizes, hbm_budget, max_slots, step_ms)
         self.index = {c[0]: i for i, c in enumerate(self.classes)}
         self.ens = Ensemble(self.classes, device=device, graph=graph)
@@ -106,6 +112,9 @@ class Server:
         self.step_ms = [None] * n    # measured seconds per step, per class (ms)
         self.steps = [0] * n         # class steps run
         self.batch_ms, self.max_batch = batch_ms, max_batch
+        self.segment_steps = segment_steps
+        self.preemptions = 0
+        self.requeue = []
 
     def close(self):
         self.ens.close()
@@ -117,16 +126,28 @@ class Server:
         si = self.free[ci].popleft()
         p = req.params()
         v = self.ens.slot(ci, si, p)
-        v.generate_ic(req.table, req.k_delta)
-        self.ens.start(ci, si, _ts_for(p), req.nsteps)
+        ckpt = getattr(req, "ckpt", None)
+        if ckpt is None:
+            v.generate_ic(req.table, req.k_delta)
+            ts = _ts_for(p)
+            req.steps_before = 0
+        else:
+            ts = v.restore(ckpt)  # a pre-empted request resumes exactly
+            req.ckpt = None
+        left = req.nsteps - req.steps_before
+        req.segment = min(left, self.segment_steps) if self.segment_steps else left
+        self.ens.start(ci, si, ts, req.segment)  # ts leaves advanced through the segment
+        req.ts_end = ts
         req.done_steps = 0
         self.running[(ci, si)] = req
         return True
 
     def poll(self):
         """Finished requests (with results) of every class whose queued
-        steps have run."""
+        steps have run; requests whose segment ended with steps left are
+        checkpointed and listed in ``self.requeue``."""
         done = []
+        self.requeue = []
         for ci in range(len(self.classes)):
             if not self.busy[ci] or not self.ens.class_done(ci):
                 continue
@@ -140,11 +161,17 @@ class Server:
                 running, req.done_steps = self.ens.status(ci, si)
                 if not running:
                     v = self.ens.views[(ci, si)]
-                    req.result = _result(v, req)
+                    req.steps_before += req.segment
+                    if req.steps_before < req.nsteps:
+                        req.ckpt = v.checkpoint(req.ts_end)
+                        self.requeue.append(req)
+                        self.preemptions += 1
+                    else:
+                        req.result = _result(v, req)
+                        done.append(req)
                     self.ens.release(ci, si)
                     self.free[ci].append(si)
                     del self.running[(ci, si)]
-                    done.append(req)
         return done
 
     def launch(self):
@@ -152,7 +179,7 @@ class Server:
         for ci in range(len(self.classes)):
             if self.busy[ci]:
                 continue
-            rem = [r.nsteps - r.done_steps for (c, _), r in self.running.items() if c == ci]
+            rem = [r.segment - r.done_steps for (c, _), r in self.running.items() if c == ci]
             if not rem:
                 continue
             k = 1 if self.step_ms[ci] is None else int(self.batch_ms / max(self.step_ms[ci], 1e-3))
@@ -165,14 +192,15 @@ class Server:
 
 
 def serve(requests, hbm_budget: float = 40e9, device: int = 0, graph: bool = True, realtime: bool = True,
-          max_slots: int = 64):
+          max_slots: int = 64, segment_steps: int = None):
     """Run the request stream through a Server.  realtime: requests become
     visible at their arrival times (wall clock from the start); otherwise all
-    are queued at t = 0 (saturated throughput).  Returns (requests with
-    .latency and .result, makespan seconds, server stats)."""
+    are queued at t = 0 (saturated throughput).  segment_steps: pre-empt
+    every request after that many steps (see Server).  Returns (requests
+    with .latency and .result, makespan seconds, server stats)."""
     prepare_tables(requests)
     sizes = sorted({r.ng for r in requests})
-    srv = Server(sizes, hbm_budget, device, graph, max_slots)
+    srv = Server(sizes, hbm_budget, device, graph, max_slots, segment_steps=segment_steps)
     try:
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         waiting = collections.deque()
@@ -186,6 +214,7 @@ def serve(requests, hbm_budget: float = 40e9, device: int = 0, graph: bool = Tru
                 r.finish = time.perf_counter() - t0
                 r.latency = r.finish - (r.arrival if realtime else 0.0)
                 finished.append(r)
+            waiting.extend(srv.requeue)  # pre-empted: back of the queue
             # first come first served within what fits (a class takes new
             # requests between its batches)
             still = collections.deque()
@@ -199,6 +228,7 @@ def serve(requests, hbm_budget: float = 40e9, device: int = 0, graph: bool = Tru
                 time.sleep(max(0.0, min(pending[0].arrival - (time.perf_counter() - t0), 0.01)))
         makespan = time.perf_counter() - t0
         return finished, makespan, {"ticks": max(srv.steps), "steps_per_class": list(srv.steps),
+                                    "preemptions": srv.preemptions,
                                     "classes": srv.classes, "launches": srv.ens.kernel_launches()}
     finally:
         srv.close()

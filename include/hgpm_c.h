@@ -126,6 +126,19 @@ int hgpm_store_state_device(hgpm_ctx* ctx, float* x_dev, float* v_dev);
 /* Linear cell index (ix*ng+iy)*ng+iz of every particle's CIC base cell
  * (the reference's `int i = x` truncation, cic_pm.cu:52-54).              */
 int hgpm_get_cells(hgpm_ctx* ctx, int32_t* cells_host);
+/* Restart from a particle dump: reads the file serial::writeOutput writes
+ * (io.cu:12-44: raw float3 x[np^3] then float3 v[np^3]) into the context,
+ * like hgpm_load_state.  Positions re-split from float3 as on any load.   */
+int hgpm_read_output(hgpm_ctx* ctx, const char* fname);
+/* Checkpoints (no counterpart in the reference): the exact device state
+ * (packed cells, offsets, velocities) and a time stepper, to and from a
+ * host buffer of hgpm_checkpoint_bytes(ctx).  A run of s steps,
+ * checkpointed, loaded into a context of the same NG/NP and continued for n
+ * steps with the saved stepper is bit-identical to s + n steps run at once
+ * (resume after pre-emption; the float3 dump above is not exact).         */
+size_t hgpm_checkpoint_bytes(const hgpm_ctx* ctx);
+int hgpm_checkpoint_save(hgpm_ctx* ctx, const hgpm_timestepper* ts, void* host_buf, size_t bytes);
+int hgpm_checkpoint_load(hgpm_ctx* ctx, hgpm_timestepper* ts_out, const void* host_buf, size_t bytes);
 
 /* ---- PM phases -----------------------------------------------------------*/
 /* serial::UpdatePositions (pm_actions.cpp:287-314, update_positions_pm.cu:3-20) */

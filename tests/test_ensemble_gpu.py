@@ -68,6 +68,20 @@ def test_per_class_stepping_equals_alone(graph):
         _same(a, b)
 
 
+def test_serving_preemption_equals_alone():
+    """Requests pre-empted every 4 steps (checkpoint to host, slot freed,
+    resumed later from the checkpoint) end bit-identical to runs alone."""
+    reqs = S.request_stream(8, rate=500.0, seed=13, sizes=(32, 48), steps=(5, 11))
+    got, _, stats = S.serve(reqs, hbm_budget=1e9, realtime=False, max_slots=2, segment_steps=4)
+    assert len(got) == 8 and stats["preemptions"] >= 8
+    alone, _ = S.serve_one_at_a_time(S.request_stream(8, rate=500.0, seed=13, sizes=(32, 48), steps=(5, 11)),
+                                     realtime=False)
+    by_tag = {r.tag: r for r in got}
+    for r in alone:
+        g = by_tag[r.tag].result
+        assert np.array_equal(g["n"], r.result["n"]) and np.array_equal(g["P"], r.result["P"])
+
+
 def test_slot_reuse_and_errors():
     boxes = _boxes()[:2]
     classes, _ = E.class_layout(boxes)

@@ -188,6 +188,47 @@ def test_ic_table_too_short_is_an_error():
             s.generate_ic(np.ones(100), k[1] - k[0])
 
 
+def test_checkpoint_resume_is_bit_identical(tmp_path):
+    """s steps, checkpoint to a host buffer, restore in a fresh context and n
+    more steps equal s + n steps at once; the float3 dump reader restores
+    exactly what the dump holds."""
+    hp, op = _pair(32)
+    x0, v0, *_ = oracle_ics(op)
+
+    def ts0():
+        t = H.Timestepper(hp)
+        t.set_initial_z(hp.z_ini)
+        t.reverse_half_step()
+        t.advance_half_step()
+        return t
+
+    with H.Simulation(hp) as a:
+        a.load_state(x0, v0)
+        ta = ts0()
+        a.run_steps(ta, 7)
+        xa, va = a.store_state()
+    with H.Simulation(hp) as b:
+        b.load_state(x0, v0)
+        tb = ts0()
+        b.run_steps(tb, 3)
+        buf = b.checkpoint(tb)
+        b.write_output(str(tmp_path / "dump"))
+        xd, vd = b.store_state()
+    with H.Simulation(hp) as c:
+        tc = c.restore(buf)
+        assert tc.aa == tb.aa
+        c.run_steps(tc, 4)
+        xc, vc = c.store_state()
+        c.read_output(str(tmp_path / "dump"))
+        xr, vr = c.store_state()
+    assert np.array_equal(xa, xc) and np.array_equal(va, vc)
+    assert np.array_equal(xr, xd) and np.array_equal(vr, vd)
+    hp48, _ = _pair(48)
+    with H.Simulation(hp48) as d:
+        with pytest.raises(H.HgpmError, match="does not fit"):
+            d.restore(buf)
+
+
 def test_step_host_roundtrip_equals_device_resident():
     hp, op = _pair(32)
     x0, v0, *_ = oracle_ics(op)
