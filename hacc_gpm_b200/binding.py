@@ -52,6 +52,10 @@ class _Params(C.Structure):
         ("pks", C.c_ubyte * HGPM_MAX_STEPS), ("dumps", C.c_ubyte * HGPM_MAX_STEPS),
         ("dump_init", C.c_int), ("dump_final", C.c_int),
         ("ref_quirks", C.c_int),
+        ("do_analysis", C.c_int),
+        ("analysis", C.c_ubyte * HGPM_MAX_STEPS),
+        ("analysis_dir", C.c_char * HGPM_PATH_MAX),
+        ("analysis_py", C.c_char * HGPM_PATH_MAX),
     ]
 
 
@@ -119,6 +123,7 @@ def lib() -> C.CDLL:
         "hgpm_power_spectrum": (C.c_int, [vp, C.c_int, C.c_int, P(C.c_double), P(C.c_double), P(C.c_int64)]),
         "hgpm_write_pk": (C.c_int, [C.c_char_p, C.c_int, P(C.c_double), P(C.c_double), P(C.c_int64)]),
         "hgpm_read_output": (C.c_int, [vp, C.c_char_p]),
+        "hgpm_analysis_rows": (C.c_int, [vp, P(C.c_float)]),
         "hgpm_checkpoint_bytes": (C.c_size_t, [vp]),
         "hgpm_checkpoint_save": (C.c_int, [vp, P(_Timestepper), vp, C.c_size_t]),
         "hgpm_checkpoint_load": (C.c_int, [vp, P(_Timestepper), vp, C.c_size_t]),
@@ -224,6 +229,7 @@ class Timestepper:
         lib().hgpm_ts_init(C.byref(self._raw), C.byref(params._raw))
 
     aa = property(lambda s: s._raw.aa)
+    z = property(lambda s: s._raw.z)
     adot = property(lambda s: s._raw.adot)
     fscal = property(lambda s: s._raw.fscal)
     deltaT = property(lambda s: s._raw.deltaT)
@@ -357,6 +363,13 @@ class Simulation:
 
     def store_state_device(self, x_ptr: int, v_ptr: int):
         self._ck(self.L.hgpm_store_state_device(self._h, C.c_void_p(x_ptr), C.c_void_p(v_ptr)))
+
+    def analysis_rows(self) -> np.ndarray:
+        """PyAnalysis's rows (py_analysis.cu:10-22): (np^3, 7) float32,
+        columns tag, x, y, z, vx, vy, vz."""
+        out = np.empty((self.npart, 7), np.float32)
+        self._ck(self.L.hgpm_analysis_rows(self._h, _f(out)))
+        return out
 
     def read_output(self, fname: str):
         """Load the state from a ``serial::writeOutput`` dump (io.cu:12-44)."""

@@ -121,7 +121,13 @@ extern "C" int hgpm_params_parse(const char* text, hgpm_params* out, char* err, 
         } else if (!strcmp(key, "PARTICLE_DUMP")) {
             int rc = mark_steps(p.dumps, value, err, errlen, key);
             if (rc) return rc;
-        } else if (!strcmp(key, "DUMP_INIT")) p.dump_init = 1;
+        } else if (!strcmp(key, "ANALYSIS_STEPS")) {
+            int rc = mark_steps(p.analysis, value, err, errlen, key);
+            if (rc) return rc;
+        } else if (!strcmp(key, "ANALYSIS_DIR")) snprintf(p.analysis_dir, sizeof(p.analysis_dir), "%s", value);
+        else if (!strcmp(key, "ANALYSIS_PY")) snprintf(p.analysis_py, sizeof(p.analysis_py), "%s", value);
+        else if (!strcmp(key, "DO_ANALYSIS")) p.do_analysis = 1;
+        else if (!strcmp(key, "DUMP_INIT")) p.dump_init = 1;
         else if (!strcmp(key, "DUMP_FINAL")) p.dump_final = 1;
         else if (!strcmp(key, "IPK")) snprintf(p.ipk, sizeof(p.ipk), "%s", value);
         else if (!strcmp(key, "OL")) p.ol = atof(value);
@@ -586,6 +592,22 @@ extern "C" int hgpm_checkpoint_load(hgpm_ctx* c, hgpm_timestepper* ts, const voi
     c->have_state = true;
     c->win_valid = false;
     if (ts) *ts = h.ts;
+    return HGPM_OK;
+}
+
+extern "C" int hgpm_analysis_rows(hgpm_ctx* c, float* rows) {
+    if (!c || !rows) return HGPM_ERR_ARG;
+    std::vector<float> x(c->npart * 3), v(c->npart * 3);
+    int rc = hgpm_store_state(c, x.data(), v.data());
+    if (rc) return rc;
+    for (size_t i = 0; i < c->npart; ++i) {
+        float* r = rows + 7 * i;
+        r[0] = (float)i;
+        for (int a = 0; a < 3; ++a) {
+            r[1 + a] = x[3 * i + a];
+            r[4 + a] = v[3 * i + a];
+        }
+    }
     return HGPM_OK;
 }
 

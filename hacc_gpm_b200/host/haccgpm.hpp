@@ -25,6 +25,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 
 #include "hgpm_c.h"
 
@@ -53,6 +54,9 @@ struct Params {
     bool dumps[HGPM_MAX_STEPS];
     char ipk[HGPM_PATH_MAX];
     bool do_analysis;
+    bool analysis[HGPM_MAX_STEPS];
+    char analysis_dir[HGPM_PATH_MAX];
+    char analysis_py[HGPM_PATH_MAX];
     int lastStep;
     int pkFolds;
     int world_rank, world_size;
@@ -125,6 +129,17 @@ void printTimers(CPUTimer_t init, CPUTimer_t total);
 // kick (bit-identical to the UpdatePositions/CIC/SolveGradient/
 // UpdateVelocities/UpdatePositions sequence); ts advances as that loop does.
 void RunSteps(Params& params, MemoryManager& mem, Timestepper& ts, int nsteps);
+
+// PyAnalysis (py_analysis.cu:3-27): with DO_ANALYSIS, at every step that
+// ANALYSIS_STEPS marks, the particles' rows (tag, x, y, z, vx, vy, vz; tag
+// the lattice index) go to the analysis code with the step, a and z.  The
+// reference passes them to Python through pycosmotools (a submodule absent
+// here); here the receiver is any callable.
+using AnalysisHook = std::function<void(const float* rows, int64_t n, int ncols, int step, double aa, double z)>;
+void Analysis(Params& params, MemoryManager& mem, Timestepper& ts, int step, const AnalysisHook& hook);
+// The driver's receiver: the rows as raw float32 [n][ncols] in
+// "<dir>/analysis.<step>" (dir "." when ANALYSIS_DIR is unset).
+void WriteAnalysisRows(const char* dir, const float* rows, int64_t n, int ncols, int step);
 
 }  // namespace serial
 }  // namespace HACCGPM

@@ -6,7 +6,9 @@
 // Writes what the reference's serial() writes: "<prefix>.params" (echo),
 // "<prefix>.pk.ini.fold.0", "<prefix>.pk.<step>.fold.0" for PK_DUMP steps,
 // "<prefix>.pk.fin.fold.0", and "<prefix>.particles.{ini,<step>,fin}" when
-// DUMP_INIT / PARTICLE_DUMP / DUMP_FINAL ask for them.  The phase calls are
+// DUMP_INIT / PARTICLE_DUMP / DUMP_FINAL ask for them (pk files for every
+// fold up to PK_FOLDS), and with DO_ANALYSIS the analysis rows of the
+// ANALYSIS_STEPS steps as "<ANALYSIS_DIR>/analysis.<step>".  The phase calls are
 // the reference's, one per line of its loop; --fused runs the steps between
 // two outputs through serial::RunSteps instead (same results, bit for bit:
 // consecutive drifts fold into the kick kernel).
@@ -45,7 +47,9 @@ static int serial(const char* params_file, bool fused) {
         if (fused) {
             // run to the next step that writes something
             int end = step;
-            while (end < params.lastStep - 1 && !params.pks[end] && !params.dumps[end]) ++end;
+            while (end < params.lastStep - 1 && !params.pks[end] && !params.dumps[end] &&
+                   !(params.do_analysis && params.analysis[end]))
+                ++end;
             serial::RunSteps(params, mem, ts, end - step + 1);
             step = end;
         } else {
@@ -65,6 +69,11 @@ static int serial(const char* params_file, bool fused) {
             snprintf(stepstr, sizeof(stepstr), "%s.particles.%d", params.prefix, step);
             serial::writeOutput(params, mem, stepstr);
         }
+        // driver_pm.cpp:137-139: the analysis rows, here written for the
+        // analysis code to read (ANALYSIS_DIR/analysis.<step>)
+        serial::Analysis(params, mem, ts, step, [&](const float* rows, int64_t n, int ncols, int s, double, double) {
+            serial::WriteAnalysisRows(params.analysis_dir, rows, n, ncols, s);
+        });
         ++step;
     }
 

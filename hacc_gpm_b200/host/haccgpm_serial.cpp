@@ -68,6 +68,10 @@ static void from_c(Params& p, const hgpm_params& c) {
     p.overload = c.overload;
     p.pk_bins = c.pk_bins;
     p.pk_log = c.pk_log != 0;
+    p.do_analysis = c.do_analysis != 0;
+    for (int i = 0; i < HGPM_MAX_STEPS; ++i) p.analysis[i] = c.analysis[i] != 0;
+    memcpy(p.analysis_dir, c.analysis_dir, sizeof(p.analysis_dir));
+    memcpy(p.analysis_py, c.analysis_py, sizeof(p.analysis_py));
 }
 
 hgpm_params to_c(const Params& p) {
@@ -105,6 +109,10 @@ hgpm_params to_c(const Params& p) {
     c.ol = p.ol;
     c.pk_bins = p.pk_bins;
     c.pk_log = p.pk_log ? 1 : 0;
+    c.do_analysis = p.do_analysis ? 1 : 0;
+    for (int i = 0; i < HGPM_MAX_STEPS; ++i) c.analysis[i] = p.analysis[i] ? 1 : 0;
+    memcpy(c.analysis_dir, p.analysis_dir, sizeof(c.analysis_dir));
+    memcpy(c.analysis_py, p.analysis_py, sizeof(c.analysis_py));
     hgpm_params_derive(&c);
     return c;
 }
@@ -264,6 +272,24 @@ void writeOutput(Params&, MemoryManager& mem, char* fname, int) {
 }
 
 double get_fscal(double m_aa, double m_adot, double m_omega_cb) { return hgpm_get_fscal(m_aa, m_adot, m_omega_cb, 1); }
+
+void Analysis(Params& params, MemoryManager& mem, Timestepper& ts, int step, const AnalysisHook& hook) {
+    if (!params.do_analysis || step < 0 || step >= HGPM_MAX_STEPS || !params.analysis[step] || !hook) return;
+    printf("Doing Analysis Step\n");
+    const int64_t n = (int64_t)params.np * params.np * params.np;
+    std::vector<float> rows((size_t)n * 7);
+    check(mem.ctx, hgpm_analysis_rows(mem.ctx, rows.data()), "Analysis");
+    hook(rows.data(), n, 7, step, ts.aa, ts.z);
+}
+
+void WriteAnalysisRows(const char* dir, const float* rows, int64_t n, int ncols, int step) {
+    char fname[2 * HGPM_PATH_MAX];
+    snprintf(fname, sizeof(fname), "%s/analysis.%d", (dir && dir[0]) ? dir : ".", step);
+    FILE* fp = fopen(fname, "wb");
+    if (!fp) die("Analysis", fname);
+    fwrite(rows, sizeof(float) * ncols, (size_t)n, fp);
+    fclose(fp);
+}
 
 void RunSteps(Params&, MemoryManager& mem, Timestepper& ts, int nsteps) {
     hgpm_timestepper t = ts.to_c();

@@ -63,6 +63,12 @@ typedef struct hgpm_params {
     int dump_init, dump_final;
     int ref_quirks;                 /* 1 (default): float dtdy / float growth
                                        exactly as the reference; 0: FP64    */
+    /* analysis hook (params.cpp:195-214): DO_ANALYSIS, ANALYSIS_STEPS,
+       ANALYSIS_DIR, ANALYSIS_PY */
+    int do_analysis;
+    unsigned char analysis[HGPM_MAX_STEPS];
+    char analysis_dir[HGPM_PATH_MAX];
+    char analysis_py[HGPM_PATH_MAX];
 } hgpm_params;
 
 /* Replaces HACCGPM::read_params (src/simulation/params.cpp:72-250).
@@ -123,6 +129,10 @@ int hgpm_store_state(hgpm_ctx* ctx, float* x_host, float* v_host);
 /* Same as above, but pointers are DEVICE pointers (stream-ordered).        */
 int hgpm_load_state_device(hgpm_ctx* ctx, const float* x_dev, const float* v_dev);
 int hgpm_store_state_device(hgpm_ctx* ctx, float* x_dev, float* v_dev);
+/* The rows PyAnalysis hands to the analysis code (py_analysis.cu:10-22):
+ * per particle, in lattice order, 7 floats (tag, x, y, z, vx, vy, vz), tag
+ * the particle's lattice index (exact as a float up to 2^24 particles).   */
+int hgpm_analysis_rows(hgpm_ctx* ctx, float* rows_host);
 /* Linear cell index (ix*ng+iy)*ng+iz of every particle's CIC base cell
  * (the reference's `int i = x` truncation, cic_pm.cu:52-54).              */
 int hgpm_get_cells(hgpm_ctx* ctx, int32_t* cells_host);

@@ -110,6 +110,35 @@ def test_driver_writes_every_fold(tmp_path):
 
 
 @pytest.mark.gpu
+def test_analysis_hook_and_python_driver(tmp_path):
+    """DO_ANALYSIS / ANALYSIS_STEPS (PyAnalysis, py_analysis.cu:3-27): the C++
+    driver writes the rows (tag, x, y, z, vx, vy, vz) of the marked steps;
+    the Python driver hands the same rows to a callable and writes the same
+    pk and particle files."""
+    from hacc_gpm_b200 import driver as D
+
+    extra = "LAST_STEP 5\nPK_DUMP 2\nPARTICLE_DUMP 3\nDUMP_FINAL\nPK_FOLDS 1\nDO_ANALYSIS\nANALYSIS_STEPS 1,3\n"
+    dc, _ = _case(tmp_path, "cpp", extra=extra + "ANALYSIS_DIR %s\n" % (tmp_path / "cpp"))
+    r = subprocess.run([_driver(), str(dc / "input.params"), "--fused"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    dp, _ = _case(tmp_path, "py", extra=extra)
+    seen = {}
+    D.serial(str(dp / "input.params"), analysis=lambda rows, step, a, z: seen.__setitem__(step, (rows.copy(), a, z)))
+    assert sorted(seen) == [1, 3]
+    n3 = 32 ** 3
+    for step, (rows, a, z) in seen.items():
+        assert rows.shape == (n3, 7) and np.array_equal(rows[:, 0], np.arange(n3, dtype=np.float32))
+        assert 0 < a < 1 and z > 0
+        cpp = np.fromfile(str(dc / ("analysis.%d" % step)), dtype="<f4").reshape(n3, 7)
+        assert np.array_equal(cpp, rows)
+    dump3 = np.fromfile(str(dp / "run.particles.3"), dtype="<f4")
+    assert np.array_equal(seen[3][0][:, 1:4].reshape(-1), dump3[:3 * n3])
+    for f in ("run.pk.ini.fold.0", "run.pk.ini.fold.1", "run.pk.2.fold.0", "run.pk.fin.fold.1", "run.particles.3",
+              "run.particles.fin"):
+        assert (dc / f).read_bytes() == (dp / f).read_bytes(), f
+
+
+@pytest.mark.gpu
 def test_driver_fused_equals_plain(tmp_path):
     runs = []
     for name, flags in (("a", []), ("b", ["--fused"])):
