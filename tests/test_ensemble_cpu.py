@@ -59,3 +59,16 @@ def test_capacity_by_footprint():
 def test_bad_class_rejected_without_gpu():
     with pytest.raises(H.HgpmError, match="NG/NP must be one of"):
         E.Ensemble([(20, 20, 2)])
+
+
+def test_capacity_capped_by_batched_step_time():
+    """With step_ms the large classes hold only the slots whose batched step
+    takes about that long (256^3: ~0.95 ms each, so 2 at 2 ms); the small
+    classes keep their memory share."""
+    sizes = (32, 64, 128, 256)
+    free = S.class_capacity(sizes, 40e9, max_slots=64)
+    capped = S.class_capacity(sizes, 40e9, max_slots=64, step_ms=2.0)
+    by = {ng: n for ng, _, n in capped}
+    assert by[256] == 2 and by[128] == round(2.0 / (S.STEP_MS_PER_UNIT * 2 * 128 ** 3))
+    assert by[32] == 64 and by[64] == 64
+    assert all(c[2] <= f[2] for c, f in zip(capped, free))
