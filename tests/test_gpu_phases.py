@@ -46,7 +46,7 @@ def test_drift_matches_oracle(ng):
     assert np.array_equal(vg, v)
 
 
-@pytest.mark.parametrize("ng,np_side", [(32, 32), (48, 48), (64, 32)])
+@pytest.mark.parametrize("ng,np_side", [(32, 32), (48, 48), (64, 32), (32, 64), (24, 48)])
 def test_deposit_deterministic_and_matches_oracle(ng, np_side):
     x, v = lattice_state(np_side, ng, disp=1.5, seed=5)
     with make(ng, np_side) as s:
@@ -137,7 +137,7 @@ def test_deposit_configurations_bit_identical(ng, disp, monkeypatch):
     assert np.array_equal(out[0], out[1])
 
 
-@pytest.mark.parametrize("ng,np_side,disp", [(32, 32, 1.0), (48, 48, 1.0), (64, 32, 1.0), (64, 64, 0.3),
+@pytest.mark.parametrize("ng,np_side,disp", [(32, 32, 1.0), (48, 48, 1.0), (64, 32, 1.0), (32, 64, 1.0), (64, 64, 0.3),
                                              (64, 64, 4.0)])
 def test_kick_variants_bit_identical(ng, np_side, disp, monkeypatch):
     """Tiled (shared-memory force window), flat (global gather) and float4
