@@ -98,6 +98,38 @@ template <bool INV> struct Dft<8, INV> {
 // NS = product of the radices of the previous stages.  TP: radix-4/8
 // twiddles beyond the loaded powers formed as products (fewer loads, more
 // registers; a pass whose registers are capped keeps TP false).
+// Twiddles and radix-R DFT of butterfly k (k = j % NS) of a stage, in place
+// on the R values of the butterfly.
+template <int N, int NS, int R, bool INV, int TWS, bool TP>
+__device__ __forceinline__ void stage_butterfly(float2* v, int k, const float2* __restrict__ tw) {
+    if (NS > 1) {
+        const int m = k * (N / (NS * R));  // twiddle r is tw[r * m]
+        if (TP && (R == 8 || R == 4)) {
+            // powers 1, 2 (and 4) from the table, the rest as products
+            // (one extra rounding each): fewer loads per butterfly
+            float2 w[R];
+            w[1] = __ldg(&tw[TWS * m]);
+            w[2] = __ldg(&tw[TWS * 2 * m]);
+            w[3] = cmul(w[1], w[2]);
+            if (R == 8) {
+                w[4] = __ldg(&tw[TWS * 4 * m]);
+                w[5] = cmul(w[1], w[4]);
+                w[6] = cmul(w[2], w[4]);
+                w[7] = cmul(w[3], w[4]);
+            }
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[r] = INV ? cmulc(v[r], w[r]) : cmul(v[r], w[r]);
+        } else {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                const float2 w = __ldg(&tw[TWS * (r * m)]);
+                v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
+            }
+        }
+    }
+    Dft<R, INV>::run(v);
+}
+
 template <int N, int C, int ES, int NS, int R, bool INV, int NT, int TWS, bool TP>
 __device__ __forceinline__ void fft_stage(float2* __restrict__ buf, const float2* __restrict__ tw) {
     constexpr int NB = N / R;        // butterflies per line
@@ -121,35 +153,51 @@ __device__ __forceinline__ void fft_stage(float2* __restrict__ buf, const float2
         if ((TOT % NT) == 0 || b < TOT) {
             const int c = b % C, j = b / C;
             const int k = j % NS;
-            if (NS > 1) {
-                const int m = k * (N / (NS * R));  // twiddle r is tw[r * m]
-                if (TP && (R == 8 || R == 4)) {
-                    // powers 1, 2 (and 4) from the table, the rest as products
-                    // (one extra rounding each): fewer loads per butterfly
-                    float2 w[R];
-                    w[1] = __ldg(&tw[TWS * m]);
-                    w[2] = __ldg(&tw[TWS * 2 * m]);
-                    w[3] = cmul(w[1], w[2]);
-                    if (R == 8) {
-                        w[4] = __ldg(&tw[TWS * 4 * m]);
-                        w[5] = cmul(w[1], w[4]);
-                        w[6] = cmul(w[2], w[4]);
-                        w[7] = cmul(w[3], w[4]);
-                    }
-#pragma unroll
-                    for (int r = 1; r < R; ++r) v[t][r] = INV ? cmulc(v[t][r], w[r]) : cmul(v[t][r], w[r]);
-                } else {
-#pragma unroll
-                    for (int r = 1; r < R; ++r) {
-                        const float2 w = __ldg(&tw[TWS * (r * m)]);
-                        v[t][r] = INV ? cmulc(v[t][r], w) : cmul(v[t][r], w);
-                    }
-                }
-            }
-            Dft<R, INV>::run(v[t]);
+            stage_butterfly<N, NS, R, INV, TWS, TP>(v[t], k, tw);
             const int base = (j / NS) * NS * R + k;
 #pragma unroll
             for (int r = 0; r < R; ++r) buf[(base + r * NS) * ES + c] = v[t][r];
+        }
+    }
+    __syncthreads();
+}
+
+// The last stage of a forward transform, a per-mode operator and the first
+// stage of the inverse transform in one pass.  With the forward radices
+// R_1..R_L, the last forward stage (NS = N / R_L) leaves butterfly j's outputs
+// at modes j + r N / R_L, which are exactly the inputs of butterfly j of an
+// inverse stage of radix R_L with NS = 1; the inverse then runs the radices in
+// reverse order.  So the operator is applied in registers and the tile makes
+// one shared-memory round trip instead of three.  op(e, c, v): mode e of line
+// c.
+template <int N, int C, int ES, int R, int NT, int TWS, bool TP, class F>
+__device__ __forceinline__ void fft_turn_stage(float2* __restrict__ buf, const float2* __restrict__ tw, const F& op) {
+    constexpr int NB = N / R, NS = N / R;
+    constexpr int TOT = NB * C;
+    constexpr int PER = (TOT + NT - 1) / NT;
+    float2 v[PER][R];
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int b = tid + t * NT;
+        if ((TOT % NT) == 0 || b < TOT) {
+            const int c = b % C, j = b / C;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[t][r] = buf[(j + r * NB) * ES + c];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int b = tid + t * NT;
+        if ((TOT % NT) == 0 || b < TOT) {
+            const int c = b % C, j = b / C;
+            stage_butterfly<N, NS, R, false, TWS, TP>(v[t], j, tw);
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[t][r] = op(j + r * NS, c, v[t][r]);
+            stage_butterfly<N, 1, R, true, TWS, TP>(v[t], 0, tw);
+#pragma unroll
+            for (int r = 0; r < R; ++r) buf[(j * R + r) * ES + c] = v[t][r];
         }
     }
     __syncthreads();
@@ -184,11 +232,44 @@ template <> struct Plan<512> { using type = RSeq<8, 8, 8>; };
 template <> struct Plan<768> { using type = RSeq<3, 8, 8, 4>; };
 template <> struct Plan<1024> { using type = RSeq<8, 8, 4, 4>; };
 
+// Radix sequence helpers: all but the last radix, the last radix, reversal.
+template <int R, class S> struct SeqCons;
+template <int R, int... Ts> struct SeqCons<R, RSeq<Ts...>> { using type = RSeq<R, Ts...>; };
+template <class S> struct SeqInit;
+template <int R> struct SeqInit<RSeq<R>> { using type = RSeq<>; };
+template <int R, int R2, int... Rs> struct SeqInit<RSeq<R, R2, Rs...>> {
+    using type = typename SeqCons<R, typename SeqInit<RSeq<R2, Rs...>>::type>::type;
+};
+template <class S> struct SeqLast;
+template <int R> struct SeqLast<RSeq<R>> { static constexpr int value = R; };
+template <int R, int R2, int... Rs> struct SeqLast<RSeq<R, R2, Rs...>> {
+    static constexpr int value = SeqLast<RSeq<R2, Rs...>>::value;
+};
+template <class S, class Acc = RSeq<>> struct SeqRev;
+template <int... As> struct SeqRev<RSeq<>, RSeq<As...>> { using type = RSeq<As...>; };
+template <int R, int... Rs, int... As> struct SeqRev<RSeq<R, Rs...>, RSeq<As...>> {
+    using type = typename SeqRev<RSeq<Rs...>, RSeq<R, As...>>::type;
+};
+
 // Transform all C lines of the tile (natural order in, natural order out).
 // Caller must __syncthreads() after filling the tile; returns synchronised.
 template <int N, int C, int ES, bool INV, int NT, int TWS = 1, bool TP = true>
 __device__ __forceinline__ void fft_tile(float2* buf, const float2* __restrict__ tw) {
     fft_stages<N, C, ES, INV, NT, TWS, TP, 1>(buf, tw, typename Plan<N>::type{});
+}
+
+// Forward transform, op(e, c, v) on every mode e of every line c, inverse
+// transform (radices in reverse order), with the last forward and first
+// inverse stages fused around op (fft_turn_stage).  Natural order in and out;
+// caller synchronises after filling the tile; returns synchronised.
+template <int N, int C, int ES, int NT, int TWS, bool TP, class F>
+__device__ __forceinline__ void fft_tile_fwd_op_inv(float2* buf, const float2* __restrict__ tw, const F& op) {
+    using P = typename Plan<N>::type;
+    using Init = typename SeqInit<P>::type;
+    constexpr int RL = SeqLast<P>::value;
+    fft_stages<N, C, ES, false, NT, TWS, TP, 1>(buf, tw, Init{});
+    fft_turn_stage<N, C, ES, RL, NT, TWS, TP>(buf, tw, op);
+    fft_stages<N, C, ES, true, NT, TWS, TP, RL>(buf, tw, typename SeqRev<Init>::type{});
 }
 
 }  // namespace hgpm

@@ -26,7 +26,10 @@ struct PotentialOp {
     __device__ __forceinline__ float2 pre(int ix, int iy, int iz, float2 v) const {
         const double s = __ldg(&cosq[ix]) + __ldg(&cosq[iy]) + __ldg(&cosq[iz]);
         const float g = (s == 0.0) ? 0.f : (float)(coeff / s);
-        return make_float2(v.x * g, v.y * g);
+        // explicit roundings: the product is never contracted into the
+        // butterfly arithmetic around it, so every kernel that applies this
+        // operator between its transforms gets the same bits
+        return make_float2(__fmul_rn(v.x, g), __fmul_rn(v.y, g));
     }
     __device__ __forceinline__ float2 comp(int, int, int, int, float2 t) const { return t; }
 };

@@ -172,24 +172,18 @@ __global__ void __launch_bounds__(NT, 768 / NT) xpotential_tma_kernel(const __gr
         const TileIdx ti = tile_of(t, nchunks, NG);
         const int iy = ti.plane, col0 = ti.chunk * CT;
         float2* tile = in[cur];
-        fft_tile<NG, CT, CT, false, NT, 1, true>(tile, tw);
-        // t = G rho_k (PotentialOp::pre with the table in shared memory)
+        // forward x FFT, t = G rho_k (PotentialOp::pre with the table in
+        // shared memory, in registers between the two transforms), the
+        // potential's inverse x FFT; the gradient is taken in real space
+        // (gradient_kernel)
         const double cy = cosq[iy];
-        for (int i = threadIdx.x; i < NG * CT; i += NT) {
-            const int ix = i / CT, iz = col0 + i % CT;
-            float2 v = make_float2(0.f, 0.f);
-            if (iz < ncols) {
-                const double sum = cosq[ix] + cy + cosq[iz];
-                const float g = (sum == 0.0) ? 0.f : (float)(coeff / sum);
-                v = tile[i];
-                v = make_float2(v.x * g, v.y * g);
-            }
-            tile[i] = v;
-        }
-        __syncthreads();
-        // the potential's inverse x transform; the gradient is taken in real
-        // space (gradient_kernel)
-        fft_tile<NG, CT, CT, true, NT, 1, true>(tile, tw);
+        fft_tile_fwd_op_inv<NG, CT, CT, NT, 1, true>(tile, tw, [&](int ix, int c, float2 v) {
+            const int iz = col0 + c;
+            if (iz >= ncols) return make_float2(0.f, 0.f);
+            const double sum = cosq[ix] + cy + cosq[iz];
+            const float g = (sum == 0.0) ? 0.f : (float)(coeff / sum);
+            return make_float2(__fmul_rn(v.x, g), __fmul_rn(v.y, g));  // as PotentialOp::pre
+        });
         store_rows<NG, CT, NT>(tile, out + (size_t)iy * zs + col0, rs, ncols - col0);
         // the next TMA load into this buffer follows generic-proxy writes
         fence_async_shared();
