@@ -80,10 +80,11 @@ KERNEL_NAMES = {
     "deposit": "deposit_tiled_kernel<16,1,512,2> + deposit_spill_kernel<16,1,1024> (queued wide blocks)",
     "fft_z_fwd": "zpass_r2c_kernel<NG,1>",
     "fft_y_fwd": "strided_tma_kernel<NG,0,0>",
-    "poisson_x": "xpotential_tma_kernel<NG,512> (forward x, Green's function, inverse x)",
+    "poisson_x": "xpotential_tma_kernel<NG,256> (forward x, Green's function, inverse x)",
     "fft_y_inv": "strided_tma_kernel<NG,1,0>",
-    "fft_z_inv": "zpass_c2r_kernel<NG> (the potential) + gradient_kernel (central differences, float4 force)",
-    "kick_drift": "kick_spill_kernel<16> (flat: one particle per thread, float4 force gathers)",
+    "fft_z_inv": "zpass_c2r_kernel<NG> (the potential) + gradient_kernel<8,3,2> (central differences, float4 force)",
+    "kick_drift": "kick_flat_nt_kernel<16,1024> (flat: one particle per thread, four x-planes per CTA, "
+                  "float4 force gathers)",
 }
 
 
