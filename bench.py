@@ -83,8 +83,8 @@ KERNEL_NAMES = {
     "poisson_x": "xpotential_tma_kernel<NG,256> (forward x, Green's function, inverse x)",
     "fft_y_inv": "strided_tma_kernel<NG,1,0>",
     "fft_z_inv": "zpass_c2r_kernel<NG> (the potential) + gradient_kernel<8,3,2> (central differences, float4 force)",
-    "kick_drift": "kick_flat_nt_kernel<16,1024> (flat: one particle per thread, four x-planes per CTA, "
-                  "float4 force gathers)",
+    "kick_drift": "kick_flat_nt_kernel<16,1024,4> (flat: one particle per thread, a 16^3 block per CTA run "
+                  "as four units of four x-planes, float4 force gathers)",
 }
 
 

@@ -728,35 +728,43 @@ __global__ void __launch_bounds__(256) kick_spill_kernel(ParticleSoA p, int ng, 
     }
 }
 
-// Flat kick over every block with NT threads per CTA: a work item is NT / B^2
+// Flat kick over every block with NT threads per CTA: a unit is NT / B^2
 // consecutive Lagrangian x-planes of a block, so the force-grid planes that
 // neighbouring x-planes share are gathered by warps of the same SM and meet
 // in its L1 (kick_spill_kernel's 256-thread items put neighbouring planes on
-// different SMs).  Arithmetic as kick_spill_kernel, bit for bit.
-template <int B, int NT>
+// different SMs); a CTA takes runs of R consecutive units, the next particle
+// always loaded one unit ahead.  Arithmetic as kick_spill_kernel, bit for
+// bit.
+template <int B, int NT, int R = 1>
 __global__ void __launch_bounds__(NT, 1024 / NT) kick_flat_nt_kernel(ParticleSoA p, int ng, const float4* __restrict__ f,
                                                                    double deltaT, double fscal, float pf_a, float pf_b,
                                                                    int ndrift, int nblocks, Slots sl, KickSched ks) {
     constexpr int B3 = B * B * B, SUB = B3 / NT;
     const int slot = blockIdx.y;
     if (slot_idle(sl, slot)) return;
-    const int n = nblocks * SUB;
-    if ((int)blockIdx.x >= n) return;
+    const int n = nblocks * SUB;  // units of NT particles; a CTA takes runs of R consecutive units
+    if ((int)blockIdx.x * R >= n) return;
     p = offset_soa(p, (size_t)slot * sl.s0);
     f += (size_t)slot * sl.s1;
     float dtf;
     kick_scalars(ks, slot, deltaT, fscal, dtf, pf_a, pf_b, ndrift);
-    auto index = [&](int w) { return (size_t)(w / SUB) * B3 + (w % SUB) * NT + threadIdx.x; };
-    size_t inext = index(blockIdx.x);
+    auto index = [&](int u) { return (size_t)(u / SUB) * B3 + (u % SUB) * NT + threadIdx.x; };
+    auto unit = [&](int k) { return ((int)blockIdx.x + (k / R) * (int)gridDim.x) * R + k % R; };
+    int k = 0;
+    size_t inext = index(unit(0));
     PState next = load_p(p, inext);
-    for (int w = blockIdx.x; w < n; w += gridDim.x) {
+    for (;;) {
         const size_t i = inext;
         const PState cur = next;
-        if (w + (int)gridDim.x < n) {
-            inext = index(w + gridDim.x);
+        const int un = unit(k + 1);
+        const bool more = un < n;
+        if (more) {
+            inext = index(un);
             next = load_p(p, inext);
         }
         finish_p(p, i, cur, gather_global(f, cur, KickWeights(cur, dtf), ng), pf_a, pf_b, ndrift, ng);
+        if (!more) break;
+        ++k;
     }
 }
 
@@ -1054,11 +1062,12 @@ static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const fl
     const int sp_grid = num_sms() * blocks_per_sm_once((const void*)ksp, 256, 0);
     if (force_flat) {
         if constexpr (B == 16) {
-            // four x-planes of a block per 1024-thread CTA: measured at 512^3
-            // mid-run 2.15 ms against 2.18 (two planes, 512 threads) and 2.28
-            // (one plane, kick_spill_kernel's 256 threads)
+            // 1024-thread CTAs, each taking a whole block as four units of four
+            // x-planes: measured at 512^3 mid-run 2.03 ms, against 2.04 (runs
+            // of two units), 2.08 (one unit), 2.18 (two planes per 512-thread
+            // CTA) and 2.25-2.28 (one plane, kick_spill_kernel's 256 threads)
             const int nblocks = (np_side / B) * (np_side / B) * (np_side / B);
-            auto kf = kick_flat_nt_kernel<B, 1024>;
+            auto kf = kick_flat_nt_kernel<B, 1024, 4>;
             const int grid = num_sms() * blocks_per_sm_once((const void*)kf, 1024, 0);
             kf<<<dim3(grid, nslots), 1024, 0, s>>>(p, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, nblocks, sl, ks);
             return cudaGetLastError();
