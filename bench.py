@@ -57,7 +57,7 @@ NSTEPS_RUN = 100  # step size of the run the timed steps belong to (z 50 -> 0 in
 MID_STEP = 45     # the timed steps start here (the mid-run cost is the run's average)
 
 # Algorithmic bytes per launch of each kernel (precision-form state:
-# x = 12 B offset + 4 B cell, v = 12 B; FP32 grids).  Sum = 72 Np + 64 Ng.
+# x = 12 B offset + 4 B cell, v = 12 B; FP32 grids).  Sum = 72 Np + 56 Ng.
 def alg_bytes(np3, ng3):
     """Algorithmic bytes per phase: each input read once, each output
     written once (FP32, 12 B per force vector).  The gradient is taken in
