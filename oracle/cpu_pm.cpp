@@ -1,6 +1,6 @@
 // cpu_pm.cpp — OpenMP C++ transcription of HACC_GPM's serial PM step.
 //
-// TEST / BASELINE INFRASTRUCTURE ONLY.  The reference has no CPU or FFTW
+// TEST AND CPU-BASELINE INFRASTRUCTURE ONLY.  The reference has no CPU or FFTW
 // path; this program restates its serial CUDA routines on the host, in the
 // reference's own layout and precision (float3 positions and velocities, a
 // float complex grid, float atomics), so that bench.py can time "the

@@ -1,6 +1,6 @@
 """FP64 CPU restatement of HACC_GPM's serial particle-mesh path.
 
-TEST INFRASTRUCTURE ONLY.  This module is the checker that the CUDA path is
+TEST INFRASTRUCTURE ONLY.  This module is the oracle that the CUDA path is
 compared against.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
 ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` may import it; the
 product (``hacc_gpm_b200`` and its C-ABI library) never does.

@@ -13,8 +13,9 @@ packs its outputs:
   fin_x/v  positions/velocities after NSTEPS steps of its run loop
   pk_ini   its P(k) CSV lines of the ICs, pk_fin of the final state
 
-Usage (on the GPU box, from the repository root):
-    python tests/golden/make_refgpu_fixtures.py --out gpurun_out/golden
+Usage (on a machine with a B200 and the built refpm, from the repository
+root; the .npz files then go to tests/golden/):
+    python tests/golden/make_refgpu_fixtures.py --out refgpu_out
 Every input is seeded; PK_FOLDS is 0 (fold > 0 writes out of bounds in the
 reference's BinPower).
 """
@@ -104,7 +105,7 @@ def make_case(name, out):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default="gpurun_out/golden")
+    ap.add_argument("--out", default="refgpu_out")
     ap.add_argument("--cases", default=",".join(CASES))
     a = ap.parse_args()
     if not os.path.exists(REFPM):

@@ -9,7 +9,7 @@ import numpy as np
 from hacc_gpm_b200 import ipk as ipkmod
 from oracle import pm_oracle as O
 
-# Tolerances (north star): fields 1e-5 relative to the field's max, final
+# Parity bars: fields 1e-5 relative to the field's max, final
 # positions 1e-4 of the box side, P(k) 0.1 % per bin.
 FIELD_RTOL = 1e-5
 POS_BOX_TOL = 1e-4

@@ -16,9 +16,9 @@ CASES = ("a32", "b24")
 IC_POS_CELLS = 1e-5      # Zel'dovich positions, absolute, in cells
 IC_VEL_REL = 1e-5        # velocities, relative to the max
 RHO_REL = 1e-6           # density, relative to the max (reference: float atomics)
-FORCE_REL = 1e-5         # force grids, relative to the max (north star: 1e-5 on the field)
-POS_BOX = 1e-4           # positions after N steps, fraction of the box (north star)
-PK_REL = 1e-3            # P(k) per bin (north star: 0.1 %)
+FORCE_REL = 1e-5         # force grids, relative to the max (the 1e-5 field bar)
+POS_BOX = 1e-4           # positions after N steps, fraction of the box
+PK_REL = 1e-3            # P(k) per bin (0.1 %)
 
 
 class Case:

@@ -1,7 +1,7 @@
 """Reference match: the B200 path against outputs of the reference's own
 serial CUDA path on identical inputs (its cuRAND noise and its ICs), through
-the C-ABI.  Bars in tests/refgpu.py (north star: 1e-5 on fields, 1e-4 of the
-box on positions after N steps, 0.1 % per P(k) bin)."""
+the C-ABI.  Bars in tests/refgpu.py (1e-5 on fields, 1e-4 of the box on
+positions after N steps, 0.1 % per P(k) bin)."""
 import numpy as np
 import pytest
 
