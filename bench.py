@@ -2,29 +2,39 @@
 """Headline benchmark: PM steps per second of particles at 512^3.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--config NS|C] [--workload step|ensemble|serve]
 
 One process per GPU (torchrun for N > 1).  Each rank advances its own
 independent box (replicas: the step itself has no collective), so scaling
-is weak.  The workload is a 100-step run from z = 50 to z = 0; the cost of
-a step grows as the particles cluster (about 7 ms early, 10.6 ms at z = 0 on
-one B200), and the middle of the run costs about the run's average.  So
-the run is advanced untimed to step 45 - W, then W warm-up steps, then
-exactly K timed steps (CUDA events on the box's stream, barrier +
-synchronize on both sides, max over ranks; per-kernel events inside the
-same region).  value = particle updates of all ranks / that time.  The
-whole 100-step run is also timed once ("full_run").
+is weak.  --config NS (default): 512^3 particles on a 512^3 grid, L = 512
+Mpc/h, a 100-step run from z = 50 to z = 0.  --config C: 512^3 particles on a
+1024^3 grid, L = 1000 Mpc/h, a 200-step run from z = 50.  The cost of a step
+grows as the particles cluster and the middle of the run costs about the
+run's average, so the run is advanced untimed to step MID - W (45 of 100, 90
+of 200), then W warm-up steps, then exactly K timed steps (CUDA events on
+the box's stream, barrier + synchronize on both sides, max over ranks;
+per-kernel events inside the same region).  value = particle updates of all
+ranks / that time.  The ICs are the reference's own: EH no-wiggle Zel'dovich
+displacements from its cuRAND white noise for SEED 21082001 (+ rank).  The
+whole run is also timed once ("full_run").
 
 Also reported (rank 0): per-kernel timings and the roofline of the dominant
 kernel against the measured HBM peak, the end-to-end number through the
 C-ABI with host buffers (hgpm_step_host: H2D of the state, one step, D2H of
 the state, every step), the CPU baseline (the OpenMP C++ transcription of
-the reference's serial step on this host's cores), kernel launch count and
-SM clocks sampled during the timed region.
+the reference's serial step on this host's cores, on the same state), kernel
+launch count, SM clocks sampled during the timed region, and (N = 1,
+--config NS) the batched forms: the 96-box ensemble and the serving loop
+against the same work one box at a time ("forms"; --no-forms skips them).
 
 --impl reference times the reference's algorithm on the host cores (the
-reference has no CPU path; oracle/_bin/cpu_pm is its OpenMP transcription).
+reference has no CPU path; oracle/_bin/cpu_pm is its OpenMP transcription)
+on the same state and steps: the reference's own serial CUDA code
+(oracle/_ref/refpm, built from its sources) makes the ICs from the same SEED
+and advances them to the first warm-up step, then the transcription runs
+the W warm-up and K timed steps.  Its line carries the same config.
 
---workload ensemble | serve (1 GPU) measure the batched forms instead:
+--workload ensemble | serve (1 GPU) print only the batched form's line:
   ensemble  96 boxes, ng = np from {32, 48, 64, 96, 128}, L ~ U[64, 512],
             sigma8 ~ U[0.7, 0.9], z 100, 64 steps each: sims/hour batched
             (one launch per phase per size class, CUDA graph) against the
@@ -48,13 +58,24 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "particle-updates/s at 512^3"
 UNIT = "particle-updates/s"
-NG = NP = 512
-RL = 512.0
+SEED = 21082001
 Z_INI = 50.0
-NSTEPS_RUN = 100  # step size of the run the timed steps belong to (z 50 -> 0 in 100 steps)
-MID_STEP = 45     # the timed steps start here (the mid-run cost is the run's average)
+# the box of each --config: (ng, np, rl, steps in the run, first timed step)
+CONFIGS = {"NS": (512, 512, 512.0, 100, 45), "C": (1024, 512, 1000.0, 200, 90)}
+NG, NP, RL, NSTEPS_RUN, MID_STEP = CONFIGS["NS"]
+
+
+def metric_name():
+    if NG == NP:
+        return "particle-updates/s at %d^3" % NP
+    return "particle-updates/s at %d^3 particles on a %d^3 grid" % (NP, NG)
+
+
+def first_warmup_step(steps, warmup):
+    """The run is advanced untimed to this step; W warm-up steps follow, then
+    the K timed steps."""
+    return max(0, min(MID_STEP, NSTEPS_RUN - steps) - warmup)
 
 # Algorithmic bytes per launch of each kernel (precision-form state:
 # x = 12 B offset + 4 B cell, v = 12 B; FP32 grids).  Sum = 72 Np + 56 Ng.
@@ -77,7 +98,8 @@ def alg_bytes(np3, ng3):
 
 # The kernels of each phase (one launch each per step, unless noted).
 KERNEL_NAMES = {
-    "deposit": "deposit_tiled_kernel<16,1,512,2> + deposit_spill_kernel<16,1,1024> (queued wide blocks)",
+    "deposit": "deposit_col_kernel<16,4,4> (autotuned choice; 32-bit windows, x-half split) + "
+               "deposit_spill_kernel<16,1,1024> (queued wide blocks)",
     "fft_z_fwd": "zpass_r2c_kernel<NG,1>",
     "fft_y_fwd": "strided_tma_kernel<NG,0,0>",
     "poisson_x": "xpotential_tma_kernel<NG,256> (forward x, Green's function, inverse x)",
@@ -146,38 +168,82 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(steps=1, warmup=0, ng=None, np_side=None):
-    ng = NG if ng is None else ng  # the box size set by --size (read at call time)
-    np_side = NP if np_side is None else np_side
+def cosmo_args(params):
+    """Cosmology of the run for the CPU transcription's time stepper."""
+    return ["--omega-cb", repr(params.omega_cb), "--omega-m", repr(params.omega_matter),
+            "--omega-r", repr(params.omega_radiation), "--f-nu", repr(params.f_nu_massless)]
+
+
+def cpu_baseline(steps=1, warmup=0, load=None, start_step=0, cosmo=()):
+    """The OpenMP C++ transcription of the reference's serial step on all host
+    threads: `warmup` + `steps` steps from `load` (x then v, float3, lattice
+    order) at step `start_step` of the run, or from a seeded lattice."""
     exe = os.path.join(ROOT, "oracle", "_bin", "cpu_pm")
     if not os.path.exists(exe):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "cpu"], check=True)
-    out = subprocess.run([exe, "--ng", str(ng), "--np", str(np_side), "--rl", str(RL), "--zini", str(Z_INI),
-                          "--nsteps-total", str(NSTEPS_RUN), "--steps", str(steps), "--warmup", str(warmup)],
-                         capture_output=True, text=True, check=True)
+    cmd = [exe, "--ng", str(NG), "--np", str(NP), "--rl", str(RL), "--zini", str(Z_INI),
+           "--nsteps-total", str(NSTEPS_RUN), "--steps", str(steps), "--warmup", str(warmup), *cosmo]
+    if load:
+        cmd += ["--load", load, "--start-step", str(start_step)]
+    out = subprocess.run(cmd, capture_output=True, text=True, check=True)
     return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def run_params_text(rank=0, prefix="run", ipk="run.ipk", extra=""):
+    from hacc_gpm_b200 import ipk as ipkmod
+    return ipkmod.lcdm_params_text(NG, NP, RL, Z_INI, NSTEPS_RUN, seed=SEED + rank, prefix=prefix, ipk=ipk,
+                                   extra=extra)
+
+
+def run_ipk(params):
+    """The .ipk of the run (EH no-wiggle, sigma8-normalised, at z_ini)."""
+    from hacc_gpm_b200 import ipk as ipkmod
+    return ipkmod.make_ipk(ipkmod.cosmo_from_params(params), Z_INI, k_max=20.0, k_bins=20000)
+
+
+def reference_state(start, d):
+    """The reference's own serial CUDA path (oracle/_ref/refpm, compiled from
+    its sources; GPU) makes the ICs of SEED and runs `start` steps of its
+    serial() loop, dumping x, v (writeOutput's float3 layout) after the last.
+    Returns the dump's path, or None when the harness or a GPU is absent."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "refpm")
+    if not os.path.exists(exe) or start < 1:
+        return None
+    import numpy as np
+    from oracle import pm_oracle as O
+    pre = os.path.join(d, "r")
+    txt = run_params_text(prefix=pre, ipk=pre + ".ipk",
+                          extra="LAST_STEP %d\nPARTICLE_DUMP %d\n" % (start, start - 1))
+    h, tab = run_ipk(O.parse_params_text(txt))
+    np.concatenate([h, tab]).astype("<f8").tofile(pre + ".ipk")
+    pf = pre + ".in"
+    with open(pf, "w") as f:
+        f.write(txt)
+    r = subprocess.run([exe, "run", pf], capture_output=True, text=True, timeout=900)
+    dump = "%s.particles.%d" % (pre, start - 1)
+    if r.returncode != 0 or not os.path.exists(dump):
+        return None
+    return dump
 
 
 def reference_gpu():
     """The reference's own serial CUDA step (oracle/_ref/refpm, compiled from
     the HACC_GPM sources when they were present at build time) on this GPU:
-    the same run (512^3 by default), steps 46-55 (mid-run) and the whole
-    100-step run.
-    Context for the GPU-to-GPU comparison; None when the harness is absent."""
+    the same run, K = 10 steps from the first timed step (mid-run) and the
+    whole run.  Context for the GPU-to-GPU comparison; None when the harness
+    is absent."""
     exe = os.path.join(ROOT, "oracle", "_ref", "refpm")
     if not os.path.exists(exe):
         return None
     import numpy as np
-
-    from hacc_gpm_b200 import ipk as ipkmod
     from oracle import pm_oracle as O
     out = {}
     with tempfile.TemporaryDirectory() as d:
-        txt = ipkmod.lcdm_params_text(NG, NP, RL, Z_INI, NSTEPS_RUN, prefix=os.path.join(d, "r"),
-                                      ipk=os.path.join(d, "r.ipk"))
-        h, tab = ipkmod.make_ipk(ipkmod.cosmo_from_params(O.parse_params_text(txt)), Z_INI, k_max=20.0)
-        np.concatenate([h, tab]).astype("<f8").tofile(os.path.join(d, "r.ipk"))
-        pf = os.path.join(d, "r.in")
+        pre = os.path.join(d, "r")
+        txt = run_params_text(prefix=pre, ipk=pre + ".ipk")
+        h, tab = run_ipk(O.parse_params_text(txt))
+        np.concatenate([h, tab]).astype("<f8").tofile(pre + ".ipk")
+        pf = pre + ".in"
         with open(pf, "w") as f:
             f.write(txt)
         for key, (w, k) in (("mid", (MID_STEP, 10)), ("full", (0, NSTEPS_RUN))):
@@ -192,39 +258,62 @@ def reference_gpu():
     return out
 
 
+def bench_config(steps, warmup):
+    """The workload both arms report (identical dicts)."""
+    start = first_warmup_step(steps, warmup)
+    return {"workload": "PM step (deposit, R2C FFT, Poisson+gradient, C2R FFT, gather+kick+drift), "
+                        "%d^3 particles on a %d^3 grid, L=%g Mpc/h, flat LCDM (Om 0.31, h 0.68, ns 0.96, "
+                        "sigma8 0.81), %d-step run from z=%g" % (NP, NG, RL, NSTEPS_RUN, Z_INI),
+            "np": NP, "ng": NG, "rl": RL,
+            "ics": "EH no-wiggle Zel'dovich from the reference's cuRAND white noise, SEED %d (+ rank)" % SEED,
+            "timed": "steps %d-%d of the run after %d warm-up steps (mid-run cost = run average)"
+                     % (start + warmup, start + warmup + steps - 1, warmup),
+            "l2": "inputs larger than L2 (%.2g GB particle state, %.2g GB grids)" % (28 * NP ** 3 / 1e9,
+                                                                                    40 * NG ** 3 / 1e9)}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    steps = max(1, min(args.steps, 3))
-    r = cpu_baseline(steps=steps, warmup=1 if args.warmup > 0 else 0)
-    v = NP ** 3 / r["sec_per_step"]
+    from hacc_gpm_b200 import binding as Bd
+    params = Bd.parse_params(run_params_text())
+    start = first_warmup_step(args.steps, args.warmup)
     gpu = None
+    with tempfile.TemporaryDirectory() as d:
+        dump = None
+        try:
+            import torch
+            if torch.cuda.is_available():
+                dump = reference_state(start, d)
+        except Exception:
+            dump = None
+        r = cpu_baseline(steps=args.steps, warmup=args.warmup, load=dump, start_step=start,
+                         cosmo=cosmo_args(params))
     try:
         import torch
         if torch.cuda.is_available() and not args.no_full:
             gpu = reference_gpu()
     except Exception as e:  # the CPU arm stands on its own
         gpu = {"error": str(e)[:200]}
+    v = NP ** 3 / r["sec_per_step"]
+    state = ("the run's state after %d steps from the reference's own serial CUDA path (refpm) on the same SEED"
+             % start) if dump else "a seeded perturbed lattice (the reference harness was not available)"
     print(json.dumps({
-        "impl": "reference", "metric": METRIC if NP == 512 else "particle-updates/s at %d^3" % NP, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": r["steps"],
-        "warmup": 1 if args.warmup > 0 else 0, "ms_per_step": r["sec_per_step"] * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic: seeded perturbed lattice",
-        "config": dict(step_config(), parallelism="host cores (OpenMP)"),
+        "impl": "reference", "metric": metric_name(), "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": r["steps"], "warmup": args.warmup, "ms_per_step": r["sec_per_step"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded EH no-wiggle Zel'dovich ICs (the reference's cuRAND white noise)",
+        "config": bench_config(args.steps, args.warmup),
+        "execution": "the OpenMP C++ transcription of the reference's serial step on %d host threads" % r["threads"],
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["threads"], "kind": "port",
-                         "sample": "%d full %d^3 step(s) of the OpenMP C++ transcription of the reference's serial "
-                                   "step (float3 layout, float atomics, C2C FFTs), after 1 warm-up" % (r["steps"], NP)},
+                         "sample": "%d full %d^3 steps (after %d warm-up) of the OpenMP C++ transcription of the "
+                                   "reference's serial step (float3 layout, float atomics, C2C FFTs) from %s"
+                                   % (r["steps"], NP, args.warmup, state)},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "same_state": bool(dump),
         "reference_gpu": gpu,
     }))
-
-
-def step_config():
-    """The workload both arms report: one PM step of the box."""
-    return {"workload": "PM step (deposit, R2C FFT, Poisson+gradient, 3 C2R FFTs, gather+kick+drift), "
-                        "%d^3 particles on a %d^3 grid, L=%g Mpc/h, flat LCDM, ICs at z=50, %d-step run"
-                        % (NP, NG, RL, NSTEPS_RUN),
-            "np": NP, "ng": NG, "rl": RL}
 
 
 def _check_same(a, b):
@@ -240,58 +329,62 @@ def _check_same(a, b):
     return worst, counts
 
 
-def run_forms(args):
-    """The batched ensemble and the serving loop (1 GPU)."""
+def form_ensemble():
+    """96 mixed boxes batched against the same boxes one at a time."""
     import torch
 
     from hacc_gpm_b200 import ensemble as E
+    boxes = E.prepare_tables(E.ensemble_boxes(96))
+    warm = E.prepare_tables(E.ensemble_boxes(10, master_seed=1))
+    for b in warm:
+        b.nsteps = 3
+    E.run_serial(warm)
+    E.run_batched(warm)
+    torch.cuda.synchronize()
+    serial, t_serial = E.timed(E.run_serial, boxes)
+    batched, t_batch = E.timed(E.run_batched, boxes)
+    st_serial, st_batch = {}, {}
+    E.run_serial(boxes, stages=st_serial)
+    E.run_batched(boxes, stages=st_batch)
+    worst, counts = _check_same(batched, serial)
+    classes, _ = E.class_layout(boxes)
+    return {
+        "metric": "ensemble sims/hour (96 mixed boxes, 64 steps each)", "value": 96 / t_batch * 3600.0,
+        "unit": "sims/hour", "higher_is_better": True, "n_gpus": 1,
+        "one_at_a_time": {"value": 96 / t_serial * 3600.0, "seconds": t_serial},
+        "batched_seconds": t_batch, "speedup_vs_one_at_a_time": t_serial / t_batch,
+        "stages_s": {"batched": st_batch, "one_at_a_time": st_serial},
+        "speedup_compute_only": (sum(v for k, v in st_serial.items() if k != "create") /
+                                 sum(v for k, v in st_batch.items() if k != "create")),
+        "pk_max_rel_diff_vs_one_at_a_time": worst, "pk_counts_equal": counts,
+        "config": {"workload": "96 boxes, ng = np uniform over {32,48,64,96,128}, L ~ U[64,512] Mpc/h, "
+                               "sigma8 ~ U[0.7,0.9], seeds 1000+i, EH ICs at z=100, 64 steps, P(k) 32 bins",
+                   "classes": classes, "timed": "ICs + 64 steps + final P(k) of every box (host-side "
+                                                ".ipk tables prepared beforehand for both)",
+                   "batched": "one launch per phase per size class, classes on parallel streams, "
+                              "CUDA graph per step"},
+        "dtype": "f32", "data": "synthetic: seeded EH no-wiggle Zel'dovich ICs",
+    }
+
+
+def form_serve(nreq):
+    """A Poisson request stream served with continuous batching against the
+    same stream one request at a time."""
+    import torch
+
     from hacc_gpm_b200 import serve as S
-    torch.cuda.set_device(0)
-    if args.workload == "ensemble":
-        boxes = E.prepare_tables(E.ensemble_boxes(96))
-        warm = E.prepare_tables(E.ensemble_boxes(10, master_seed=1))
-        for b in warm:
-            b.nsteps = 3
-        E.run_serial(warm)
-        E.run_batched(warm)
-        torch.cuda.synchronize()
-        serial, t_serial = E.timed(E.run_serial, boxes)
-        batched, t_batch = E.timed(E.run_batched, boxes)
-        st_serial, st_batch = {}, {}
-        E.run_serial(boxes, stages=st_serial)
-        E.run_batched(boxes, stages=st_batch)
-        worst, counts = _check_same(batched, serial)
-        classes, _ = E.class_layout(boxes)
-        print(json.dumps({
-            "metric": "ensemble sims/hour (96 mixed boxes, 64 steps each)", "value": 96 / t_batch * 3600.0,
-            "unit": "sims/hour", "higher_is_better": True, "n_gpus": 1,
-            "one_at_a_time": {"value": 96 / t_serial * 3600.0, "seconds": t_serial},
-            "batched_seconds": t_batch, "speedup_vs_one_at_a_time": t_serial / t_batch,
-            "stages_s": {"batched": st_batch, "one_at_a_time": st_serial},
-            "speedup_compute_only": (sum(v for k, v in st_serial.items() if k != "create") /
-                                     sum(v for k, v in st_batch.items() if k != "create")),
-            "pk_max_rel_diff_vs_one_at_a_time": worst, "pk_counts_equal": counts,
-            "config": {"workload": "96 boxes, ng = np uniform over {32,48,64,96,128}, L ~ U[64,512] Mpc/h, "
-                                   "sigma8 ~ U[0.7,0.9], seeds 1000+i, EH ICs at z=100, 64 steps, P(k) 32 bins",
-                       "classes": classes, "timed": "ICs + 64 steps + final P(k) of every box (host-side "
-                                                    ".ipk tables prepared beforehand for both)",
-                       "batched": "one launch per phase per size class, classes on parallel streams, "
-                                  "CUDA graph per step"},
-            "dtype": "f32", "data": "synthetic: seeded EH no-wiggle Zel'dovich ICs (Philox white noise)",
-        }))
-        return
-    reqs = S.request_stream(args.requests)
+    reqs = S.request_stream(nreq)
     warm = S.request_stream(8, rate=1000.0, seed=3, steps=(2, 3))
     S.serve(warm, realtime=False)
     S.serve_one_at_a_time(S.request_stream(8, rate=1000.0, seed=3, steps=(2, 3)), realtime=False)
     torch.cuda.synchronize()
     got, mk, stats = S.serve(reqs)
-    one, mk1 = S.serve_one_at_a_time(S.request_stream(args.requests))
-    sat, mks, _ = S.serve(S.request_stream(args.requests), realtime=False)
-    sat1, mks1 = S.serve_one_at_a_time(S.request_stream(args.requests), realtime=False)
+    one, mk1 = S.serve_one_at_a_time(S.request_stream(nreq))
+    sat, mks, _ = S.serve(S.request_stream(nreq), realtime=False)
+    sat1, mks1 = S.serve_one_at_a_time(S.request_stream(nreq), realtime=False)
     worst, counts = _check_same(sorted(got, key=lambda r: r.tag), sorted(one, key=lambda r: r.tag))
     out = S.latency_summary(got, mk)
-    print(json.dumps({
+    return {
         "metric": "serving p99 completion latency (Poisson 20 req/s)", "value": out["p99_s"], "unit": "s",
         "higher_is_better": False, "n_gpus": 1, "batched": out, "one_at_a_time": S.latency_summary(one, mk1),
         "saturated": {"batched_sims_per_hour": len(sat) / mks * 3600.0,
@@ -299,14 +392,21 @@ def run_forms(args):
         "pk_max_rel_diff_vs_one_at_a_time": worst, "pk_counts_equal": counts,
         "config": {"workload": "%d requests, Poisson arrivals 20/s (seed 7), ng = np log-uniform over "
                                "{32,48,64,96,128,192,256}, L = ng Mpc/h, steps U[20,200], Om U[0.25,0.35], "
-                               "sigma8 U[0.7,0.9], EH ICs at z=50" % args.requests,
+                               "sigma8 U[0.7,0.9], EH ICs at z=50" % nreq,
                    "classes": stats["classes"],
                    "admission": "slots per size class from a 40 GB HBM budget split over the classes by footprint "
                                 "per slot, at most the slots whose batched step is ~2 ms of GPU time",
                    "scheduling": "each class on its own stream at its own pace (batches of ~1 ms), stream "
                                  "priority by box size (smaller first)"},
         "dtype": "f32", "data": "synthetic",
-    }))
+    }
+
+
+def run_forms(args):
+    """--workload ensemble | serve: the batched form's own line (1 GPU)."""
+    import torch
+    torch.cuda.set_device(0)
+    print(json.dumps(form_ensemble() if args.workload == "ensemble" else form_serve(args.requests)))
 
 
 def main():
@@ -315,20 +415,25 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="NS", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-full", action="store_true", help="skip the whole-run timing")
-    ap.add_argument("--size", type=int, default=512, help="np = ng (profiling runs use a smaller box)")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched ensemble and serving forms")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (built-in or cached choices)")
+    ap.add_argument("--size", type=int, default=0, help="np = ng = rl (profiling runs use a smaller box)")
     ap.add_argument("--workload", default="step", choices=["step", "ensemble", "serve"])
     ap.add_argument("--requests", type=int, default=160, help="serve: requests in the stream")
     args = ap.parse_args()
     if args.workload != "step":
         run_forms(args)
         return
-    global NG, NP, RL
-    NG = NP = args.size
-    RL = float(args.size)
+    global NG, NP, RL, NSTEPS_RUN, MID_STEP
+    NG, NP, RL, NSTEPS_RUN, MID_STEP = CONFIGS[args.config]
+    if args.size:
+        NG = NP = args.size
+        RL = float(args.size)
     if args.impl == "reference":
         run_reference(args)
         return
@@ -344,11 +449,9 @@ def main():
     barrier, allmax = rk.barrier, rk.allmax
 
     import hacc_gpm_b200 as H
-    from hacc_gpm_b200 import ipk as ipkmod
 
-    txt = ipkmod.lcdm_params_text(NG, NP, RL, Z_INI, NSTEPS_RUN, seed=21082001 + rank)
-    params = H.parse_params(txt)
-    header, table = ipkmod.make_ipk(ipkmod.cosmo_from_params(params), Z_INI, k_max=20.0, k_bins=20000)
+    params = H.parse_params(run_params_text(rank))
+    header, table = run_ipk(params)
     sim = H.Simulation(params, device=local)
     sim.generate_ic(table, header[3])
     ts = H.Timestepper(params)
@@ -357,9 +460,12 @@ def main():
     ts.advance_half_step()
     stream = torch.cuda.ExternalStream(sim.stream)
 
-    # untimed advance to the middle of the run, then warm-up
-    start = max(0, min(MID_STEP, NSTEPS_RUN - args.steps) - args.warmup)
+    # untimed advance to the middle of the run, the autotuner on that state
+    # (it times every configuration of the tunable phases and leaves the
+    # state unchanged), then warm-up
+    start = first_warmup_step(args.steps, args.warmup)
     sim.run_steps(ts, start)
+    tuned = sim.autotune(reps=3) if not args.no_tune else sim.tuned_choices()
     sim.run_steps(ts, args.warmup)
     sim.sync()
 
@@ -398,7 +504,8 @@ def main():
         # events bracket the phase (all its kernels) once per step
         avg = ph_ms[k] / args.steps
         phases[k] = {"ms_per_step": avg, "kernels": n, "alg_bytes": b,
-                     "alg_gbs": b / (avg * 1e-3) / 1e9 if b else 0.0}
+                     "alg_gbs": b / (avg * 1e-3) / 1e9 if b else 0.0,
+                     "frac_of_peak": (b / (avg * 1e-3) / 1e9 / peak) if b else None}
     dom = max(phases, key=lambda k: phases[k]["ms_per_step"])
     d = phases[dom]
     roofline = {"bound": "hbm", "kernel": KERNEL_NAMES[dom].replace("NG", str(NG)), "phase": dom,
@@ -408,13 +515,31 @@ def main():
     step_ms = ms_max / args.steps
     b_step = sum(alg_bytes(np3, ng3).values())  # 72 Np + 56 Ng
     step_roof = {"alg_bytes_per_step": b_step, "achieved_gbs": b_step / (step_ms * 1e-3) / 1e9,
-                 "frac": b_step / (step_ms * 1e-3) / 1e9 / peak, "peak": peak}
+                 "frac": b_step / (step_ms * 1e-3) / 1e9 / peak, "peak": peak,
+                 "survey_bytes_per_step": 72 * np3 + 64 * ng3,
+                 "survey_frac": (72 * np3 + 64 * ng3) / (step_ms * 1e-3) / 1e9 / peak}
     tp = os.path.join(ROOT, "profiles", "traffic_%d.json" % NG)
-    if os.path.exists(tp):
+    if os.path.exists(tp) and NG == NP:
         with open(tp) as f:
             traf = json.load(f)
         if dom in traf:
             roofline["traffic"] = traf[dom]
+
+    # the CPU baseline on this state (rank 0, N = 1): 2 steps of the OpenMP
+    # transcription from the state the timed steps ended with
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        with tempfile.TemporaryDirectory() as dtmp:
+            dump = os.path.join(dtmp, "state")
+            xh, vh = sim.store_state()
+            np.concatenate([xh.ravel(), vh.ravel()]).astype("<f4").tofile(dump)
+            del xh, vh
+            at = start + args.warmup + args.steps
+            r = cpu_baseline(steps=2, warmup=0, load=dump, start_step=at, cosmo=cosmo_args(params))
+        cpu = {"value": np3 / r["sec_per_step"], "unit": UNIT, "cores": r["threads"], "kind": "port",
+               "sample": "2 full %d^3 steps (steps %d-%d of the run, the state this GPU run reached) of the "
+                         "OpenMP C++ transcription of the reference's serial step (float3 layout, float atomics, "
+                         "C2C FFTs) on %d host threads" % (NP, at, at + 1, r["threads"])}
 
     # end to end through the C-ABI with pinned host buffers, every step:
     # H2D state -> one step -> D2H state
@@ -440,7 +565,7 @@ def main():
                "h2d_bytes_per_step": 24 * np3, "d2h_bytes_per_step": 24 * np3, "steps": args.e2e_steps,
                "path": "hgpm_step_host (C-ABI, pinned float3 x,v in and out every step)"}
 
-    # the whole 100-step run once (fresh ICs), for the run-average cost
+    # the whole run once (fresh ICs), for the run-average cost
     full = None
     if not args.no_full:
         sim.generate_ic(table, header[3])
@@ -457,30 +582,25 @@ def main():
         f1.synchronize()
         fms = allmax(f0.elapsed_time(f1))
         full = {"steps": NSTEPS_RUN, "ms_per_step": fms / NSTEPS_RUN,
-                "value": world * np3 * NSTEPS_RUN / (fms * 1e-3), "unit": UNIT, "z": "50 -> 0"}
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        r = cpu_baseline(steps=1, warmup=0)
-        cpu = {"value": np3 / r["sec_per_step"], "unit": UNIT, "cores": r["threads"], "kind": "port",
-               "sample": "1 full %d^3 step of the OpenMP C++ transcription of the reference's serial step "
-                         "(float3 layout, float atomics, C2C FFTs) on %d host threads" % (NP, r["threads"])}
+                "value": world * np3 * NSTEPS_RUN / (fms * 1e-3), "unit": UNIT, "z": "%g -> 0" % Z_INI}
 
     sim.close()
+    forms = None
+    if rank == 0 and world == 1 and args.config == "NS" and not args.size and not args.no_forms:
+        forms = {"ensemble": form_ensemble(), "serve": form_serve(args.requests)}
     rk.close()
     if rank != 0:
         return
     out = {
-        "metric": METRIC if NP == 512 else "particle-updates/s at %d^3" % NP, "value": value, "unit": UNIT,
+        "metric": metric_name(), "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic: seeded EH no-wiggle Zel'dovich ICs (Philox white noise), random per rank",
-        "config": dict(step_config(), parallelism="replicas (one independent box per GPU)",
-                       l2="inputs larger than L2 (%.2g GB particle state, %.2g GB grids)"
-                          % (28 * NP ** 3 / 1e9, 40 * NG ** 3 / 1e9),
-                       timed="K steps from step 45 of the 100-step run (mid-run cost = run average)"),
+        "data": "synthetic: seeded EH no-wiggle Zel'dovich ICs (the reference's cuRAND white noise), seed + rank",
+        "config": bench_config(args.steps, args.warmup),
+        "execution": "replicas (one independent box per GPU)",
         "roofline": roofline, "step_roofline": step_roof, "phases": phases, "cpu_baseline": cpu, "e2e": e2e,
         "full_run": full, "timed_steps": run_state, "gpu_launches": int(launches), "clocks": clk,
+        "autotuned": tuned, "forms": forms,
     }
     print(json.dumps(out))
 

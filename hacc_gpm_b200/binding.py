@@ -23,6 +23,8 @@ LIB_PATH = os.path.join(HERE, "_lib", "libhgpm.so")
 HGPM_MAX_STEPS = 1000
 HGPM_PATH_MAX = 300
 HGPM_NPHASE = 9
+TUNE_KNOBS = 4
+TUNE_NAMES = ("deposit", "kick", "y_pass", "x_pass")
 PHASES = ("drift", "deposit", "fft_z_fwd", "fft_y_fwd", "poisson_x", "fft_y_inv", "fft_z_inv", "kick_drift", "pk")
 
 
@@ -56,6 +58,7 @@ class _Params(C.Structure):
         ("analysis", C.c_ubyte * HGPM_MAX_STEPS),
         ("analysis_dir", C.c_char * HGPM_PATH_MAX),
         ("analysis_py", C.c_char * HGPM_PATH_MAX),
+        ("noise", C.c_int),
     ]
 
 
@@ -154,6 +157,12 @@ def lib() -> C.CDLL:
         "hgpm_ens_step_class": (C.c_int, [vp, C.c_int, C.c_int]),
         "hgpm_ens_class_done": (C.c_int, [vp, C.c_int, P(C.c_int)]),
         "hgpm_ens_sync_class": (C.c_int, [vp, C.c_int]),
+        "hgpm_autotune": (C.c_int, [vp, C.c_int, C.c_int, P(C.c_int), P(C.c_double)]),
+        "hgpm_tuned_choices": (C.c_int, [vp, P(C.c_int)]),
+        "hgpm_tune_pick": (C.c_int, [P(C.c_double), C.c_int, C.c_int, C.c_double]),
+        "hgpm_tune_cache_lookup": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int, P(C.c_int)]),
+        "hgpm_tune_cache_store": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int, P(C.c_int),
+                                            P(C.c_double)]),
         "hgpm_sizeof_params": (C.c_size_t, []),
         "hgpm_sizeof_timestepper": (C.c_size_t, []),
     }
@@ -480,3 +489,17 @@ class Simulation:
 
     def kernel_launches(self, reset=False) -> int:
         return self.L.hgpm_kernel_launches(self._h, int(reset))
+
+    def autotune(self, reps: int = 3, store: bool = False) -> dict:
+        """Time every configuration of the tunable phases on the current
+        state (left unchanged), apply the winners (hgpm_autotune); store:
+        also append them to the tuning cache."""
+        ch = (C.c_int * TUNE_KNOBS)()
+        ms = (C.c_double * TUNE_KNOBS)()
+        self._ck(self.L.hgpm_autotune(self._h, int(reps), int(store), ch, ms))
+        return {k: {"choice": int(ch[i]), "ms": float(ms[i])} for i, k in enumerate(TUNE_NAMES)}
+
+    def tuned_choices(self) -> dict:
+        ch = (C.c_int * TUNE_KNOBS)()
+        self._ck(self.L.hgpm_tuned_choices(self._h, ch))
+        return {k: int(ch[i]) for i, k in enumerate(TUNE_NAMES)}

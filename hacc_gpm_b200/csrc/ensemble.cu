@@ -76,7 +76,8 @@ struct hgpm_ensemble {
     std::vector<EnsClass> cls;
     bool use_graph = false;
     cudaGraphExec_t exec = nullptr;
-    int kick_variant = 1;
+    int kick_choice = 0;   // kick and deposit candidates (HGPM_KICK / HGPM_DEPOSIT)
+    int dep_choice = -1;
     int64_t launches = 0;
     std::string err;
 };
@@ -243,7 +244,9 @@ extern "C" int hgpm_ens_create(int nclass, const int* ng, const int* np, const i
         if (nslots[i] <= 0 || nslots[i] > 65535 / 3) return efail(E, HGPM_ERR_ARG, "class %d: bad slot count", i);
     }
     const char* kv = getenv("HGPM_KICK");
-    if (kv && kv[0] >= '0' && kv[0] <= '2') E->kick_variant = kv[0] - '0';
+    if (kv && kv[0] >= '0' && kv[0] <= '9' && atoi(kv) < kick_candidates(np[0], ng[0])) E->kick_choice = atoi(kv);
+    const char* dv = getenv("HGPM_DEPOSIT");
+    if (dv && dv[0] >= '0' && dv[0] <= '9') E->dep_choice = atoi(dv);
     ECK(cudaSetDevice(device));
     ECK(cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking));
     ECK(cudaEventCreateWithFlags(&E->fork, cudaEventDisableTiming));
@@ -352,7 +355,8 @@ extern "C" int hgpm_ens_slot(hgpm_ensemble* E, int ci, int slot, const hgpm_para
         c->pk_nparts = 4 * 148;
         c->tma = false;  // batched passes are the plain ones; views match them
         c->xtma = false;
-        c->kick_variant = E->kick_variant;
+        c->kick_choice = E->kick_choice;
+        c->dep_choice = E->dep_choice;
         k.views[slot] = c;
     }
     c->p = *p;
@@ -443,7 +447,7 @@ static int class_step(hgpm_ensemble* E, EnsClass& k, cudaStream_t s) {
     p.vz = (float*)(b + 6 * a);
     const int* act = k.d_active;
     ECK(launch_deposit(p, k.np, ng, mass, k.rho64, k.blkwin, k.dep_spill, s,
-                       Slots{act, k.part_stride, k.ncell, k.win_stride}, S));
+                       Slots{act, k.part_stride, k.ncell, k.win_stride}, S, E->dep_choice));
     ECK(launch_zfwd(ng, k.rho64, true, k.spec, ng * ng, k.zs, mean, k.tw_ng, s, Slots{act, k.ncell, k.spec_elems}, S));
     ECK(launch_strided(ng, false, k.spec, M + 1, (size_t)k.zs, (size_t)ng * k.zs, ng, 0, 1, k.tw_ng, s,
                        Slots{act, k.spec_elems, 0}, S));
@@ -456,11 +460,11 @@ static int class_step(hgpm_ensemble* E, EnsClass& k, cudaStream_t s) {
     ECK(launch_zinv(ng, k.fspec, phi, ng * ng, k.zs, 0, 0, 1, 1.0f, k.tw_ng, s,
                     Slots{act, 3 * k.spec_elems, 6 * k.spec_elems}, S));
     ECK(launch_gradient(ng, phi, f4, s, Slots{act, 6 * k.spec_elems, k.force_elems / 4}, S));
-    ECK(launch_kick_drift(p, k.np, ng, f4, 0.0, 0.0, 0.f, 0.f, 0, E->kick_variant, k.blkwin, true, k.kick_spill, s,
+    ECK(launch_kick_drift(p, k.np, ng, f4, 0.0, 0.0, 0.f, 0.f, 0, E->kick_choice, k.blkwin, true, k.kick_spill, s,
                           Slots{act, k.part_stride, k.force_elems / 4, k.win_stride},
                           KickSched{k.d_sched, k.d_step, HGPM_MAX_STEPS}, S));
     ECK(launch_slots_advance(k.d_active, k.d_step, k.d_nsteps, S, s));
-    E->launches += kStepKernels + kick_kernels(E->kick_variant, k.np, ng);
+    E->launches += kStepKernels + kick_kernels(E->kick_choice, k.np, ng);
     return HGPM_OK;
 }
 
@@ -517,7 +521,7 @@ extern "C" int hgpm_ens_step(hgpm_ensemble* E, int nsteps) {
             ECK(ie);
         }
         int per = 0;
-        for (auto& k : E->cls) per += kStepKernels + kick_kernels(E->kick_variant, k.np, k.ng);
+        for (auto& k : E->cls) per += kStepKernels + kick_kernels(E->kick_choice, k.np, k.ng);
         for (int i = 0; i < nsteps; ++i) {
             ECK(cudaGraphLaunch(E->exec, E->stream));
             E->launches += per;
@@ -568,7 +572,7 @@ extern "C" int hgpm_ens_step_class(hgpm_ensemble* E, int ci, int nsteps) {
         }
         for (int i = 0; i < nsteps; ++i) {
             ECK(cudaGraphLaunch(k.exec, k.stream));
-            E->launches += kStepKernels + kick_kernels(E->kick_variant, k.np, k.ng);
+            E->launches += kStepKernels + kick_kernels(E->kick_choice, k.np, k.ng);
         }
     } else {
         for (int i = 0; i < nsteps; ++i)

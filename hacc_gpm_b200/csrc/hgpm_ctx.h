@@ -46,12 +46,14 @@ struct hgpm_ctx {
     bool win_valid = false;  // blkwin describes the current positions
     // kernel variants (environment, read at creation): HGPM_NO_TMA=1 selects the
     // plain strided y passes, HGPM_XTMA=0|1 the plain/TMA-fed fused x pass
-    // (default 1, the TMA-fed one: 0.95 vs 0.99 ms at 512^3),
-    // HGPM_KICK=1|2: flat gathers from the float4 force grid (default) /
-    // float4 shared windows per Lagrangian block with a flat spill pass
+    // (default 1, the TMA-fed one: 0.95 vs 0.99 ms at 512^3).  The deposit
+    // and kick candidates (bit-identical results) are chosen by the autotuner
+    // (hgpm_autotune, or its cache), else HGPM_DEPOSIT / HGPM_KICK, else the
+    // built-in defaults (-1 / 0).
     bool tma = true;
     bool xtma = true;
-    int kick_variant = 1;
+    int dep_choice = -1;
+    int kick_choice = 0;
     float* stage = nullptr;     // AoS float3 x, v staging (lazy)
     double* pk_part = nullptr;  // P(k) partial sums (lazy)
     unsigned long long* pk_pcnt = nullptr;
@@ -135,3 +137,6 @@ static_assert(PH_PK + 1 == HGPM_NPHASE, "phase ids");
 int ctx_set_rl_tables(hgpm_ctx* c);
 // Unit-mass CIC weight scale (ng/np)^3 of pm_actions.cpp:229-230.
 float ctx_cic_mass(int ng, int np);
+// Apply the autotuner's cached entry for this context's size and device
+// (autotune.cu); returns 1 if one was applied.
+int ctx_apply_tuned(hgpm_ctx* c);

@@ -6,10 +6,14 @@
 namespace hgpm {
 
 constexpr int kThreads = 256;            // threads per CTA for all pass kernels
-// int64 fixed-point density: value * 2^31 (a unit-mass CIC weight fits a u32)
+// int64 fixed-point density: value * 2^31.  Each CIC weight (times the
+// particle mass) is rounded to 2^-24, the FP32 resolution of a unit weight,
+// and stored shifted by kQShift, so a unit weight is 2^24 in a 32-bit
+// shared-memory window and 2^31 in the int64 grid.
 constexpr double kFixScale = 2147483648.0;
 constexpr double kFixInv = 1.0 / 2147483648.0;
-constexpr float kFixScaleF = 2147483648.0f;
+constexpr float kQ24F = 16777216.0f;
+constexpr int kQShift = 7;
 
 // Particle positions are a packed cell (10 bits per axis, ng <= 1024) plus
 // an FP32 offset in [0, 1) per axis.

@@ -77,19 +77,25 @@ int deposit_cap_cells(int np_side, int ng);
 // kick reads it back when have_rec (positions unchanged since the deposit),
 // else measures and writes it.
 int window_records(int np_side, int ng);  // ints per box
-// Kernels one launch_kick_drift call launches: flat (variant 1) one, the
-// windowed variants two (windowed + spill).
-inline int kick_kernels(int variant, int, int) { return variant == 1 ? 1 : 2; }
+// Kick configurations: every candidate gives bit-identical results.
+// kick_candidates: how many; kick_kernels: kernels one launch_kick_drift
+// call of candidate `choice` launches (the windowed one two: windowed + spill).
+int kick_candidates(int np_side, int ng);
+int kick_kernels(int choice, int np_side, int ng);
+// Deposit configurations (bit-identical int64 grids): how many, and the
+// default (used when the choice is -1).
+int deposit_candidates(int np_side, int ng);
+int deposit_default(int np_side, int ng);
 // Blocks too wide for a kernel's window are queued in `spill` (the deposit's
 // and the kick's own lists) and run one particle per thread after the
 // windowed pass, inside the same launcher.
 cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
                            int* blkwin, const SpillList& spill, cudaStream_t s, const Slots& sl = Slots{},
-                           int nslots = 1);
-// f: the float4 (F_x, F_y, F_z, 0) force grid.  variant 1 forces the flat
-// (one particle per thread, global gathers) path for the whole box.
+                           int nslots = 1, int choice = -1);
+// f: the float4 (F_x, F_y, F_z, 0) force grid.  choice: kick candidate
+// (0 = default).
 cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float4* f, double deltaT,
-                              double fscal, float pf_a, float pf_b, int ndrift, int variant, int* blkwin,
+                              double fscal, float pf_a, float pf_b, int ndrift, int choice, int* blkwin,
                               bool have_rec, const SpillList& spill, cudaStream_t s, const Slots& sl = Slots{},
                               const KickSched& ks = KickSched{}, int nslots = 1);
 // Batched step bookkeeping: each active slot's step counter advances and a
@@ -97,7 +103,9 @@ cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const f
 cudaError_t launch_slots_advance(int* active, int* step, const int* nsteps, int nslots, cudaStream_t s);
 cudaError_t launch_density(const unsigned long long* rho64, float* rho, size_t n, cudaStream_t s);
 cudaError_t launch_ktables(int ng, double* cosq, float* sk, float* pkw, cudaStream_t s);
-cudaError_t launch_noise(float* out, size_t n, uint32_t seed, cudaStream_t s);
+// White noise of the ICs: kind HGPM_NOISE_CURAND (curand_init(seed, i, 0) +
+// curand_normal_double, as the reference) or HGPM_NOISE_PHILOX.
+cudaError_t launch_noise(float* out, size_t n, int seed, int kind, cudaStream_t s);
 cudaError_t launch_place(const float* sgrid, size_t scomp, const ParticleSoA& p, int np_side, int ng, float delta_f,
                          float velmul, cudaStream_t s);
 

@@ -6,6 +6,7 @@
 // in [0, 1) per axis; the offset equals the reference's `x - (int)x`
 // (cic_pm.cu:52-58) bit for bit when a state is loaded.
 #include <cuda_runtime.h>
+#include <curand_kernel.h>
 #include <stdint.h>
 #include <math.h>
 
@@ -215,9 +216,10 @@ constexpr int kWinRec = 8;
 // CTAs per SM.  The deposit counts the blocks above it.
 constexpr int kWin4Cap = 6912;
 
-// 8 fixed-point corner weights, index (a*2+b)*2+c for corner (+a, +b, +c)
-template <bool SMALL>
-__device__ __forceinline__ void cic_fixed(float dx, float dy, float dz, float mass, unsigned long long q[8]) {
+// 8 corner weights ((w_x w_y) w_z) * mass rounded to 2^-24, index (a*2+b)*2+c
+// for corner (+a, +b, +c).  Q32: every value < 2^32 (mass < 256).
+template <bool Q32>
+__device__ __forceinline__ void cic_q24(float dx, float dy, float dz, float mass, unsigned long long q[8]) {
     const float wx[2] = {1.f - dx, dx}, wy[2] = {1.f - dy, dy}, wz[2] = {1.f - dz, dz};
 #pragma unroll
     for (int a = 0; a < 2; ++a)
@@ -227,10 +229,20 @@ __device__ __forceinline__ void cic_fixed(float dx, float dy, float dz, float ma
             for (int cc = 0; cc < 2; ++cc) {
                 float mul = __fmul_rn(__fmul_rn(wx[a], wy[b]), wz[cc]);
                 if (mass != 1.f) mul = __fmul_rn(mul, mass);  // exact when mass is 1 (ng = np)
-                // SMALL: mass <= 1, so mul * 2^31 < 2^32 fits an unsigned int
-                q[(a * 2 + b) * 2 + cc] = SMALL ? (unsigned long long)__float2uint_rn(mul * kFixScaleF)
-                                                : (unsigned long long)__float2ull_rn(mul * kFixScaleF);
+                // the product by 2^24 is exact, so only the rounding to an integer rounds
+                q[(a * 2 + b) * 2 + cc] = Q32 ? (unsigned long long)__float2uint_rn(mul * kQ24F)
+                                              : (unsigned long long)__float2ull_rn(mul * kQ24F);
             }
+}
+
+// The same weights on the int64 grid's 2^31 scale.  SMALL (mass <= 1): each
+// value, and the sum of two (the x-chain merges an upper-x weight < 1 with a
+// lower-x weight <= 1), is below 2^32.
+template <bool SMALL>
+__device__ __forceinline__ void cic_fixed(float dx, float dy, float dz, float mass, unsigned long long q[8]) {
+    cic_q24<SMALL>(dx, dy, dz, mass, q);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) q[j] <<= kQShift;
 }
 
 // Window cell update.  SMALL (every contribution < 2^32): the low and high
@@ -340,10 +352,331 @@ __global__ void __launch_bounds__(NT, MINB) deposit_tiled_kernel(ParticleSoA p, 
             if (v != 0ull) atomicAdd(&rho[map.global(i)], v);
         }
     } else if (tid == 0) {
-        // too wide for the window: queued for deposit_spill_kernel
+        // too wide for the window: queued (whole) for deposit_spill_kernel
         const int slot = blockIdx.y;
-        spill.items[(size_t)slot * spill.nblocks + atomicAdd(&spill.cnt[slot], 1)] = blk;
+        spill.items[(size_t)slot * spill.nblocks + atomicAdd(&spill.cnt[slot], 1)] = blk * 4;
     }
+}
+
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// deposit_tiled_kernel with one 32-bit word per window cell: the weights are
+// added as 2^-24 integers (cic_q24) with one shared atomic per corner instead
+// of two 16-bit halves.  A corner adds at most mass * 2^24, so a cell can wrap
+// only where the block puts 256 units of weight x mass into it (256 times the
+// mean density from one block, in dense cores late in a run).  Before the
+// flush the CTA compares the 64-bit sum of its window with the sum of every
+// value it added; a block that wrapped is queued, like a block too wide for the
+// window, for deposit_spill_kernel, whose 16-bit-split window is exact.  Needs
+// mass <= 64 (two merged corners below 2^32).  CHAIN: the x-chain merge of
+// deposit_tiled_kernel; otherwise each particle adds its 8 corners.
+template <int B, int NT, int MINB, bool CHAIN, int PF = 1>
+__global__ void __launch_bounds__(NT, MINB) deposit_w32_kernel(ParticleSoA p, int np_side, int ng, float mass,
+                                                               unsigned long long* __restrict__ rho, int cap_cells,
+                                                               int* __restrict__ blkwin, SpillList spill, Slots sl) {
+    constexpr int B3 = B * B * B, BB = B * B;
+    constexpr int PPT = B3 / NT;
+    static_assert(NT % BB == 0 && B3 % NT == 0, "a thread owns one x-run of PPT particles");
+    extern __shared__ unsigned long long win[];
+    __shared__ int bb[6];
+    __shared__ long long wsum[NT / 32];
+    if (slot_idle(sl, blockIdx.y)) return;
+    const int tid = threadIdx.x;
+    const int nb = np_side / B;
+    const int blk = blockIdx.x;
+    p = offset_soa(p, (size_t)blockIdx.y * sl.s0 + (size_t)blk * B3);
+    rho += (size_t)blockIdx.y * sl.s1;
+    const int bz = blk % nb, by = (blk / nb) % nb, bx = blk / (nb * nb);
+    const int ox = (int)((long long)bx * B * ng / np_side);
+    const int oy = (int)((long long)by * B * ng / np_side);
+    const int oz = (int)((long long)bz * B * ng / np_side);
+    int l0[3], w[3];
+    block_window<NT, PPT>(p.cell, 0, ox, oy, oz, ng, bb, l0, w);
+    if (blkwin && tid < 6) blkwin[(size_t)blockIdx.y * sl.s2 + (size_t)blk * kWinRec + tid] = tid < 3 ? l0[tid] : w[tid - 3];
+    const int wy = w[1], wz = w[2];
+    const int gx0 = wrap_once(ox + l0[0], ng), gy0 = wrap_once(oy + l0[1], ng), gz0 = wrap_once(oz + l0[2], ng);
+    const long long vol = (long long)w[0] * wy * wz;
+    if (tid == 0 && spill.over && vol > kWin4Cap) atomicAdd(&spill.over[blockIdx.y], 1);
+    if (vol > cap_cells) {
+        if (tid == 0) spill.items[(size_t)blockIdx.y * spill.nblocks + atomicAdd(&spill.cnt[blockIdx.y], 1)] = blk * 4;
+        return;
+    }
+    unsigned* w0 = reinterpret_cast<unsigned*>(win);
+    for (int i = tid; i < vol; i += NT) w0[i] = 0u;
+    __syncthreads();
+    const int syz = wy * wz;
+    const int off[4] = {0, 1, wz, wz + 1};  // (b, c) corner offsets in the window
+    unsigned long long added = 0ull;        // every value this thread adds
+    unsigned pend[4] = {0u, 0u, 0u, 0u};
+    int pw = -1;  // window index of the pending (upper-x) face; -1: none
+    const int i0 = (tid / BB) * PPT * BB + tid % BB;
+    // the particles PF ahead are in flight in a register ring (PF = 1: the
+    // next one; PF > 1 unrolls the run so the ring indices are static)
+    uint32_t rc[PF];
+    float rx[PF], ry[PF], rz[PF];
+#pragma unroll
+    for (int k = 0; k < PF; ++k) {
+        if (k < PPT) {
+            const int idx = i0 + k * BB;
+            rc[k] = __ldg(&p.cell[idx]);
+            rx[k] = __ldg(&p.ox[idx]);
+            ry[k] = __ldg(&p.oy[idx]);
+            rz[k] = __ldg(&p.oz[idx]);
+        }
+    }
+#pragma unroll(PF > 1 ? PPT : 1)
+    for (int k = 0; k < PPT; ++k) {
+        const int r = PF > 1 ? k % PF : 0;
+        const uint32_t c = rc[r];
+        const float cx = rx[r], cy = ry[r], cz = rz[r];
+        if (k + PF < PPT) {
+            const int nidx = i0 + (k + PF) * BB;
+            rc[r] = __ldg(&p.cell[nidx]);
+            rx[r] = __ldg(&p.ox[nidx]);
+            ry[r] = __ldg(&p.oy[nidx]);
+            rz[r] = __ldg(&p.oz[nidx]);
+        }
+        unsigned long long q64[8];
+        cic_q24<true>(cx, cy, cz, mass, q64);
+        unsigned q[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            q[j] = (unsigned)q64[j];
+            added += q64[j];
+        }
+        const int cw = (win_rel(cell_x(c), gx0, ng) * wy + win_rel(cell_y(c), gy0, ng)) * wz +
+                       win_rel(cell_z(c), gz0, ng);
+        if (CHAIN) {
+            if (pw == cw) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) q[j] += pend[j];
+            } else if (pw >= 0) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) atomicAdd(&w0[pw + off[j]], pend[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) atomicAdd(&w0[cw + off[j]], q[j]);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) pend[j] = q[4 + j];
+            pw = cw + syz;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) atomicAdd(&w0[cw + (j >> 2) * syz + off[j & 3]], q[j]);
+        }
+    }
+    if (CHAIN) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) atomicAdd(&w0[pw + off[j]], pend[j]);
+    }
+    __syncthreads();
+    // wrap check: the window's 64-bit sum equals the sum of the added values
+    // unless a cell wrapped (a wrap only lowers it)
+    long long d = -(long long)added;
+    for (int i = tid; i < vol; i += NT) d += (long long)w0[i];
+    d = warp_sum_ll(d);
+    if ((tid & 31) == 0) wsum[tid >> 5] = d;
+    __syncthreads();
+    long long tot = 0;
+#pragma unroll
+    for (int k = 0; k < NT / 32; ++k) tot += wsum[k];
+    if (tot != 0) {
+        if (tid == 0) spill.items[(size_t)blockIdx.y * spill.nblocks + atomicAdd(&spill.cnt[blockIdx.y], 1)] = blk * 4;
+        return;
+    }
+    const WinMap map(wy, wz, gx0, gy0, gz0, ng);
+    for (int i = tid; i < vol; i += NT) {
+        const unsigned v = w0[i];
+        if (v != 0u) atomicAdd(&rho[map.global(i)], (unsigned long long)v << kQShift);
+    }
+}
+
+// Column deposit: 32-bit windows (as deposit_w32_kernel) with one thread per
+// (y, z) column of the block, which walks the column's B particles along x
+// with the next PF in flight in a register ring.  A block whose window is
+// wider than the cap but whose two x-halves (x < B/2, x >= B/2) each fit is
+// deposited as two halves, one after the other, each with its own window,
+// wrap check and flush; only blocks whose halves do not fit either (or that
+// wrap) go to deposit_spill_kernel.
+template <int B, int PF>
+__device__ __forceinline__ unsigned long long column_adds(const ParticleSoA& p, int i0, int k0, int len, float mass,
+                                                          unsigned* __restrict__ w0, int gx0, int gy0, int gz0,
+                                                          int wy, int wz, int ng) {
+    constexpr int BB = B * B;
+    const int syz = wy * wz;
+    unsigned long long added = 0ull;
+    uint32_t rc[PF];
+    float rx[PF], ry[PF], rz[PF];
+#pragma unroll
+    for (int j = 0; j < PF; ++j) {
+        if (j < len) {
+            const int idx = i0 + (k0 + j) * BB;
+            rc[j] = __ldg(&p.cell[idx]);
+            rx[j] = __ldg(&p.ox[idx]);
+            ry[j] = __ldg(&p.oy[idx]);
+            rz[j] = __ldg(&p.oz[idx]);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < B; ++j) {
+        if (j < len) {
+            const int r = j % PF;
+            const uint32_t c = rc[r];
+            const float cx = rx[r], cy = ry[r], cz = rz[r];
+            if (j + PF < len) {
+                const int idx = i0 + (k0 + j + PF) * BB;
+                rc[r] = __ldg(&p.cell[idx]);
+                rx[r] = __ldg(&p.ox[idx]);
+                ry[r] = __ldg(&p.oy[idx]);
+                rz[r] = __ldg(&p.oz[idx]);
+            }
+            unsigned long long q[8];
+            cic_q24<true>(cx, cy, cz, mass, q);
+            const int cw = (win_rel(cell_x(c), gx0, ng) * wy + win_rel(cell_y(c), gy0, ng)) * wz +
+                           win_rel(cell_z(c), gz0, ng);
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b)
+#pragma unroll
+                    for (int cc = 0; cc < 2; ++cc) {
+                        const unsigned long long v = q[(a * 2 + b) * 2 + cc];
+                        added += v;
+                        atomicAdd(&w0[cw + a * syz + b * wz + cc], (unsigned)v);
+                    }
+        }
+    }
+    return added;
+}
+
+// Zero the window, add the column range [k0, k0 + len), check for wraps and
+// flush; returns false (nothing flushed) if a cell wrapped.  Called by every
+// thread of the CTA.
+template <int B, int PF>
+__device__ __forceinline__ bool column_pass(const ParticleSoA& p, int i0, int k0, int len, float mass,
+                                            unsigned* __restrict__ w0, long long* wsum, const int* box, int ox,
+                                            int oy, int oz, int ng, unsigned long long* __restrict__ rho) {
+    constexpr int NT = B * B;
+    const int tid = threadIdx.x;
+    const int wx = box[3] - box[0] + 2, wy = box[4] - box[1] + 2, wz = box[5] - box[2] + 2;
+    const int gx0 = wrap_once(ox + box[0], ng), gy0 = wrap_once(oy + box[1], ng), gz0 = wrap_once(oz + box[2], ng);
+    const int vol = wx * wy * wz;
+    for (int i = tid; i < vol; i += NT) w0[i] = 0u;
+    __syncthreads();
+    const unsigned long long added = column_adds<B, PF>(p, i0, k0, len, mass, w0, gx0, gy0, gz0, wy, wz, ng);
+    __syncthreads();
+    long long d = -(long long)added;
+    for (int i = tid; i < vol; i += NT) d += (long long)w0[i];
+    d = warp_sum_ll(d);
+    if ((tid & 31) == 0) wsum[tid >> 5] = d;
+    __syncthreads();
+    long long tot = 0;
+#pragma unroll
+    for (int k = 0; k < NT / 32; ++k) tot += wsum[k];
+    if (tot == 0) {
+        const WinMap map(wy, wz, gx0, gy0, gz0, ng);
+        for (int i = tid; i < vol; i += NT) {
+            const unsigned v = w0[i];
+            if (v != 0u) atomicAdd(&rho[map.global(i)], (unsigned long long)v << kQShift);
+        }
+    }
+    __syncthreads();  // the window is reused by the next pass
+    return tot == 0;
+}
+
+template <int B, int MINB, int PF>
+__global__ void __launch_bounds__(B * B, MINB) deposit_col_kernel(ParticleSoA p, int np_side, int ng, float mass,
+                                                                  unsigned long long* __restrict__ rho, int cap_cells,
+                                                                  int* __restrict__ blkwin, SpillList spill, Slots sl) {
+    constexpr int B3 = B * B * B, NT = B * B;
+    extern __shared__ unsigned long long win[];
+    __shared__ int bb[18];  // (min xyz, max xyz) of the block, then of each x-half
+    __shared__ long long wsum[NT / 32];
+    if (slot_idle(sl, blockIdx.y)) return;
+    const int tid = threadIdx.x;
+    const int nb = np_side / B;
+    const int blk = blockIdx.x;
+    p = offset_soa(p, (size_t)blockIdx.y * sl.s0 + (size_t)blk * B3);
+    rho += (size_t)blockIdx.y * sl.s1;
+    const int bz = blk % nb, by = (blk / nb) % nb, bx = blk / (nb * nb);
+    const int ox = (int)((long long)bx * B * ng / np_side);
+    const int oy = (int)((long long)by * B * ng / np_side);
+    const int oz = (int)((long long)bz * B * ng / np_side);
+    if (tid < 18) bb[tid] = (tid % 6) < 3 ? 0x7fffffff : -0x7fffffff;
+    __syncthreads();
+    {
+        // bounding boxes of the two x-halves of the thread's column
+        int mn[2][3], mx[2][3];
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                mn[h][a] = 0x7fffffff;
+                mx[h][a] = -0x7fffffff;
+            }
+#pragma unroll
+        for (int k = 0; k < B; ++k) {
+            const int h = k >= B / 2;
+            const uint32_t c = __ldg(&p.cell[tid + k * NT]);
+            const int r[3] = {nearest_image(cell_x(c) - ox, ng), nearest_image(cell_y(c) - oy, ng),
+                              nearest_image(cell_z(c) - oz, ng)};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                mn[h][a] = min(mn[h][a], r[a]);
+                mx[h][a] = max(mx[h][a], r[a]);
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                mn[h][a] = __reduce_min_sync(0xffffffffu, mn[h][a]);
+                mx[h][a] = __reduce_max_sync(0xffffffffu, mx[h][a]);
+            }
+        if ((tid & 31) == 0) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    atomicMin(&bb[6 + 6 * h + a], mn[h][a]);
+                    atomicMax(&bb[9 + 6 * h + a], mx[h][a]);
+                    atomicMin(&bb[a], mn[h][a]);
+                    atomicMax(&bb[3 + a], mx[h][a]);
+                }
+        }
+    }
+    __syncthreads();
+    const int wx = bb[3] - bb[0] + 2, wy = bb[4] - bb[1] + 2, wz = bb[5] - bb[2] + 2;
+    if (blkwin && tid < 6) {
+        const int rec = tid < 3 ? bb[tid] : bb[tid] - bb[tid - 3] + 2;
+        blkwin[(size_t)blockIdx.y * sl.s2 + (size_t)blk * kWinRec + tid] = rec;
+    }
+    const long long vol = (long long)wx * wy * wz;
+    if (tid == 0 && spill.over && vol > kWin4Cap) atomicAdd(&spill.over[blockIdx.y], 1);
+    unsigned* w0 = reinterpret_cast<unsigned*>(win);
+    // queued part: 0 the whole block, 2 its upper x-half (the lower half
+    // flushed); at most one item per block
+    int queue = -1;
+    if (vol <= cap_cells) {
+        if (!column_pass<B, PF>(p, tid, 0, B, mass, w0, wsum, bb, ox, oy, oz, ng, rho)) queue = 0;
+    } else {
+        auto hvol = [&](int h) {
+            const int* q = bb + 6 + 6 * h;
+            return (long long)(q[3] - q[0] + 2) * (q[4] - q[1] + 2) * (q[5] - q[2] + 2);
+        };
+        if (hvol(0) <= cap_cells && hvol(1) <= cap_cells) {
+            if (!column_pass<B, PF>(p, tid, 0, B / 2, mass, w0, wsum, bb + 6, ox, oy, oz, ng, rho)) queue = 0;
+            else if (!column_pass<B, PF>(p, tid, B / 2, B / 2, mass, w0, wsum, bb + 12, ox, oy, oz, ng, rho))
+                queue = 2;
+        } else {
+            queue = 0;
+        }
+    }
+    if (queue >= 0 && tid == 0)
+        spill.items[(size_t)blockIdx.y * spill.nblocks + atomicAdd(&spill.cnt[blockIdx.y], 1)] = blk * 4 + queue;
 }
 
 // The 8 fixed-point corner weights of one particle added straight to the
@@ -396,7 +729,10 @@ __global__ void __launch_bounds__(NT, 1) deposit_spill_kernel(ParticleSoA p, int
     const int g = tid / BB, r = tid % BB;  // x group and (y, z) of the thread's chain
     const int nb = np_side / B;
     for (int t = blockIdx.x; t < cnt; t += gridDim.x) {
-        const int blk = __ldg(&items[t]);
+        // item = block * 4 + part: 0 the whole block, 2 its upper x-half only
+        const int item = __ldg(&items[t]);
+        const int blk = item >> 2;
+        const int xlo = (item & 3) == 2 ? B / 2 : 0;
         const int* rec = recs + (size_t)blk * kWinRec;
         const int wx = __ldg(&rec[3]), wy = __ldg(&rec[4]), wz = __ldg(&rec[5]);
         const int bz = blk % nb, by = (blk / nb) % nb, bx = blk / (nb * nb);
@@ -421,6 +757,10 @@ __global__ void __launch_bounds__(NT, 1) deposit_spill_kernel(ParticleSoA p, int
                 const uint32_t c = __ldg(&pb.cell[i]);
                 unsigned long long q[8];
                 cic_fixed<SMALL>(__ldg(&pb.ox[i]), __ldg(&pb.oy[i]), __ldg(&pb.oz[i]), mass, q);
+                if (g * PPT + k < xlo) {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) q[j] = 0ull;  // outside the queued part
+                }
                 const int cw = (win_rel(cell_x(c), gx0, ng) * wy + win_rel(cell_y(c), gy0, ng)) * wz +
                                win_rel(cell_z(c), gz0, ng);
                 if (pw == cw) {
@@ -449,8 +789,9 @@ __global__ void __launch_bounds__(NT, 1) deposit_spill_kernel(ParticleSoA p, int
 #pragma unroll
             for (int k = 0; k < PPT; ++k) {
                 const int i = (g * PPT + k) * BB + r;
-                deposit_global<SMALL>(rho, __ldg(&pb.cell[i]), __ldg(&pb.ox[i]), __ldg(&pb.oy[i]), __ldg(&pb.oz[i]),
-                                      mass, ng);
+                if (g * PPT + k >= xlo)
+                    deposit_global<SMALL>(rho, __ldg(&pb.cell[i]), __ldg(&pb.ox[i]), __ldg(&pb.oy[i]),
+                                          __ldg(&pb.oz[i]), mass, ng);
             }
         }
     }
@@ -831,6 +1172,18 @@ __global__ void noise_kernel(float* __restrict__ out, size_t n, uint32_t seed) {
     out[i] = (float)philox_normal((uint64_t)i, seed);
 }
 
+// The reference's white noise (GenerateRealRandom, rng_initializer.cu:38-49),
+// drawn by calling cuRAND's device API the same way: the default generator
+// state, seeded with (seed, subsequence = the cell's linear index, offset 0),
+// one curand_normal_double per cell, stored as float.
+__global__ void noise_curand_kernel(float* __restrict__ out, int n, int seed) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    curandState st;
+    curand_init(seed, i, 0, &st);
+    out[i] = (float)curand_normal_double(&st);
+}
+
 // placeParticles (place_particles_initializer.cu:23-65): lattice point q of
 // particle idx (get_index with np), x = q*(ng/np) + delta*s (wrapped),
 // v = velmul * s.  The position is formed in FP64 and split into cell + offset.
@@ -996,30 +1349,85 @@ static int num_sms() {
     return cached[dev];
 }
 
-// Windowed deposit configurations (B = 16: HGPM_DEPOSIT=0|1|2, default 1;
-// B = 8: always 0): 0) 256 threads, 3 CTAs per SM, 9216-cell (72 KB) window;
-// 1) 512 threads, 2 CTAs per SM, 13824 cells (110.6 KB); 2) 1024 threads, one
-// CTA per SM, kBigCap cells (216 KB).  Measured over a 512^3 run: 1 is the
-// fastest (8.02 / 7.88 / 8.34 ms per step averaged over the run for 0 / 1 / 2).
+// Windowed deposit configurations.  The kernels share one signature; a
+// configuration is (kernel, threads per CTA, window cells, bytes per window
+// cell).
+using DepositFn = void (*)(ParticleSoA, int, int, float, unsigned long long*, int, int*, SpillList, Slots);
+struct DepositCfg {
+    DepositFn fn;
+    int nt, cap, cell_bytes;
+};
+
+constexpr int kDepositCands = 8;
+
+// Candidates per block side; index = HGPM_DEPOSIT (or the tuned choice).
+//   16^3 blocks: 0-2 (lo, hi) 16-bit-split windows (deposit_tiled_kernel) with
+//   256 / 512 / 1024 threads; 3-4 32-bit windows (deposit_w32_kernel), 512
+//   threads x-chained, 256 threads with a 4-deep load ring; 5-7 column
+//   kernels (deposit_col_kernel, 256 threads, x-half split): 4 CTAs per SM
+//   with a 4- or 2-deep ring, 3 CTAs per SM with 18432-cell windows.
+//   8^3 blocks: 0 split window, 1 32-bit window (256 threads, 13312 cells),
+//   2 column kernel (64 threads, 4096 cells), 3 32-bit window (512 threads,
+//   kBigCap cells).
+// The 32-bit windows need mass <= 64; otherwise the split window of the same
+// thread count runs.
+template <int B, bool SMALL>
+static int deposit_candidates(int cap_default, bool w32, DepositCfg* out) {
+    int n = 0;
+    if constexpr (B == 16) {
+        out[n++] = {deposit_tiled_kernel<B, SMALL, 256, 3>, 256, cap_default, 8};
+        out[n++] = {deposit_tiled_kernel<B, SMALL, 512, 2>, 512, 13824, 8};
+        out[n++] = {deposit_tiled_kernel<B, SMALL, 1024, 1>, 1024, kBigCap, 8};
+        if (w32) {
+            out[n++] = {deposit_w32_kernel<B, 512, 2, true>, 512, 13824, 4};
+            out[n++] = {deposit_w32_kernel<B, 256, 4, true, 4>, 256, 13312, 4};
+            out[n++] = {deposit_col_kernel<B, 4, 4>, 256, 13312, 4};
+            out[n++] = {deposit_col_kernel<B, 4, 2>, 256, 13312, 4};
+            out[n++] = {deposit_col_kernel<B, 3, 4>, 256, 18432, 4};
+        } else {
+            // the split window with the same threads per CTA
+            const int same_nt[5] = {1, 0, 0, 0, 0};
+            for (int i = 0; i < 5; ++i) out[n + i] = out[same_nt[i]];
+            n += 5;
+        }
+    } else {
+        out[n++] = {deposit_tiled_kernel<B, SMALL, 256, 3>, 256, cap_default, 8};
+        if (w32) {
+            out[n++] = {deposit_w32_kernel<B, 256, 4, true, 2>, 256, 13312, 4};
+            out[n++] = {deposit_col_kernel<B, 12, 4>, B * B, 4096, 4};
+            out[n++] = {deposit_w32_kernel<B, 512, 2, true, 1>, 512, kBigCap, 4};
+        } else {
+            out[n++] = out[0];
+            out[n++] = out[0];
+            out[n++] = out[0];
+        }
+    }
+    return n;
+}
+
+// Default candidate (measured mid-run): 16^3 blocks the column kernel (1.46
+// ms at 512^3 against 2.22 for the split window with 512 threads); 8^3
+// blocks with more cells than particles per axis (their windows span twice
+// the block) the 32-bit 256-thread kernel with 13312-cell windows, otherwise
+// the column kernel.
+template <int B>
+static int deposit_default_choice(int np_side, int ng) {
+    if (B == 16) return 5;
+    return ng > np_side ? 1 : 2;
+}
+
 template <int B, bool SMALL>
 static cudaError_t deposit_impl(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
                                 int cap, int* blkwin, const SpillList& spill, const Slots& sl, int nslots,
-                                cudaStream_t s) {
-    const char* env = getenv("HGPM_DEPOSIT");
-    int mode = B == 16 ? 1 : 0;
-    if (B == 16 && env && env[0] >= '0' && env[0] <= '2') mode = env[0] - '0';
-    auto k = deposit_tiled_kernel<B, SMALL, 256, 3>;
-    int nt = 256;
-    if (mode == 1) {
-        cap = 13824;
-        k = deposit_tiled_kernel<B, SMALL, 512, 2>;
-        nt = 512;
-    } else if (mode == 2) {
-        cap = kBigCap;
-        k = deposit_tiled_kernel<B, SMALL, 1024, 1>;
-        nt = 1024;
-    }
-    const int smem = cap * 8;
+                                int choice, cudaStream_t s) {
+    DepositCfg cands[kDepositCands];
+    const int ncand = deposit_candidates<B, SMALL>(cap, mass <= 64.0f, cands);
+    const int mode = choice >= 0 && choice < ncand ? choice : deposit_default_choice<B>(np_side, ng);
+    const DepositCfg& cfg = cands[mode];
+    const DepositFn k = cfg.fn;
+    const int nt = cfg.nt;
+    cap = cfg.cap;
+    const int smem = cap * cfg.cell_bytes;
     cudaError_t e = smem_attr_once((const void*)k, smem);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(spill.cnt, 0, sizeof(int) * nslots, s);
@@ -1038,39 +1446,79 @@ static cudaError_t deposit_impl(const ParticleSoA& p, int np_side, int ng, float
     return cudaGetLastError();
 }
 
+int deposit_candidates(int np_side, int ng) { return block_side(np_side, ng) == 16 ? kDepositCands : 4; }
+
+int deposit_default(int np_side, int ng) {
+    return block_side(np_side, ng) == 16 ? deposit_default_choice<16>(np_side, ng)
+                                         : deposit_default_choice<8>(np_side, ng);
+}
+
 cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
-                           int* blkwin, const SpillList& spill, cudaStream_t s, const Slots& sl, int nslots) {
+                           int* blkwin, const SpillList& spill, cudaStream_t s, const Slots& sl, int nslots,
+                           int choice) {
     if (!blkwin || !spill.cnt || !spill.items) return cudaErrorInvalidValue;
     const int B = block_side(np_side, ng);
     const int cap = deposit_cap_cells(np_side, ng);
     // SMALL needs every window add (a weight, or two merged x-chain weights,
     // each < mass*2^31) below 2^32: mass <= 1
     const bool small = mass <= 1.0f;
-    if (B == 16) return small ? deposit_impl<16, true>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl, nslots, s)
-                              : deposit_impl<16, false>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl, nslots, s);
-    return small ? deposit_impl<8, true>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl, nslots, s)
-                 : deposit_impl<8, false>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl, nslots, s);
+    if (B == 16) return small ? deposit_impl<16, true>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl, nslots, choice, s)
+                              : deposit_impl<16, false>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl, nslots, choice, s);
+    return small ? deposit_impl<8, true>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl, nslots, choice, s)
+                 : deposit_impl<8, false>(p, np_side, ng, mass, rho, cap, blkwin, spill, sl, nslots, choice, s);
 }
+// Kick candidates per block side; all run the same FP32 arithmetic in the
+// same order (bit-identical).  16^3 blocks: 0-2 flat 1024-thread CTAs taking
+// a block as four four-plane units in runs of 4 / 2 / 1 (kick_flat_nt_kernel;
+// measured at 512^3 mid-run 2.03 / 2.04 / 2.08 ms), 3 flat 256-thread items
+// (kick_spill_kernel, 2.25 ms), 4 windowed (kick_win4_kernel + the flat
+// kernel for the queued blocks).  8^3 blocks: 0 flat 256-thread items, 1-2
+// flat 512-thread CTAs (a whole block per unit) in runs of 1 / 2, 3 flat
+// 256-thread CTAs in runs of 4, 4 windowed.
+constexpr int kKickCands = 5;
+constexpr int kKickWindowed = 4;
+
+int kick_candidates(int np_side, int ng) {
+    (void)np_side;
+    (void)ng;
+    return kKickCands;
+}
+
+int kick_kernels(int choice, int np_side, int ng) {
+    (void)np_side;
+    (void)ng;
+    return choice == kKickWindowed ? 2 : 1;
+}
+
+template <int B, int NT, int R>
+static cudaError_t kick_flat_launch(const ParticleSoA& p, int np_side, int ng, const float4* f, double deltaT,
+                                    double fscal, float pf_a, float pf_b, int ndrift, const Slots& sl,
+                                    const KickSched& ks, int nslots, cudaStream_t s) {
+    const int nblocks = (np_side / B) * (np_side / B) * (np_side / B);
+    auto kf = kick_flat_nt_kernel<B, NT, R>;
+    const int grid = num_sms() * blocks_per_sm_once((const void*)kf, NT, 0);
+    kf<<<dim3(grid, nslots), NT, 0, s>>>(p, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, nblocks, sl, ks);
+    return cudaGetLastError();
+}
+
 template <int B>
 static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const float4* f, double deltaT, double fscal,
-                             float pf_a, float pf_b, int ndrift, bool force_flat, int* blkwin, bool have_rec,
+                             float pf_a, float pf_b, int ndrift, int choice, int* blkwin, bool have_rec,
                              const SpillList& spill, const Slots& sl, const KickSched& ks, int nslots,
                              cudaStream_t s) {
     constexpr int NT = 512;
     auto ksp = kick_spill_kernel<B>;
     // persistent grid of exactly the resident CTAs (no second round)
     const int sp_grid = num_sms() * blocks_per_sm_once((const void*)ksp, 256, 0);
-    if (force_flat) {
+    if (choice != kKickWindowed) {
         if constexpr (B == 16) {
-            // 1024-thread CTAs, each taking a whole block as four units of four
-            // x-planes: measured at 512^3 mid-run 2.03 ms, against 2.04 (runs
-            // of two units), 2.08 (one unit), 2.18 (two planes per 512-thread
-            // CTA) and 2.25-2.28 (one plane, kick_spill_kernel's 256 threads)
-            const int nblocks = (np_side / B) * (np_side / B) * (np_side / B);
-            auto kf = kick_flat_nt_kernel<B, 1024, 4>;
-            const int grid = num_sms() * blocks_per_sm_once((const void*)kf, 1024, 0);
-            kf<<<dim3(grid, nslots), 1024, 0, s>>>(p, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, nblocks, sl, ks);
-            return cudaGetLastError();
+            if (choice == 0) return kick_flat_launch<B, 1024, 4>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
+            if (choice == 1) return kick_flat_launch<B, 1024, 2>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
+            if (choice == 2) return kick_flat_launch<B, 1024, 1>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
+        } else {
+            if (choice == 1) return kick_flat_launch<B, 512, 1>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
+            if (choice == 2) return kick_flat_launch<B, 512, 2>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
+            if (choice == 3) return kick_flat_launch<B, 256, 4>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
         }
         ksp<<<dim3(sp_grid, nslots), 256, 0, s>>>(p, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, 0, 1, spill, sl, ks);
         return cudaGetLastError();
@@ -1089,25 +1537,25 @@ static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const fl
     if (per_slot < 1) per_slot = 1;
     if (per_slot > nb * nb * nb) per_slot = nb * nb * nb;
     k<<<dim3(per_slot, nslots), NT, smem, s>>>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, blkwin,
-                                                 have_rec ? 1 : 0, force_flat ? 1 : 0, spill, sl, ks);
+                                                 have_rec ? 1 : 0, 0, spill, sl, ks);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    ksp<<<dim3(sp_grid, nslots), 256, 0, s>>>(p, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, have_rec ? 1 : 0,
-                                               force_flat ? 1 : 0, spill, sl, ks);
+    ksp<<<dim3(sp_grid, nslots), 256, 0, s>>>(p, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, have_rec ? 1 : 0, 0, spill,
+                                               sl, ks);
     return cudaGetLastError();
 }
 
 cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float4* f, double deltaT,
-                              double fscal, float pf_a, float pf_b, int ndrift, int variant, int* blkwin,
+                              double fscal, float pf_a, float pf_b, int ndrift, int choice, int* blkwin,
                               bool have_rec, const SpillList& spill, cudaStream_t s, const Slots& sl,
                               const KickSched& ks, int nslots) {
     if (!spill.cnt || !spill.items || !spill.next || !blkwin) return cudaErrorInvalidValue;
-    const bool flat = variant == 1;
+    if (choice < 0 || choice >= kKickCands) choice = 0;
     if (block_side(np_side, ng) == 16)
-        return kick_impl<16>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, flat, blkwin, have_rec, spill, sl,
-                             ks, nslots, s);
-    return kick_impl<8>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, flat, blkwin, have_rec, spill, sl, ks,
-                        nslots, s);
+        return kick_impl<16>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, choice, blkwin, have_rec, spill,
+                             sl, ks, nslots, s);
+    return kick_impl<8>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, choice, blkwin, have_rec, spill, sl,
+                        ks, nslots, s);
 }
 __global__ void slots_advance_kernel(int* __restrict__ active, int* __restrict__ step,
                                      const int* __restrict__ nsteps, int nslots) {
@@ -1131,8 +1579,13 @@ cudaError_t launch_ktables(int ng, double* cosq, float* sk, float* pkw, cudaStre
     ktables_kernel<<<nblk(ng, 128), 128, 0, s>>>(ng, cosq, sk, pkw);
     return cudaGetLastError();
 }
-cudaError_t launch_noise(float* out, size_t n, uint32_t seed, cudaStream_t s) {
-    noise_kernel<<<nblk(n, 256), 256, 0, s>>>(out, n, seed);
+cudaError_t launch_noise(float* out, size_t n, int seed, int kind, cudaStream_t s) {
+    if (kind == 0) {
+        if (n > 0x7fffffffu) return cudaErrorInvalidValue;  // the reference's int cell index
+        noise_curand_kernel<<<nblk(n, 256), 256, 0, s>>>(out, (int)n, seed);
+    } else {
+        noise_kernel<<<nblk(n, 256), 256, 0, s>>>(out, n, (uint32_t)seed);
+    }
     return cudaGetLastError();
 }
 cudaError_t launch_place(const float* sgrid, size_t scomp, const ParticleSoA& p, int np_side, int ng, float delta_f,

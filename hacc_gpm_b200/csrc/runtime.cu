@@ -131,6 +131,14 @@ extern "C" int hgpm_params_parse(const char* text, hgpm_params* out, char* err, 
         else if (!strcmp(key, "DUMP_FINAL")) p.dump_final = 1;
         else if (!strcmp(key, "IPK")) snprintf(p.ipk, sizeof(p.ipk), "%s", value);
         else if (!strcmp(key, "OL")) p.ol = atof(value);
+        else if (!strcmp(key, "NOISE")) {
+            if (!strcmp(value, "CURAND")) p.noise = HGPM_NOISE_CURAND;
+            else if (!strcmp(value, "PHILOX")) p.noise = HGPM_NOISE_PHILOX;
+            else {
+                set_err(err, errlen, "NOISE must be CURAND or PHILOX, not %s", value);
+                return HGPM_ERR_ARG;
+            }
+        }
         // unknown keys are ignored, as in the reference
     }
     if (p.np == 0) {
@@ -355,7 +363,10 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
         const char* xt = getenv("HGPM_XTMA");
         c->xtma = !(xt && xt[0] == '0');
         const char* kv = getenv("HGPM_KICK");
-        if (kv && kv[0] >= '0' && kv[0] <= '2') c->kick_variant = kv[0] - '0';
+        if (kv && kv[0] >= '0' && kv[0] <= '9' && atoi(kv) < kick_candidates(p->np, p->ng)) c->kick_choice = atoi(kv);
+        const char* dv = getenv("HGPM_DEPOSIT");
+        if (dv && dv[0] >= '0' && dv[0] <= '9' && atoi(dv) < deposit_candidates(p->np, p->ng)) c->dep_choice = atoi(dv);
+        ctx_apply_tuned(c);
     }
     c->blk = block_side(c->np, c->ng);
     c->npart = (size_t)c->np * c->np * c->np;
@@ -663,7 +674,8 @@ static double mean_density(const hgpm_ctx* c) {
 
 static int deposit_impl(hgpm_ctx* c) {
     if (c->rho_dirty) CK(cudaMemsetAsync(c->rho64, 0, c->ncell * 8, c->stream));
-    CK(launch_deposit(c->part, c->np, c->ng, cic_mass(c->ng, c->np), c->rho64, c->blkwin, c->dep_spill, c->stream));
+    CK(launch_deposit(c->part, c->np, c->ng, cic_mass(c->ng, c->np), c->rho64, c->blkwin, c->dep_spill, c->stream,
+                      Slots{}, 1, c->dep_choice));
     c->win_valid = true;
     count(c, PH_DEPOSIT, 2);  // windowed pass + spill pass
     c->rho_dirty = true;
@@ -768,9 +780,9 @@ extern "C" int hgpm_kick_drift(hgpm_ctx* c, double deltaT, double fscal, float p
     if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
     PhaseScope ps(c, PH_KICK);
     CK(launch_kick_drift(c->part, c->np, c->ng, reinterpret_cast<const float4*>(c->force), deltaT, fscal, pf_a, pf_b,
-                         ndrift, c->kick_variant, c->blkwin, c->win_valid, c->kick_spill, c->stream));
+                         ndrift, c->kick_choice, c->blkwin, c->win_valid, c->kick_spill, c->stream));
     if (ndrift > 0) c->win_valid = false;
-    count(c, PH_KICK, kick_kernels(c->kick_variant, c->np, c->ng));
+    count(c, PH_KICK, kick_kernels(c->kick_choice, c->np, c->ng));
     return HGPM_OK;
 }
 
@@ -991,7 +1003,7 @@ static int ic_common(hgpm_ctx* c, const float* noise_host, const double* table, 
         if (noise_host) {
             e = cudaMemcpyAsync(noise, noise_host, npart * 4, cudaMemcpyHostToDevice, c->stream);
         } else {
-            e = launch_noise(noise, npart, (uint32_t)c->p.seed, c->stream);
+            e = launch_noise(noise, npart, c->p.seed, c->p.noise, c->stream);
             count(c, PH_PK, 1);
         }
         if (e != cudaSuccess) { rc = fail(c, HGPM_ERR_CUDA, "ic noise: %s", cudaGetErrorString(e)); break; }
@@ -1039,7 +1051,7 @@ extern "C" int hgpm_ic_from_noise(hgpm_ctx* c, const float* noise, const double*
 
 extern "C" int hgpm_ic_noise(hgpm_ctx* c, float* out) {
     if (!c || !out) return HGPM_ERR_ARG;
-    CK(launch_noise(c->force, c->npart, (uint32_t)c->p.seed, c->stream));
+    CK(launch_noise(c->force, c->npart, c->p.seed, c->p.noise, c->stream));
     count(c, PH_PK, 1);
     CK(cudaMemcpyAsync(out, c->force, c->npart * 4, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));

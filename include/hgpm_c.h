@@ -69,7 +69,16 @@ typedef struct hgpm_params {
     unsigned char analysis[HGPM_MAX_STEPS];
     char analysis_dir[HGPM_PATH_MAX];
     char analysis_py[HGPM_PATH_MAX];
+    /* NOISE (new key): white-noise source of hgpm_ic_generate.
+       HGPM_NOISE_CURAND (default): the reference's own draws,
+       curand_init(SEED, cell, 0) then curand_normal_double per cell
+       (rng_initializer.cu:38-49), so a SEED gives the reference's universe;
+       HGPM_NOISE_PHILOX: counter-based Philox4x32-10 (Box-Muller).      */
+    int noise;
 } hgpm_params;
+
+#define HGPM_NOISE_CURAND 0
+#define HGPM_NOISE_PHILOX 1
 
 /* Replaces HACCGPM::read_params (src/simulation/params.cpp:72-250).
  * Does not print or write the .params echo; see hgpm_params_save.        */
@@ -292,6 +301,44 @@ int hgpm_ens_sync_class(hgpm_ensemble* ens, int cls);
  * address (cudaGetSymbolAddress) and should be made before any stream
  * capture.  Stream-ordered on `stream` (a cudaStream_t, NULL = legacy).     */
 int hgpm_cic_density_noalloc(const float* x_dev, int np_side, int ng, float* rho_dev, void* stream);
+
+/* ---- autotuner --------------------------------------------------------------
+ * No counterpart in the reference, whose one launch knob is BLOCK_SIZE
+ * (params.cpp:164, applied to every kernel by InvokeGPUKernel,
+ * haccgpm.hpp:59).  Each knob below has candidates that give bit-identical
+ * results and differ only in speed:
+ *   HGPM_TUNE_DEPOSIT  deposit window kernel / CTA shape / window cap,
+ *   HGPM_TUNE_KICK     kick gather scheme / CTA shape / units per CTA turn,
+ *   HGPM_TUNE_YPASS    1 = TMA-fed persistent y pass, 0 = plain strided,
+ *   HGPM_TUNE_XPASS    1 = TMA-fed persistent x pass, 0 = plain.
+ * hgpm_autotune times every candidate `reps` times on the context's current
+ * particle state (which it leaves unchanged), keeps a knob's default unless
+ * another candidate is faster by more than 2 %, applies the winners to the
+ * context and, when `store`, appends them to the cache file
+ * ($HGPM_TUNE_CACHE, else tune_cache.txt beside the library) under (device
+ * name, SM count, ng, np).  hgpm_create applies the last cached entry for
+ * its size and device unless HGPM_NO_TUNE_CACHE is set (or the knob's
+ * environment variable HGPM_DEPOSIT / HGPM_KICK / HGPM_NO_TMA / HGPM_XTMA
+ * pins it).  choices / best_ms (may be NULL) receive the picks and their
+ * ms per launch.                                                          */
+#define HGPM_TUNE_KNOBS 4
+#define HGPM_TUNE_DEPOSIT 0
+#define HGPM_TUNE_KICK 1
+#define HGPM_TUNE_YPASS 2
+#define HGPM_TUNE_XPASS 3
+int hgpm_autotune(hgpm_ctx* ctx, int reps, int store, int choices[HGPM_TUNE_KNOBS], double best_ms[HGPM_TUNE_KNOBS]);
+/* The knobs a context uses now (after env, cache or tuning).              */
+int hgpm_tuned_choices(const hgpm_ctx* ctx, int choices[HGPM_TUNE_KNOBS]);
+/* The tuner's pick: the fastest of n timings (ms <= 0: not measured),
+ * unless the default `def` is within a fraction `tol` of it.              */
+int hgpm_tune_pick(const double* ms, int n, int def, double tol);
+/* Cache file access (host only): lookup returns 1 and fills choices when a
+ * line for (device, sms, ng, np) exists (the last one wins), else 0;
+ * store appends one line.  device: one token without blanks.              */
+int hgpm_tune_cache_lookup(const char* path, const char* device, int sms, int ng, int np,
+                           int choices[HGPM_TUNE_KNOBS]);
+int hgpm_tune_cache_store(const char* path, const char* device, int sms, int ng, int np,
+                          const int choices[HGPM_TUNE_KNOBS], const double ms[HGPM_TUNE_KNOBS]);
 
 /* ---- ABI checks ------------------------------------------------------------
  * sizeof of the public structs, for bindings that mirror them.            */

@@ -11,6 +11,11 @@
 //
 // usage: cpu_pm --ng N --np N --rl L --steps K --warmup W [--threads T]
 //               [--zini z] [--zfin z] [--nsteps-total S] [--seed s]
+//               [--load FILE --start-step S]
+//               [--omega-cb x --omega-m x --omega-r x --f-nu x]
+// --load reads x then v (float3, lattice order: writeOutput's layout,
+// io.cu:12-44) instead of the seeded perturbed lattice, and the time stepper
+// starts S steps into the run (2S half steps of timestepper.cpp:49-57).
 // Prints one JSON line: per-step seconds of the timed steps.
 #include <omp.h>
 
@@ -279,11 +284,23 @@ int main(int argc, char** argv) {
     const double zfin = arg_d(argc, argv, "--zfin", 0.0);
     const int ntot = (int)arg_d(argc, argv, "--nsteps-total", 100);
     const int seed = (int)arg_d(argc, argv, "--seed", 21082001);
+    const char* load = nullptr;
+    for (int i = 1; i + 1 < argc; ++i)
+        if (!strcmp(argv[i], "--load")) load = argv[i + 1];
+    const int start_step = (int)arg_d(argc, argv, "--start-step", 0);
     if (threads > 0) omp_set_num_threads(threads);
     (void)rl;
     const size_t npart = (size_t)np * np * np, nc = (size_t)ng * ng * ng;
-    // seeded perturbed lattice in Lagrangian order (synthetic ICs)
     std::vector<F3> x(npart), v(npart);
+    if (load) {
+        FILE* f = fopen(load, "rb");
+        if (!f || fread(x.data(), sizeof(F3), npart, f) != npart || fread(v.data(), sizeof(F3), npart, f) != npart) {
+            fprintf(stderr, "cpu_pm: cannot read %s\n", load);
+            return 2;
+        }
+        fclose(f);
+    } else
+    // seeded perturbed lattice in Lagrangian order (synthetic ICs)
 #pragma omp parallel
     {
         std::mt19937 gen(seed + omp_get_thread_num());
@@ -304,13 +321,14 @@ int main(int argc, char** argv) {
     std::vector<float> grad(4 * nc);
     Fft1 f(ng);
     TS ts;
-    ts.om_cb = 0.31;
-    ts.om_m = 0.31;
-    ts.om_r = 5.3e-5;
-    ts.fnu = 0.69;
+    ts.om_cb = arg_d(argc, argv, "--omega-cb", 0.31);
+    ts.om_m = arg_d(argc, argv, "--omega-m", 0.31);
+    ts.om_r = arg_d(argc, argv, "--omega-r", 5.3e-5);
+    ts.fnu = arg_d(argc, argv, "--f-nu", 0.69);
     ts.deltaT = ((1 / (zfin + 1)) - (1 / (zini + 1))) / (double)ntot;
     ts.aa = 1.0 / (zini + 1.0);
     ts.upd();
+    for (int s = 0; s < 2 * start_step; ++s) ts.half();
     const float gp = (float)ng / (float)np;
     const float mass = gp * gp * gp;
     std::vector<double> times;

@@ -7,8 +7,9 @@ product (``hacc_gpm_b200`` and its C-ABI library) never does.
 
 Every function restates one piece of the reference's serial path in float64
 NumPy, citing the reference file:line it follows (paths are relative to the
-HACC_GPM project root).  FFTs are ``numpy.fft`` in complex128 with the same
-sign and normalisation conventions as the reference's cuFFT calls
+HACC_GPM project root).  FFTs are complex128 (``scipy.fft`` on all host
+threads when SciPy is present, else ``numpy.fft``: the same transforms) with
+the same sign and normalisation conventions as the reference's cuFFT calls
 (``src/fft_tools/cuda/ffts.cu:271`` forward = e^{-ikx}, ``:423`` inverse,
 unnormalised).
 
@@ -31,6 +32,17 @@ import struct
 from dataclasses import dataclass, field
 
 import numpy as np
+
+try:
+    import scipy.fft as _sfft
+
+    def _fftn(a):
+        return _sfft.fftn(a, workers=-1)
+
+    def _ifftn(a):
+        return _sfft.ifftn(a, workers=-1)
+except ImportError:  # pragma: no cover
+    _fftn, _ifftn = np.fft.fftn, np.fft.ifftn
 
 MAX_STEPS = 1000  # src/haccgpm.hpp:106
 
@@ -320,7 +332,7 @@ def solve_gradient(rho: np.ndarray, ref_quirks: bool = False) -> np.ndarray:
     (unnormalised, 1/ng^3 sits in G), real part into the force grid
     (transform_density_field_initializer.cu:14-28).  Returns (3, ng, ng, ng)."""
     ng = rho.shape[0]
-    rk = np.fft.fftn(rho.astype(np.complex128))
+    rk = _fftn(rho.astype(np.complex128))
     g = greens(ng, ref_quirks)
     k1 = signed_index(ng) * (2.0 * np.pi / ng)
     sk = np.sin(k1)
@@ -329,7 +341,7 @@ def solve_gradient(rho: np.ndarray, ref_quirks: bool = False) -> np.ndarray:
     for dim in range(3):
         c = -sk.reshape(shapes[dim]) * g
         fk = 1j * c * rk  # (-c*Im, c*Re) == i*c*rho
-        out[dim] = np.fft.ifftn(fk).real * ng ** 3  # unnormalised inverse
+        out[dim] = _ifftn(fk).real * ng ** 3  # unnormalised inverse
     return out
 
 
@@ -393,6 +405,19 @@ def pk_bin_edges(ng: int, rl: float, nbins: int, folds: int = 0):
     return min_k, delta, centres
 
 
+def pk_log_bin_edges(ng: int, rl: float, nbins: int):
+    """Log-spaced bins over the reference's k range (power.cu:174-187:
+    minK = 2pi/rl, maxK = sqrt(3 (ng/2)^2 d^2)): width ln(maxK/minK)/nbins in
+    ln k, centres minK exp((i + 1/2) width).  The reference bins linearly
+    only; PK_LOG is a key this project adds (config C's 64 log bins)."""
+    d = 2.0 * np.pi / rl
+    min_k = d
+    max_k = math.sqrt(3 * ((ng // 2) * (ng // 2) * d * d))
+    dl = math.log(max_k / min_k) / nbins
+    centres = np.array([min_k * math.exp(dl * (i + 0.5)) for i in range(nbins)])
+    return min_k, dl, centres
+
+
 def pk_cic_filter(ng: int) -> np.ndarray:
     """get_pk_cic_filter (filter_power.cu:3-32): prod_axis [sin(k/2)/(k/2)]^-4,
     k = signed index * 2pi/ng, factor 1 at k = 0."""
@@ -430,7 +455,7 @@ def fold_positions(x: np.ndarray, ng: int, fold: int) -> np.ndarray:
 
 
 def power_spectrum(x: np.ndarray, ng: int, np_side: int, rl: float, nbins: int = 221,
-                   folds: int = 0, fold: int = 0, ref_quirks: bool = True):
+                   folds: int = 0, fold: int = 0, ref_quirks: bool = True, log_bins: bool = False):
     """One fold of serial::GetPowerSpectrum (power.cu:152-246): CIC of the
     particles folded `fold` times, forward FFT, scalePower (|d|^2 (1/ng^3)
     (rl/ng), scale_power.cu:3-12), PkCICFilter, BinPower (k in the fold's
@@ -438,20 +463,32 @@ def power_spectrum(x: np.ndarray, ng: int, np_side: int, rl: float, nbins: int =
     edges from rl/2^max(folds, fold) and the scale from the unfolded rl, as
     the reference (power.cu:174-187, 215); otherwise both from the fold's
     box.  Negative bin indices (reference: writes before its arrays) are
-    dropped.  Sums in float64 (the reference sums in float).  Returns
+    dropped.  Sums in float64 (the reference sums in float).  log_bins:
+    pk_log_bin_edges over the fold's box, index (int)(ln(|k|/minK)/width)
+    with |k| formed in float as calc_power_bins does.  Returns
     (k_centres, P, counts) for all bins (empty bins give P=nan)."""
     rl_f = rl / (2.0 ** fold)
     nf = max(folds, fold)
     xf = fold_positions(x, ng, fold) if fold else x
     rho = cic_deposit(xf, ng, cic_mass(ng, np_side))
-    rk = np.fft.fftn(rho)
+    rk = _fftn(rho)
     scale = (1.0 / float(ng * ng * ng)) * ((rl if ref_quirks else rl_f) / ng)
     pw = (rk.real ** 2 + rk.imag ** 2) * scale * pk_cic_filter(ng)
-    if ref_quirks:
+    if log_bins:
+        min_k, dl, centres = pk_log_bin_edges(ng, rl / (2.0 ** nf) if ref_quirks else rl_f, nbins)
+        kf = kmodes_f32(ng, 2.0 * np.pi / rl_f)
+        s2 = (kf[:, None, None] * kf[:, None, None] + kf[None, :, None] * kf[None, :, None]).astype(np.float32) \
+            + kf[None, None, :] * kf[None, None, :]
+        kmag = np.sqrt(s2.astype(np.float32)).astype(np.float64)
+        with np.errstate(divide="ignore"):
+            idx = np.trunc(np.log(kmag / min_k) / dl)
+        idx = np.where(np.isfinite(idx), idx, -1).astype(np.int64)
+    elif ref_quirks:
         min_k, delta, centres = pk_bin_edges(ng, rl, nbins, nf)
+        idx = pk_bin_index(ng, rl_f, min_k, delta)
     else:
         min_k, delta, centres = pk_bin_edges(ng, rl_f, nbins, 0)
-    idx = pk_bin_index(ng, rl_f, min_k, delta)
+        idx = pk_bin_index(ng, rl_f, min_k, delta)
     mask = np.ones((ng, ng, ng), dtype=bool)
     mask[0, 0, 0] = False
     mask[ng // 2, ng // 2, ng // 2] = False
@@ -565,7 +602,7 @@ def displacement_from_noise(noise: np.ndarray, table, k_delta, rl, delta):
     s_dim = -i k_dim delta_k / (k^2 delta), inverse FFT, times 1/n^3.
     Returns s with shape (3, n, n, n)."""
     n = noise.shape[0]
-    dk = np.fft.fftn(noise.astype(np.complex128))
+    dk = _fftn(noise.astype(np.complex128))
     dk *= np.sqrt(interp_pk(table, k_delta, n, rl))
     kf = kmodes_f32(n, 2.0 * np.pi / rl).astype(np.float64)
     kx, ky, kz = kf[:, None, None], kf[None, :, None], kf[None, None, :]
@@ -577,7 +614,7 @@ def displacement_from_noise(noise: np.ndarray, table, k_delta, rl, delta):
     s = np.empty((3, n, n, n))
     for dim, kd in enumerate((kx, ky, kz)):
         sk = -1j * cur * kd  # (Im*k, -Re*k)
-        s[dim] = (np.fft.ifftn(sk) * n ** 3).real / float(n ** 3)
+        s[dim] = (_ifftn(sk) * n ** 3).real / float(n ** 3)
     return s
 
 

@@ -58,6 +58,16 @@ def test_params_errors(built_lib):
         H.parse_params("NG 32\nNP 32\nPK_DUMP 5,2000\n")  # step outside MAX_STEPS
 
 
+def test_params_noise_key(built_lib):
+    """NOISE selects the IC white noise: the reference's cuRAND draws by
+    default, Philox on request; anything else is an error."""
+    assert H.parse_params("NG 32\nNP 32\n").noise == 0
+    assert H.parse_params("NG 32\nNP 32\nNOISE CURAND\n").noise == 0
+    assert H.parse_params("NG 32\nNP 32\nNOISE PHILOX\n").noise == 1
+    with pytest.raises(H.HgpmError, match="NOISE"):
+        H.parse_params("NG 32\nNP 32\nNOISE MT19937\n")
+
+
 def test_params_save_format(built_lib, tmp_path):
     p = H.read_params(os.path.join(GOLD, "ref_test_run_params"))
     p.prefix = str(tmp_path / "echo")

@@ -37,3 +37,21 @@ def test_help_runs_without_a_gpu():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--help"], capture_output=True, text=True,
                        timeout=120)
     assert r.returncode == 0 and "--impl" in r.stdout
+
+
+def test_both_arms_report_the_same_config():
+    """The b200 line and the --impl reference line carry the same config
+    dict for the same --steps/--warmup: the timed steps start at the same
+    step of the same run."""
+    b = _bench()
+    assert b.bench_config(20, 5) == b.bench_config(20, 5)
+    assert b.first_warmup_step(20, 5) == 40 and b.first_warmup_step(10, 3) == 42
+    c = b.bench_config(20, 5)
+    assert "steps 45-64" in c["timed"] and c["np"] == 512 and c["ng"] == 512
+
+
+def test_config_c_box():
+    b = _bench()
+    ng, np_side, rl, nrun, mid = b.CONFIGS["C"]
+    assert (ng, np_side, rl, nrun) == (1024, 512, 1000.0, 200)
+    assert mid < nrun

@@ -122,30 +122,37 @@ def test_fused_x_pass_variants_bit_identical(ng, monkeypatch):
     assert np.array_equal(out[0], out[1])
 
 
-@pytest.mark.parametrize("ng,disp", [(32, 0.3), (64, 0.3), (64, 2.0), (64, 6.0)])
-def test_deposit_configurations_bit_identical(ng, disp, monkeypatch):
-    """The 256-thread / 72 KB and 512-thread / 110 KB windowed deposits (and
-    their spill passes, reached with disp 2 and 6) give the same int64 grid."""
-    x, v = lattice_state(ng, ng, disp=disp, vel=1.0, seed=23)
+@pytest.mark.parametrize("ng,np_side,disp", [(32, 32, 0.3), (64, 64, 0.3), (64, 64, 2.0), (64, 64, 6.0),
+                                             (64, 32, 1.0), (48, 48, 1.0), (64, 32, 5.0)])
+def test_deposit_configurations_bit_identical(ng, np_side, disp, monkeypatch):
+    """Every deposit candidate (split, 32-bit and column windows, with and
+    without x-half splitting; their spill passes, reached with disp 2 to 6)
+    gives the same int64 grid; 16^3 blocks (np = ng = 32, 64) and 8^3 blocks
+    (np < ng, np = 48)."""
+    x, v = lattice_state(np_side, ng, disp=disp, vel=1.0, seed=23)
     out = []
-    for flag in ("0", "1"):
-        monkeypatch.setenv("HGPM_DEPOSIT", flag)
-        with make(ng, ng) as s:
+    n = 8 if np_side % 16 == 0 and ng <= np_side else 4
+    for flag in range(n):
+        monkeypatch.setenv("HGPM_DEPOSIT", str(flag))
+        with make(ng, np_side) as s:
+            assert s.tuned_choices()["deposit"] == flag
             s.load_state(x, v)
             s.cic()
             out.append(s.get_density())
-    assert np.array_equal(out[0], out[1])
+    for o in out[1:]:
+        assert np.array_equal(out[0], o)
 
 
 @pytest.mark.parametrize("ng,np_side,disp", [(32, 32, 1.0), (48, 48, 1.0), (64, 32, 1.0), (32, 64, 1.0), (64, 64, 0.3),
                                              (64, 64, 4.0)])
 def test_kick_variants_bit_identical(ng, np_side, disp, monkeypatch):
-    """Tiled (shared-memory force window), flat (global gather) and float4
-    window kicks run the same FP32 arithmetic in the same order; disp 4
-    spreads blocks past the window caps (global-gather fallback)."""
+    """Every kick candidate (flat global gathers with different CTA shapes
+    and unit runs, the float4-window kick) runs the same FP32 arithmetic in
+    the same order; disp 4 spreads blocks past the window caps (global-gather
+    fallback)."""
     x, v = lattice_state(np_side, ng, disp=disp, vel=1.0, seed=17)
     out = []
-    for flag in ("0", "1", "2"):
+    for flag in ("0", "1", "2", "3", "4"):
         monkeypatch.setenv("HGPM_KICK", flag)
         with make(ng, np_side) as s:
             s.load_state(x, v)
@@ -217,3 +224,41 @@ def test_errors_are_status_codes_not_crashes():
             s.solve_gradient()
         with pytest.raises(H.HgpmError):
             s.load_state(np.zeros((5, 3), np.float32), np.zeros((5, 3), np.float32))
+
+
+@pytest.mark.parametrize("ng,np_side", [(64, 64), (64, 32)])
+def test_autotune_leaves_state_and_results_unchanged(ng, np_side, tmp_path, monkeypatch):
+    """hgpm_autotune times every candidate on the live state: the state is
+    the same afterwards, the picks are valid, steps after tuning equal steps
+    without it bit for bit, and a stored pick is applied to the next context
+    of that size."""
+    for k in ("HGPM_DEPOSIT", "HGPM_KICK", "HGPM_NO_TMA", "HGPM_XTMA"):
+        monkeypatch.delenv(k, raising=False)
+    monkeypatch.setenv("HGPM_TUNE_CACHE", str(tmp_path / "tune.txt"))
+    hp = H.parse_params(params_text(ng, np_side))
+    x, v = lattice_state(np_side, ng, disp=2.0, vel=1.0, seed=29)
+
+    def run(tune):
+        with H.Simulation(hp) as s:
+            s.load_state(x, v)
+            picks = None
+            if tune:
+                picks = s.autotune(reps=2, store=True)
+                x1, v1 = s.store_state()
+                assert np.array_equal(x1, x) and np.array_equal(v1, v)
+            ts = H.Timestepper(hp)
+            ts.set_initial_z(hp.z_ini)
+            ts.reverse_half_step()
+            ts.advance_half_step()
+            s.run_steps(ts, 3)
+            return s.store_state(), picks
+
+    (xa, va), picks = run(True)
+    monkeypatch.setenv("HGPM_NO_TUNE_CACHE", "1")
+    (xb, vb), _ = run(False)
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+    assert all(p["ms"] > 0 for p in picks.values())
+    monkeypatch.delenv("HGPM_NO_TUNE_CACHE")
+    with H.Simulation(hp) as s:
+        got = s.tuned_choices()
+    assert got == {k: p["choice"] for k, p in picks.items()}

@@ -162,7 +162,8 @@ def test_ic_from_noise_matches_oracle(ng, np_side, rl):
 
 
 def test_ic_philox_noise_matches_oracle():
-    hp, op = _pair(32)
+    hp, op = _pair(32, extra="NOISE PHILOX\n")
+    assert hp.noise == 1
     with H.Simulation(hp) as s:
         g = s.ic_noise().reshape(-1)
     o = O.philox_normal(32 ** 3, op.seed)

@@ -29,6 +29,25 @@ def test_ics_from_reference_noise(case):
     assert np.abs(v - case["ics_v"]).max() / np.abs(case["ics_v"]).max() < R.IC_VEL_REL
 
 
+def test_curand_noise_is_the_references(case):
+    """Default NOISE (CURAND): the same SEED draws the reference's white
+    noise bit for bit (rng_initializer.cu:38-49)."""
+    with _sim(case) as s:
+        assert s.params.noise == 0
+        g = s.ic_noise().reshape(case["noise"].shape)
+    assert np.array_equal(g, case["noise"])
+
+
+def test_seeded_ics_are_the_references(case):
+    """hgpm_ic_generate from the params file and .ipk alone (no noise
+    replay) lands on the reference's ICs within the IC bars."""
+    with _sim(case) as s:
+        s.generate_ic(case.ipk_table, case.ipk_header[3])
+        x, v = s.store_state()
+    assert np.abs(O.periodic_diff(x, case["ics_x"], case.ng)).max() < R.IC_POS_CELLS
+    assert np.abs(v - case["ics_v"]).max() / np.abs(case["ics_v"]).max() < R.IC_VEL_REL
+
+
 def test_cells_density_force(case):
     with _sim(case) as s:
         s.load_state(case["ics_x"], case["ics_v"])
