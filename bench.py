@@ -341,8 +341,15 @@ def form_ensemble():
     E.run_serial(warm)
     E.run_batched(warm)
     torch.cuda.synchronize()
-    serial, t_serial = E.timed(E.run_serial, boxes)
-    batched, t_batch = E.timed(E.run_batched, boxes)
+    # each arm twice, alternately; the faster of each is kept (the first pass
+    # after the 512^3 box is freed can pay one-time allocation costs)
+    reps = {"one_at_a_time": [], "batched": []}
+    for _ in range(2):
+        serial, t = E.timed(E.run_serial, boxes)
+        reps["one_at_a_time"].append(t)
+        batched, t = E.timed(E.run_batched, boxes)
+        reps["batched"].append(t)
+    t_serial, t_batch = min(reps["one_at_a_time"]), min(reps["batched"])
     st_serial, st_batch = {}, {}
     E.run_serial(boxes, stages=st_serial)
     E.run_batched(boxes, stages=st_batch)
@@ -352,8 +359,9 @@ def form_ensemble():
         "metric": "ensemble sims/hour (96 mixed boxes, 64 steps each)", "value": 96 / t_batch * 3600.0,
         "unit": "sims/hour", "higher_is_better": True, "n_gpus": 1,
         "one_at_a_time": {"value": 96 / t_serial * 3600.0, "seconds": t_serial},
-        "batched_seconds": t_batch, "speedup_vs_one_at_a_time": t_serial / t_batch,
+        "batched_seconds": t_batch, "speedup_vs_one_at_a_time": t_serial / t_batch, "seconds_per_pass": reps,
         "stages_s": {"batched": st_batch, "one_at_a_time": st_serial},
+        "speedup_steps_only": st_serial["steps"] / st_batch["steps"],
         "speedup_compute_only": (sum(v for k, v in st_serial.items() if k != "create") /
                                  sum(v for k, v in st_batch.items() if k != "create")),
         "pk_max_rel_diff_vs_one_at_a_time": worst, "pk_counts_equal": counts,

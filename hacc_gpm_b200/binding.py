@@ -163,6 +163,7 @@ def lib() -> C.CDLL:
         "hgpm_tune_cache_lookup": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int, P(C.c_int)]),
         "hgpm_tune_cache_store": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int, P(C.c_int),
                                             P(C.c_double)]),
+        "hgpm_test_wait_timeout": (C.c_int, [vp, C.c_uint]),
         "hgpm_sizeof_params": (C.c_size_t, []),
         "hgpm_sizeof_timestepper": (C.c_size_t, []),
     }
@@ -489,6 +490,11 @@ class Simulation:
 
     def kernel_launches(self, reset=False) -> int:
         return self.L.hgpm_kernel_launches(self._h, int(reset))
+
+    def test_wait_timeout(self, polls: int = 1000):
+        """Queue a bounded wait that nothing completes (the time-out path of
+        the TMA passes); the next sync() raises HgpmError."""
+        self._ck(self.L.hgpm_test_wait_timeout(self._h, int(polls)))
 
     def autotune(self, reps: int = 3, store: bool = False) -> dict:
         """Time every configuration of the tunable phases on the current

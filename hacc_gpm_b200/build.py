@@ -80,6 +80,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
         deps = [drv_src, shim_src, LIB, os.path.join(HERE, "host", "haccgpm.hpp"), os.path.join(ROOT, "include", "hgpm_c.h")]
         if force or not _newer(DRIVER, [d for d in deps if os.path.exists(d)]):
             run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(HERE, "host"),
+                 "-I", os.path.join(os.path.dirname(os.path.dirname(nvcc())), "include"),
                  drv_src, shim_src, "-L", LIBDIR, "-lhgpm", "-Wl,-rpath,$ORIGIN", "-o", DRIVER])
     return LIB
 

@@ -34,26 +34,34 @@ namespace {
 
 std::mutex g_cache_mu;
 
-// Device name with blanks replaced (one token in the cache file).
-std::string device_token(int dev) {
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return "unknown";
-    std::string s(prop.name);
-    for (auto& ch : s)
-        if (ch == ' ' || ch == '\t') ch = '_';
-    return s;
+// Device name with blanks replaced (one token in the cache file) and SM
+// count, looked up once per device (cudaGetDeviceProperties takes
+// milliseconds, and every context creation consults the cache).
+struct DeviceKey {
+    bool known = false;
+    std::string name;
+    int sms = 0;
+};
+std::mutex g_dev_mu;
+DeviceKey g_dev[64];
+
+const DeviceKey& device_key(int dev) {
+    static const DeviceKey unknown{true, "unknown", 0};
+    if (dev < 0 || dev >= 64) return unknown;
+    std::lock_guard<std::mutex> g(g_dev_mu);
+    DeviceKey& k = g_dev[dev];
+    if (!k.known) {
+        cudaDeviceProp prop;
+        k.name = cudaGetDeviceProperties(&prop, dev) == cudaSuccess ? std::string(prop.name) : "unknown";
+        for (auto& ch : k.name)
+            if (ch == ' ' || ch == '\t') ch = '_';
+        if (cudaDeviceGetAttribute(&k.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) k.sms = 0;
+        k.known = true;
+    }
+    return k;
 }
 
-int device_sms(int dev) {
-    int n = 0;
-    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-    return n;
-}
-
-// The cache file: $HGPM_TUNE_CACHE, else tune_cache.txt beside the library.
-std::string cache_path() {
-    const char* env = getenv("HGPM_TUNE_CACHE");
-    if (env && env[0]) return env;
+std::string lib_dir_cache() {
     Dl_info info;
     if (dladdr(reinterpret_cast<void*>(&hgpm_autotune), &info) && info.dli_fname) {
         std::string p(info.dli_fname);
@@ -62,6 +70,17 @@ std::string cache_path() {
     }
     return "tune_cache.txt";
 }
+
+// The cache file: $HGPM_TUNE_CACHE, else tune_cache.txt beside the library.
+std::string cache_path() {
+    const char* env = getenv("HGPM_TUNE_CACHE");
+    if (env && env[0]) return env;
+    static std::string beside_lib;
+    static std::once_flag once;
+    std::call_once(once, [] { beside_lib = lib_dir_cache(); });
+    return beside_lib;
+}
+
 
 }  // namespace
 
@@ -116,9 +135,8 @@ extern "C" int hgpm_tune_cache_store(const char* path, const char* device, int s
 int ctx_apply_tuned(hgpm_ctx* c) {
     if (getenv("HGPM_NO_TUNE_CACHE")) return 0;
     int ch[HGPM_TUNE_KNOBS];
-    const std::string dev = device_token(c->device);
-    if (hgpm_tune_cache_lookup(cache_path().c_str(), dev.c_str(), device_sms(c->device), c->ng, c->np, ch) != 1)
-        return 0;
+    const DeviceKey& dk = device_key(c->device);
+    if (hgpm_tune_cache_lookup(cache_path().c_str(), dk.name.c_str(), dk.sms, c->ng, c->np, ch) != 1) return 0;
     if (!getenv("HGPM_DEPOSIT") && ch[HGPM_TUNE_DEPOSIT] >= 0 && ch[HGPM_TUNE_DEPOSIT] < deposit_candidates(c->np, c->ng))
         c->dep_choice = ch[HGPM_TUNE_DEPOSIT];
     if (!getenv("HGPM_KICK") && ch[HGPM_TUNE_KICK] >= 0 && ch[HGPM_TUNE_KICK] < kick_candidates(c->np, c->ng))
@@ -250,8 +268,8 @@ extern "C" int hgpm_autotune(hgpm_ctx* c, int reps, int store, int choices[HGPM_
     if (best_ms)
         for (int k = 0; k < HGPM_TUNE_KNOBS; ++k) best_ms[k] = pms[k];
     if (store) {
-        const std::string dev = device_token(c->device);
-        if (hgpm_tune_cache_store(cache_path().c_str(), dev.c_str(), device_sms(c->device), ng, np, pick, pms))
+        const DeviceKey& dk = device_key(c->device);
+        if (hgpm_tune_cache_store(cache_path().c_str(), dk.name.c_str(), dk.sms, ng, np, pick, pms))
             return fail(c, HGPM_ERR_IO, "hgpm_autotune: cannot write the cache %s", cache_path().c_str());
     }
     return HGPM_OK;

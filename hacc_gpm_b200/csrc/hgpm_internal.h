@@ -59,6 +59,9 @@ cudaError_t launch_xpk(int ng, const float2* in, int ncols, size_t rs, size_t ps
 // lines when isx); err is set if a bounded mbarrier wait times out.
 cudaError_t launch_strided_tma(int ng, bool inv, bool isx, float2* data, int ncols, int zs, size_t cs, int ncomp,
                                const float2* tw, int* err, cudaStream_t s);
+// A bounded mbarrier wait that nothing completes (tests of the time-out
+// path): sets *err after `polls` polls.
+cudaError_t launch_wait_timeout_probe(int* err, unsigned polls, cudaStream_t s);
 // Persistent TMA-fed launch_xpotential (single box).
 cudaError_t launch_xpotential_tma(int ng, float2* in, float2* out, int ncols, int zs, const float2* tw,
                                   const double* cosq, double coeff, int* err, cudaStream_t s);

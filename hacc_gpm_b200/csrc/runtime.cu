@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -322,17 +323,33 @@ static std::vector<float2> twiddles(int n) {
 
 static int even_pad(int v) { return (v + 15) / 16 * 16; }
 
+// Device bytes of one context: every buffer hgpm_create allocates (sized as
+// it sizes them: spectra and the force grid cover the larger of the ng and
+// np grids, which the ICs use), plus the ones made on first use (the float3
+// staging of hgpm_load_state / hgpm_store_state, the P(k) partial sums, the
+// RL and .ipk tables), each rounded up to the 2 MiB granularity of large
+// device allocations.
 extern "C" size_t hgpm_footprint_bytes(int ng, int np) {
-    size_t ncell = (size_t)ng * ng * ng, npart = (size_t)np * np * np;
-    size_t zs = even_pad(ng / 2 + 1);
-    size_t nspec = (size_t)ng * ng * zs;
+    const size_t ncell = (size_t)ng * ng * ng, npart = (size_t)np * np * np;
+    const size_t nspec = (size_t)ng * ng * even_pad(ng / 2 + 1);
+    const size_t nspec_np = (size_t)np * np * even_pad(np / 2 + 1);
+    const size_t spec_elems = std::max(nspec, nspec_np);
+    const size_t force_elems = 4 * std::max(ncell, npart);
+    const size_t nblocks = (size_t)window_records(np, ng) / 8;
+    const size_t page = 2u << 20;
+    auto r = [&](size_t b) { return (b + page - 1) / page * page; };
     size_t b = 0;
-    b += npart * 7 * 4;        // particle SoA
-    b += ncell * 8;            // int64 density
-    b += nspec * 8 * 4;        // spectrum + 3 force spectra
-    b += ncell * 4 * 4;        // force grid (float4 per cell)
-    b += (size_t)ng * 64;      // tables
-    b += (size_t)window_records(np, ng) * 4;  // per-block CIC windows
+    b += r((npart * 4 + 255) / 256 * 256 * 7);          // particle SoA (one block)
+    b += r(ncell * 8);                                  // int64 density
+    b += r(spec_elems * 8);                             // spectrum
+    b += r(spec_elems * 8 * 3);                         // potential / IC spectra
+    b += r(force_elems * 4);                            // float4 force grid
+    b += r((size_t)window_records(np, ng) * 4);         // per-block CIC windows
+    b += r((4 + 2 * nblocks) * 4);                      // spill queues and counters
+    b += r((size_t)ng * 8 * 2 + (size_t)np * 8 + (size_t)ng * 8 + (size_t)ng * 12 + (size_t)np * 4 + 8);  // tables
+    b += r(npart * 6 * 4);                              // float3 staging (first host load/store)
+    b += r((size_t)4 * 148 * pk_max_bins() * 16 + (size_t)pk_max_bins() * 16);  // P(k) partial sums
+    b += r(20000 * 8);                                  // .ipk table (20000 bins)
     return b;
 }
 
@@ -496,6 +513,12 @@ static int sync_check(hgpm_ctx* c) {
 extern "C" int hgpm_sync(hgpm_ctx* c) {
     if (!c) return HGPM_ERR_ARG;
     return sync_check(c);
+}
+
+extern "C" int hgpm_test_wait_timeout(hgpm_ctx* c, unsigned polls) {
+    if (!c || polls == 0 || polls > (1u << 20)) return HGPM_ERR_ARG;
+    CK(launch_wait_timeout_probe(c->d_err + 1, polls, c->stream));
+    return HGPM_OK;
 }
 
 // ===========================================================================

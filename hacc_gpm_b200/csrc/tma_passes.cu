@@ -199,6 +199,27 @@ __global__ void __launch_bounds__(NT, 768 / NT) xpotential_tma_kernel(const __gr
 }
 
 // ---------------------------------------------------------------------------
+// The time-out path of the passes' bounded waits, for tests: thread 0 arms an
+// mbarrier for a 16-byte copy that is never issued, polls it `polls` times
+// as the passes do, and on time-out sets the error flag and returns (no
+// fault, nothing left in flight).
+__global__ void wait_timeout_probe_kernel(int* __restrict__ err, unsigned polls) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    fence_async_shared();
+    mbar_expect_tx(&bar, 16u);
+    bool done = false;
+    for (unsigned i = 0; i < polls && !done; ++i) done = mbar_try_wait(&bar, 0);
+    if (!done) atomicExch(err, 1);
+}
+
+cudaError_t launch_wait_timeout_probe(int* err, unsigned polls, cudaStream_t s) {
+    wait_timeout_probe_kernel<<<1, 32, 0, s>>>(err, polls);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
 static bool encode_fn() {

@@ -24,15 +24,25 @@
 //     > 0) are dropped (REF_QUIRKS 0: each fold binned in its own box).
 #pragma once
 
+// the headers the reference's haccgpm.hpp brings to its callers (the
+// driver calls cudaFree(0) and strlen through them)
+#include <cuda_runtime.h>
+#include <stdio.h>
 #include <cstdint>
+#include <cstring>
 #include <functional>
 
 #include "hgpm_c.h"
 
+// Wall-clock timer as the reference declares it, at global scope
+// (src/haccgpm.hpp:18): microseconds since an arbitrary origin.
+typedef unsigned long long CPUTimer_t;
+CPUTimer_t CPUTimer();
+
 namespace HACCGPM {
 
-typedef int64_t CPUTimer_t;  // microseconds since an arbitrary origin (timers.cpp)
-CPUTimer_t CPUTimer();
+using ::CPUTimer;
+using ::CPUTimer_t;
 
 // src/haccgpm.hpp:118-174, the fields the serial path reads.  `c` holds the
 // same values in the C-ABI layout; every call re-derives it from the named
@@ -60,6 +70,11 @@ struct Params {
     int lastStep;
     int pkFolds;
     int world_rank, world_size;
+    // the one-rank decomposition (the multi-rank fields of the reference's
+    // struct): a single 1x1x1 grid of ranks holding the whole ng^3 grid
+    int local_grid_size[3];
+    int grid_dims[3];
+    int grid_coords[3];
     bool dump_init, dump_final;
     double ol;
     int overload;

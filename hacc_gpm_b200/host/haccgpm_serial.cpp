@@ -7,6 +7,11 @@
 #include <cstring>
 #include <vector>
 
+CPUTimer_t CPUTimer() {
+    using namespace std::chrono;
+    return (CPUTimer_t)duration_cast<microseconds>(steady_clock::now().time_since_epoch()).count();
+}
+
 namespace HACCGPM {
 
 static void die(const char* what, const char* msg) {
@@ -16,11 +21,6 @@ static void die(const char* what, const char* msg) {
 
 static void check(hgpm_ctx* ctx, int rc, const char* what) {
     if (rc != HGPM_OK) die(what, ctx ? hgpm_last_error(ctx) : "invalid argument");
-}
-
-CPUTimer_t CPUTimer() {
-    using namespace std::chrono;
-    return duration_cast<microseconds>(steady_clock::now().time_since_epoch()).count();
 }
 
 static void from_c(Params& p, const hgpm_params& c) {
@@ -62,6 +62,11 @@ static void from_c(Params& p, const hgpm_params& c) {
     p.pkFolds = c.pk_folds;
     p.world_rank = 0;
     p.world_size = 1;
+    for (int a = 0; a < 3; ++a) {
+        p.local_grid_size[a] = p.ng;
+        p.grid_dims[a] = 1;
+        p.grid_coords[a] = 0;
+    }
     p.dump_init = c.dump_init != 0;
     p.dump_final = c.dump_final != 0;
     p.ol = c.ol;

@@ -46,25 +46,34 @@ def request_stream(n: int, rate: float = 20.0, seed: int = 7, sizes=(32, 48, 64,
     return out
 
 
-# GPU milliseconds of one PM step per particle + cell (7.6 ms for a 512^3 box
-# with a 512^3 grid on one B200), for the concurrency cap below
-STEP_MS_PER_UNIT = 7.6 / (2 * 512 ** 3)
+# GPU milliseconds of one PM step per particle + cell, for the concurrency
+# cap below: the mid-run 512^3 step on one B200 (5.7 ms for 512^3 particles
+# on a 512^3 grid, bench.py).
+STEP_MS_PER_UNIT = 5.7 / (2 * 512 ** 3)
 
 
-def class_capacity(sizes, hbm_budget: float, max_slots: int = 64, step_ms: float = None):
-    """Slots per size class by footprint: the budget is split evenly over the
-    classes, and what a class leaves unused (it stops at its cap) is split
-    again over the classes that can still take a slot, until no share buys
-    one.  Every class gets at least one slot.  The cap is max_slots and, with
-    step_ms, the slots whose batched step takes about step_ms of GPU time:
-    more large boxes at once would only share the GPU further and lengthen
-    every one of their runs (the serving p99)."""
+def class_capacity(sizes, hbm_budget: float, max_slots: int = 64, step_ms: float = None,
+                   ms_per_unit: float = STEP_MS_PER_UNIT):
+    """Slots per size class by footprint: every class first gets one slot,
+    then the budget left is split evenly over the classes, and what a class
+    leaves unused (it stops at its cap) is split again over the classes that
+    can still take a slot, until no share buys one.  If one slot of every
+    class does not fit the budget, ValueError (admission is by footprint: no
+    class is given memory it does not have).  The cap is max_slots and, with
+    step_ms, the slots whose batched step takes about step_ms of GPU time
+    (ms_per_unit per particle + cell): more large boxes at once would only
+    share the GPU further and lengthen every one of their runs (the serving
+    p99)."""
     per = {ng: Ensemble.footprint_bytes(ng, ng, 1) for ng in sizes}
+    one = sum(per.values())
+    if one > hbm_budget:
+        raise ValueError("one slot of each size class (%s) needs %.3g GB, above the %.3g GB budget"
+                         % (", ".join("%d^3" % ng for ng in sizes), one / 1e9, hbm_budget / 1e9))
     cap = {ng: max_slots if step_ms is None else
-           int(max(1, min(max_slots, round(step_ms / (STEP_MS_PER_UNIT * 2 * ng ** 3))))) for ng in sizes}
-    n = {ng: 0 for ng in sizes}
-    left = float(hbm_budget)
-    open_ = list(sizes)
+           int(max(1, min(max_slots, round(step_ms / (ms_per_unit * 2 * ng ** 3))))) for ng in sizes}
+    n = {ng: 1 for ng in sizes}
+    left = float(hbm_budget) - one
+    open_ = [ng for ng in sizes if n[ng] < cap[ng]]
     while open_:
         share = left / len(open_)
         gave = False
@@ -77,7 +86,7 @@ def class_capacity(sizes, hbm_budget: float, max_slots: int = 64, step_ms: float
         open_ = [ng for ng in open_ if n[ng] < cap[ng] and per[ng] <= left]
         if not gave:
             break
-    return [(ng, ng, int(max(1, n[ng]))) for ng in sizes]
+    return [(ng, ng, int(n[ng])) for ng in sizes]
 
 
 class Server:

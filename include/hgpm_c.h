@@ -299,7 +299,9 @@ int hgpm_ens_sync_class(hgpm_ensemble* ens, int cls);
  * whose work overlaps on the GPU (different streams, or different host
  * threads) race.  The first call on each device looks up the array's device
  * address (cudaGetSymbolAddress) and should be made before any stream
- * capture.  Stream-ordered on `stream` (a cudaStream_t, NULL = legacy).     */
+ * capture; the address is kept for the life of the process, so after a
+ * cudaDeviceReset of a device this entry point must not be called on that
+ * device again.  Stream-ordered on `stream` (a cudaStream_t, NULL = legacy). */
 int hgpm_cic_density_noalloc(const float* x_dev, int np_side, int ng, float* rho_dev, void* stream);
 
 /* ---- autotuner --------------------------------------------------------------
@@ -339,6 +341,15 @@ int hgpm_tune_cache_lookup(const char* path, const char* device, int sms, int ng
                            int choices[HGPM_TUNE_KNOBS]);
 int hgpm_tune_cache_store(const char* path, const char* device, int sms, int ng, int np,
                           const int choices[HGPM_TUNE_KNOBS], const double ms[HGPM_TUNE_KNOBS]);
+
+/* ---- time-out path, for tests ------------------------------------------------
+ * No counterpart in the reference.  Every mbarrier wait of the TMA-fed
+ * passes is bounded; on time-out the pass sets an error flag and returns,
+ * and the next hgpm_sync reports HGPM_ERR_CUDA ("... timed out ...") and
+ * clears the flag, with the context still usable.  This queues a one-thread
+ * kernel whose bounded wait (polls <= 2^20) nothing completes, so a test can
+ * take that path without a fault.                                         */
+int hgpm_test_wait_timeout(hgpm_ctx* ctx, unsigned polls);
 
 /* ---- ABI checks ------------------------------------------------------------
  * sizeof of the public structs, for bindings that mirror them.            */

@@ -139,8 +139,31 @@ def test_create_rejects_bad_sizes_without_touching_gpu(built_lib):
         H.Simulation(p)
 
 
+def _alloc_sizes(ng, np_side):
+    """The buffers hgpm_create makes and the ones made on first use (float3
+    staging, P(k) partial sums), sized as runtime.cu sizes them."""
+    pad = lambda v: (v + 15) // 16 * 16
+    ncell, npart = ng ** 3, np_side ** 3
+    spec = max(ng * ng * pad(ng // 2 + 1), np_side ** 2 * pad(np_side // 2 + 1))
+    b = 16 if (np_side % 16 == 0 and ng <= np_side) else 8
+    nblocks = (np_side // b) ** 3
+    return [(npart * 4 + 255) // 256 * 256 * 7, ncell * 8, spec * 8, 3 * spec * 8, 16 * max(ncell, npart),
+            nblocks * 8 * 4, (4 + 2 * nblocks) * 4, npart * 24, 4 * 148 * 1024 * 16]
+
+
+def test_footprint_covers_the_allocations(built_lib):
+    """The admission model counts every buffer a context allocates, with the
+    spectra and force grid sized by the larger of the ng and np grids."""
+    for ng, np_side in ((32, 32), (32, 64), (64, 32), (48, 96), (512, 512), (1024, 512)):
+        need = sum(_alloc_sizes(ng, np_side))
+        got = H.footprint_bytes(ng, np_side)
+        assert need <= got <= need + 32 * 2 ** 21, (ng, np_side, need, got)
+    assert H.footprint_bytes(32, 64) > H.footprint_bytes(32, 32)
+
+
 def test_footprint_model_monotone(built_lib):
     a = H.footprint_bytes(64, 64)
     b = H.footprint_bytes(128, 128)
-    assert 7 * a < b < 9 * a
-    assert H.footprint_bytes(512, 512) / 2 ** 30 < 10
+    assert 4 * a < b < 9 * a
+    assert 7 * b < H.footprint_bytes(256, 256) < 9 * b
+    assert H.footprint_bytes(512, 512) / 2 ** 30 < 12

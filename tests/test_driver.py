@@ -55,6 +55,33 @@ def test_echo_and_exit_on_error(tmp_path):
     assert (d / "run.params").read_text() == (d / "py.params").read_text().replace(str(d / "py"), str(d / "run"))
 
 
+REF_DRIVER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "ref_driver")
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(REF_DRIVER), reason="the reference driver was not built (make -C oracle refdrv)")
+def test_reference_driver_on_the_drop_in(tmp_path):
+    """The reference's own src/driver_pm.cpp (main and serial(), compiled
+    unchanged with -DNOPYTHON against host/haccgpm.hpp and libhgpm.so by
+    oracle/Makefile) runs on the B200 path and writes the same files, byte
+    for byte, as this project's driver on the same params."""
+    extra = "LAST_STEP 5\nPK_DUMP 1,3\nPARTICLE_DUMP 2\nDUMP_INIT\nDUMP_FINAL\n"
+    da, _ = _case(tmp_path, "ref", extra=extra)
+    db, _ = _case(tmp_path, "ours", extra=extra)
+    ra = subprocess.run([REF_DRIVER, str(da / "input.params")], capture_output=True, text=True, timeout=300)
+    assert ra.returncode == 0, ra.stderr[-2000:]
+    assert "RUNNING IN SERIAL MODE" in ra.stdout
+    rb = subprocess.run([_driver(), str(db / "input.params")], capture_output=True, text=True, timeout=300)
+    assert rb.returncode == 0, rb.stderr[-2000:]
+    files = ("run.pk.ini.fold.0", "run.pk.1.fold.0", "run.pk.3.fold.0", "run.pk.fin.fold.0", "run.particles.ini",
+             "run.particles.2", "run.particles.fin")
+    for f in files:
+        assert (da / f).exists() and filecmp.cmp(da / f, db / f, shallow=False), f
+    echo_a = (da / "run.params").read_text().replace(str(da), "DIR")
+    echo_b = (db / "run.params").read_text().replace(str(db), "DIR")
+    assert echo_a == echo_b
+
+
 @pytest.mark.gpu
 def test_driver_files_match_api(tmp_path):
     d, txt = _case(tmp_path, "plain")

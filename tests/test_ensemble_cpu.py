@@ -53,7 +53,21 @@ def test_capacity_by_footprint():
     # below its cap could still take a slot from what is left
     assert all(n == 64 or f > 8e9 - used for (_, _, n), f in zip(caps, per))
     assert caps[2][2] > 2e9 // per[2]
-    assert E.Ensemble.footprint_bytes(64, 64, 4) > 4 * H.footprint_bytes(64, 64) * 0.9
+    # every slot carries a box's whole device state: particles, int64
+    # density, four half spectra and the float4 force grid
+    n = 64
+    per_slot = (E.Ensemble.footprint_bytes(n, n, 8) - E.Ensemble.footprint_bytes(n, n, 4)) / 4
+    state = 28 * n ** 3 + 8 * n ** 3 + 4 * 8 * n * n * ((n // 2 + 1 + 15) // 16 * 16) + 16 * n ** 3
+    assert per_slot >= state
+    assert H.footprint_bytes(n, n) >= state
+
+
+def test_capacity_refuses_a_budget_below_one_slot_each():
+    per = E.Ensemble.footprint_bytes(256, 256, 1)
+    with pytest.raises(ValueError, match="budget"):
+        S.class_capacity([32, 256], per * 0.5)
+    caps = S.class_capacity([32, 256], per * 1.5)
+    assert [c[2] for c in caps][1] == 1 and caps[0][2] >= 1
 
 
 def test_bad_class_rejected_without_gpu():
@@ -63,12 +77,14 @@ def test_bad_class_rejected_without_gpu():
 
 def test_capacity_capped_by_batched_step_time():
     """With step_ms the large classes hold only the slots whose batched step
-    takes about that long (256^3: ~0.95 ms each, so 2 at 2 ms); the small
+    takes about that long (256^3: ~0.7 ms each, so 3 at 2 ms); the small
     classes keep their memory share."""
     sizes = (32, 64, 128, 256)
     free = S.class_capacity(sizes, 40e9, max_slots=64)
     capped = S.class_capacity(sizes, 40e9, max_slots=64, step_ms=2.0)
     by = {ng: n for ng, _, n in capped}
-    assert by[256] == 2 and by[128] == round(2.0 / (S.STEP_MS_PER_UNIT * 2 * 128 ** 3))
+    for ng in (128, 256):
+        assert by[ng] == round(2.0 / (S.STEP_MS_PER_UNIT * 2 * ng ** 3))
+    assert by[256] == 3
     assert by[32] == 64 and by[64] == 64
     assert all(c[2] <= f[2] for c, f in zip(capped, free))

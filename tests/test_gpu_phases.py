@@ -262,3 +262,28 @@ def test_autotune_leaves_state_and_results_unchanged(ng, np_side, tmp_path, monk
     with H.Simulation(hp) as s:
         got = s.tuned_choices()
     assert got == {k: p["choice"] for k, p in picks.items()}
+
+
+def test_bounded_wait_time_out_reported_and_context_usable():
+    """A bounded mbarrier wait that nothing completes sets the error flag;
+    hgpm_sync reports it once and clears it, and the context stays usable:
+    the next solve matches a fresh context's bit for bit."""
+    ng = 32
+    x, v = lattice_state(ng, ng, disp=1.0, seed=31)
+    with make(ng) as s:
+        s.load_state(x, v)
+        s.sync()
+        s.test_wait_timeout(1000)
+        with pytest.raises(H.HgpmError, match="timed out"):
+            s.sync()
+        s.sync()  # the flag was cleared
+        s.cic()
+        s.solve_gradient()
+        f1 = s.get_force()
+        s.sync()
+    with make(ng) as s:
+        s.load_state(x, v)
+        s.cic()
+        s.solve_gradient()
+        f2 = s.get_force()
+    assert np.array_equal(f1, f2)
