@@ -240,7 +240,7 @@ extern "C" int hgpm_ens_create(int nclass, const int* ng, const int* np, const i
     E->device = device;
     for (int i = 0; i < nclass; ++i) {
         if (!fft_size_supported(ng[i]) || !fft_size_supported(np[i]))
-            return efail(E, HGPM_ERR_ARG, "class %d: NG/NP must be one of 16,24,32,48,64,96,128,192,256,384,512,768,1024", i);
+            return efail(E, HGPM_ERR_ARG, "class %d: NG/NP must be one of " HGPM_SIZES_TEXT, i);
         if (nslots[i] <= 0 || nslots[i] > 65535 / 3) return efail(E, HGPM_ERR_ARG, "class %d: bad slot count", i);
     }
     const char* kv = getenv("HGPM_KICK");

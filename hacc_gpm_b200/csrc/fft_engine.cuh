@@ -5,7 +5,7 @@
 // i.e. lines are columns with unit stride between lines.  Every pass kernel
 // (z R2C/C2R lines, y and x strided lines) stages its data into this layout
 // and calls fft_tile<>.  The transform is a Stockham autosort mixed-radix
-// FFT (radices 2, 3, 4, 8): each stage reads R values per butterfly into
+// FFT (radices 2, 3, 4, 5, 8): each stage reads R values per butterfly into
 // registers, synchronises, twiddles, does the radix-R DFT in registers and
 // writes back in place in Stockham order.  Threads are mapped line-fastest
 // so a half-warp touches 16 consecutive lines of one element (conflict-free
@@ -67,6 +67,30 @@ template <bool INV> struct Dft<4, INV> {
         v[2] = csub(a0, b0);
         v[1] = cadd(a1, b1);
         v[3] = csub(a1, b1);
+    }
+};
+
+// Radix 5 from the DFT definition: with t1 = v1 + v4, t2 = v2 + v3,
+// t3 = v1 - v4, t4 = v2 - v3, c_k = cos(2 pi k/5), s_k = sin(2 pi k/5),
+//   X0 = v0 + t1 + t2,
+//   X1, X4 = a1 -+ i b1,  a1 = v0 + c1 t1 + c2 t2,  b1 = s1 t3 + s2 t4,
+//   X2, X3 = a2 -+ i b2,  a2 = v0 + c2 t1 + c1 t2,  b2 = s2 t3 - s1 t4
+// (forward, exp(-2 pi i jk/5); the inverse flips the sign of i).
+template <bool INV> struct Dft<5, INV> {
+    static __device__ __forceinline__ void run(float2* v) {
+        const float c1 = 0.30901699437494742410f, c2 = -0.80901699437494742410f;
+        const float s1 = 0.95105651629515357212f, s2 = 0.58778525229247312917f;
+        const float2 t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+        const float2 t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+        const float2 a1 = make_float2(v[0].x + c1 * t1.x + c2 * t2.x, v[0].y + c1 * t1.y + c2 * t2.y);
+        const float2 a2 = make_float2(v[0].x + c2 * t1.x + c1 * t2.x, v[0].y + c2 * t1.y + c1 * t2.y);
+        const float2 b1 = rot90<INV>(make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y));
+        const float2 b2 = rot90<INV>(make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y));
+        v[0] = cadd(v[0], cadd(t1, t2));
+        v[1] = cadd(a1, b1);
+        v[4] = csub(a1, b1);
+        v[2] = cadd(a2, b2);
+        v[3] = csub(a2, b2);
     }
 };
 
@@ -214,7 +238,8 @@ __device__ __forceinline__ void fft_stages(float2* buf, const float2* tw, RSeq<R
     fft_stages<N, C, ES, INV, NT, TWS, TP, NS * R>(buf, tw, RSeq<Rs...>{});
 }
 
-// Radix plans for the supported lengths (2^a 3^b, 8..1024).
+// Radix plans for the supported lengths (2^a 3^b 5^c, 8..1024; the grid
+// sides and their halves, the z passes' complex lengths).
 template <int N> struct Plan;
 template <> struct Plan<8> { using type = RSeq<8>; };
 template <> struct Plan<12> { using type = RSeq<3, 4>; };
@@ -231,6 +256,23 @@ template <> struct Plan<384> { using type = RSeq<3, 8, 4, 4>; };
 template <> struct Plan<512> { using type = RSeq<8, 8, 8>; };
 template <> struct Plan<768> { using type = RSeq<3, 8, 8, 4>; };
 template <> struct Plan<1024> { using type = RSeq<8, 8, 4, 4>; };
+template <> struct Plan<20> { using type = RSeq<5, 4>; };
+template <> struct Plan<40> { using type = RSeq<5, 8>; };
+template <> struct Plan<60> { using type = RSeq<3, 5, 4>; };
+template <> struct Plan<80> { using type = RSeq<5, 4, 4>; };
+template <> struct Plan<100> { using type = RSeq<5, 5, 4>; };
+template <> struct Plan<120> { using type = RSeq<3, 5, 8>; };
+template <> struct Plan<160> { using type = RSeq<5, 8, 4>; };
+template <> struct Plan<200> { using type = RSeq<5, 5, 8>; };
+template <> struct Plan<240> { using type = RSeq<3, 5, 4, 4>; };
+template <> struct Plan<320> { using type = RSeq<5, 8, 8>; };
+template <> struct Plan<400> { using type = RSeq<5, 5, 4, 4>; };
+template <> struct Plan<480> { using type = RSeq<3, 5, 8, 4>; };
+template <> struct Plan<500> { using type = RSeq<5, 5, 5, 4>; };
+template <> struct Plan<640> { using type = RSeq<5, 8, 4, 4>; };
+template <> struct Plan<800> { using type = RSeq<5, 5, 8, 4>; };
+template <> struct Plan<960> { using type = RSeq<3, 5, 8, 8>; };
+template <> struct Plan<1000> { using type = RSeq<5, 5, 5, 8>; };
 
 // Radix sequence helpers: all but the last radix, the last radix, reversal.
 template <int R, class S> struct SeqCons;

@@ -646,8 +646,6 @@ static cudaError_t xpk_impl(const float2* in, int ncols, size_t rs, size_t ps, c
     return cudaGetLastError();
 }
 
-#define HGPM_SIZES(X) X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
-
 bool fft_size_supported(int ng) {
     switch (ng) {
 #define X(n) case n:

@@ -20,6 +20,15 @@ struct PkArgs {
     double scale;        // (1/ng^3) * (rl/ng), scale_power.cu:8
 };
 
+// Grid sides with compiled FFT passes: 2^a 3^b 5^c multiples of 8 up to 1024
+// (the reference's sizing tool, mem_calc.py:6-22, picks such sides; the
+// Lagrangian particle blocks need multiples of 8 and the packed cell index
+// 10 bits per axis).
+#define HGPM_SIZES(X)                                                                                       \
+    X(16) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(120) X(128) X(160) X(192) X(200) X(240) X(256) X(320) \
+    X(384) X(400) X(480) X(512) X(640) X(768) X(800) X(960) X(1000) X(1024)
+#define HGPM_SIZES_TEXT                                                                                     \
+    "16,24,32,40,48,64,80,96,120,128,160,192,200,240,256,320,384,400,480,512,640,768,800,960,1000,1024"
 bool fft_size_supported(int ng);
 // cudaFuncAttributeMaxDynamicSharedMemorySize for `func` on the current
 // device, set once per (device, kernel) rather than before every launch.

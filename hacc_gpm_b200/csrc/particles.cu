@@ -501,13 +501,18 @@ __global__ void __launch_bounds__(NT, MINB) deposit_w32_kernel(ParticleSoA p, in
 // deposited as two halves, one after the other, each with its own window,
 // wrap check and flush; only blocks whose halves do not fit either (or that
 // wrap) go to deposit_spill_kernel.
-template <int B, int PF>
+// Adds the column range [k0, k0 + len) into the window.  RET: each atomic
+// returns the cell's old value and a wrap (old + q < old) is recorded in
+// *wrapped; otherwise the sum of the added values is returned for the
+// caller's window-sum check.
+template <int B, int PF, bool RET>
 __device__ __forceinline__ unsigned long long column_adds(const ParticleSoA& p, int i0, int k0, int len, float mass,
                                                           unsigned* __restrict__ w0, int gx0, int gy0, int gz0,
-                                                          int wy, int wz, int ng) {
+                                                          int wy, int wz, int ng, bool* wrapped) {
     constexpr int BB = B * B;
     const int syz = wy * wz;
     unsigned long long added = 0ull;
+    bool wr = false;
     uint32_t rc[PF];
     float rx[PF], ry[PF], rz[PF];
 #pragma unroll
@@ -543,19 +548,25 @@ __device__ __forceinline__ unsigned long long column_adds(const ParticleSoA& p, 
                 for (int b = 0; b < 2; ++b)
 #pragma unroll
                     for (int cc = 0; cc < 2; ++cc) {
-                        const unsigned long long v = q[(a * 2 + b) * 2 + cc];
-                        added += v;
-                        atomicAdd(&w0[cw + a * syz + b * wz + cc], (unsigned)v);
+                        const unsigned v = (unsigned)q[(a * 2 + b) * 2 + cc];
+                        if (RET) {
+                            const unsigned old = atomicAdd(&w0[cw + a * syz + b * wz + cc], v);
+                            wr |= old + v < old;
+                        } else {
+                            added += v;
+                            atomicAdd(&w0[cw + a * syz + b * wz + cc], v);
+                        }
                     }
         }
     }
+    if (RET) *wrapped = wr;
     return added;
 }
 
 // Zero the window, add the column range [k0, k0 + len), check for wraps and
 // flush; returns false (nothing flushed) if a cell wrapped.  Called by every
 // thread of the CTA.
-template <int B, int PF>
+template <int B, int PF, bool RET>
 __device__ __forceinline__ bool column_pass(const ParticleSoA& p, int i0, int k0, int len, float mass,
                                             unsigned* __restrict__ w0, long long* wsum, const int* box, int ox,
                                             int oy, int oz, int ng, unsigned long long* __restrict__ rho) {
@@ -566,16 +577,22 @@ __device__ __forceinline__ bool column_pass(const ParticleSoA& p, int i0, int k0
     const int vol = wx * wy * wz;
     for (int i = tid; i < vol; i += NT) w0[i] = 0u;
     __syncthreads();
-    const unsigned long long added = column_adds<B, PF>(p, i0, k0, len, mass, w0, gx0, gy0, gz0, wy, wz, ng);
-    __syncthreads();
-    long long d = -(long long)added;
-    for (int i = tid; i < vol; i += NT) d += (long long)w0[i];
-    d = warp_sum_ll(d);
-    if ((tid & 31) == 0) wsum[tid >> 5] = d;
-    __syncthreads();
+    bool wrapped = false;
+    const unsigned long long added =
+        column_adds<B, PF, RET>(p, i0, k0, len, mass, w0, gx0, gy0, gz0, wy, wz, ng, &wrapped);
     long long tot = 0;
+    if (RET) {
+        tot = __syncthreads_or(wrapped) ? 1 : 0;
+    } else {
+        __syncthreads();
+        long long d = -(long long)added;
+        for (int i = tid; i < vol; i += NT) d += (long long)w0[i];
+        d = warp_sum_ll(d);
+        if ((tid & 31) == 0) wsum[tid >> 5] = d;
+        __syncthreads();
 #pragma unroll
-    for (int k = 0; k < NT / 32; ++k) tot += wsum[k];
+        for (int k = 0; k < NT / 32; ++k) tot += wsum[k];
+    }
     if (tot == 0) {
         const WinMap map(wy, wz, gx0, gy0, gz0, ng);
         for (int i = tid; i < vol; i += NT) {
@@ -587,7 +604,7 @@ __device__ __forceinline__ bool column_pass(const ParticleSoA& p, int i0, int k0
     return tot == 0;
 }
 
-template <int B, int MINB, int PF>
+template <int B, int MINB, int PF, bool RET = false>
 __global__ void __launch_bounds__(B * B, MINB) deposit_col_kernel(ParticleSoA p, int np_side, int ng, float mass,
                                                                   unsigned long long* __restrict__ rho, int cap_cells,
                                                                   int* __restrict__ blkwin, SpillList spill, Slots sl) {
@@ -661,15 +678,15 @@ __global__ void __launch_bounds__(B * B, MINB) deposit_col_kernel(ParticleSoA p,
     // flushed); at most one item per block
     int queue = -1;
     if (vol <= cap_cells) {
-        if (!column_pass<B, PF>(p, tid, 0, B, mass, w0, wsum, bb, ox, oy, oz, ng, rho)) queue = 0;
+        if (!column_pass<B, PF, RET>(p, tid, 0, B, mass, w0, wsum, bb, ox, oy, oz, ng, rho)) queue = 0;
     } else {
         auto hvol = [&](int h) {
             const int* q = bb + 6 + 6 * h;
             return (long long)(q[3] - q[0] + 2) * (q[4] - q[1] + 2) * (q[5] - q[2] + 2);
         };
         if (hvol(0) <= cap_cells && hvol(1) <= cap_cells) {
-            if (!column_pass<B, PF>(p, tid, 0, B / 2, mass, w0, wsum, bb + 6, ox, oy, oz, ng, rho)) queue = 0;
-            else if (!column_pass<B, PF>(p, tid, B / 2, B / 2, mass, w0, wsum, bb + 12, ox, oy, oz, ng, rho))
+            if (!column_pass<B, PF, RET>(p, tid, 0, B / 2, mass, w0, wsum, bb + 6, ox, oy, oz, ng, rho)) queue = 0;
+            else if (!column_pass<B, PF, RET>(p, tid, B / 2, B / 2, mass, w0, wsum, bb + 12, ox, oy, oz, ng, rho))
                 queue = 2;
         } else {
             queue = 0;
@@ -1173,15 +1190,24 @@ __global__ void noise_kernel(float* __restrict__ out, size_t n, uint32_t seed) {
 }
 
 // The reference's white noise (GenerateRealRandom, rng_initializer.cu:38-49),
-// drawn by calling cuRAND's device API the same way: the default generator
-// state, seeded with (seed, subsequence = the cell's linear index, offset 0),
-// one curand_normal_double per cell, stored as float.
-__global__ void noise_curand_kernel(float* __restrict__ out, int n, int seed) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    curandState st;
-    curand_init(seed, i, 0, &st);
-    out[i] = (float)curand_normal_double(&st);
+// drawn through cuRAND's device API: the default generator state seeded with
+// (seed, subsequence = the cell's linear index, offset 0), one
+// curand_normal_double per cell, stored as float.  T threads (a power of two)
+// draw cells t, t + T, t + 2T, ...: a thread seeds its first cell with
+// curand_init and reaches each next one with skipahead_sequence(T).
+// Subsequence skips compose, so every cell gets exactly the state
+// curand_init(seed, cell, 0) gives it, for one jump per cell instead of
+// curand_init's skip over the whole cell index.
+__global__ void noise_curand_kernel(float* __restrict__ out, int n, int seed, int T) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T || t >= n) return;
+    curandState base;
+    curand_init(seed, t, 0, &base);
+    for (int c = t; c < n; c += T) {
+        curandState st = base;
+        out[c] = (float)curand_normal_double(&st);
+        if (c + T < n) skipahead_sequence((unsigned long long)T, &base);
+    }
 }
 
 // placeParticles (place_particles_initializer.cu:23-65): lattice point q of
@@ -1358,17 +1384,18 @@ struct DepositCfg {
     int nt, cap, cell_bytes;
 };
 
-constexpr int kDepositCands = 8;
+constexpr int kDepositCands = 9;
 
 // Candidates per block side; index = HGPM_DEPOSIT (or the tuned choice).
 //   16^3 blocks: 0-2 (lo, hi) 16-bit-split windows (deposit_tiled_kernel) with
 //   256 / 512 / 1024 threads; 3-4 32-bit windows (deposit_w32_kernel), 512
-//   threads x-chained, 256 threads with a 4-deep load ring; 5-7 column
+//   threads x-chained, 256 threads with a 4-deep load ring; 5-8 column
 //   kernels (deposit_col_kernel, 256 threads, x-half split): 4 CTAs per SM
-//   with a 4- or 2-deep ring, 3 CTAs per SM with 18432-cell windows.
+//   with a 4- or 2-deep ring, 3 CTAs per SM with 18432-cell windows, and 4
+//   CTAs per SM detecting wraps from the atomics' returned values.
 //   8^3 blocks: 0 split window, 1 32-bit window (256 threads, 13312 cells),
 //   2 column kernel (64 threads, 4096 cells), 3 32-bit window (512 threads,
-//   kBigCap cells).
+//   kBigCap cells), 4 column kernel with returned-value wrap detection.
 // The 32-bit windows need mass <= 64; otherwise the split window of the same
 // thread count runs.
 template <int B, bool SMALL>
@@ -1384,11 +1411,12 @@ static int deposit_candidates(int cap_default, bool w32, DepositCfg* out) {
             out[n++] = {deposit_col_kernel<B, 4, 4>, 256, 13312, 4};
             out[n++] = {deposit_col_kernel<B, 4, 2>, 256, 13312, 4};
             out[n++] = {deposit_col_kernel<B, 3, 4>, 256, 18432, 4};
+            out[n++] = {deposit_col_kernel<B, 4, 4, true>, 256, 13312, 4};
         } else {
             // the split window with the same threads per CTA
-            const int same_nt[5] = {1, 0, 0, 0, 0};
-            for (int i = 0; i < 5; ++i) out[n + i] = out[same_nt[i]];
-            n += 5;
+            const int same_nt[6] = {1, 0, 0, 0, 0, 0};
+            for (int i = 0; i < 6; ++i) out[n + i] = out[same_nt[i]];
+            n += 6;
         }
     } else {
         out[n++] = {deposit_tiled_kernel<B, SMALL, 256, 3>, 256, cap_default, 8};
@@ -1396,10 +1424,9 @@ static int deposit_candidates(int cap_default, bool w32, DepositCfg* out) {
             out[n++] = {deposit_w32_kernel<B, 256, 4, true, 2>, 256, 13312, 4};
             out[n++] = {deposit_col_kernel<B, 12, 4>, B * B, 4096, 4};
             out[n++] = {deposit_w32_kernel<B, 512, 2, true, 1>, 512, kBigCap, 4};
+            out[n++] = {deposit_col_kernel<B, 12, 4, true>, B * B, 4096, 4};
         } else {
-            out[n++] = out[0];
-            out[n++] = out[0];
-            out[n++] = out[0];
+            for (int i = 0; i < 4; ++i) out[n++] = out[0];
         }
     }
     return n;
@@ -1446,7 +1473,7 @@ static cudaError_t deposit_impl(const ParticleSoA& p, int np_side, int ng, float
     return cudaGetLastError();
 }
 
-int deposit_candidates(int np_side, int ng) { return block_side(np_side, ng) == 16 ? kDepositCands : 4; }
+int deposit_candidates(int np_side, int ng) { return block_side(np_side, ng) == 16 ? kDepositCands : 5; }
 
 int deposit_default(int np_side, int ng) {
     return block_side(np_side, ng) == 16 ? deposit_default_choice<16>(np_side, ng)
@@ -1582,7 +1609,10 @@ cudaError_t launch_ktables(int ng, double* cosq, float* sk, float* pkw, cudaStre
 cudaError_t launch_noise(float* out, size_t n, int seed, int kind, cudaStream_t s) {
     if (kind == 0) {
         if (n > 0x7fffffffu) return cudaErrorInvalidValue;  // the reference's int cell index
-        noise_curand_kernel<<<nblk(n, 256), 256, 0, s>>>(out, (int)n, seed);
+        // threads: the largest power of two <= n / 16 (at least 32, at most 2^20)
+        int T = 32;
+        while (T < (1 << 20) && (size_t)T * 2 * 16 <= n) T *= 2;
+        noise_curand_kernel<<<nblk(T, 256), 256, 0, s>>>(out, (int)n, seed, T);
     } else {
         noise_kernel<<<nblk(n, 256), 256, 0, s>>>(out, n, (uint32_t)seed);
     }

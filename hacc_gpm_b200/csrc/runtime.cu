@@ -366,8 +366,8 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
         *out = c;  // return the context so the caller can read the message
         return code;
     };
-    if (!fft_size_supported(p->ng)) return bad(HGPM_ERR_ARG, "NG must be one of 16,24,32,48,64,96,128,192,256,384,512,768,1024");
-    if (!fft_size_supported(p->np)) return bad(HGPM_ERR_ARG, "NP must be one of 16,24,32,48,64,96,128,192,256,384,512,768,1024");
+    if (!fft_size_supported(p->ng)) return bad(HGPM_ERR_ARG, "NG must be one of " HGPM_SIZES_TEXT);
+    if (!fft_size_supported(p->np)) return bad(HGPM_ERR_ARG, "NP must be one of " HGPM_SIZES_TEXT);
     if (p->rl <= 0) return bad(HGPM_ERR_ARG, "RL must be positive");
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return bad(HGPM_ERR_CUDA, cudaGetErrorString(e));

@@ -313,7 +313,7 @@ cudaError_t launch_xpotential_tma(int ng, float2* in, float2* out, int ncols, in
     switch (ng) {
 #define X(n) \
     case n: return xpotential_tma_impl<n>(in, out, ncols, zs, tw, cosq, coeff, err, s);
-        X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
+        HGPM_SIZES(X)
 #undef X
     }
     return cudaErrorInvalidValue;
@@ -324,7 +324,7 @@ cudaError_t launch_strided_tma(int ng, bool inv, bool isx, float2* data, int nco
     switch (ng) {
 #define X(n) \
     case n: return tma_impl<n>(inv, isx, data, ncols, zs, cs, ncomp, tw, err, s);
-        X(16) X(24) X(32) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) X(768) X(1024)
+        HGPM_SIZES(X)
 #undef X
     }
     return cudaErrorInvalidValue;

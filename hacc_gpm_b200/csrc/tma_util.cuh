@@ -10,10 +10,19 @@ namespace hgpm {
 constexpr int kTmaThreads = 256;
 constexpr unsigned kMaxPolls = 1u << 22;
 
+// Rows per TMA box: the largest divisor d of n with d <= 256 (a box
+// dimension) whose box of ct complex columns is a whole number of 128-byte
+// lines (d * ct * 8 % 128 == 0), so every box's shared-memory destination,
+// b * d * ct * 8 bytes into a 1024-aligned tile, is 128-byte aligned.
+constexpr int box_rows(int n, int ct, int d = 256) {
+    return d <= 1 ? 1 : ((n % d == 0 && (d * ct * 8) % 128 == 0) ? d : box_rows(n, ct, d - 1));
+}
+
 template <int NG> struct TmaCfg {
     static constexpr int CT = NG <= 256 ? 16 : (NG <= 512 ? 8 : 4);  // complex columns per tile
-    // rows per TMA box: a divisor of NG that is <= 256 (384 -> 2 x 192)
-    static constexpr int RB = NG <= 256 ? NG : (NG % 256 == 0 ? 256 : NG / 2);
+    // rows per TMA box (384 -> 2 x 192, 1000 -> 5 x 200)
+    static constexpr int RB = box_rows(NG, CT);
+    static_assert(NG % RB == 0 && RB <= 256 && (RB * CT * 8) % 128 == 0, "TMA box rows");
     static constexpr int NBOX = NG / RB;
     static constexpr int TILE_BYTES = NG * CT * 8;
     static constexpr int SMEM = 2 * TILE_BYTES + 1024;               // + alignment slack

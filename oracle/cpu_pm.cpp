@@ -36,7 +36,7 @@ struct F3 {
 };
 
 // ---------------------------------------------------------------------------
-// 1D FFT (Stockham, radices 4/2/3), forward sign -1, unnormalised
+// 1D FFT (Stockham, radices 4/2/3/5), forward sign -1, unnormalised
 // ---------------------------------------------------------------------------
 struct Fft1 {
     int n;
@@ -47,6 +47,7 @@ struct Fft1 {
         while (m % 4 == 0) { radices.push_back(4); m /= 4; }
         while (m % 2 == 0) { radices.push_back(2); m /= 2; }
         while (m % 3 == 0) { radices.push_back(3); m /= 3; }
+        while (m % 5 == 0) { radices.push_back(5); m /= 5; }
         if (m != 1) { fprintf(stderr, "unsupported FFT size %d\n", n); exit(2); }
         tw.resize(n);
         for (int k = 0; k < n; ++k) tw[k] = cf((float)cos(-2 * M_PI * k / n), (float)sin(-2 * M_PI * k / n));
@@ -60,15 +61,25 @@ struct Fft1 {
             const int nb = n / r;
             for (int j = 0; j < nb; ++j) {
                 const int k = j % ns;
-                cf v[4];
+                cf v[5];
                 for (int q = 0; q < r; ++q) v[q] = src[j + q * nb];
                 if (ns > 1)
                     for (int q = 1; q < r; ++q) {
                         cf w = tw[q * k * (n / (ns * r))];
                         v[q] *= (sign < 0 ? w : std::conj(w));
                     }
-                cf y[4];
-                if (r == 2) {
+                cf y[5];
+                if (r == 5) {
+                    // the radix-5 DFT from its definition (sum over the five inputs)
+                    for (int q = 0; q < 5; ++q) {
+                        cf acc = 0;
+                        for (int t = 0; t < 5; ++t) {
+                            const double ang = sign * 2 * M_PI * (double)((q * t) % 5) / 5.0;
+                            acc += v[t] * cf((float)cos(ang), (float)sin(ang));
+                        }
+                        y[q] = acc;
+                    }
+                } else if (r == 2) {
                     y[0] = v[0] + v[1];
                     y[1] = v[0] - v[1];
                 } else if (r == 4) {

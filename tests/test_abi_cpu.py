@@ -133,8 +133,12 @@ def test_write_pk_format_matches_oracle(built_lib, tmp_path):
     assert got == O.format_pk_lines(k, P, n)
 
 
-def test_create_rejects_bad_sizes_without_touching_gpu(built_lib):
-    p = H.parse_params(ipkmod.lcdm_params_text(40, 40, 40.0, 50.0, 5))
+@pytest.mark.parametrize("ng", [20, 44, 56, 1008, 1280])
+def test_create_rejects_bad_sizes_without_touching_gpu(built_lib, ng):
+    """Sides outside the compiled 2^a 3^b 5^c multiples of 8 up to 1024 (20:
+    not a multiple of 8; 44, 56: factors 11, 7; 1008: a factor 7; 1280: above
+    the 10-bit packed cell) are refused before any device work."""
+    p = H.parse_params(ipkmod.lcdm_params_text(ng, ng, float(ng), 50.0, 5))
     with pytest.raises(H.HgpmError, match="NG must be one of"):
         H.Simulation(p)
 

@@ -9,8 +9,10 @@ to (j/NS)*NS*R + k + r*NS.  For every supported length this checks that:
     inverse DFT,
   * forward, then a per-mode operator in the turn stage, then inverse equals
     N * ifft(op * fft(x)), which is what the fused x pass computes.
-The GPU tests compare the kernels with the oracle at 16-128 and 512; this
-also covers 192, 256, 384, 768 and 1024.
+The GPU tests compare the kernels with the oracle at 16-160 and 512; this
+also covers every other compiled length up to 1024.  The radix-5
+butterfly's algebra (Dft<5> in fft_engine.cuh) is restated too and checked
+against the DFT definition.
 """
 import os
 import re
@@ -79,7 +81,7 @@ def run(x, N, radices, inv, tw, ns=1):
 @pytest.mark.parametrize("N", sorted(plans()))
 def test_plan_forward_inverse_and_turn(N):
     P = plans()[N]
-    assert int(np.prod(P)) == N and all(r in (2, 3, 4, 8) for r in P)
+    assert int(np.prod(P)) == N and all(r in (2, 3, 4, 5, 8) for r in P)
     tw = np.exp(-2j * np.pi * np.arange(N) / N)
     rng = np.random.default_rng(N)
     x = rng.standard_normal(N) + 1j * rng.standard_normal(N)
@@ -93,5 +95,39 @@ def test_plan_forward_inverse_and_turn(N):
     assert np.allclose(y, N * np.fft.ifft(g * np.fft.fft(x)), atol=1e-9 * N * N)
 
 
+def compiled_sizes():
+    txt = open(os.path.join(os.path.dirname(HDR), "hgpm_internal.h")).read()
+    body = txt[txt.index("#define HGPM_SIZES(X)"):txt.index("#define HGPM_SIZES_TEXT")]
+    return sorted(int(n) for n in re.findall(r"X\((\d+)\)", body))
+
+
 def test_every_supported_grid_side_has_a_plan():
-    assert set(plans()) >= {16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024}
+    """Every compiled grid side and its half (the z passes' complex length)
+    has a plan; the sides are 2^a 3^b 5^c multiples of 8 up to 1024."""
+    sides = compiled_sizes()
+    assert set(sides) >= {16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 768, 1024, 40, 80, 160, 320, 640, 1000}
+    for n in sides:
+        m = n
+        for r in (2, 3, 5):
+            while m % r == 0:
+                m //= r
+        assert m == 1 and n % 8 == 0 and n <= 1024
+    assert set(plans()) >= set(sides) | {n // 2 for n in sides}
+
+
+def test_radix5_butterfly_algebra():
+    """Dft<5>: t1 = v1 + v4, t2 = v2 + v3, t3 = v1 - v4, t4 = v2 - v3;
+    X0 = v0 + t1 + t2, X1/X4 = a1 -/+ i b1, X2/X3 = a2 -/+ i b2 with
+    a1 = v0 + c1 t1 + c2 t2, a2 = v0 + c2 t1 + c1 t2, b1 = s1 t3 + s2 t4,
+    b2 = s2 t3 - s1 t4 (forward; the inverse flips i)."""
+    c1, c2 = np.cos(2 * np.pi / 5), np.cos(4 * np.pi / 5)
+    s1, s2 = np.sin(2 * np.pi / 5), np.sin(4 * np.pi / 5)
+    rng = np.random.default_rng(5)
+    for inv in (False, True):
+        v = rng.standard_normal(5) + 1j * rng.standard_normal(5)
+        t1, t2, t3, t4 = v[1] + v[4], v[2] + v[3], v[1] - v[4], v[2] - v[3]
+        a1, a2 = v[0] + c1 * t1 + c2 * t2, v[0] + c2 * t1 + c1 * t2
+        rot = (1j if inv else -1j)
+        b1, b2 = rot * (s1 * t3 + s2 * t4), rot * (s2 * t3 - s1 * t4)
+        X = np.array([v[0] + t1 + t2, a1 + b1, a2 + b2, a2 - b2, a1 - b1])
+        assert np.allclose(X, dft(v, inv), atol=1e-12)

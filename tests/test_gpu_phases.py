@@ -13,7 +13,7 @@ from tests.helpers import FIELD_RTOL, lattice_state, params_text, rel_max_err
 
 pytestmark = pytest.mark.gpu
 
-SIZES = [16, 24, 32, 48, 64, 96, 128]
+SIZES = [16, 24, 32, 40, 48, 64, 80, 96, 120, 128, 160, 200]
 
 
 def make(ng, np_side=None, rl=None, extra=""):
@@ -61,18 +61,23 @@ def test_deposit_deterministic_and_matches_oracle(ng, np_side):
     assert r1.astype(np.float64).sum() == pytest.approx(ro.sum(), rel=1e-7)
 
 
-def test_deposit_hot_cell_exact():
-    """All particles in one cell (late-time clustering extreme): the integer
-    accumulation stays exact."""
-    ng = 32
-    x = np.full((ng ** 3, 3), 5.5, np.float32)
-    v = np.zeros_like(x)
-    with make(ng) as s:
-        s.load_state(x, v)
-        s.cic()
-        r = s.get_density()
-    assert np.count_nonzero(r) == 8
-    assert r[5, 5, 5] == np.float32(ng ** 3 / 8)
+@pytest.mark.parametrize("ng,np_side,ncand", [(32, 32, 9), (64, 32, 5)])
+def test_deposit_hot_cell_exact(ng, np_side, ncand, monkeypatch):
+    """All particles in one cell (late-time clustering extreme): the 32-bit
+    windows wrap, every candidate detects it and sends the block to the
+    exact pass, and the integer accumulation stays exact."""
+    for pos, cells in ((5.5, 8), (5.0, 1)):
+        x = np.full((np_side ** 3, 3), pos, np.float32)
+        v = np.zeros_like(x)
+        for cand in range(ncand):
+            monkeypatch.setenv("HGPM_DEPOSIT", str(cand))
+            with make(ng, np_side) as s:
+                s.load_state(x, v)
+                s.cic()
+                r = s.get_density()
+            mass = (ng / np_side) ** 3
+            assert np.count_nonzero(r) == cells, (pos, cand)
+            assert r[5, 5, 5] == np.float32(np_side ** 3 * mass / cells), (pos, cand)
 
 
 @pytest.mark.parametrize("ng", SIZES)
@@ -88,7 +93,7 @@ def test_solve_gradient_matches_oracle(ng):
     assert rel_max_err(f, fo) < FIELD_RTOL
 
 
-@pytest.mark.parametrize("ng", [48, 64, 128])
+@pytest.mark.parametrize("ng", [48, 64, 80, 128, 320])
 def test_tma_and_plain_strided_passes_bit_identical(ng, monkeypatch):
     """The persistent TMA-fed y passes and the plain strided kernels run the
     same per-line transform, so forces are bit-identical."""
@@ -131,7 +136,7 @@ def test_deposit_configurations_bit_identical(ng, np_side, disp, monkeypatch):
     (np < ng, np = 48)."""
     x, v = lattice_state(np_side, ng, disp=disp, vel=1.0, seed=23)
     out = []
-    n = 8 if np_side % 16 == 0 and ng <= np_side else 4
+    n = 9 if np_side % 16 == 0 and ng <= np_side else 5
     for flag in range(n):
         monkeypatch.setenv("HGPM_DEPOSIT", str(flag))
         with make(ng, np_side) as s:

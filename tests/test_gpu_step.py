@@ -22,7 +22,9 @@ def _pair(ng, np_side=None, rl=None, z_ini=50.0, nsteps=100, extra=""):
 
 
 @pytest.mark.parametrize("ng,np_side,rl,z,n", [(32, 32, 32.0, 50.0, 10), (48, 48, 96.0, 100.0, 8),
-                                               (64, 32, 64.0, 50.0, 5), (32, 64, 32.0, 50.0, 5)])
+                                               (64, 32, 64.0, 50.0, 5), (32, 64, 32.0, 50.0, 5),
+                                               (40, 40, 40.0, 50.0, 6), (80, 40, 160.0, 50.0, 5),
+                                               (160, 80, 160.0, 50.0, 4)])
 def test_run_steps_match_oracle(ng, np_side, rl, z, n):
     hp, op = _pair(ng, np_side, rl, z_ini=z)
     x0, v0, *_ = oracle_ics(op)
@@ -82,7 +84,7 @@ def test_whole_step_deterministic():
     assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
 
 
-@pytest.mark.parametrize("ng,nbins,log_bins", [(32, 221, False), (48, 40, False), (64, 32, True)])
+@pytest.mark.parametrize("ng,nbins,log_bins", [(32, 221, False), (48, 40, False), (64, 32, True), (40, 60, False)])
 def test_power_spectrum_matches_oracle(ng, nbins, log_bins):
     hp, op = _pair(ng, rl=2.0 * ng, z_ini=20.0)
     x0, v0, *_ = oracle_ics(op)
@@ -150,7 +152,8 @@ def test_power_spectrum_deterministic_and_leaves_state():
     assert np.array_equal(x1, x0) and np.array_equal(v1, v0)
 
 
-@pytest.mark.parametrize("ng,np_side,rl", [(32, 32, 32.0), (48, 48, 64.0), (64, 32, 128.0), (32, 64, 64.0)])
+@pytest.mark.parametrize("ng,np_side,rl", [(32, 32, 32.0), (48, 48, 64.0), (64, 32, 128.0), (32, 64, 64.0),
+                                         (40, 40, 80.0), (80, 80, 80.0)])
 def test_ic_from_noise_matches_oracle(ng, np_side, rl):
     hp, op = _pair(ng, np_side, rl, z_ini=50.0)
     xo, vo, noise, table, header = oracle_ics(op)
