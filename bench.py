@@ -34,7 +34,9 @@ on the same state and steps: the reference's own serial CUDA code
 and advances them to the first warm-up step, then the transcription runs
 the W warm-up and K timed steps.  Its line carries the same config.
 
---workload ensemble | serve (1 GPU) print only the batched form's line:
+--workload ensemble | serve print only the batched form's line (under
+torchrun each rank takes its share of the boxes / requests, whole boxes by
+predicted cost; makespans are the slowest rank's):
   ensemble  96 boxes, ng = np from {32, 48, 64, 96, 128}, L ~ U[64, 512],
             sigma8 ~ U[0.7, 0.9], z 100, 64 steps each: sims/hour batched
             (one launch per phase per size class, CUDA graph) against the
@@ -98,8 +100,8 @@ def alg_bytes(np3, ng3):
 
 # The kernels of each phase (one launch each per step, unless noted).
 KERNEL_NAMES = {
-    "deposit": "deposit_col_kernel<16,4,4> (autotuned choice; 32-bit windows, x-half split) + "
-               "deposit_spill_kernel<16,1,1024> (queued wide blocks)",
+    "deposit": "deposit_col_kernel<16,4,4,1> (autotuned choice; 32-bit windows, x-half split, wraps from the "
+               "atomics' returned values) + deposit_spill_kernel<16,1,1024> (queued blocks)",
     "fft_z_fwd": "zpass_r2c_kernel<NG,1>",
     "fft_y_fwd": "strided_tma_kernel<NG,0,0>",
     "poisson_x": "xpotential_tma_kernel<NG,256> (forward x, Green's function, inverse x)",
@@ -329,12 +331,17 @@ def _check_same(a, b):
     return worst, counts
 
 
-def form_ensemble():
-    """96 mixed boxes batched against the same boxes one at a time."""
+def form_ensemble(rk=None):
+    """96 mixed boxes batched against the same boxes one at a time.  Under
+    torchrun each rank takes its share of the boxes (ensemble.shard: whole
+    boxes by predicted cost, no collective on the data path); times are the
+    slowest rank's."""
     import torch
 
     from hacc_gpm_b200 import ensemble as E
-    boxes = E.prepare_tables(E.ensemble_boxes(96))
+    from hacc_gpm_b200.replicas import Ranks
+    rk = rk or Ranks("nccl")
+    boxes = E.prepare_tables(E.shard(E.ensemble_boxes(96), rk.rank, rk.world))
     warm = E.prepare_tables(E.ensemble_boxes(10, master_seed=1))
     for b in warm:
         b.nsteps = 3
@@ -342,22 +349,26 @@ def form_ensemble():
     E.run_batched(warm)
     torch.cuda.synchronize()
     # each arm twice, alternately; the faster of each is kept (the first pass
-    # after the 512^3 box is freed can pay one-time allocation costs)
+    # after a large box is freed can pay one-time allocation costs)
     reps = {"one_at_a_time": [], "batched": []}
     for _ in range(2):
+        rk.barrier()
         serial, t = E.timed(E.run_serial, boxes)
-        reps["one_at_a_time"].append(t)
+        reps["one_at_a_time"].append(rk.allmax(t))
+        rk.barrier()
         batched, t = E.timed(E.run_batched, boxes)
-        reps["batched"].append(t)
+        reps["batched"].append(rk.allmax(t))
     t_serial, t_batch = min(reps["one_at_a_time"]), min(reps["batched"])
     st_serial, st_batch = {}, {}
     E.run_serial(boxes, stages=st_serial)
     E.run_batched(boxes, stages=st_batch)
     worst, counts = _check_same(batched, serial)
+    worst = rk.allmax(worst)
+    counts = rk.allsum(0.0 if counts else 1.0) == 0.0
     classes, _ = E.class_layout(boxes)
     return {
         "metric": "ensemble sims/hour (96 mixed boxes, 64 steps each)", "value": 96 / t_batch * 3600.0,
-        "unit": "sims/hour", "higher_is_better": True, "n_gpus": 1,
+        "unit": "sims/hour", "higher_is_better": True, "n_gpus": rk.world,
         "one_at_a_time": {"value": 96 / t_serial * 3600.0, "seconds": t_serial},
         "batched_seconds": t_batch, "speedup_vs_one_at_a_time": t_serial / t_batch, "seconds_per_pass": reps,
         "stages_s": {"batched": st_batch, "one_at_a_time": st_serial},
@@ -367,54 +378,97 @@ def form_ensemble():
         "pk_max_rel_diff_vs_one_at_a_time": worst, "pk_counts_equal": counts,
         "config": {"workload": "96 boxes, ng = np uniform over {32,48,64,96,128}, L ~ U[64,512] Mpc/h, "
                                "sigma8 ~ U[0.7,0.9], seeds 1000+i, EH ICs at z=100, 64 steps, P(k) 32 bins",
-                   "classes": classes, "timed": "ICs + 64 steps + final P(k) of every box (host-side "
-                                                ".ipk tables prepared beforehand for both)",
+                   "classes_rank0": classes, "timed": "ICs + 64 steps + final P(k) of every box (host-side "
+                                                      ".ipk tables prepared beforehand for both)",
                    "batched": "one launch per phase per size class, classes on parallel streams, "
-                              "CUDA graph per step"},
+                              "CUDA graph per step",
+                   "parallelism": "replicas: %d rank(s), whole boxes per rank by predicted cost" % rk.world},
         "dtype": "f32", "data": "synthetic: seeded EH no-wiggle Zel'dovich ICs",
     }
 
 
-def form_serve(nreq):
+def form_serve(nreq, rk=None):
     """A Poisson request stream served with continuous batching against the
-    same stream one request at a time."""
+    same stream one request at a time.  Under torchrun each rank serves its
+    share of the requests (ensemble.shard) on its own GPU, from a common
+    start after a barrier; latencies are gathered, makespans are the
+    slowest rank's."""
     import torch
 
+    from hacc_gpm_b200 import ensemble as E
     from hacc_gpm_b200 import serve as S
-    reqs = S.request_stream(nreq)
+    from hacc_gpm_b200.replicas import Ranks
+    rk = rk or Ranks("nccl")
+
+    def mine():
+        return E.shard(S.request_stream(nreq), rk.rank, rk.world)
+
     warm = S.request_stream(8, rate=1000.0, seed=3, steps=(2, 3))
     S.serve(warm, realtime=False)
     S.serve_one_at_a_time(S.request_stream(8, rate=1000.0, seed=3, steps=(2, 3)), realtime=False)
     torch.cuda.synchronize()
-    got, mk, stats = S.serve(reqs)
-    one, mk1 = S.serve_one_at_a_time(S.request_stream(nreq))
-    sat, mks, _ = S.serve(S.request_stream(nreq), realtime=False)
-    sat1, mks1 = S.serve_one_at_a_time(S.request_stream(nreq), realtime=False)
+    rk.barrier()
+    got, mk, stats = S.serve(mine())
+    mk = rk.allmax(mk)
+    rk.barrier()
+    one, mk1 = S.serve_one_at_a_time(mine())
+    mk1 = rk.allmax(mk1)
+    rk.barrier()
+    sat, mks, _ = S.serve(mine(), realtime=False)
+    mks = rk.allmax(mks)
+    # one at a time, saturated, twice: its per-request context allocation
+    # makes passes differ by up to 2x; the faster pass is the baseline
+    passes = []
+    for _ in range(2):
+        rk.barrier()
+        sat1, t1 = S.serve_one_at_a_time(mine(), realtime=False)
+        passes.append(rk.allmax(t1))
+    mks1 = min(passes)
     worst, counts = _check_same(sorted(got, key=lambda r: r.tag), sorted(one, key=lambda r: r.tag))
-    out = S.latency_summary(got, mk)
+    worst = rk.allmax(worst)
+    counts = rk.allsum(0.0 if counts else 1.0) == 0.0
+
+    class _L:
+        def __init__(self, lat):
+            self.latency = lat
+
+    def everyone(reqs):
+        return [_L(x) for part in rk.gather([r.latency for r in reqs]) for x in part]
+
+    out = S.latency_summary(everyone(got), mk)
     return {
         "metric": "serving p99 completion latency (Poisson 20 req/s)", "value": out["p99_s"], "unit": "s",
-        "higher_is_better": False, "n_gpus": 1, "batched": out, "one_at_a_time": S.latency_summary(one, mk1),
-        "saturated": {"batched_sims_per_hour": len(sat) / mks * 3600.0,
-                      "one_at_a_time_sims_per_hour": len(sat1) / mks1 * 3600.0, "speedup": mks1 / mks},
+        "higher_is_better": False, "n_gpus": rk.world, "batched": out,
+        "one_at_a_time": S.latency_summary(everyone(one), mk1),
+        "saturated": {"batched_sims_per_hour": nreq / mks * 3600.0,
+                      "one_at_a_time_sims_per_hour": nreq / mks1 * 3600.0, "speedup": mks1 / mks,
+                      "one_at_a_time_seconds_per_pass": passes, "batched_seconds": mks},
         "pk_max_rel_diff_vs_one_at_a_time": worst, "pk_counts_equal": counts,
         "config": {"workload": "%d requests, Poisson arrivals 20/s (seed 7), ng = np log-uniform over "
                                "{32,48,64,96,128,192,256}, L = ng Mpc/h, steps U[20,200], Om U[0.25,0.35], "
                                "sigma8 U[0.7,0.9], EH ICs at z=50" % nreq,
-                   "classes": stats["classes"],
+                   "classes_rank0": stats["classes"],
                    "admission": "slots per size class from a 40 GB HBM budget split over the classes by footprint "
                                 "per slot, at most the slots whose batched step is ~2 ms of GPU time",
                    "scheduling": "each class on its own stream at its own pace (batches of ~1 ms), stream "
-                                 "priority by box size (smaller first)"},
+                                 "priority by box size (smaller first)",
+                   "parallelism": "replicas: %d rank(s), whole requests per rank by predicted cost" % rk.world},
         "dtype": "f32", "data": "synthetic",
     }
 
 
 def run_forms(args):
-    """--workload ensemble | serve: the batched form's own line (1 GPU)."""
+    """--workload ensemble | serve: the batched form's own line (one rank per
+    GPU under torchrun; rank 0 prints)."""
     import torch
-    torch.cuda.set_device(0)
-    print(json.dumps(form_ensemble() if args.workload == "ensemble" else form_serve(args.requests)))
+
+    from hacc_gpm_b200.replicas import Ranks
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rk = Ranks("nccl")
+    out = form_ensemble(rk) if args.workload == "ensemble" else form_serve(args.requests, rk)
+    rk.close()
+    if rk.rank == 0:
+        print(json.dumps(out))
 
 
 def main():
@@ -595,7 +649,7 @@ def main():
     sim.close()
     forms = None
     if rank == 0 and world == 1 and args.config == "NS" and not args.size and not args.no_forms:
-        forms = {"ensemble": form_ensemble(), "serve": form_serve(args.requests)}
+        forms = {"ensemble": form_ensemble(rk), "serve": form_serve(args.requests, rk)}
     rk.close()
     if rank != 0:
         return

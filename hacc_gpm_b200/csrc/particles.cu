@@ -718,6 +718,42 @@ __device__ __forceinline__ void deposit_global(unsigned long long* __restrict__ 
             for (int cc = 0; cc < 2; ++cc) atomicAdd(&rho[sx[a] + sy[b] + sz[cc]], q[(a * 2 + b) * 2 + cc]);
 }
 
+// Direct deposit: one CTA per Lagrangian block records the block's window
+// (for the windowed kick, as the windowed deposits do), then every particle
+// adds its 8 fixed-point weights straight to the int64 grid.  Where a window
+// would hold about one contribution per cell (more cells than particles per
+// axis: each particle's corners are mostly its own) this skips the window's
+// zeroing and flush; the sums are the same integers (bit-identical grids).
+template <int B, bool SMALL, int NT>
+__global__ void __launch_bounds__(NT) deposit_direct_kernel(ParticleSoA p, int np_side, int ng, float mass,
+                                                            unsigned long long* __restrict__ rho, int cap_cells,
+                                                            int* __restrict__ blkwin, SpillList spill, Slots sl) {
+    constexpr int B3 = B * B * B;
+    constexpr int PPT = B3 / NT;
+    static_assert(B3 % NT == 0, "whole particles per thread");
+    (void)cap_cells;
+    __shared__ int bb[6];
+    if (slot_idle(sl, blockIdx.y)) return;
+    const int tid = threadIdx.x;
+    const int nb = np_side / B;
+    const int blk = blockIdx.x;
+    p = offset_soa(p, (size_t)blockIdx.y * sl.s0 + (size_t)blk * B3);
+    rho += (size_t)blockIdx.y * sl.s1;
+    const int bz = blk % nb, by = (blk / nb) % nb, bx = blk / (nb * nb);
+    const int ox = (int)((long long)bx * B * ng / np_side);
+    const int oy = (int)((long long)by * B * ng / np_side);
+    const int oz = (int)((long long)bz * B * ng / np_side);
+    int l0[3], w[3];
+    block_window<NT, PPT>(p.cell, 0, ox, oy, oz, ng, bb, l0, w);
+    if (blkwin && tid < 6) blkwin[(size_t)blockIdx.y * sl.s2 + (size_t)blk * kWinRec + tid] = tid < 3 ? l0[tid] : w[tid - 3];
+    if (tid == 0 && spill.over && (long long)w[0] * w[1] * w[2] > kWin4Cap) atomicAdd(&spill.over[blockIdx.y], 1);
+#pragma unroll 2
+    for (int k = 0; k < PPT; ++k) {
+        const int i = tid + k * NT;
+        deposit_global<SMALL>(rho, __ldg(&p.cell[i]), __ldg(&p.ox[i]), __ldg(&p.oy[i]), __ldg(&p.oz[i]), mass, ng);
+    }
+}
+
 // Blocks queued by deposit_tiled_kernel (window wider than its own): a
 // persistent grid of one CTA per SM with a kBigCap-cell window (216 KB) takes
 // them from the queue one at a time.  A thread walks PPT x-adjacent particles
@@ -1384,7 +1420,7 @@ struct DepositCfg {
     int nt, cap, cell_bytes;
 };
 
-constexpr int kDepositCands = 9;
+constexpr int kDepositCands = 10;
 
 // Candidates per block side; index = HGPM_DEPOSIT (or the tuned choice).
 //   16^3 blocks: 0-2 (lo, hi) 16-bit-split windows (deposit_tiled_kernel) with
@@ -1392,10 +1428,12 @@ constexpr int kDepositCands = 9;
 //   threads x-chained, 256 threads with a 4-deep load ring; 5-8 column
 //   kernels (deposit_col_kernel, 256 threads, x-half split): 4 CTAs per SM
 //   with a 4- or 2-deep ring, 3 CTAs per SM with 18432-cell windows, and 4
-//   CTAs per SM detecting wraps from the atomics' returned values.
+//   CTAs per SM detecting wraps from the atomics' returned values; 9 direct
+//   (deposit_direct_kernel: no window, every weight to the int64 grid).
 //   8^3 blocks: 0 split window, 1 32-bit window (256 threads, 13312 cells),
 //   2 column kernel (64 threads, 4096 cells), 3 32-bit window (512 threads,
-//   kBigCap cells), 4 column kernel with returned-value wrap detection.
+//   kBigCap cells), 4 column kernel with returned-value wrap detection, 5
+//   direct.
 // The 32-bit windows need mass <= 64; otherwise the split window of the same
 // thread count runs.
 template <int B, bool SMALL>
@@ -1418,6 +1456,7 @@ static int deposit_candidates(int cap_default, bool w32, DepositCfg* out) {
             for (int i = 0; i < 6; ++i) out[n + i] = out[same_nt[i]];
             n += 6;
         }
+        out[n++] = {deposit_direct_kernel<B, SMALL, 512>, 512, 0, 0};
     } else {
         out[n++] = {deposit_tiled_kernel<B, SMALL, 256, 3>, 256, cap_default, 8};
         if (w32) {
@@ -1428,18 +1467,21 @@ static int deposit_candidates(int cap_default, bool w32, DepositCfg* out) {
         } else {
             for (int i = 0; i < 4; ++i) out[n++] = out[0];
         }
+        out[n++] = {deposit_direct_kernel<B, SMALL, 256>, 256, 0, 0};
     }
     return n;
 }
 
-// Default candidate (measured mid-run): 16^3 blocks the column kernel (1.46
-// ms at 512^3 against 2.22 for the split window with 512 threads); 8^3
+// Default candidate (measured mid-run): 16^3 blocks the column kernel with
+// returned-value wrap detection (1.41 ms at 512^3, against 1.46 with the
+// window-sum check and 2.22 for the split window with 512 threads); 8^3
 // blocks with more cells than particles per axis (their windows span twice
-// the block) the 32-bit 256-thread kernel with 13312-cell windows, otherwise
-// the column kernel.
+// the block) the 32-bit 256-thread kernel with 13312-cell windows (6.9 ms
+// for 512^3 particles on a 1024^3 grid, against 8.3-11.8 for the other
+// windows), otherwise the column kernel.
 template <int B>
 static int deposit_default_choice(int np_side, int ng) {
-    if (B == 16) return 5;
+    if (B == 16) return 8;
     return ng > np_side ? 1 : 2;
 }
 
@@ -1473,7 +1515,7 @@ static cudaError_t deposit_impl(const ParticleSoA& p, int np_side, int ng, float
     return cudaGetLastError();
 }
 
-int deposit_candidates(int np_side, int ng) { return block_side(np_side, ng) == 16 ? kDepositCands : 5; }
+int deposit_candidates(int np_side, int ng) { return block_side(np_side, ng) == 16 ? kDepositCands : 6; }
 
 int deposit_default(int np_side, int ng) {
     return block_side(np_side, ng) == 16 ? deposit_default_choice<16>(np_side, ng)

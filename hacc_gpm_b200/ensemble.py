@@ -270,8 +270,9 @@ def run_batched(boxes, device: int = 0, graph: bool = True, keep_state: bool = F
 
 
 def shard(boxes, rank: int, world: int):
-    """This rank's share of an ensemble on `world` GPUs (replicas: whole boxes
-    per GPU, split by predicted cost; no collective on the data path)."""
+    """This rank's share of an ensemble (or a request stream) on `world` GPUs
+    (replicas: whole boxes per GPU, split by predicted cost; no collective on
+    the data path).  Every rank computes the same split."""
     from .replicas import box_cost, partition
 
     parts = partition([box_cost(b.ng, b.np_side or b.ng, b.nsteps) for b in boxes], world)

@@ -58,6 +58,15 @@ class Ranks:
         self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
         return float(t.item())
 
+    def gather(self, obj):
+        """Every rank's obj, in rank order, on every rank (host-side results:
+        latencies, per-rank summaries; no data-path use)."""
+        if self.dist is None:
+            return [obj]
+        out = [None] * self.world
+        self.dist.all_gather_object(out, obj)
+        return out
+
     def close(self):
         if self.dist is not None:
             self.dist.destroy_process_group()

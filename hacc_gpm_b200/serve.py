@@ -201,15 +201,16 @@ class Server:
 
 
 def serve(requests, hbm_budget: float = 40e9, device: int = 0, graph: bool = True, realtime: bool = True,
-          max_slots: int = 64, segment_steps: int = None):
+          max_slots: int = 64, segment_steps: int = None, **server_kw):
     """Run the request stream through a Server.  realtime: requests become
     visible at their arrival times (wall clock from the start); otherwise all
     are queued at t = 0 (saturated throughput).  segment_steps: pre-empt
-    every request after that many steps (see Server).  Returns (requests
-    with .latency and .result, makespan seconds, server stats)."""
+    every request after that many steps (see Server); server_kw: the other
+    Server settings (batch_ms, max_batch, step_ms).  Returns (requests with
+    .latency and .result, makespan seconds, server stats)."""
     prepare_tables(requests)
     sizes = sorted({r.ng for r in requests})
-    srv = Server(sizes, hbm_budget, device, graph, max_slots, segment_steps=segment_steps)
+    srv = Server(sizes, hbm_budget, device, graph, max_slots, segment_steps=segment_steps, **server_kw)
     try:
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         waiting = collections.deque()

@@ -61,7 +61,7 @@ def test_deposit_deterministic_and_matches_oracle(ng, np_side):
     assert r1.astype(np.float64).sum() == pytest.approx(ro.sum(), rel=1e-7)
 
 
-@pytest.mark.parametrize("ng,np_side,ncand", [(32, 32, 9), (64, 32, 5)])
+@pytest.mark.parametrize("ng,np_side,ncand", [(32, 32, 10), (64, 32, 6)])
 def test_deposit_hot_cell_exact(ng, np_side, ncand, monkeypatch):
     """All particles in one cell (late-time clustering extreme): the 32-bit
     windows wrap, every candidate detects it and sends the block to the
@@ -131,12 +131,12 @@ def test_fused_x_pass_variants_bit_identical(ng, monkeypatch):
                                              (64, 32, 1.0), (48, 48, 1.0), (64, 32, 5.0)])
 def test_deposit_configurations_bit_identical(ng, np_side, disp, monkeypatch):
     """Every deposit candidate (split, 32-bit and column windows, with and
-    without x-half splitting; their spill passes, reached with disp 2 to 6)
-    gives the same int64 grid; 16^3 blocks (np = ng = 32, 64) and 8^3 blocks
-    (np < ng, np = 48)."""
+    without x-half splitting, and the direct one without a window; the spill
+    passes, reached with disp 2 to 6) gives the same int64 grid; 16^3 blocks
+    (np = ng = 32, 48, 64) and 8^3 blocks (np < ng)."""
     x, v = lattice_state(np_side, ng, disp=disp, vel=1.0, seed=23)
     out = []
-    n = 9 if np_side % 16 == 0 and ng <= np_side else 5
+    n = 10 if np_side % 16 == 0 and ng <= np_side else 6
     for flag in range(n):
         monkeypatch.setenv("HGPM_DEPOSIT", str(flag))
         with make(ng, np_side) as s:
