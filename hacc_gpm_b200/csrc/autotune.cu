@@ -7,7 +7,9 @@
 // particles are:
 //   deposit  window kernel, threads per CTA, window cap, load ring depth
 //            (launch_deposit candidates),
-//   kick     flat / windowed gathers, CTA shape, units per CTA turn
+//   kick     flat / windowed gathers from the force grid, or gathers from
+//            the real potential (no force grid: the gradient kernel's time
+//            is charged to the others), CTA shape, units per CTA turn
 //            (launch_kick_drift candidates),
 //   y pass   TMA-fed persistent or plain strided transform,
 //   x pass   TMA-fed persistent or plain fused Poisson transform.
@@ -247,21 +249,29 @@ extern "C" int hgpm_autotune(hgpm_ctx* c, int reps, int store, int choices[HGPM_
     rc = hgpm_sync(c);
     if (rc) return rc;
     {
+        // the force grid and the potential from the solve above (the grid
+        // formed here whichever kick the context had); a candidate that
+        // gathers the force grid is charged the gradient kernel that makes it
+        const float* phi = reinterpret_cast<const float*>(c->fspec + (size_t)ng * ng * c->zs);
+        float4* f4 = reinterpret_cast<float4*>(c->force);
+        const double grad_ms = time_launches(c, reps, [&] { return launch_gradient(ng, phi, f4, c->stream); }, &e);
+        CK(e);
         const int n = kick_candidates(np, ng);
         std::vector<double> ms(n, -1.0);
-        const float4* f4 = reinterpret_cast<const float4*>(c->force);
         for (int i = 0; i < n; ++i) {
             ms[i] = time_launches(c, reps, [&] {
                 // zero kick and drift factors: v + 0 and x + 0 leave the state as it is
                 return launch_kick_drift(c->part, np, ng, f4, 0.0, 0.0, 0.f, 0.f, 2, i, c->blkwin, c->win_valid,
-                                         c->kick_spill, c->stream);
+                                         c->kick_spill, c->stream, Slots{}, KickSched{}, 1, phi);
             }, &e);
             CK(e);
+            if (!kick_uses_phi(i)) ms[i] += grad_ms;
         }
         pick[HGPM_TUNE_KICK] = hgpm_tune_pick(ms.data(), n, 0, tol);
         pms[HGPM_TUNE_KICK] = ms[pick[HGPM_TUNE_KICK]];
     }
     c->kick_choice = pick[HGPM_TUNE_KICK];
+    c->force_valid = true;  // the force grid timed above is the current one
     CK(cudaStreamSynchronize(c->stream));
     if (choices)
         for (int k = 0; k < HGPM_TUNE_KNOBS; ++k) choices[k] = pick[k];

@@ -44,6 +44,11 @@ struct hgpm_ctx {
     int* blkwin = nullptr;   // per-block CIC windows of the last deposit
     SpillList dep_spill, kick_spill;  // blocks too wide for the windows
     bool win_valid = false;  // blkwin describes the current positions
+    // the real potential of the last solve (in the second force spectrum's
+    // space) is current; the float4 force grid has been formed from it (a
+    // kick that gathers the potential leaves it to hgpm_get_force)
+    bool phi_valid = false;
+    bool force_valid = false;
     // kernel variants (environment, read at creation): HGPM_NO_TMA=1 selects the
     // plain strided y passes, HGPM_XTMA=0|1 the plain/TMA-fed fused x pass
     // (default 1, the TMA-fed one: 0.95 vs 0.99 ms at 512^3).  The deposit

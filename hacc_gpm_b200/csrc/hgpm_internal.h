@@ -94,6 +94,9 @@ int window_records(int np_side, int ng);  // ints per box
 // call of candidate `choice` launches (the windowed one two: windowed + spill).
 int kick_candidates(int np_side, int ng);
 int kick_kernels(int choice, int np_side, int ng);
+// Candidates that gather the real potential instead of the float4 force
+// grid (the step then skips gradient_kernel).
+bool kick_uses_phi(int choice);
 // Deposit configurations (bit-identical int64 grids): how many, and the
 // default (used when the choice is -1).
 int deposit_candidates(int np_side, int ng);
@@ -104,12 +107,13 @@ int deposit_default(int np_side, int ng);
 cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass, unsigned long long* rho,
                            int* blkwin, const SpillList& spill, cudaStream_t s, const Slots& sl = Slots{},
                            int nslots = 1, int choice = -1);
-// f: the float4 (F_x, F_y, F_z, 0) force grid.  choice: kick candidate
-// (0 = default).
+// f: the float4 (F_x, F_y, F_z, 0) force grid; phi (may be null): the real
+// potential, for the candidates that gather it (with phi null they fall
+// back to candidate 0).  choice: kick candidate (0 = default).
 cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float4* f, double deltaT,
                               double fscal, float pf_a, float pf_b, int ndrift, int choice, int* blkwin,
                               bool have_rec, const SpillList& spill, cudaStream_t s, const Slots& sl = Slots{},
-                              const KickSched& ks = KickSched{}, int nslots = 1);
+                              const KickSched& ks = KickSched{}, int nslots = 1, const float* phi = nullptr);
 // Batched step bookkeeping: each active slot's step counter advances and a
 // slot that has run nsteps[slot] steps goes idle.
 cudaError_t launch_slots_advance(int* active, int* step, const int* nsteps, int nslots, cudaStream_t s);

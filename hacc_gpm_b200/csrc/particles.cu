@@ -1162,6 +1162,100 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_flat_nt_kernel(ParticleSoA
     }
 }
 
+// The CIC-weighted force of a particle gathered from the real potential phi
+// instead of the float4 force grid: each corner's force is formed from phi as
+// gradient_kernel forms it, F_d = 0.5f * (phi(c - e_d) - phi(c + e_d)), and
+// accumulated in gather_global's order, so the result is bit-identical to
+// gradient_kernel followed by gather_global.  The 8 corners need phi on the
+// 32 points of the 4^3 cube around the cell without its edges and corners:
+// the four inner z columns (z-1 .. z+2) and the x and y faces.  4 bytes per
+// point from a 4-byte grid instead of 16 bytes per corner from a 16-byte
+// grid, and no force grid to write.
+__device__ __forceinline__ float3 gather_phi(const float* __restrict__ phi, const PState& c, const KickWeights& w,
+                                             int ng) {
+    const int ix = cell_x(c.c), iy = cell_y(c.c), iz = cell_z(c.c);
+    const int xm = ix == 0 ? ng - 1 : ix - 1, x1 = ix + 1 == ng ? 0 : ix + 1, x2 = x1 + 1 == ng ? 0 : x1 + 1;
+    const int ym = iy == 0 ? ng - 1 : iy - 1, y1 = iy + 1 == ng ? 0 : iy + 1, y2 = y1 + 1 == ng ? 0 : y1 + 1;
+    const int zm = iz == 0 ? ng - 1 : iz - 1, z1 = iz + 1 == ng ? 0 : iz + 1, z2 = z1 + 1 == ng ? 0 : z1 + 1;
+    const size_t sx[4] = {(size_t)xm * ng * ng, (size_t)ix * ng * ng, (size_t)x1 * ng * ng, (size_t)x2 * ng * ng};
+    const size_t sy[4] = {(size_t)ym * ng, (size_t)iy * ng, (size_t)y1 * ng, (size_t)y2 * ng};
+    const int sz[4] = {zm, iz, z1, z2};
+    // P[a][b][t]: phi(x_a, y_b, z_{t-1}) on the inner columns; X[e][b][cc],
+    // Y[a][e][cc]: the x and y faces (e = 0: x-1 / y-1, e = 1: x+2 / y+2)
+    float P[2][2][4], X[2][2][2], Y[2][2][2];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int t = 0; t < 4; ++t) P[a][b][t] = __ldg(&phi[sx[1 + a] + sy[1 + b] + sz[t]]);
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                X[e][b][cc] = __ldg(&phi[sx[3 * e] + sy[1 + b] + sz[1 + cc]]);
+                Y[b][e][cc] = __ldg(&phi[sx[1 + b] + sy[3 * e] + sz[1 + cc]]);
+            }
+    float3 dv = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const float wab = __fmul_rn(w.wx[a], w.wy[b]);
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const float lo_x = a == 0 ? X[0][b][cc] : P[0][b][1 + cc];
+                const float hi_x = a == 0 ? P[1][b][1 + cc] : X[1][b][cc];
+                const float lo_y = b == 0 ? Y[a][0][cc] : P[a][0][1 + cc];
+                const float hi_y = b == 0 ? P[a][1][1 + cc] : Y[a][1][cc];
+                const float fx = 0.5f * (lo_x - hi_x);
+                const float fy = 0.5f * (lo_y - hi_y);
+                const float fz = 0.5f * (P[a][b][cc] - P[a][b][cc + 2]);
+                const float mul = __fmul_rn(wab, w.wz[cc]);
+                dv.x = fmaf(mul, fx, dv.x);
+                dv.y = fmaf(mul, fy, dv.y);
+                dv.z = fmaf(mul, fz, dv.z);
+            }
+        }
+    return dv;
+}
+
+// kick_flat_nt_kernel gathering from the real potential (gather_phi).
+template <int B, int NT, int R = 1>
+__global__ void __launch_bounds__(NT, 1024 / NT) kick_phi_kernel(ParticleSoA p, int ng, const float* __restrict__ phi,
+                                                               double deltaT, double fscal, float pf_a, float pf_b,
+                                                               int ndrift, int nblocks, Slots sl, KickSched ks) {
+    constexpr int B3 = B * B * B, SUB = B3 / NT;
+    const int slot = blockIdx.y;
+    if (slot_idle(sl, slot)) return;
+    const int n = nblocks * SUB;
+    if ((int)blockIdx.x * R >= n) return;
+    p = offset_soa(p, (size_t)slot * sl.s0);
+    phi += (size_t)slot * sl.s1;
+    float dtf;
+    kick_scalars(ks, slot, deltaT, fscal, dtf, pf_a, pf_b, ndrift);
+    auto index = [&](int u) { return (size_t)(u / SUB) * B3 + (u % SUB) * NT + threadIdx.x; };
+    auto unit = [&](int k) { return ((int)blockIdx.x + (k / R) * (int)gridDim.x) * R + k % R; };
+    int k = 0;
+    size_t inext = index(unit(0));
+    PState next = load_p(p, inext);
+    for (;;) {
+        const size_t i = inext;
+        const PState cur = next;
+        const int un = unit(k + 1);
+        const bool more = un < n;
+        if (more) {
+            inext = index(un);
+            next = load_p(p, inext);
+        }
+        finish_p(p, i, cur, gather_phi(phi, cur, KickWeights(cur, dtf), ng), pf_a, pf_b, ndrift, ng);
+        if (!more) break;
+        ++k;
+    }
+}
+
 __global__ void density_kernel(const unsigned long long* __restrict__ rho64, float* __restrict__ rho, size_t n) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -1544,14 +1638,19 @@ cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass
 // kernel for the queued blocks).  8^3 blocks: 0 flat 256-thread items, 1-2
 // flat 512-thread CTAs (a whole block per unit) in runs of 1 / 2, 3 flat
 // 256-thread CTAs in runs of 4, 4 windowed.
-constexpr int kKickCands = 5;
+constexpr int kKickCands = 7;
 constexpr int kKickWindowed = 4;
+// candidates 5 and 6 gather from the real potential (kick_phi_kernel): the
+// step then needs no force grid (kick_uses_phi)
+constexpr int kKickPhiFirst = 5;
 
 int kick_candidates(int np_side, int ng) {
     (void)np_side;
     (void)ng;
     return kKickCands;
 }
+
+bool kick_uses_phi(int choice) { return choice >= kKickPhiFirst && choice < kKickCands; }
 
 int kick_kernels(int choice, int np_side, int ng) {
     (void)np_side;
@@ -1570,11 +1669,31 @@ static cudaError_t kick_flat_launch(const ParticleSoA& p, int np_side, int ng, c
     return cudaGetLastError();
 }
 
+template <int B, int NT, int R>
+static cudaError_t kick_phi_launch(const ParticleSoA& p, int np_side, int ng, const float* phi, double deltaT,
+                                   double fscal, float pf_a, float pf_b, int ndrift, const Slots& sl,
+                                   const KickSched& ks, int nslots, cudaStream_t s) {
+    const int nblocks = (np_side / B) * (np_side / B) * (np_side / B);
+    auto kf = kick_phi_kernel<B, NT, R>;
+    const int grid = num_sms() * blocks_per_sm_once((const void*)kf, NT, 0);
+    kf<<<dim3(grid, nslots), NT, 0, s>>>(p, ng, phi, deltaT, fscal, pf_a, pf_b, ndrift, nblocks, sl, ks);
+    return cudaGetLastError();
+}
+
 template <int B>
-static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const float4* f, double deltaT, double fscal,
-                             float pf_a, float pf_b, int ndrift, int choice, int* blkwin, bool have_rec,
-                             const SpillList& spill, const Slots& sl, const KickSched& ks, int nslots,
+static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const float4* f, const float* phi,
+                             double deltaT, double fscal, float pf_a, float pf_b, int ndrift, int choice, int* blkwin,
+                             bool have_rec, const SpillList& spill, const Slots& sl, const KickSched& ks, int nslots,
                              cudaStream_t s) {
+    if (kick_uses_phi(choice)) {
+        if constexpr (B == 16) {
+            if (choice == 5) return kick_phi_launch<B, 1024, 4>(p, np_side, ng, phi, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
+            return kick_phi_launch<B, 1024, 2>(p, np_side, ng, phi, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
+        } else {
+            if (choice == 5) return kick_phi_launch<B, 512, 1>(p, np_side, ng, phi, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
+            return kick_phi_launch<B, 512, 2>(p, np_side, ng, phi, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
+        }
+    }
     constexpr int NT = 512;
     auto ksp = kick_spill_kernel<B>;
     // persistent grid of exactly the resident CTAs (no second round)
@@ -1617,14 +1736,15 @@ static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const fl
 cudaError_t launch_kick_drift(const ParticleSoA& p, int np_side, int ng, const float4* f, double deltaT,
                               double fscal, float pf_a, float pf_b, int ndrift, int choice, int* blkwin,
                               bool have_rec, const SpillList& spill, cudaStream_t s, const Slots& sl,
-                              const KickSched& ks, int nslots) {
+                              const KickSched& ks, int nslots, const float* phi) {
     if (!spill.cnt || !spill.items || !spill.next || !blkwin) return cudaErrorInvalidValue;
     if (choice < 0 || choice >= kKickCands) choice = 0;
+    if (kick_uses_phi(choice) && !phi) choice = 0;
     if (block_side(np_side, ng) == 16)
-        return kick_impl<16>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, choice, blkwin, have_rec, spill,
-                             sl, ks, nslots, s);
-    return kick_impl<8>(p, np_side, ng, f, deltaT, fscal, pf_a, pf_b, ndrift, choice, blkwin, have_rec, spill, sl,
-                        ks, nslots, s);
+        return kick_impl<16>(p, np_side, ng, f, phi, deltaT, fscal, pf_a, pf_b, ndrift, choice, blkwin, have_rec,
+                             spill, sl, ks, nslots, s);
+    return kick_impl<8>(p, np_side, ng, f, phi, deltaT, fscal, pf_a, pf_b, ndrift, choice, blkwin, have_rec, spill,
+                        sl, ks, nslots, s);
 }
 __global__ void slots_advance_kernel(int* __restrict__ active, int* __restrict__ step,
                                      const int* __restrict__ nsteps, int nslots) {

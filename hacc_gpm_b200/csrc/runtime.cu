@@ -773,18 +773,34 @@ extern "C" int hgpm_solve_gradient(hgpm_ctx* c) {
     }
     {
         // the real potential (in the space of the second force spectrum), then
-        // the force grid by central differences
+        // the force grid by central differences, unless the kick gathers the
+        // potential itself (hgpm_get_force then forms the grid on demand)
         PhaseScope ps(c, PH_ZINV);
         float* phi = reinterpret_cast<float*>(c->fspec + cs);
         CK(launch_zinv(ng, c->fspec, phi, ng * ng, c->zs, 0, 0, 1, 1.0f, c->tw_ng, c->stream));
-        CK(launch_gradient(ng, phi, reinterpret_cast<float4*>(c->force), c->stream));
-        count(c, PH_ZINV, 2);
+        c->phi_valid = true;
+        c->force_valid = false;
+        if (!kick_uses_phi(c->kick_choice)) {
+            CK(launch_gradient(ng, phi, reinterpret_cast<float4*>(c->force), c->stream));
+            c->force_valid = true;
+        }
+        count(c, PH_ZINV, c->force_valid ? 2 : 1);
     }
     return HGPM_OK;
 }
 
+// The real potential of the last solve, or null.
+static const float* ctx_phi(const hgpm_ctx* c) {
+    return c->phi_valid ? reinterpret_cast<const float*>(c->fspec + (size_t)c->ng * c->ng * c->zs) : nullptr;
+}
+
 extern "C" int hgpm_get_force(hgpm_ctx* c, float* f) {
     if (!c || !f) return HGPM_ERR_ARG;
+    if (!c->force_valid && c->phi_valid) {
+        CK(launch_gradient(c->ng, ctx_phi(c), reinterpret_cast<float4*>(c->force), c->stream));
+        count(c, PH_ZINV, 1);
+        c->force_valid = true;
+    }
     // the device grid is float4 (F_x, F_y, F_z, 0) per cell; the ABI returns
     // three planes
     std::vector<float4> g(c->ncell);
@@ -803,7 +819,8 @@ extern "C" int hgpm_kick_drift(hgpm_ctx* c, double deltaT, double fscal, float p
     if (!c->have_state) return fail(c, HGPM_ERR_STATE, "no particle state loaded");
     PhaseScope ps(c, PH_KICK);
     CK(launch_kick_drift(c->part, c->np, c->ng, reinterpret_cast<const float4*>(c->force), deltaT, fscal, pf_a, pf_b,
-                         ndrift, c->kick_choice, c->blkwin, c->win_valid, c->kick_spill, c->stream));
+                         ndrift, c->kick_choice, c->blkwin, c->win_valid, c->kick_spill, c->stream, Slots{},
+                         KickSched{}, 1, ctx_phi(c)));
     if (ndrift > 0) c->win_valid = false;
     count(c, PH_KICK, kick_kernels(c->kick_choice, c->np, c->ng));
     return HGPM_OK;
@@ -1022,6 +1039,8 @@ static int ic_common(hgpm_ctx* c, const float* noise_host, const double* table, 
     int rc = HGPM_OK;
     do {
         float* noise = c->force;  // scratch: the force grids are rebuilt every solve
+        c->phi_valid = false;     // the IC spectra and displacements overwrite both
+        c->force_valid = false;
         cudaError_t e;
         if (noise_host) {
             e = cudaMemcpyAsync(noise, noise_host, npart * 4, cudaMemcpyHostToDevice, c->stream);
@@ -1074,6 +1093,7 @@ extern "C" int hgpm_ic_from_noise(hgpm_ctx* c, const float* noise, const double*
 
 extern "C" int hgpm_ic_noise(hgpm_ctx* c, float* out) {
     if (!c || !out) return HGPM_ERR_ARG;
+    c->force_valid = false;  // the noise is drawn into the force grid's space
     CK(launch_noise(c->force, c->npart, c->p.seed, c->p.noise, c->stream));
     count(c, PH_PK, 1);
     CK(cudaMemcpyAsync(out, c->force, c->npart * 4, cudaMemcpyDeviceToHost, c->stream));

@@ -152,12 +152,13 @@ def test_deposit_configurations_bit_identical(ng, np_side, disp, monkeypatch):
                                              (64, 64, 4.0)])
 def test_kick_variants_bit_identical(ng, np_side, disp, monkeypatch):
     """Every kick candidate (flat global gathers with different CTA shapes
-    and unit runs, the float4-window kick) runs the same FP32 arithmetic in
-    the same order; disp 4 spreads blocks past the window caps (global-gather
-    fallback)."""
+    and unit runs, the float4-window kick, the gathers of the real potential
+    that form each corner's force as the gradient kernel does) runs the same
+    FP32 arithmetic in the same order; disp 4 spreads blocks past the window
+    caps (global-gather fallback)."""
     x, v = lattice_state(np_side, ng, disp=disp, vel=1.0, seed=17)
     out = []
-    for flag in ("0", "1", "2", "3", "4"):
+    for flag in ("0", "1", "2", "3", "4", "5", "6"):
         monkeypatch.setenv("HGPM_KICK", flag)
         with make(ng, np_side) as s:
             s.load_state(x, v)
@@ -292,3 +293,21 @@ def test_bounded_wait_time_out_reported_and_context_usable():
         s.solve_gradient()
         f2 = s.get_force()
     assert np.array_equal(f1, f2)
+
+
+@pytest.mark.parametrize("ng,np_side", [(32, 32), (64, 32)])
+def test_force_grid_on_demand_with_potential_kick(ng, np_side, monkeypatch):
+    """With a kick that gathers the potential the solve writes no force grid;
+    hgpm_get_force forms it from the potential, equal bit for bit to the
+    grid the default solve writes."""
+    x, v = lattice_state(np_side, ng, disp=1.5, vel=1.0, seed=37)
+    out = []
+    for flag in ("0", "5"):
+        monkeypatch.setenv("HGPM_KICK", flag)
+        with make(ng, np_side) as s:
+            assert s.tuned_choices()["kick"] == int(flag)
+            s.load_state(x, v)
+            s.cic()
+            s.solve_gradient()
+            out.append(s.get_force())
+    assert np.array_equal(out[0], out[1])
