@@ -151,6 +151,7 @@ def lib() -> C.CDLL:
         "hgpm_ens_release": (C.c_int, [vp, C.c_int, C.c_int]),
         "hgpm_ens_step": (C.c_int, [vp, C.c_int]),
         "hgpm_ens_use_graph": (C.c_int, [vp, C.c_int]),
+        "hgpm_ens_multi_launch": (C.c_int, [vp, C.c_int]),
         "hgpm_ens_sync": (C.c_int, [vp]),
         "hgpm_ens_status": (C.c_int, [vp, C.c_int, C.c_int, P(C.c_int), P(C.c_int)]),
         "hgpm_ens_kernel_launches": (C.c_int64, [vp, C.c_int]),

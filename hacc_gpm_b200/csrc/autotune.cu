@@ -144,7 +144,7 @@ int ctx_apply_tuned(hgpm_ctx* c) {
     if (!getenv("HGPM_KICK") && ch[HGPM_TUNE_KICK] >= 0 && ch[HGPM_TUNE_KICK] < kick_candidates(c->np, c->ng))
         c->kick_choice = ch[HGPM_TUNE_KICK];
     if (!getenv("HGPM_NO_TMA")) c->tma = ch[HGPM_TUNE_YPASS] != 0;
-    if (!getenv("HGPM_XTMA")) c->xtma = ch[HGPM_TUNE_XPASS] != 0;
+    if (!getenv("HGPM_XTMA") && ch[HGPM_TUNE_XPASS] >= 0 && ch[HGPM_TUNE_XPASS] <= 1) c->xmode = ch[HGPM_TUNE_XPASS];
     return 1;
 }
 
@@ -221,7 +221,7 @@ extern "C" int hgpm_autotune(hgpm_ctx* c, int reps, int store, int choices[HGPM_
         pick[HGPM_TUNE_YPASS] = hgpm_tune_pick(ms, 2, 1, tol);
         pms[HGPM_TUNE_YPASS] = ms[pick[HGPM_TUNE_YPASS]];
     }
-    // x pass with the Green's function: 1 = TMA-fed, 0 = plain
+    // x pass with the Green's function: 0 = plain, 1 = TMA-fed
     {
         double ms[2];
         const double coeff = 0.5 / ((double)ng * ng * ng);
@@ -239,7 +239,7 @@ extern "C" int hgpm_autotune(hgpm_ctx* c, int reps, int store, int choices[HGPM_
     }
     c->dep_choice = pick[HGPM_TUNE_DEPOSIT];
     c->tma = pick[HGPM_TUNE_YPASS] != 0;
-    c->xtma = pick[HGPM_TUNE_XPASS] != 0;
+    c->xmode = pick[HGPM_TUNE_XPASS];
     // a real force grid from the current positions for the kick candidates
     c->rho_dirty = true;
     int rc = hgpm_deposit(c);
@@ -249,29 +249,53 @@ extern "C" int hgpm_autotune(hgpm_ctx* c, int reps, int store, int choices[HGPM_
     rc = hgpm_sync(c);
     if (rc) return rc;
     {
-        // the force grid and the potential from the solve above (the grid
-        // formed here whichever kick the context had); a candidate that
-        // gathers the force grid is charged the gradient kernel that makes it
-        const float* phi = reinterpret_cast<const float*>(c->fspec + (size_t)ng * ng * c->zs);
+        // the potential from the spectrum of the solve above, then the force
+        // grid (both formed here whichever kick the context had); a candidate
+        // that gathers the force grid is charged the gradient kernel that
+        // makes it
+        float* phi = reinterpret_cast<float*>(c->fspec + (size_t)ng * ng * c->zs);
         float4* f4 = reinterpret_cast<float4*>(c->force);
+        const double z1 = time_launches(c, reps, [&] {
+            return launch_zinv(ng, c->fspec, phi, ng * ng, c->zs, 0, 0, 1, 1.0f, c->tw_ng, c->stream);
+        }, &e);
+        CK(e);
         const double grad_ms = time_launches(c, reps, [&] { return launch_gradient(ng, phi, f4, c->stream); }, &e);
         CK(e);
         const int n = kick_candidates(np, ng);
         std::vector<double> ms(n, -1.0);
-        for (int i = 0; i < n; ++i) {
-            ms[i] = time_launches(c, reps, [&] {
+        auto time_kick = [&](int i, const float* pot) {
+            const double t = time_launches(c, reps, [&] {
                 // zero kick and drift factors: v + 0 and x + 0 leave the state as it is
                 return launch_kick_drift(c->part, np, ng, f4, 0.0, 0.0, 0.f, 0.f, 2, i, c->blkwin, c->win_valid,
-                                         c->kick_spill, c->stream, Slots{}, KickSched{}, 1, phi);
+                                         c->kick_spill, c->stream, Slots{}, KickSched{}, 1, pot);
             }, &e);
+            return t;
+        };
+        for (int i = 0; i < n; ++i) {
+            if (kick_uses_phi2(i)) continue;
+            ms[i] = time_kick(i, phi);
             CK(e);
             if (!kick_uses_phi(i)) ms[i] += grad_ms;
+        }
+        // the paired potential (in the force grid's space, so after the
+        // candidates that gather the grid), charged the extra bytes its z
+        // pass writes over the plain one
+        const double z2 = time_launches(c, reps, [&] { return launch_zinv_pair(ng, c->fspec, c->force, c->zs, c->tw_ng, c->stream); }, &e);
+        CK(e);
+        for (int i = 0; i < n; ++i) {
+            if (!kick_uses_phi2(i)) continue;
+            ms[i] = time_kick(i, c->force) + (z2 - z1);
+            CK(e);
         }
         pick[HGPM_TUNE_KICK] = hgpm_tune_pick(ms.data(), n, 0, tol);
         pms[HGPM_TUNE_KICK] = ms[pick[HGPM_TUNE_KICK]];
     }
     c->kick_choice = pick[HGPM_TUNE_KICK];
-    c->force_valid = true;  // the force grid timed above is the current one
+    // the potential is the current one; the force grid's space now holds the
+    // paired potential
+    c->phi_valid = true;
+    c->force_valid = false;
+    c->phi2_valid = true;
     CK(cudaStreamSynchronize(c->stream));
     if (choices)
         for (int k = 0; k < HGPM_TUNE_KNOBS; ++k) choices[k] = pick[k];
@@ -290,6 +314,6 @@ extern "C" int hgpm_tuned_choices(const hgpm_ctx* c, int choices[HGPM_TUNE_KNOBS
     choices[HGPM_TUNE_DEPOSIT] = c->dep_choice >= 0 ? c->dep_choice : deposit_default(c->np, c->ng);
     choices[HGPM_TUNE_KICK] = c->kick_choice;
     choices[HGPM_TUNE_YPASS] = c->tma ? 1 : 0;
-    choices[HGPM_TUNE_XPASS] = c->xtma ? 1 : 0;
+    choices[HGPM_TUNE_XPASS] = c->xmode;
     return HGPM_OK;
 }

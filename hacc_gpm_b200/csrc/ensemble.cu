@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "hgpm_ctx.h"
+#include "multi_class.h"
 
 namespace {
 
@@ -78,6 +79,9 @@ struct hgpm_ensemble {
     cudaGraphExec_t exec = nullptr;
     int kick_choice = 0;   // kick and deposit candidates (HGPM_KICK / HGPM_DEPOSIT)
     int dep_choice = -1;
+    // hgpm_ens_step as one launch per phase across all classes (multi_class.h)
+    // when every class is supported; else one launch per phase per class
+    bool multi = true;
     int64_t launches = 0;
     std::string err;
 };
@@ -354,7 +358,7 @@ extern "C" int hgpm_ens_slot(hgpm_ensemble* E, int ci, int slot, const hgpm_para
         c->pk_cnt = k.pk_cnt;
         c->pk_nparts = 4 * 148;
         c->tma = false;  // batched passes are the plain ones; views match them
-        c->xtma = false;
+        c->xmode = 0;
         c->kick_choice = E->kick_choice;
         c->dep_choice = E->dep_choice;
         k.views[slot] = c;
@@ -468,9 +472,66 @@ static int class_step(hgpm_ensemble* E, EnsClass& k, cudaStream_t s) {
     return HGPM_OK;
 }
 
+static bool multi_ok(const hgpm_ensemble* E) {
+    if (!E->multi || E->cls.empty() || E->cls.size() > (size_t)kMaxMC) return false;
+    for (const auto& k : E->cls)
+        if (!mc_class_supported(k.ng, k.np)) return false;
+    return true;
+}
+
+// The classes as a multi-class table (multi_class.h).
+static MCTable multi_table(hgpm_ensemble* E) {
+    MCTable t;
+    t.n = (int)E->cls.size();
+    for (int i = 0; i < t.n; ++i) {
+        EnsClass& k = E->cls[i];
+        MCClass& c = t.c[i];
+        const int S = k.nslots;
+        c.ng = k.ng;
+        c.np = k.np;
+        c.nslots = S;
+        c.nblocks = (k.np / 16) * (k.np / 16) * (k.np / 16);
+        c.zs = k.zs;
+        c.mass = ctx_cic_mass(k.ng, k.np);
+        c.mean = (double)c.mass * (double)k.npart / (double)k.ncell;
+        c.active = k.d_active;
+        c.step = k.d_step;
+        c.nsteps = k.d_nsteps;
+        char* b = (char*)k.part_block;
+        const size_t a = k.part_stride * 4 * (size_t)S;
+        c.p.cell = (uint32_t*)b;
+        c.p.ox = (float*)(b + a);
+        c.p.oy = (float*)(b + 2 * a);
+        c.p.oz = (float*)(b + 3 * a);
+        c.p.vx = (float*)(b + 4 * a);
+        c.p.vy = (float*)(b + 5 * a);
+        c.p.vz = (float*)(b + 6 * a);
+        c.part_stride = k.part_stride;
+        c.rho64 = k.rho64;
+        c.ncell = k.ncell;
+        c.spec = k.spec;
+        c.fspec = k.fspec;
+        c.spec_elems = k.spec_elems;
+        c.blkwin = k.blkwin;
+        c.win_stride = k.win_stride;
+        c.spill = k.dep_spill;
+        c.tw = k.tw_ng;
+        c.cosq = k.cosq;
+        c.sched = k.d_sched;
+        c.pitch = HGPM_MAX_STEPS;
+    }
+    return t;
+}
+
 // Fork the class streams off the ensemble stream, run every class that has a
-// started slot, join back.
+// started slot, join back (or, multi-class, every phase once on the ensemble
+// stream).
 static int enqueue_step(hgpm_ensemble* E, bool all_classes) {
+    if (multi_ok(E)) {
+        ECK(mc_step(multi_table(E), E->stream));
+        E->launches += kMCStepLaunches;
+        return HGPM_OK;
+    }
     ECK(cudaEventRecord(E->fork, E->stream));
     for (auto& k : E->cls) {
         bool any = all_classes;
@@ -483,6 +544,16 @@ static int enqueue_step(hgpm_ensemble* E, bool all_classes) {
         ECK(cudaStreamWaitEvent(E->stream, k.join, 0));
     }
     return HGPM_OK;
+}
+
+extern "C" int hgpm_ens_multi_launch(hgpm_ensemble* E, int on) {
+    if (!E) return HGPM_ERR_ARG;
+    E->multi = on != 0;
+    if (E->exec) {  // the captured step was made for the other form
+        cudaGraphExecDestroy(E->exec);
+        E->exec = nullptr;
+    }
+    return multi_ok(E) ? 1 : 0;
 }
 
 extern "C" int hgpm_ens_use_graph(hgpm_ensemble* E, int on) {
@@ -521,7 +592,9 @@ extern "C" int hgpm_ens_step(hgpm_ensemble* E, int nsteps) {
             ECK(ie);
         }
         int per = 0;
-        for (auto& k : E->cls) per += kStepKernels + kick_kernels(E->kick_choice, k.np, k.ng);
+        if (multi_ok(E)) per = kMCStepLaunches;
+        else
+            for (auto& k : E->cls) per += kStepKernels + kick_kernels(E->kick_choice, k.np, k.ng);
         for (int i = 0; i < nsteps; ++i) {
             ECK(cudaGraphLaunch(E->exec, E->stream));
             E->launches += per;

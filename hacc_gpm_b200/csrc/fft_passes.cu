@@ -18,6 +18,7 @@
 #include "hgpm_device.cuh"
 #include "hgpm_internal.h"
 #include "kspace_ops.cuh"
+#include "multi_class.h"
 
 namespace hgpm {
 
@@ -143,18 +144,15 @@ __device__ __forceinline__ void store_tile_comp(const float2* __restrict__ tile,
 // (value * 2^32); it is converted to float delta = rho - mean in FP64 and the
 // accumulator is zeroed for the next deposit.  Otherwise input is float.
 // ---------------------------------------------------------------------------
+// The CTA's work (line group bx of one box) as a device function: the
+// single-class kernel below and the multi-class pass (mc_zfwd_kernel) run
+// the same code.
 template <int NG, bool FIX>
-__global__ void __launch_bounds__(kThreads, 4) zpass_r2c_kernel(void* __restrict__ in_, float2* __restrict__ out,
-                                                             int nlines, int zs, double mean,
-                                                             const float2* __restrict__ tw, Slots sl) {
+__device__ __forceinline__ void zpass_r2c_body(void* __restrict__ in_, float2* __restrict__ out, int nlines, int zs,
+                                               double mean, const float2* __restrict__ tw, int bx) {
     constexpr int M = NG / 2, L = Cfg<NG>::L, ES = L + 1;
     float2* buf = reinterpret_cast<float2*>(hgpm_smem);
-    if (slot_idle(sl, blockIdx.y)) return;
-    // slot stride s0 counts input elements (int64 when FIX, float otherwise)
-    in_ = FIX ? (void*)(reinterpret_cast<unsigned long long*>(in_) + (size_t)blockIdx.y * sl.s0)
-              : (void*)(reinterpret_cast<float*>(in_) + (size_t)blockIdx.y * sl.s0);
-    out += (size_t)blockIdx.y * sl.s1;
-    const int line0 = blockIdx.x * L;
+    const int line0 = bx * L;
     constexpr int TOT = L * M;
     constexpr int PER = (TOT + kThreads - 1) / kThreads;
     if (FIX) {
@@ -220,24 +218,32 @@ __global__ void __launch_bounds__(kThreads, 4) zpass_r2c_kernel(void* __restrict
     }
 }
 
+template <int NG, bool FIX>
+__global__ void __launch_bounds__(kThreads, 4) zpass_r2c_kernel(void* __restrict__ in_, float2* __restrict__ out,
+                                                             int nlines, int zs, double mean,
+                                                             const float2* __restrict__ tw, Slots sl) {
+    if (slot_idle(sl, blockIdx.y)) return;
+    // slot stride s0 counts input elements (int64 when FIX, float otherwise)
+    in_ = FIX ? (void*)(reinterpret_cast<unsigned long long*>(in_) + (size_t)blockIdx.y * sl.s0)
+              : (void*)(reinterpret_cast<float*>(in_) + (size_t)blockIdx.y * sl.s0);
+    out += (size_t)blockIdx.y * sl.s1;
+    zpass_r2c_body<NG, FIX>(in_, out, nlines, zs, mean, tw, blockIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 // z pass, inverse C2R, ncomp components, unnormalised * scale;
 // blockIdx.y = slot * ncomp + component.
 // X[0] and X[ng/2] are taken as real (Hermitian extension), which makes the
 // result equal to the real part of the reference's full C2C inverse.
 // ---------------------------------------------------------------------------
-template <int NG>
-__global__ void __launch_bounds__(kThreads) zpass_c2r_kernel(const float2* __restrict__ in, float* __restrict__ out,
-                                                             int nlines, int zs, size_t in_cs, size_t out_cs,
-                                                             float scale, const float2* __restrict__ tw, int ncomp,
-                                                             Slots sl) {
+// PAIR: out holds nlines * NG pairs, cell z of a line (phi(z), phi(z+1 mod
+// NG)) (the paired potential the pair-gathering kick reads).
+template <int NG, bool PAIR = false>
+__device__ __forceinline__ void zpass_c2r_body(const float2* __restrict__ in, float* __restrict__ out, int nlines,
+                                               int zs, float scale, const float2* __restrict__ tw, int bx) {
     constexpr int M = NG / 2, L = Cfg<NG>::L, ES = L + 1;
     float2* buf = reinterpret_cast<float2*>(hgpm_smem);
-    const int slot = blockIdx.y / ncomp, comp = blockIdx.y % ncomp;
-    if (slot_idle(sl, slot)) return;
-    in += (size_t)slot * sl.s0 + (size_t)comp * in_cs;
-    out += (size_t)slot * sl.s1 + (size_t)comp * out_cs;
-    const int line0 = blockIdx.x * L;
+    const int line0 = bx * L;
     constexpr int H = M / 2 + 1;
     constexpr int TOT = L * H;
     constexpr int PER = (TOT + kThreads - 1) / kThreads;
@@ -286,29 +292,63 @@ __global__ void __launch_bounds__(kThreads) zpass_c2r_kernel(const float2* __res
         const int line = line0 + l;
         if (line >= nlines) continue;
         const float2 z = buf[m * ES + l];
-        reinterpret_cast<float2*>(out + (size_t)line * NG)[m] = make_float2(z.x * scale, z.y * scale);
+        if (PAIR) {
+            // cells 2m and 2m+1: (phi(2m), phi(2m+1)), (phi(2m+1), phi(2m+2))
+            const float nx = buf[(m + 1 == M ? 0 : m + 1) * ES + l].x * scale;
+            reinterpret_cast<float4*>(out + (size_t)line * NG * 2)[m] =
+                make_float4(z.x * scale, z.y * scale, z.y * scale, nx);
+        } else {
+            reinterpret_cast<float2*>(out + (size_t)line * NG)[m] = make_float2(z.x * scale, z.y * scale);
+        }
     }
+}
+
+template <int NG>
+__global__ void __launch_bounds__(kThreads) zpass_c2r_pair_kernel(const float2* __restrict__ in,
+                                                                  float* __restrict__ out, int nlines, int zs,
+                                                                  const float2* __restrict__ tw) {
+    zpass_c2r_body<NG, true>(in, out, nlines, zs, 1.0f, tw, blockIdx.x);
+}
+
+template <int NG>
+__global__ void __launch_bounds__(kThreads) zpass_c2r_kernel(const float2* __restrict__ in, float* __restrict__ out,
+                                                             int nlines, int zs, size_t in_cs, size_t out_cs,
+                                                             float scale, const float2* __restrict__ tw, int ncomp,
+                                                             Slots sl) {
+    const int slot = blockIdx.y / ncomp, comp = blockIdx.y % ncomp;
+    if (slot_idle(sl, slot)) return;
+    in += (size_t)slot * sl.s0 + (size_t)comp * in_cs;
+    out += (size_t)slot * sl.s1 + (size_t)comp * out_cs;
+    zpass_c2r_body<NG>(in, out, nlines, zs, scale, tw, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
 // strided pass (y or x lines), in place,
 // blockIdx = (column chunk, plane, slot * ncomp + comp)
 // ---------------------------------------------------------------------------
-template <int NG, bool INV>
-__global__ void __launch_bounds__(Cfg<NG>::NTS, 2) strided_kernel(float2* __restrict__ data, int ncols, size_t rs,
-                                                               size_t ps, size_t cs, const float2* __restrict__ tw,
-                                                               int ncomp, Slots sl) {
-    constexpr int C = Cfg<NG>::CS, NT = Cfg<NG>::NTS;
+// Column chunk bx of plane by of one component of one box, NT threads.
+template <int NG, bool INV, int NT>
+__device__ __forceinline__ void strided_body(float2* __restrict__ data, int ncols, size_t rs, size_t ps,
+                                             const float2* __restrict__ tw, int bx, int by) {
+    constexpr int C = Cfg<NG>::CS;
     float2* tile = reinterpret_cast<float2*>(hgpm_smem);
-    const int slot = blockIdx.z / ncomp, comp = blockIdx.z % ncomp;
-    if (slot_idle(sl, slot)) return;
-    const int col0 = blockIdx.x * C;
-    float2* g = data + (size_t)slot * sl.s0 + (size_t)comp * cs + (size_t)blockIdx.y * ps + col0;
+    const int col0 = bx * C;
+    float2* g = data + (size_t)by * ps + col0;
     const int nvalid = ncols - col0;
     load_tile<NG, C, NT>(tile, g, rs, nvalid);
     __syncthreads();
     fft_tile<NG, C, C, INV, NT>(tile, tw);
     store_tile<NG, C, NT>(tile, g, rs, nvalid);
+}
+
+template <int NG, bool INV>
+__global__ void __launch_bounds__(Cfg<NG>::NTS, 2) strided_kernel(float2* __restrict__ data, int ncols, size_t rs,
+                                                               size_t ps, size_t cs, const float2* __restrict__ tw,
+                                                               int ncomp, Slots sl) {
+    const int slot = blockIdx.z / ncomp, comp = blockIdx.z % ncomp;
+    if (slot_idle(sl, slot)) return;
+    strided_body<NG, INV, Cfg<NG>::NTS>(data + (size_t)slot * sl.s0 + (size_t)comp * cs, ncols, rs, ps, tw,
+                                        blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -321,6 +361,34 @@ __global__ void __launch_bounds__(Cfg<NG>::NTS, 2) strided_kernel(float2* __rest
 // tile instead of three.
 // plane = ky index, rows = kx index, columns = kz index; blockIdx.z = slot.
 // ---------------------------------------------------------------------------
+// One-output x pass on a loaded tile: forward x FFT, pre() in registers,
+// inverse x FFT, the same stages and arithmetic as xpotential_tma_kernel (bit
+// for bit).
+template <int NG, int NT, class Op>
+__device__ __forceinline__ void xone_after_load(float2* __restrict__ tile, float2* __restrict__ out, size_t rs,
+                                                int nvalid, const float2* __restrict__ tw, const Op& op, int iy,
+                                                int col0) {
+    constexpr int C = Cfg<NG>::CX;
+    fft_tile_fwd_op_inv<NG, C, C, NT, 1, true>(tile, tw,
+                                              [&](int ix, int c, float2 v) { return op.pre(ix, iy, col0 + c, v); });
+    store_tile<NG, C, NT>(tile, out, rs, nvalid);
+}
+
+// The one-output x pass of column chunk bx of plane (ky) by of one box.
+template <int NG, int NT, class Op>
+__device__ __forceinline__ void xone_body(const float2* __restrict__ in, float2* __restrict__ out, int ncols,
+                                          size_t rs, size_t ps, const float2* __restrict__ tw, const Op& op, int bx,
+                                          int by) {
+    constexpr int C = Cfg<NG>::CX;
+    float2* tile = reinterpret_cast<float2*>(hgpm_smem);
+    const int col0 = bx * C;
+    const size_t off = (size_t)by * ps + col0;
+    const int nvalid = ncols - col0;
+    load_tile<NG, C, NT>(tile, in + off, rs, nvalid);
+    __syncthreads();
+    xone_after_load<NG, NT>(tile, out + off, rs, nvalid, tw, op, by, col0);
+}
+
 template <int NG, class Op>
 __global__ void __launch_bounds__(Cfg<NG>::NTX) xfused_kernel(const float2* __restrict__ in, float2* __restrict__ out,
                                                               int ncols, size_t rs, size_t ps, size_t out_cs,
@@ -338,11 +406,7 @@ __global__ void __launch_bounds__(Cfg<NG>::NTX) xfused_kernel(const float2* __re
     load_tile<NG, C, NT>(tile, in + off, rs, nvalid);
     __syncthreads();
     if constexpr (Op::kOut == 1) {
-        // one output: forward x FFT, pre() in registers, inverse x FFT, the
-        // same stages and arithmetic as xpotential_tma_kernel (bit for bit)
-        fft_tile_fwd_op_inv<NG, C, C, NT, 1, true>(
-            tile, tw, [&](int ix, int c, float2 v) { return op.pre(ix, iy, col0 + c, v); });
-        store_tile<NG, C, NT>(tile, out + off, rs, nvalid);
+        xone_after_load<NG, NT>(tile, out + off, rs, nvalid, tw, op, iy, col0);
         return;
     }
     // the three-output IC pass, whose registers are tight, reads every
@@ -597,6 +661,16 @@ static cudaError_t zinv_impl(const float2* in, float* out, int nlines, int zs, s
 }
 
 template <int NG>
+static cudaError_t zinv_pair_impl(const float2* in, float* out, int nlines, int zs, const float2* tw, cudaStream_t s) {
+    using G = Cfg<NG>;
+    auto k = zpass_c2r_pair_kernel<NG>;
+    cudaError_t e = ensure_smem(k, G::ZSMEM);
+    if (e != cudaSuccess) return e;
+    k<<<cdiv(nlines, G::L), kThreads, G::ZSMEM, s>>>(in, out, nlines, zs, tw);
+    return cudaGetLastError();
+}
+
+template <int NG>
 static cudaError_t strided_impl(bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
                                 int ncomp, const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
     using G = Cfg<NG>;
@@ -679,6 +753,16 @@ cudaError_t launch_zinv(int ng, const float2* in, float* out, int nlines, int zs
     return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_zinv_pair(int ng, const float2* in, float* out, int zs, const float2* tw, cudaStream_t s) {
+    switch (ng) {
+#define X(n) \
+    case n: return zinv_pair_impl<n>(in, out, n * n, zs, tw, s);
+        HGPM_SIZES(X)
+#undef X
+    }
+    return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
                            int ncomp, const float2* tw, cudaStream_t s, const Slots& sl, int nslots) {
     switch (ng) {
@@ -747,5 +831,155 @@ cudaError_t launch_xpk(int ng, const float2* in, int ncols, size_t rs, size_t ps
 }
 
 int pk_max_bins() { return 1024; }
+
+}  // namespace hgpm
+
+// ===========================================================================
+// Multi-class FFT passes (multi_class.h): one persistent launch per pass over
+// the work units of every class and slot; each CTA serves one class, whose
+// unit u is slot u / per and local unit u % per.  The body is the one the
+// single-class kernel runs (the z passes with 256 threads, the y and x passes
+// with 512, for every size: a butterfly's arithmetic does not depend on which
+// thread does it).
+// ===========================================================================
+namespace hgpm {
+
+namespace {
+
+// threads and minimum CTAs per SM of each pass: z passes 256 x 2 (the class
+// fields a CTA keeps in registers push the single-class kernels' 64 to 128
+// without spills), y and x passes 512 x 2 (as the single-class ones at 128^3
+// and above)
+template <int PASS> constexpr int mc_threads() { return PASS == 0 || PASS == 4 ? 256 : 512; }
+template <int PASS> constexpr int mc_minb() { return 2; }
+
+__device__ __forceinline__ float* mc_phi(const MCClass& c, int slot) {
+    return reinterpret_cast<float*>(c.fspec + c.spec_elems) + (size_t)slot * 6 * c.spec_elems;
+}
+
+// One unit of each pass for one grid side.
+template <int NG>
+__device__ __forceinline__ void mc_zfwd_unit(const MCClass& c, int slot, int lu) {
+    zpass_r2c_body<NG, true>(c.rho64 + (size_t)slot * c.ncell, c.spec + (size_t)slot * c.spec_elems, NG * NG, c.zs,
+                             c.mean, c.tw, lu);
+}
+template <int NG, bool INV>
+__device__ __forceinline__ void mc_ypass_unit(const MCClass& c, int slot, int lu) {
+    float2* data = INV ? c.fspec + (size_t)slot * 3 * c.spec_elems : c.spec + (size_t)slot * c.spec_elems;
+    constexpr int ncols = NG / 2 + 1, nch = (ncols + Cfg<NG>::CS - 1) / Cfg<NG>::CS;
+    strided_body<NG, INV, 512>(data, ncols, (size_t)c.zs, (size_t)NG * c.zs, c.tw, lu % nch, lu / nch);
+}
+template <int NG>
+__device__ __forceinline__ void mc_xpot_unit(const MCClass& c, int slot, int lu) {
+    constexpr int ncols = NG / 2 + 1, nch = (ncols + Cfg<NG>::CX - 1) / Cfg<NG>::CX;
+    const PotentialOp op{c.cosq, 0.5 / ((double)NG * NG * NG)};
+    xone_body<NG, 512>(c.spec + (size_t)slot * c.spec_elems, c.fspec + (size_t)slot * 3 * c.spec_elems, ncols,
+                       (size_t)NG * c.zs, (size_t)c.zs, c.tw, op, lu % nch, lu / nch);
+}
+template <int NG>
+__device__ __forceinline__ void mc_zinv_unit(const MCClass& c, int slot, int lu) {
+    zpass_c2r_body<NG>(c.fspec + (size_t)slot * 3 * c.spec_elems, mc_phi(c, slot), NG * NG, c.zs, 1.0f, c.tw, lu);
+}
+
+// PASS: 0 z forward, 1 y forward, 2 x with the Green's function, 3 y
+// inverse, 4 z inverse.  CTA b of nb serving class c takes units b, b + nb, ...
+template <int NG, int PASS>
+__device__ __forceinline__ void mc_fft_class(const MCClass& c, int per, int b, int nb) {
+    const int total = per * c.nslots;
+    for (int u = b; u < total; u += nb) {
+        const int slot = u / per, lu = u - slot * per;
+        if (c.active && !c.active[slot]) continue;  // the whole CTA skips
+        if (PASS == 0) mc_zfwd_unit<NG>(c, slot, lu);
+        else if (PASS == 1) mc_ypass_unit<NG, false>(c, slot, lu);
+        else if (PASS == 2) mc_xpot_unit<NG>(c, slot, lu);
+        else if (PASS == 3) mc_ypass_unit<NG, true>(c, slot, lu);
+        else mc_zinv_unit<NG>(c, slot, lu);
+        __syncthreads();  // shared memory is reused by the next unit
+    }
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(mc_threads<PASS>(), mc_minb<PASS>()) mc_fft_kernel(const __grid_constant__ MCTable t) {
+    int k = 0;
+    while (k + 1 < t.n && (int)blockIdx.x >= t.g0[k + 1]) ++k;
+    const MCClass& c = t.c[k];
+    const int b = blockIdx.x - t.g0[k], nb = t.g0[k + 1] - t.g0[k];
+    switch (c.ng) {
+#define X(n) \
+    case n: mc_fft_class<n, PASS>(c, t.per[k], b, nb); break;
+        HGPM_MC_SIZES(X)
+#undef X
+    }
+}
+
+// Per-size unit counts and shared memory of the passes (host).
+struct MCPassGeom {
+    int zunits, yunits, xunits;  // per slot
+    int zsmem, ysmem, xsmem;
+};
+MCPassGeom mc_geom(int ng) {
+    switch (ng) {
+#define X(n)                                                                                            \
+    case n: {                                                                                           \
+        const int ncols = n / 2 + 1;                                                                    \
+        return MCPassGeom{(n * n + Cfg<n>::L - 1) / Cfg<n>::L, (ncols + Cfg<n>::CS - 1) / Cfg<n>::CS * n, \
+                          (ncols + Cfg<n>::CX - 1) / Cfg<n>::CX * n, Cfg<n>::ZSMEM, Cfg<n>::SSMEM,        \
+                          n * Cfg<n>::CX * 8};                                                          \
+    }
+        HGPM_MC_SIZES(X)
+#undef X
+    }
+    return MCPassGeom{0, 0, 0, 0, 0, 0};
+}
+
+// Persistent launch of `kern` (`threads` per CTA, `smem` bytes): the resident
+// CTAs shared out by the classes' unit counts (at least one each).
+cudaError_t mc_launch(const void* kern, MCTable t, const int* units, int threads, int smem, cudaStream_t s) {
+    int total = 0;
+    for (int k = 0; k < t.n; ++k) total += units[k] * t.c[k].nslots;
+    if (total == 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    if (e != cudaSuccess) return e;
+    const int grid = sms * (per_sm > 0 ? per_sm : 1);
+    t.g0[0] = 0;
+    for (int k = 0; k < t.n; ++k) {
+        const int uk = units[k] * t.c[k].nslots;
+        int gk = (int)((long long)grid * uk / total);
+        if (gk < 1) gk = 1;
+        if (gk > uk) gk = uk;
+        t.per[k] = units[k];
+        t.g0[k + 1] = t.g0[k] + gk;
+    }
+    void* args[] = {&t};
+    return cudaLaunchKernel(kern, dim3(t.g0[t.n]), dim3(threads), args, smem, s);
+}
+
+}  // namespace
+
+cudaError_t mc_launch_fft_passes(const MCTable& base, cudaStream_t s) {
+    int zu[kMaxMC], yu[kMaxMC], xu[kMaxMC];
+    int zs = 0, ys = 0, xs = 0;
+    for (int k = 0; k < base.n; ++k) {
+        const MCPassGeom g = mc_geom(base.c[k].ng);
+        if (!g.zunits) return cudaErrorInvalidValue;
+        zu[k] = g.zunits;
+        yu[k] = g.yunits;
+        xu[k] = g.xunits;
+        zs = g.zsmem > zs ? g.zsmem : zs;
+        ys = g.ysmem > ys ? g.ysmem : ys;
+        xs = g.xsmem > xs ? g.xsmem : xs;
+    }
+    cudaError_t e = mc_launch((const void*)mc_fft_kernel<0>, base, zu, mc_threads<0>(), zs, s);
+    if (e == cudaSuccess) e = mc_launch((const void*)mc_fft_kernel<1>, base, yu, mc_threads<1>(), ys, s);
+    if (e == cudaSuccess) e = mc_launch((const void*)mc_fft_kernel<2>, base, xu, mc_threads<2>(), xs, s);
+    if (e == cudaSuccess) e = mc_launch((const void*)mc_fft_kernel<3>, base, yu, mc_threads<3>(), ys, s);
+    if (e == cudaSuccess) e = mc_launch((const void*)mc_fft_kernel<4>, base, zu, mc_threads<4>(), zs, s);
+    return e;
+}
 
 }  // namespace hgpm

@@ -49,14 +49,15 @@ struct hgpm_ctx {
     // kick that gathers the potential leaves it to hgpm_get_force)
     bool phi_valid = false;
     bool force_valid = false;
+    bool phi2_valid = false;  // the paired potential, in the force grid's space
     // kernel variants (environment, read at creation): HGPM_NO_TMA=1 selects the
-    // plain strided y passes, HGPM_XTMA=0|1 the plain/TMA-fed fused x pass
-    // (default 1, the TMA-fed one: 0.95 vs 0.99 ms at 512^3).  The deposit
+    // plain strided y passes, HGPM_XTMA=0|1 the fused x pass: plain or TMA-fed
+    // (the default; 0.48 against 0.53 ms at 512^3).  The deposit
     // and kick candidates (bit-identical results) are chosen by the autotuner
     // (hgpm_autotune, or its cache), else HGPM_DEPOSIT / HGPM_KICK, else the
     // built-in defaults (-1 / 0).
     bool tma = true;
-    bool xtma = true;
+    int xmode = 1;
     int dep_choice = -1;
     int kick_choice = 0;
     float* stage = nullptr;     // AoS float3 x, v staging (lazy)

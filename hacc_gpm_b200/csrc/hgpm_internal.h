@@ -46,6 +46,9 @@ cudaError_t launch_zfwd(int ng, void* in, bool fixed, float2* out, int nlines, i
 cudaError_t launch_zinv(int ng, const float2* in, float* out, int nlines, int zs, size_t in_cs, size_t out_cs,
                         int ncomp, float scale, const float2* tw, cudaStream_t s, const Slots& sl = Slots{},
                         int nslots = 1);
+// The C2R z pass of one box writing the paired potential (2 ng^3 floats:
+// cell z of a line holds (phi(z), phi(z+1 mod ng))).
+cudaError_t launch_zinv_pair(int ng, const float2* in, float* out, int zs, const float2* tw, cudaStream_t s);
 cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
                            int ncomp, const float2* tw, cudaStream_t s, const Slots& sl = Slots{}, int nslots = 1);
 // x pass fused with the Green's function: the potential's spectrum
@@ -97,6 +100,9 @@ int kick_kernels(int choice, int np_side, int ng);
 // Candidates that gather the real potential instead of the float4 force
 // grid (the step then skips gradient_kernel).
 bool kick_uses_phi(int choice);
+// the kick gathers the paired potential (zpass_c2r with pair: cell z holds
+// (phi(z), phi(z+1)), 8 bytes per cell, in the force grid's space)
+bool kick_uses_phi2(int choice);
 // Deposit configurations (bit-identical int64 grids): how many, and the
 // default (used when the choice is -1).
 int deposit_candidates(int np_side, int ng);

@@ -16,6 +16,7 @@
 
 #include "hgpm_device.cuh"
 #include "hgpm_internal.h"
+#include "multi_class.h"
 
 namespace hgpm {
 
@@ -542,6 +543,8 @@ __device__ __forceinline__ unsigned long long column_adds(const ParticleSoA& p, 
             cic_q24<true>(cx, cy, cz, mass, q);
             const int cw = (win_rel(cell_x(c), gx0, ng) * wy + win_rel(cell_y(c), gy0, ng)) * wz +
                            win_rel(cell_z(c), gz0, ng);
+            // a particle's 8 values sum to about mass * 2^24 (< 2^31 for mass <= 64)
+            unsigned psum = 0u;
 #pragma unroll
             for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -553,10 +556,11 @@ __device__ __forceinline__ unsigned long long column_adds(const ParticleSoA& p, 
                             const unsigned old = atomicAdd(&w0[cw + a * syz + b * wz + cc], v);
                             wr |= old + v < old;
                         } else {
-                            added += v;
+                            psum += v;
                             atomicAdd(&w0[cw + a * syz + b * wz + cc], v);
                         }
                     }
+            if (!RET) added += psum;
         }
     }
     if (RET) *wrapped = wr;
@@ -564,13 +568,21 @@ __device__ __forceinline__ unsigned long long column_adds(const ParticleSoA& p, 
 }
 
 // Zero the window, add the column range [k0, k0 + len), check for wraps and
-// flush; returns false (nothing flushed) if a cell wrapped.  Called by every
-// thread of the CTA.
-template <int B, int PF, bool RET>
+// flush; returns false (nothing left in the grid) if a cell wrapped.  Called
+// by every thread of the CTA.  CHK, how a wrap is found:
+//   0  before the flush, the window's 64-bit sum against the sum of the
+//      values added (a wrapped cell changes it by a multiple of 2^32);
+//   1  from the atomics' returned values (column_adds with RET);
+//   2  the same two sums, the window's taken while flushing; a wrapped window
+//      (in practice never at the workloads' densities) is taken back out of
+//      the grid by adding the negated values, so the grid's integers are
+//      those of the other checks.
+template <int B, int PF, int CHK>
 __device__ __forceinline__ bool column_pass(const ParticleSoA& p, int i0, int k0, int len, float mass,
                                             unsigned* __restrict__ w0, long long* wsum, const int* box, int ox,
                                             int oy, int oz, int ng, unsigned long long* __restrict__ rho) {
     constexpr int NT = B * B;
+    constexpr bool RET = CHK == 1;
     const int tid = threadIdx.x;
     const int wx = box[3] - box[0] + 2, wy = box[4] - box[1] + 2, wz = box[5] - box[2] + 2;
     const int gx0 = wrap_once(ox + box[0], ng), gy0 = wrap_once(oy + box[1], ng), gz0 = wrap_once(oz + box[2], ng);
@@ -581,6 +593,31 @@ __device__ __forceinline__ bool column_pass(const ParticleSoA& p, int i0, int k0
     const unsigned long long added =
         column_adds<B, PF, RET>(p, i0, k0, len, mass, w0, gx0, gy0, gz0, wy, wz, ng, &wrapped);
     long long tot = 0;
+    if (CHK == 2) {
+        __syncthreads();
+        const WinMap map(wy, wz, gx0, gy0, gz0, ng);
+        long long d = -(long long)added;
+        for (int i = tid; i < vol; i += NT) {
+            const unsigned v = w0[i];
+            if (v != 0u) {
+                d += v;
+                atomicAdd(&rho[map.global(i)], (unsigned long long)v << kQShift);
+            }
+        }
+        d = warp_sum_ll(d);
+        if ((tid & 31) == 0) wsum[tid >> 5] = d;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < NT / 32; ++k) tot += wsum[k];
+        if (tot != 0) {
+            for (int i = tid; i < vol; i += NT) {
+                const unsigned v = w0[i];
+                if (v != 0u) atomicAdd(&rho[map.global(i)], 0ull - ((unsigned long long)v << kQShift));
+            }
+        }
+        __syncthreads();  // the window and wsum are reused by the next pass
+        return tot == 0;
+    }
     if (RET) {
         tot = __syncthreads_or(wrapped) ? 1 : 0;
     } else {
@@ -604,20 +641,21 @@ __device__ __forceinline__ bool column_pass(const ParticleSoA& p, int i0, int k0
     return tot == 0;
 }
 
-template <int B, int MINB, int PF, bool RET = false>
-__global__ void __launch_bounds__(B * B, MINB) deposit_col_kernel(ParticleSoA p, int np_side, int ng, float mass,
-                                                                  unsigned long long* __restrict__ rho, int cap_cells,
-                                                                  int* __restrict__ blkwin, SpillList spill, Slots sl) {
+// Block blk of one box: p, rho, recs (window records, may be null), the
+// box's spill queue (items, cnt) and wide-window counter (over, may be
+// null).  The single-class kernel below and the multi-class deposit run it.
+template <int B, int PF, int CHK>
+__device__ __forceinline__ void deposit_col_body(ParticleSoA p, int np_side, int ng, float mass,
+                                                 unsigned long long* __restrict__ rho, int cap_cells,
+                                                 int* __restrict__ recs, int* __restrict__ items, int* cnt,
+                                                 int* over, int blk) {
     constexpr int B3 = B * B * B, NT = B * B;
     extern __shared__ unsigned long long win[];
     __shared__ int bb[18];  // (min xyz, max xyz) of the block, then of each x-half
     __shared__ long long wsum[NT / 32];
-    if (slot_idle(sl, blockIdx.y)) return;
     const int tid = threadIdx.x;
     const int nb = np_side / B;
-    const int blk = blockIdx.x;
-    p = offset_soa(p, (size_t)blockIdx.y * sl.s0 + (size_t)blk * B3);
-    rho += (size_t)blockIdx.y * sl.s1;
+    p = offset_soa(p, (size_t)blk * B3);
     const int bz = blk % nb, by = (blk / nb) % nb, bx = blk / (nb * nb);
     const int ox = (int)((long long)bx * B * ng / np_side);
     const int oy = (int)((long long)by * B * ng / np_side);
@@ -667,33 +705,44 @@ __global__ void __launch_bounds__(B * B, MINB) deposit_col_kernel(ParticleSoA p,
     }
     __syncthreads();
     const int wx = bb[3] - bb[0] + 2, wy = bb[4] - bb[1] + 2, wz = bb[5] - bb[2] + 2;
-    if (blkwin && tid < 6) {
+    if (recs && tid < 6) {
         const int rec = tid < 3 ? bb[tid] : bb[tid] - bb[tid - 3] + 2;
-        blkwin[(size_t)blockIdx.y * sl.s2 + (size_t)blk * kWinRec + tid] = rec;
+        recs[(size_t)blk * kWinRec + tid] = rec;
     }
     const long long vol = (long long)wx * wy * wz;
-    if (tid == 0 && spill.over && vol > kWin4Cap) atomicAdd(&spill.over[blockIdx.y], 1);
+    if (tid == 0 && over && vol > kWin4Cap) atomicAdd(over, 1);
     unsigned* w0 = reinterpret_cast<unsigned*>(win);
     // queued part: 0 the whole block, 2 its upper x-half (the lower half
     // flushed); at most one item per block
     int queue = -1;
     if (vol <= cap_cells) {
-        if (!column_pass<B, PF, RET>(p, tid, 0, B, mass, w0, wsum, bb, ox, oy, oz, ng, rho)) queue = 0;
+        if (!column_pass<B, PF, CHK>(p, tid, 0, B, mass, w0, wsum, bb, ox, oy, oz, ng, rho)) queue = 0;
     } else {
         auto hvol = [&](int h) {
             const int* q = bb + 6 + 6 * h;
             return (long long)(q[3] - q[0] + 2) * (q[4] - q[1] + 2) * (q[5] - q[2] + 2);
         };
         if (hvol(0) <= cap_cells && hvol(1) <= cap_cells) {
-            if (!column_pass<B, PF, RET>(p, tid, 0, B / 2, mass, w0, wsum, bb + 6, ox, oy, oz, ng, rho)) queue = 0;
-            else if (!column_pass<B, PF, RET>(p, tid, B / 2, B / 2, mass, w0, wsum, bb + 12, ox, oy, oz, ng, rho))
+            if (!column_pass<B, PF, CHK>(p, tid, 0, B / 2, mass, w0, wsum, bb + 6, ox, oy, oz, ng, rho)) queue = 0;
+            else if (!column_pass<B, PF, CHK>(p, tid, B / 2, B / 2, mass, w0, wsum, bb + 12, ox, oy, oz, ng, rho))
                 queue = 2;
         } else {
             queue = 0;
         }
     }
-    if (queue >= 0 && tid == 0)
-        spill.items[(size_t)blockIdx.y * spill.nblocks + atomicAdd(&spill.cnt[blockIdx.y], 1)] = blk * 4 + queue;
+    if (queue >= 0 && tid == 0) items[atomicAdd(cnt, 1)] = blk * 4 + queue;
+}
+
+template <int B, int MINB, int PF, int CHK = 0>
+__global__ void __launch_bounds__(B * B, MINB) deposit_col_kernel(ParticleSoA p, int np_side, int ng, float mass,
+                                                                  unsigned long long* __restrict__ rho, int cap_cells,
+                                                                  int* __restrict__ blkwin, SpillList spill, Slots sl) {
+    const int slot = blockIdx.y;
+    if (slot_idle(sl, slot)) return;
+    deposit_col_body<B, PF, CHK>(offset_soa(p, (size_t)slot * sl.s0), np_side, ng, mass, rho + (size_t)slot * sl.s1,
+                                 cap_cells, blkwin ? blkwin + (size_t)slot * sl.s2 : nullptr,
+                                 spill.items + (size_t)slot * spill.nblocks, spill.cnt + slot,
+                                 spill.over ? spill.over + slot : nullptr, blockIdx.x);
 }
 
 // The 8 fixed-point corner weights of one particle added straight to the
@@ -761,27 +810,22 @@ __global__ void __launch_bounds__(NT) deposit_direct_kernel(ParticleSoA p, int n
 // the global grid.
 constexpr int kBigCap = 27648;
 
+// The queue of one box (p, rho, recs, items: that box's; cnt items), items
+// cta, cta + ncta, ...  Run by the single-class kernel below and by the
+// multi-class spill pass.
 template <int B, bool SMALL, int NT>
-__global__ void __launch_bounds__(NT, 1) deposit_spill_kernel(ParticleSoA p, int np_side, int ng, float mass,
-                                                              unsigned long long* __restrict__ rho,
-                                                              const int* __restrict__ blkwin, SpillList spill,
-                                                              Slots sl) {
+__device__ __forceinline__ void deposit_spill_body(ParticleSoA p, int np_side, int ng, float mass,
+                                                   unsigned long long* __restrict__ rho,
+                                                   const int* __restrict__ recs, const int* __restrict__ items,
+                                                   int cnt, int cta, int ncta) {
     constexpr int B3 = B * B * B, PPT = B3 / NT, BB = B * B;
     extern __shared__ unsigned long long win[];
-    const int slot = blockIdx.y;
-    if (slot_idle(sl, slot)) return;
-    const int cnt = __ldg(&spill.cnt[slot]);
-    if ((int)blockIdx.x >= cnt) return;
-    p = offset_soa(p, (size_t)slot * sl.s0);
-    rho += (size_t)slot * sl.s1;
-    const int* items = spill.items + (size_t)slot * spill.nblocks;
-    const int* recs = blkwin + (size_t)slot * sl.s2;
     unsigned* w0 = reinterpret_cast<unsigned*>(win);
     unsigned* w1 = w0 + kBigCap;
     const int tid = threadIdx.x;
     const int g = tid / BB, r = tid % BB;  // x group and (y, z) of the thread's chain
     const int nb = np_side / B;
-    for (int t = blockIdx.x; t < cnt; t += gridDim.x) {
+    for (int t = cta; t < cnt; t += ncta) {
         // item = block * 4 + part: 0 the whole block, 2 its upper x-half only
         const int item = __ldg(&items[t]);
         const int blk = item >> 2;
@@ -848,6 +892,20 @@ __global__ void __launch_bounds__(NT, 1) deposit_spill_kernel(ParticleSoA p, int
             }
         }
     }
+}
+
+template <int B, bool SMALL, int NT>
+__global__ void __launch_bounds__(NT, 1) deposit_spill_kernel(ParticleSoA p, int np_side, int ng, float mass,
+                                                              unsigned long long* __restrict__ rho,
+                                                              const int* __restrict__ blkwin, SpillList spill,
+                                                              Slots sl) {
+    const int slot = blockIdx.y;
+    if (slot_idle(sl, slot)) return;
+    const int cnt = __ldg(&spill.cnt[slot]);
+    if ((int)blockIdx.x >= cnt) return;
+    deposit_spill_body<B, SMALL, NT>(offset_soa(p, (size_t)slot * sl.s0), np_side, ng, mass,
+                                     rho + (size_t)slot * sl.s1, blkwin + (size_t)slot * sl.s2,
+                                     spill.items + (size_t)slot * spill.nblocks, cnt, blockIdx.x, gridDim.x);
 }
 
 // ICICKernel (icic_pm.cu:72-127) fused with up to two UpdatePosKernel drifts
@@ -1162,6 +1220,37 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_flat_nt_kernel(ParticleSoA
     }
 }
 
+// v += sum over the 8 CIC corners of w * F, each corner's force formed from
+// the gathered potential: P[a][b][t] = phi(x_a, y_b, z_{t-1}) on the inner
+// columns, X[e][b][cc] and Y[a][e][cc] the x and y faces (e = 0: x-1 / y-1,
+// e = 1: x+2 / y+2); F_d = 0.5f * (phi(-e_d) - phi(+e_d)) as gradient_kernel
+// forms it.
+__device__ __forceinline__ float3 phi_corner_kick(const float (&P)[2][2][4], const float (&X)[2][2][2],
+                                                  const float (&Y)[2][2][2], const KickWeights& w) {
+    float3 dv = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const float wab = __fmul_rn(w.wx[a], w.wy[b]);
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const float lo_x = a == 0 ? X[0][b][cc] : P[0][b][1 + cc];
+                const float hi_x = a == 0 ? P[1][b][1 + cc] : X[1][b][cc];
+                const float lo_y = b == 0 ? Y[a][0][cc] : P[a][0][1 + cc];
+                const float hi_y = b == 0 ? P[a][1][1 + cc] : Y[a][1][cc];
+                const float fx = 0.5f * (lo_x - hi_x);
+                const float fy = 0.5f * (lo_y - hi_y);
+                const float fz = 0.5f * (P[a][b][cc] - P[a][b][cc + 2]);
+                const float mul = __fmul_rn(wab, w.wz[cc]);
+                dv.x = fmaf(mul, fx, dv.x);
+                dv.y = fmaf(mul, fy, dv.y);
+                dv.z = fmaf(mul, fz, dv.z);
+            }
+        }
+    return dv;
+}
+
 // The CIC-weighted force of a particle gathered from the real potential phi
 // instead of the float4 force grid: each corner's force is formed from phi as
 // gradient_kernel forms it, F_d = 0.5f * (phi(c - e_d) - phi(c + e_d)), and
@@ -1198,32 +1287,51 @@ __device__ __forceinline__ float3 gather_phi(const float* __restrict__ phi, cons
                 X[e][b][cc] = __ldg(&phi[sx[3 * e] + sy[1 + b] + sz[1 + cc]]);
                 Y[b][e][cc] = __ldg(&phi[sx[1 + b] + sy[3 * e] + sz[1 + cc]]);
             }
-    float3 dv = make_float3(0.f, 0.f, 0.f);
+    return phi_corner_kick(P, X, Y, w);
+}
+
+// The paired potential (zpass_c2r_kernel with PAIR): cell z holds
+// (phi(z), phi(z+1)), so the 4 z values of an inner column are two 8-byte
+// loads and the 2 of a face column one: 16 loads instead of 32, the same
+// values, the same forces (bit-identical to gather_phi).
+__device__ __forceinline__ float3 gather_phi2(const float2* __restrict__ phi2, const PState& c, const KickWeights& w,
+                                              int ng) {
+    const int ix = cell_x(c.c), iy = cell_y(c.c), iz = cell_z(c.c);
+    const int xm = ix == 0 ? ng - 1 : ix - 1, x1 = ix + 1 == ng ? 0 : ix + 1, x2 = x1 + 1 == ng ? 0 : x1 + 1;
+    const int ym = iy == 0 ? ng - 1 : iy - 1, y1 = iy + 1 == ng ? 0 : iy + 1, y2 = y1 + 1 == ng ? 0 : y1 + 1;
+    const int zm = iz == 0 ? ng - 1 : iz - 1, z1 = iz + 1 == ng ? 0 : iz + 1;
+    const size_t sx[4] = {(size_t)xm * ng * ng, (size_t)ix * ng * ng, (size_t)x1 * ng * ng, (size_t)x2 * ng * ng};
+    const size_t sy[4] = {(size_t)ym * ng, (size_t)iy * ng, (size_t)y1 * ng, (size_t)y2 * ng};
+    float P[2][2][4], X[2][2][2], Y[2][2][2];
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
-            const float wab = __fmul_rn(w.wx[a], w.wy[b]);
-#pragma unroll
-            for (int cc = 0; cc < 2; ++cc) {
-                const float lo_x = a == 0 ? X[0][b][cc] : P[0][b][1 + cc];
-                const float hi_x = a == 0 ? P[1][b][1 + cc] : X[1][b][cc];
-                const float lo_y = b == 0 ? Y[a][0][cc] : P[a][0][1 + cc];
-                const float hi_y = b == 0 ? P[a][1][1 + cc] : Y[a][1][cc];
-                const float fx = 0.5f * (lo_x - hi_x);
-                const float fy = 0.5f * (lo_y - hi_y);
-                const float fz = 0.5f * (P[a][b][cc] - P[a][b][cc + 2]);
-                const float mul = __fmul_rn(wab, w.wz[cc]);
-                dv.x = fmaf(mul, fx, dv.x);
-                dv.y = fmaf(mul, fy, dv.y);
-                dv.z = fmaf(mul, fz, dv.z);
-            }
+            const float2 lo = __ldg(&phi2[sx[1 + a] + sy[1 + b] + zm]);  // z-1, z
+            const float2 hi = __ldg(&phi2[sx[1 + a] + sy[1 + b] + z1]);  // z+1, z+2
+            P[a][b][0] = lo.x;
+            P[a][b][1] = lo.y;
+            P[a][b][2] = hi.x;
+            P[a][b][3] = hi.y;
         }
-    return dv;
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const float2 xf = __ldg(&phi2[sx[3 * e] + sy[1 + b] + iz]);
+            const float2 yf = __ldg(&phi2[sx[1 + b] + sy[3 * e] + iz]);
+            X[e][b][0] = xf.x;
+            X[e][b][1] = xf.y;
+            Y[b][e][0] = yf.x;
+            Y[b][e][1] = yf.y;
+        }
+    return phi_corner_kick(P, X, Y, w);
 }
 
-// kick_flat_nt_kernel gathering from the real potential (gather_phi).
-template <int B, int NT, int R = 1>
+
+// kick_flat_nt_kernel gathering from the real potential (gather_phi), or with
+// PAIR from the paired potential (gather_phi2; phi then holds ng^3 pairs).
+template <int B, int NT, int R = 1, bool PAIR = false>
 __global__ void __launch_bounds__(NT, 1024 / NT) kick_phi_kernel(ParticleSoA p, int ng, const float* __restrict__ phi,
                                                                double deltaT, double fscal, float pf_a, float pf_b,
                                                                int ndrift, int nblocks, Slots sl, KickSched ks) {
@@ -1236,6 +1344,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_phi_kernel(ParticleSoA p, 
     phi += (size_t)slot * sl.s1;
     float dtf;
     kick_scalars(ks, slot, deltaT, fscal, dtf, pf_a, pf_b, ndrift);
+    const float2* phi2 = reinterpret_cast<const float2*>(phi);
     auto index = [&](int u) { return (size_t)(u / SUB) * B3 + (u % SUB) * NT + threadIdx.x; };
     auto unit = [&](int k) { return ((int)blockIdx.x + (k / R) * (int)gridDim.x) * R + k % R; };
     int k = 0;
@@ -1250,7 +1359,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) kick_phi_kernel(ParticleSoA p, 
             inext = index(un);
             next = load_p(p, inext);
         }
-        finish_p(p, i, cur, gather_phi(phi, cur, KickWeights(cur, dtf), ng), pf_a, pf_b, ndrift, ng);
+        const KickWeights w(cur, dtf);
+        finish_p(p, i, cur, PAIR ? gather_phi2(phi2, cur, w, ng) : gather_phi(phi, cur, w, ng), pf_a, pf_b, ndrift,
+                 ng);
         if (!more) break;
         ++k;
     }
@@ -1514,7 +1625,7 @@ struct DepositCfg {
     int nt, cap, cell_bytes;
 };
 
-constexpr int kDepositCands = 10;
+constexpr int kDepositCands = 11;
 
 // Candidates per block side; index = HGPM_DEPOSIT (or the tuned choice).
 //   16^3 blocks: 0-2 (lo, hi) 16-bit-split windows (deposit_tiled_kernel) with
@@ -1523,11 +1634,12 @@ constexpr int kDepositCands = 10;
 //   kernels (deposit_col_kernel, 256 threads, x-half split): 4 CTAs per SM
 //   with a 4- or 2-deep ring, 3 CTAs per SM with 18432-cell windows, and 4
 //   CTAs per SM detecting wraps from the atomics' returned values; 9 direct
-//   (deposit_direct_kernel: no window, every weight to the int64 grid).
+//   (deposit_direct_kernel: no window, every weight to the int64 grid); 10
+//   the column kernel with the wrap check folded into the flush.
 //   8^3 blocks: 0 split window, 1 32-bit window (256 threads, 13312 cells),
 //   2 column kernel (64 threads, 4096 cells), 3 32-bit window (512 threads,
 //   kBigCap cells), 4 column kernel with returned-value wrap detection, 5
-//   direct.
+//   direct, 6 column kernel with the check in the flush.
 // The 32-bit windows need mass <= 64; otherwise the split window of the same
 // thread count runs.
 template <int B, bool SMALL>
@@ -1543,7 +1655,7 @@ static int deposit_candidates(int cap_default, bool w32, DepositCfg* out) {
             out[n++] = {deposit_col_kernel<B, 4, 4>, 256, 13312, 4};
             out[n++] = {deposit_col_kernel<B, 4, 2>, 256, 13312, 4};
             out[n++] = {deposit_col_kernel<B, 3, 4>, 256, 18432, 4};
-            out[n++] = {deposit_col_kernel<B, 4, 4, true>, 256, 13312, 4};
+            out[n++] = {deposit_col_kernel<B, 4, 4, 1>, 256, 13312, 4};
         } else {
             // the split window with the same threads per CTA
             const int same_nt[6] = {1, 0, 0, 0, 0, 0};
@@ -1551,17 +1663,19 @@ static int deposit_candidates(int cap_default, bool w32, DepositCfg* out) {
             n += 6;
         }
         out[n++] = {deposit_direct_kernel<B, SMALL, 512>, 512, 0, 0};
+        out[n++] = w32 ? DepositCfg{deposit_col_kernel<B, 4, 4, 2>, 256, 13312, 4} : out[0];
     } else {
         out[n++] = {deposit_tiled_kernel<B, SMALL, 256, 3>, 256, cap_default, 8};
         if (w32) {
             out[n++] = {deposit_w32_kernel<B, 256, 4, true, 2>, 256, 13312, 4};
             out[n++] = {deposit_col_kernel<B, 12, 4>, B * B, 4096, 4};
             out[n++] = {deposit_w32_kernel<B, 512, 2, true, 1>, 512, kBigCap, 4};
-            out[n++] = {deposit_col_kernel<B, 12, 4, true>, B * B, 4096, 4};
+            out[n++] = {deposit_col_kernel<B, 12, 4, 1>, B * B, 4096, 4};
         } else {
             for (int i = 0; i < 4; ++i) out[n++] = out[0];
         }
         out[n++] = {deposit_direct_kernel<B, SMALL, 256>, 256, 0, 0};
+        out[n++] = w32 ? DepositCfg{deposit_col_kernel<B, 12, 4, 2>, B * B, 4096, 4} : out[0];
     }
     return n;
 }
@@ -1609,7 +1723,7 @@ static cudaError_t deposit_impl(const ParticleSoA& p, int np_side, int ng, float
     return cudaGetLastError();
 }
 
-int deposit_candidates(int np_side, int ng) { return block_side(np_side, ng) == 16 ? kDepositCands : 6; }
+int deposit_candidates(int np_side, int ng) { return block_side(np_side, ng) == 16 ? kDepositCands : 7; }
 
 int deposit_default(int np_side, int ng) {
     return block_side(np_side, ng) == 16 ? deposit_default_choice<16>(np_side, ng)
@@ -1637,12 +1751,14 @@ cudaError_t launch_deposit(const ParticleSoA& p, int np_side, int ng, float mass
 // (kick_spill_kernel, 2.25 ms), 4 windowed (kick_win4_kernel + the flat
 // kernel for the queued blocks).  8^3 blocks: 0 flat 256-thread items, 1-2
 // flat 512-thread CTAs (a whole block per unit) in runs of 1 / 2, 3 flat
-// 256-thread CTAs in runs of 4, 4 windowed.
-constexpr int kKickCands = 7;
+// 256-thread CTAs in runs of 4, 4 windowed.  Both: 5-6 the flat schedules of
+// 0 / 1 gathering the real potential, 7 the paired potential.
+constexpr int kKickCands = 8;
 constexpr int kKickWindowed = 4;
-// candidates 5 and 6 gather from the real potential (kick_phi_kernel): the
-// step then needs no force grid (kick_uses_phi)
+// candidates 5 and 6 gather from the real potential (kick_phi_kernel), 7 from
+// the paired potential: the step then needs no force grid (kick_uses_phi)
 constexpr int kKickPhiFirst = 5;
+constexpr int kKickPhi2 = 7;
 
 int kick_candidates(int np_side, int ng) {
     (void)np_side;
@@ -1651,6 +1767,7 @@ int kick_candidates(int np_side, int ng) {
 }
 
 bool kick_uses_phi(int choice) { return choice >= kKickPhiFirst && choice < kKickCands; }
+bool kick_uses_phi2(int choice) { return choice == kKickPhi2; }
 
 int kick_kernels(int choice, int np_side, int ng) {
     (void)np_side;
@@ -1669,12 +1786,12 @@ static cudaError_t kick_flat_launch(const ParticleSoA& p, int np_side, int ng, c
     return cudaGetLastError();
 }
 
-template <int B, int NT, int R>
+template <int B, int NT, int R, bool PAIR = false>
 static cudaError_t kick_phi_launch(const ParticleSoA& p, int np_side, int ng, const float* phi, double deltaT,
                                    double fscal, float pf_a, float pf_b, int ndrift, const Slots& sl,
                                    const KickSched& ks, int nslots, cudaStream_t s) {
     const int nblocks = (np_side / B) * (np_side / B) * (np_side / B);
-    auto kf = kick_phi_kernel<B, NT, R>;
+    auto kf = kick_phi_kernel<B, NT, R, PAIR>;
     const int grid = num_sms() * blocks_per_sm_once((const void*)kf, NT, 0);
     kf<<<dim3(grid, nslots), NT, 0, s>>>(p, ng, phi, deltaT, fscal, pf_a, pf_b, ndrift, nblocks, sl, ks);
     return cudaGetLastError();
@@ -1688,9 +1805,11 @@ static cudaError_t kick_impl(const ParticleSoA& p, int np_side, int ng, const fl
     if (kick_uses_phi(choice)) {
         if constexpr (B == 16) {
             if (choice == 5) return kick_phi_launch<B, 1024, 4>(p, np_side, ng, phi, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
+            if (choice == 7) return kick_phi_launch<B, 1024, 4, true>(p, np_side, ng, phi, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
             return kick_phi_launch<B, 1024, 2>(p, np_side, ng, phi, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
         } else {
             if (choice == 5) return kick_phi_launch<B, 512, 1>(p, np_side, ng, phi, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
+            if (choice == 7) return kick_phi_launch<B, 512, 1, true>(p, np_side, ng, phi, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
             return kick_phi_launch<B, 512, 2>(p, np_side, ng, phi, deltaT, fscal, pf_a, pf_b, ndrift, sl, ks, nslots, s);
         }
     }
@@ -1785,6 +1904,160 @@ cudaError_t launch_place(const float* sgrid, size_t scomp, const ParticleSoA& p,
     const size_t n = (size_t)np_side * np_side * np_side;
     place_kernel<<<nblk(n, 256), 256, 0, s>>>(sgrid, scomp, p, np_side, block_side(np_side, ng), ng, delta_f, velmul);
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Multi-class step (multi_class.h): the particle phases, each one launch over
+// every class and slot, running the single-class kernels' device bodies.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kMCDepCap = 13312;  // the column deposit's window (52 KB)
+
+// global unit u -> (class k, slot, local unit); false for an idle slot
+__device__ __forceinline__ bool mc_find(const MCTable& t, int u, int& k, int& slot, int& lu) {
+    k = 0;
+    while (k + 1 < t.n && u >= t.u0[k + 1]) ++k;
+    const int per = (t.u0[k + 1] - t.u0[k]) / t.c[k].nslots;
+    const int r = u - t.u0[k];
+    slot = r / per;
+    lu = r - slot * per;
+    return !t.c[k].active || t.c[k].active[slot];
+}
+
+__global__ void mc_prep_kernel(const __grid_constant__ MCTable t) {
+    for (int k = 0; k < t.n; ++k) {
+        const MCClass& c = t.c[k];
+        for (int i = threadIdx.x; i < c.nslots; i += blockDim.x) {
+            c.spill.cnt[i] = 0;
+            if (c.spill.over) c.spill.over[i] = 0;
+        }
+    }
+}
+
+// deposit_col_kernel<16, 4, 4, 1> over the blocks of every slot of every class
+__global__ void __launch_bounds__(256, 4) mc_deposit_kernel(const __grid_constant__ MCTable t) {
+    for (int u = blockIdx.x; u < t.u0[t.n]; u += gridDim.x) {
+        int k, slot, blk;
+        if (mc_find(t, u, k, slot, blk)) {
+            const MCClass& c = t.c[k];
+            deposit_col_body<16, 4, 1>(offset_soa(c.p, (size_t)slot * c.part_stride), c.np, c.ng, c.mass,
+                                       c.rho64 + (size_t)slot * c.ncell, kMCDepCap,
+                                       c.blkwin + (size_t)slot * c.win_stride,
+                                       c.spill.items + (size_t)slot * c.spill.nblocks, c.spill.cnt + slot,
+                                       c.spill.over ? c.spill.over + slot : nullptr, blk);
+        }
+        __syncthreads();  // bb, wsum and the window are reused by the next unit
+    }
+}
+
+// deposit_spill_kernel over every slot's queue: blockIdx.y = global slot
+__global__ void __launch_bounds__(1024, 1) mc_spill_kernel(const __grid_constant__ MCTable t) {
+    int k = 0, slot = blockIdx.y;
+    while (k < t.n && slot >= t.c[k].nslots) slot -= t.c[k++].nslots;
+    if (k >= t.n) return;
+    const MCClass& c = t.c[k];
+    if (c.active && !c.active[slot]) return;
+    const int cnt = c.spill.cnt[slot];
+    if ((int)blockIdx.x >= cnt) return;
+    deposit_spill_body<16, true, 1024>(offset_soa(c.p, (size_t)slot * c.part_stride), c.np, c.ng, c.mass,
+                                       c.rho64 + (size_t)slot * c.ncell, c.blkwin + (size_t)slot * c.win_stride,
+                                       c.spill.items + (size_t)slot * c.spill.nblocks, cnt, blockIdx.x, gridDim.x);
+}
+
+// kick_phi_kernel's arithmetic over units of 1024 particles (a quarter of a
+// 16^3 block: four Lagrangian x-planes) of every slot of every class; the
+// slot's scalars come from its schedule row.
+__global__ void __launch_bounds__(1024, 1) mc_kick_kernel(const __grid_constant__ MCTable t) {
+    constexpr int B3 = 4096, SUB = 4;
+    for (int u = blockIdx.x; u < t.u0[t.n]; u += gridDim.x) {
+        int k, slot, lu;
+        if (!mc_find(t, u, k, slot, lu)) continue;
+        const MCClass& c = t.c[k];
+        ParticleSoA p = offset_soa(c.p, (size_t)slot * c.part_stride);
+        const float* phi = reinterpret_cast<const float*>(c.fspec + c.spec_elems) + (size_t)slot * 6 * c.spec_elems;
+        float dtf, pf_a = 0.f, pf_b = 0.f;
+        int ndrift = 0;
+        kick_scalars(KickSched{c.sched, c.step, c.pitch}, slot, 0.0, 0.0, dtf, pf_a, pf_b, ndrift);
+        const size_t i = (size_t)(lu / SUB) * B3 + (lu % SUB) * 1024 + threadIdx.x;
+        const PState cur = load_p(p, i);
+        finish_p(p, i, cur, gather_phi(phi, cur, KickWeights(cur, dtf), c.ng), pf_a, pf_b, ndrift, c.ng);
+    }
+}
+
+__global__ void mc_advance_kernel(const __grid_constant__ MCTable t) {
+    for (int k = 0; k < t.n; ++k) {
+        const MCClass& c = t.c[k];
+        for (int i = threadIdx.x; i < c.nslots; i += blockDim.x) {
+            if (!c.active[i]) continue;
+            const int st = c.step[i] + 1;
+            c.step[i] = st;
+            if (st >= c.nsteps[i]) c.active[i] = 0;
+        }
+    }
+}
+
+cudaError_t mc_persistent(const void* kern, MCTable& t, int threads, int smem, cudaStream_t s) {
+    if (t.u0[t.n] == 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    if (e != cudaSuccess) return e;
+    int grid = num_sms() * (per_sm > 0 ? per_sm : 1);
+    if (grid > t.u0[t.n]) grid = t.u0[t.n];
+    void* args[] = {&t};
+    return cudaLaunchKernel(kern, dim3(grid), dim3(threads), args, smem, s);
+}
+
+}  // namespace
+
+bool mc_class_supported(int ng, int np) {
+    if (block_side(np, ng) != 16 || ng > np) return false;
+    switch (ng) {
+#define X(n) case n:
+        HGPM_MC_SIZES(X)
+#undef X
+        return true;
+        default:
+            return false;
+    }
+}
+
+cudaError_t mc_step(const MCTable& base, cudaStream_t s) {
+    if (base.n < 1 || base.n > kMaxMC) return cudaErrorInvalidValue;
+    int nslots = 0;
+    for (int k = 0; k < base.n; ++k) {
+        if (!mc_class_supported(base.c[k].ng, base.c[k].np) || base.c[k].nslots < 1) return cudaErrorInvalidValue;
+        nslots += base.c[k].nslots;
+    }
+    void* pargs[] = {const_cast<MCTable*>(&base)};
+    cudaError_t e = cudaLaunchKernel((const void*)mc_prep_kernel, dim3(1), dim3(256), pargs, 0, s);
+    if (e != cudaSuccess) return e;
+    // deposit: one unit per Lagrangian block
+    MCTable td = base;
+    td.u0[0] = 0;
+    for (int k = 0; k < base.n; ++k) td.u0[k + 1] = td.u0[k] + base.c[k].nblocks * base.c[k].nslots;
+    e = mc_persistent((const void*)mc_deposit_kernel, td, 256, kMCDepCap * 4, s);
+    if (e != cudaSuccess) return e;
+    {
+        const int per = num_sms() / nslots > 1 ? num_sms() / nslots : 1;
+        auto ks = mc_spill_kernel;
+        e = smem_attr_once((const void*)ks, kBigCap * 8);
+        if (e != cudaSuccess) return e;
+        ks<<<dim3(per, nslots), 1024, kBigCap * 8, s>>>(base);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    e = mc_launch_fft_passes(base, s);
+    if (e != cudaSuccess) return e;
+    // kick: four units per block
+    MCTable tk = base;
+    tk.u0[0] = 0;
+    for (int k = 0; k < base.n; ++k) tk.u0[k + 1] = tk.u0[k] + base.c[k].nblocks * 4 * base.c[k].nslots;
+    e = mc_persistent((const void*)mc_kick_kernel, tk, 1024, 0, s);
+    if (e != cudaSuccess) return e;
+    return cudaLaunchKernel((const void*)mc_advance_kernel, dim3(1), dim3(256), pargs, 0, s);
 }
 
 }  // namespace hgpm

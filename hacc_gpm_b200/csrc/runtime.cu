@@ -378,7 +378,7 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
         const char* nt = getenv("HGPM_NO_TMA");
         c->tma = !(nt && nt[0] == '1');
         const char* xt = getenv("HGPM_XTMA");
-        c->xtma = !(xt && xt[0] == '0');
+        if (xt && xt[0] >= '0' && xt[0] <= '1') c->xmode = xt[0] - '0';
         const char* kv = getenv("HGPM_KICK");
         if (kv && kv[0] >= '0' && kv[0] <= '9' && atoi(kv) < kick_candidates(p->np, p->ng)) c->kick_choice = atoi(kv);
         const char* dv = getenv("HGPM_DEPOSIT");
@@ -754,7 +754,7 @@ extern "C" int hgpm_solve_gradient(hgpm_ctx* c) {
     {
         PhaseScope ps(c, PH_POISSON);
         const double coeff = 0.5 / ((double)ng * ng * ng);
-        if (c->xtma)
+        if (c->xmode)
             CK(launch_xpotential_tma(ng, c->spec, c->fspec, M + 1, c->zs, c->tw_ng, c->cosq, coeff, c->d_err + 1,
                                      c->stream));
         else
@@ -777,29 +777,51 @@ extern "C" int hgpm_solve_gradient(hgpm_ctx* c) {
         // potential itself (hgpm_get_force then forms the grid on demand)
         PhaseScope ps(c, PH_ZINV);
         float* phi = reinterpret_cast<float*>(c->fspec + cs);
-        CK(launch_zinv(ng, c->fspec, phi, ng * ng, c->zs, 0, 0, 1, 1.0f, c->tw_ng, c->stream));
-        c->phi_valid = true;
         c->force_valid = false;
-        if (!kick_uses_phi(c->kick_choice)) {
-            CK(launch_gradient(ng, phi, reinterpret_cast<float4*>(c->force), c->stream));
-            c->force_valid = true;
+        if (kick_uses_phi2(c->kick_choice)) {
+            // the paired potential, in the force grid's space
+            CK(launch_zinv_pair(ng, c->fspec, c->force, c->zs, c->tw_ng, c->stream));
+            c->phi_valid = false;
+            c->phi2_valid = true;
+        } else {
+            CK(launch_zinv(ng, c->fspec, phi, ng * ng, c->zs, 0, 0, 1, 1.0f, c->tw_ng, c->stream));
+            c->phi_valid = true;
+            c->phi2_valid = false;
+            if (!kick_uses_phi(c->kick_choice)) {
+                CK(launch_gradient(ng, phi, reinterpret_cast<float4*>(c->force), c->stream));
+                c->force_valid = true;
+            }
         }
         count(c, PH_ZINV, c->force_valid ? 2 : 1);
     }
     return HGPM_OK;
 }
 
-// The real potential of the last solve, or null.
+// The potential of the last solve in the form the context's kick gathers
+// (the paired potential for the pair-gathering kick, else the real one), or
+// null (the kick then gathers the force grid).
 static const float* ctx_phi(const hgpm_ctx* c) {
+    if (kick_uses_phi2(c->kick_choice)) return c->phi2_valid ? c->force : nullptr;
     return c->phi_valid ? reinterpret_cast<const float*>(c->fspec + (size_t)c->ng * c->ng * c->zs) : nullptr;
 }
 
 extern "C" int hgpm_get_force(hgpm_ctx* c, float* f) {
     if (!c || !f) return HGPM_ERR_ARG;
+    if (!c->force_valid && !c->phi_valid && c->phi2_valid) {
+        // the real potential from the potential's spectrum, which the solve
+        // leaves in place (the grid below overwrites the paired potential)
+        const int ng = c->ng;
+        CK(launch_zinv(ng, c->fspec, reinterpret_cast<float*>(c->fspec + (size_t)ng * ng * c->zs), ng * ng, c->zs,
+                       0, 0, 1, 1.0f, c->tw_ng, c->stream));
+        count(c, PH_ZINV, 1);
+        c->phi_valid = true;
+    }
     if (!c->force_valid && c->phi_valid) {
-        CK(launch_gradient(c->ng, ctx_phi(c), reinterpret_cast<float4*>(c->force), c->stream));
+        const float* phi = reinterpret_cast<const float*>(c->fspec + (size_t)c->ng * c->ng * c->zs);
+        CK(launch_gradient(c->ng, phi, reinterpret_cast<float4*>(c->force), c->stream));
         count(c, PH_ZINV, 1);
         c->force_valid = true;
+        c->phi2_valid = false;
     }
     // the device grid is float4 (F_x, F_y, F_z, 0) per cell; the ABI returns
     // three planes
@@ -1039,8 +1061,9 @@ static int ic_common(hgpm_ctx* c, const float* noise_host, const double* table, 
     int rc = HGPM_OK;
     do {
         float* noise = c->force;  // scratch: the force grids are rebuilt every solve
-        c->phi_valid = false;     // the IC spectra and displacements overwrite both
+        c->phi_valid = false;     // the IC spectra and displacements overwrite all three
         c->force_valid = false;
+        c->phi2_valid = false;
         cudaError_t e;
         if (noise_host) {
             e = cudaMemcpyAsync(noise, noise_host, npart * 4, cudaMemcpyHostToDevice, c->stream);
@@ -1094,6 +1117,7 @@ extern "C" int hgpm_ic_from_noise(hgpm_ctx* c, const float* noise, const double*
 extern "C" int hgpm_ic_noise(hgpm_ctx* c, float* out) {
     if (!c || !out) return HGPM_ERR_ARG;
     c->force_valid = false;  // the noise is drawn into the force grid's space
+    c->phi2_valid = false;
     CK(launch_noise(c->force, c->npart, c->p.seed, c->p.noise, c->stream));
     count(c, PH_PK, 1);
     CK(cudaMemcpyAsync(out, c->force, c->npart * 4, cudaMemcpyDeviceToHost, c->stream));

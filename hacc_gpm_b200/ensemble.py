@@ -76,8 +76,10 @@ def _ts_for(params: Params) -> Timestepper:
 class Ensemble:
     """Size classes of slots on one GPU (``hgpm_ensemble``)."""
 
-    def __init__(self, classes, device: int = 0, graph: bool = True):
-        """classes: list of (ng, np, nslots)."""
+    def __init__(self, classes, device: int = 0, graph: bool = True, multi: bool = True):
+        """classes: list of (ng, np, nslots).  multi: one launch per phase
+        across all classes where every class allows it (hgpm_ens_multi_launch),
+        else one per phase per class; ``self.multi`` says which runs."""
         self.L = lib()
         self.classes = [(int(a), int(b), int(c)) for a, b, c in classes]
         n = len(self.classes)
@@ -92,6 +94,10 @@ class Ensemble:
             self.close()
             raise HgpmError("hgpm_ens_create status %d: %s" % (rc, msg))
         self.views = {}
+        rc = self.L.hgpm_ens_multi_launch(self._h, 1 if multi else 0)
+        if rc < 0:
+            self._ck(rc)
+        self.multi = rc == 1
         if graph:
             self._ck(self.L.hgpm_ens_use_graph(self._h, 1))
 
@@ -225,14 +231,15 @@ def class_layout(boxes):
 
 
 def run_batched(boxes, device: int = 0, graph: bool = True, keep_state: bool = False, ens: Ensemble = None,
-                stages: dict = None):
+                stages: dict = None, multi: bool = True):
     """All boxes as one ensemble: ICs per slot, batched steps until every box
     has run its steps, then P(k) per slot.  stages (optional dict) receives
-    seconds per stage."""
+    seconds per stage; multi: one launch per phase across the classes where
+    they allow it (Ensemble)."""
     classes, where = class_layout(boxes)
     own = ens is None
     t0 = time.perf_counter()
-    ens = ens or Ensemble(classes, device=device, graph=graph)
+    ens = ens or Ensemble(classes, device=device, graph=graph, multi=multi)
     clk = _Clock(ens.sync) if stages is not None else None
     if clk:
         clk.last = t0

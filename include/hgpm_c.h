@@ -267,6 +267,15 @@ int hgpm_ens_release(hgpm_ensemble* ens, int cls, int slot);
 /* nsteps batched steps (slots that finish go idle on the device).         */
 int hgpm_ens_step(hgpm_ensemble* ens, int nsteps);
 int hgpm_ens_use_graph(hgpm_ensemble* ens, int on);
+/* hgpm_ens_step launches each phase once for ALL classes (one persistent
+ * launch per phase over every class's and slot's work units; the
+ * potential-gather kick; ten launches per step) when `on` (the default),
+ * the ensemble has at most 8 classes and every class has 16^3 particle
+ * blocks (np a multiple of 16, ng <= np) and ng in {32, 48, 64, 96, 128,
+ * 192, 256}; otherwise once per phase per class, the classes on their own
+ * streams.  Results are bit-identical either way.  Returns 1 if the
+ * multi-class form applies to this ensemble, 0 if not, < 0 on error.     */
+int hgpm_ens_multi_launch(hgpm_ensemble* ens, int on);
 /* Wait for queued work; refresh the host copy of every slot's status.     */
 int hgpm_ens_sync(hgpm_ensemble* ens);
 int hgpm_ens_status(hgpm_ensemble* ens, int cls, int slot, int* running, int* steps_done);

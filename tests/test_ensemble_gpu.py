@@ -25,13 +25,37 @@ def _same(a, b):
     assert np.array_equal(a["n"], b["n"]) and np.array_equal(a["P"], b["P"])
 
 
-@pytest.mark.parametrize("graph", [True, False])
-def test_batched_equals_alone(graph):
+@pytest.mark.parametrize("graph,multi", [(True, True), (False, True), (True, False), (False, False)])
+def test_batched_equals_alone(graph, multi):
+    """Batched steps, as one launch per phase across all classes (multi) or
+    one per phase per class, give every box its state and P(k) alone."""
     boxes = _boxes()
     alone = E.run_serial(boxes, keep_state=True)
-    batched = E.run_batched(boxes, graph=graph, keep_state=True)
+    batched = E.run_batched(boxes, graph=graph, keep_state=True, multi=multi)
     for a, b in zip(alone, batched):
         _same(a, b)
+
+
+def test_multi_class_step_launches():
+    """The multi-class step is ten launches whatever the number of classes
+    (here three); the per-class step launches every phase once per class."""
+    boxes = _boxes()
+    classes, where = E.class_layout(boxes)
+    assert len(classes) == 3
+    counts = {}
+    for multi in (True, False):
+        with E.Ensemble(classes, graph=False, multi=multi) as ens:
+            assert ens.multi == multi
+            for b, (ci, si) in zip(boxes, where):
+                p = b.params()
+                ens.slot(ci, si, p).generate_ic(b.table, b.k_delta)
+                ens.start(ci, si, E._ts_for(p), b.nsteps)
+            ens.kernel_launches(reset=True)
+            ens.step(2)
+            ens.sync()
+            counts[multi] = ens.kernel_launches()
+    assert counts[True] == 2 * 10
+    assert counts[False] > counts[True]
 
 
 @pytest.mark.parametrize("graph", [True, False])

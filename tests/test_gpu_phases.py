@@ -61,11 +61,13 @@ def test_deposit_deterministic_and_matches_oracle(ng, np_side):
     assert r1.astype(np.float64).sum() == pytest.approx(ro.sum(), rel=1e-7)
 
 
-@pytest.mark.parametrize("ng,np_side,ncand", [(32, 32, 10), (64, 32, 6)])
+@pytest.mark.parametrize("ng,np_side,ncand", [(32, 32, 11), (64, 32, 7)])
 def test_deposit_hot_cell_exact(ng, np_side, ncand, monkeypatch):
     """All particles in one cell (late-time clustering extreme): the 32-bit
     windows wrap, every candidate detects it and sends the block to the
-    exact pass, and the integer accumulation stays exact."""
+    exact pass (the candidate that checks while flushing first takes its
+    flushed values back out of the grid), and the integer accumulation stays
+    exact."""
     for pos, cells in ((5.5, 8), (5.0, 1)):
         x = np.full((np_side ** 3, 3), pos, np.float32)
         v = np.zeros_like(x)
@@ -110,7 +112,7 @@ def test_tma_and_plain_strided_passes_bit_identical(ng, monkeypatch):
     assert np.array_equal(out[0], out[1])
 
 
-@pytest.mark.parametrize("ng", [32, 64, 128])
+@pytest.mark.parametrize("ng", [32, 64, 128, 80, 96])
 def test_fused_x_pass_variants_bit_identical(ng, monkeypatch):
     """The persistent TMA-fed Poisson x pass and the plain fused x pass give
     bit-identical forces."""
@@ -136,7 +138,7 @@ def test_deposit_configurations_bit_identical(ng, np_side, disp, monkeypatch):
     (np = ng = 32, 48, 64) and 8^3 blocks (np < ng)."""
     x, v = lattice_state(np_side, ng, disp=disp, vel=1.0, seed=23)
     out = []
-    n = 10 if np_side % 16 == 0 and ng <= np_side else 6
+    n = 11 if np_side % 16 == 0 and ng <= np_side else 7
     for flag in range(n):
         monkeypatch.setenv("HGPM_DEPOSIT", str(flag))
         with make(ng, np_side) as s:
@@ -152,13 +154,13 @@ def test_deposit_configurations_bit_identical(ng, np_side, disp, monkeypatch):
                                              (64, 64, 4.0)])
 def test_kick_variants_bit_identical(ng, np_side, disp, monkeypatch):
     """Every kick candidate (flat global gathers with different CTA shapes
-    and unit runs, the float4-window kick, the gathers of the real potential
-    that form each corner's force as the gradient kernel does) runs the same
-    FP32 arithmetic in the same order; disp 4 spreads blocks past the window
-    caps (global-gather fallback)."""
+    and unit runs, the float4-window kick, the gathers of the real or the
+    paired potential that form each corner's force as the gradient kernel
+    does) runs the same FP32 arithmetic in the same order; disp 4 spreads
+    blocks past the window caps (global-gather fallback)."""
     x, v = lattice_state(np_side, ng, disp=disp, vel=1.0, seed=17)
     out = []
-    for flag in ("0", "1", "2", "3", "4", "5", "6"):
+    for flag in ("0", "1", "2", "3", "4", "5", "6", "7"):
         monkeypatch.setenv("HGPM_KICK", flag)
         with make(ng, np_side) as s:
             s.load_state(x, v)
@@ -297,12 +299,14 @@ def test_bounded_wait_time_out_reported_and_context_usable():
 
 @pytest.mark.parametrize("ng,np_side", [(32, 32), (64, 32)])
 def test_force_grid_on_demand_with_potential_kick(ng, np_side, monkeypatch):
-    """With a kick that gathers the potential the solve writes no force grid;
-    hgpm_get_force forms it from the potential, equal bit for bit to the
-    grid the default solve writes."""
+    """With a kick that gathers the real or the paired potential the solve
+    writes no force grid; hgpm_get_force forms it (for the paired potential
+    from the potential's spectrum first), equal bit for bit to the grid the
+    force-grid kick's solve writes, and the kick after it is unchanged."""
     x, v = lattice_state(np_side, ng, disp=1.5, vel=1.0, seed=37)
     out = []
-    for flag in ("0", "5"):
+    states = []
+    for flag in ("0", "5", "7"):
         monkeypatch.setenv("HGPM_KICK", flag)
         with make(ng, np_side) as s:
             assert s.tuned_choices()["kick"] == int(flag)
@@ -310,4 +314,8 @@ def test_force_grid_on_demand_with_potential_kick(ng, np_side, monkeypatch):
             s.cic()
             s.solve_gradient()
             out.append(s.get_force())
-    assert np.array_equal(out[0], out[1])
+            s.kick_drift(0.0123, 1.7, 0.3, 0.25, 2)
+            states.append(s.store_state())
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
+    for st in states[1:]:
+        assert np.array_equal(states[0][0], st[0]) and np.array_equal(states[0][1], st[1])
