@@ -80,36 +80,73 @@ def first_warmup_step(steps, warmup):
     return max(0, min(MID_STEP, NSTEPS_RUN - steps) - warmup)
 
 # Algorithmic bytes per launch of each kernel (precision-form state:
-# x = 12 B offset + 4 B cell, v = 12 B; FP32 grids).  Sum = 72 Np + 56 Ng.
-def alg_bytes(np3, ng3):
+# x = 12 B offset + 4 B cell, v = 12 B; FP32 grids).
+def alg_bytes(np3, ng3, potential_kick=True):
     """Algorithmic bytes per phase: each input read once, each output
-    written once (FP32, 12 B per force vector).  The gradient is taken in
-    real space, so the x pass moves one spectrum in and one out (8 B/cell)
-    and the inverse z phase (C2R of the potential, 8 B/cell, then the
-    gradient, 4 + 12 B/cell) 24 B/cell: 72 Np + 56 Ng per step."""
+    written once (FP32).  The gradient is taken in real space, so the x pass
+    moves one spectrum in and one out (8 B/cell).  With a kick that gathers
+    the potential, the inverse z phase is the C2R of the potential (4 + 4
+    B/cell) and the kick reads the potential (4 B/cell): 72 Np + 32 Ng per
+    step; with the force-grid kick the inverse z phase adds the gradient (4
+    + 12 B/cell) and the kick reads the force (12 B/cell): 72 Np + 56 Ng."""
     return {
         "deposit": 16 * np3 + 4 * ng3,
         "fft_z_fwd": 8 * ng3,
         "fft_y_fwd": 0,
         "poisson_x": 8 * ng3,
         "fft_y_inv": 0,
-        "fft_z_inv": 24 * ng3,
-        "kick_drift": 56 * np3 + 12 * ng3,
+        "fft_z_inv": (8 if potential_kick else 24) * ng3,
+        "kick_drift": 56 * np3 + (4 if potential_kick else 12) * ng3,
     }
 
 
-# The kernels of each phase (one launch each per step, unless noted).
-KERNEL_NAMES = {
-    "deposit": "deposit_col_kernel<16,4,4,1> (autotuned choice; 32-bit windows, x-half split, wraps from the "
-               "atomics' returned values) + deposit_spill_kernel<16,1,1024> (queued blocks)",
-    "fft_z_fwd": "zpass_r2c_kernel<NG,1>",
-    "fft_y_fwd": "strided_tma_kernel<NG,0,0>",
-    "poisson_x": "xpotential_tma_kernel<NG,256> (forward x, Green's function, inverse x)",
-    "fft_y_inv": "strided_tma_kernel<NG,1,0>",
-    "fft_z_inv": "zpass_c2r_kernel<NG> (the potential) + gradient_kernel<8,3,2> (central differences, float4 force)",
-    "kick_drift": "kick_flat_nt_kernel<16,1024,4> (flat: one particle per thread, a 16^3 block per CTA run "
-                  "as four units of four x-planes, float4 force gathers)",
+# The kernels of each phase (one launch each per step, unless noted); the
+# deposit and kick entries follow the candidate lists of particles.cu.
+DEPOSIT_NAMES = {
+    16: ["deposit_tiled_kernel<16,S,256,3>", "deposit_tiled_kernel<16,S,512,2>", "deposit_tiled_kernel<16,S,1024,1>",
+         "deposit_w32_kernel<16,512,2,1>", "deposit_w32_kernel<16,256,4,1,4>", "deposit_col_kernel<16,4,4,0>",
+         "deposit_col_kernel<16,4,2,0>", "deposit_col_kernel<16,3,4,0>",
+         "deposit_col_kernel<16,4,4,1> (32-bit windows, x-half split, wraps from the atomics' returned values)",
+         "deposit_direct_kernel<16,S,512>", "deposit_col_kernel<16,4,4,2>"],
+    8: ["deposit_tiled_kernel<8,S,256,3>", "deposit_w32_kernel<8,256,4,1,2> (32-bit windows, 13312 cells)",
+        "deposit_col_kernel<8,12,4,0>", "deposit_w32_kernel<8,512,2,1,1>", "deposit_col_kernel<8,12,4,1>",
+        "deposit_direct_kernel<8,S,256>", "deposit_col_kernel<8,12,4,2>"],
 }
+KICK_NAMES = {
+    16: ["kick_flat_nt_kernel<16,1024,4> (float4 force gathers)", "kick_flat_nt_kernel<16,1024,2>",
+         "kick_flat_nt_kernel<16,1024,1>", "kick_spill_kernel<16>", "kick_win4_kernel<16,512> + kick_spill_kernel<16>",
+         "kick_phi_kernel<16,1024,4,0> (potential gathers)", "kick_phi_kernel<16,1024,2,0>",
+         "kick_phi_kernel<16,1024,4,1> (one particle per thread, a 16^3 block per CTA as four units of four "
+         "x-planes; 16 paired-potential gathers form the 8 corner forces)"],
+    8: ["kick_spill_kernel<8>", "kick_flat_nt_kernel<8,512,1>", "kick_flat_nt_kernel<8,512,2>",
+        "kick_flat_nt_kernel<8,256,4>", "kick_win4_kernel<8,512> + kick_spill_kernel<8>",
+        "kick_phi_kernel<8,512,1,0> (32 potential gathers form the 8 corner forces)", "kick_phi_kernel<8,512,2,0>",
+        "kick_phi_kernel<8,512,1,1> (paired potential)"],
+}
+
+
+def kernel_names(tuned, np_side, ng):
+    blk = 16 if np_side % 16 == 0 and ng <= np_side else 8
+    dep, kick = tuned["deposit"]["choice"] if isinstance(tuned["deposit"], dict) else tuned["deposit"], \
+        tuned["kick"]["choice"] if isinstance(tuned["kick"], dict) else tuned["kick"]
+    ypass = tuned["y_pass"]["choice"] if isinstance(tuned["y_pass"], dict) else tuned["y_pass"]
+    xpass = tuned["x_pass"]["choice"] if isinstance(tuned["x_pass"], dict) else tuned["x_pass"]
+    zinv = {7: "zpass_c2r_pair_kernel<NG> (the paired potential)", 5: "zpass_c2r_kernel<NG> (the potential)",
+            6: "zpass_c2r_kernel<NG> (the potential)"}.get(
+        kick, "zpass_c2r_kernel<NG> (the potential) + gradient_kernel<8,3,2> (central differences, float4 force)")
+    spill = "deposit_spill_kernel<%d,S,%d>" % (blk, 1024 if blk == 16 else 512)
+    names = {
+        "deposit": "%s + %s (queued blocks)" % (DEPOSIT_NAMES[blk][dep], spill),
+        "fft_z_fwd": "zpass_r2c_kernel<NG,1>",
+        "fft_y_fwd": "strided_tma_kernel<NG,0,0>" if ypass else "strided_kernel<NG,0>",
+        "poisson_x": ("xpotential_tma_kernel<NG,256>" if xpass else "xfused_kernel<NG,PotentialOp>") +
+                     " (forward x, Green's function, inverse x)",
+        "fft_y_inv": "strided_tma_kernel<NG,1,0>" if ypass else "strided_kernel<NG,1>",
+        "fft_z_inv": zinv,
+        "kick_drift": KICK_NAMES[blk][kick],
+    }
+    small = "1" if ng <= np_side else "0"
+    return {k: v.replace("NG", str(ng)).replace(",S,", "," + small + ",") for k, v in names.items()}
 
 
 def measured_peak():
@@ -557,7 +594,10 @@ def main():
     value = world * np3 * args.steps / (ms_max * 1e-3)
     run_state = {"first_timed_step": start + args.warmup, "a_after": ts.aa}
     peak, peak_kind = measured_peak()
-    ab = alg_bytes(np3, ng3)
+    kick_choice = tuned["kick"]["choice"] if isinstance(tuned["kick"], dict) else tuned["kick"]
+    potential_kick = kick_choice >= 5
+    names = kernel_names(tuned, NP, NG)
+    ab = alg_bytes(np3, ng3, potential_kick)
     phases = {}
     for k, b in ab.items():
         n = int(ph_n.get(k, 0))
@@ -565,27 +605,31 @@ def main():
             continue
         # events bracket the phase (all its kernels) once per step
         avg = ph_ms[k] / args.steps
-        phases[k] = {"ms_per_step": avg, "kernels": n, "alg_bytes": b,
+        phases[k] = {"ms_per_step": avg, "kernels": n, "kernel": names[k], "alg_bytes": b,
                      "alg_gbs": b / (avg * 1e-3) / 1e9 if b else 0.0,
                      "frac_of_peak": (b / (avg * 1e-3) / 1e9 / peak) if b else None}
     dom = max(phases, key=lambda k: phases[k]["ms_per_step"])
     d = phases[dom]
-    roofline = {"bound": "hbm", "kernel": KERNEL_NAMES[dom].replace("NG", str(NG)), "phase": dom,
+    roofline = {"bound": "hbm", "kernel": names[dom], "phase": dom,
                 "achieved": d["alg_gbs"], "peak": peak, "unit": "GB/s", "frac": d["alg_gbs"] / peak,
                 "peak_kind": peak_kind, "traffic": None, "alg_bytes_per_launch": d["alg_bytes"],
                 "ms_per_launch": d["ms_per_step"]}
     step_ms = ms_max / args.steps
-    b_step = sum(alg_bytes(np3, ng3).values())  # 72 Np + 56 Ng
+    b_step = sum(ab.values())  # 72 Np + 32 Ng (potential kick) or 72 Np + 56 Ng
     step_roof = {"alg_bytes_per_step": b_step, "achieved_gbs": b_step / (step_ms * 1e-3) / 1e9,
                  "frac": b_step / (step_ms * 1e-3) / 1e9 / peak, "peak": peak,
                  "survey_bytes_per_step": 72 * np3 + 64 * ng3,
                  "survey_frac": (72 * np3 + 64 * ng3) / (step_ms * 1e-3) / 1e9 / peak}
+    # DRAM bytes per launch from an ncu capture (profiles/traffic_<NG>.json:
+    # per phase the kernel captured and its bytes), used only when the
+    # captured kernel is the one this run timed
     tp = os.path.join(ROOT, "profiles", "traffic_%d.json" % NG)
     if os.path.exists(tp) and NG == NP:
         with open(tp) as f:
             traf = json.load(f)
-        if dom in traf:
-            roofline["traffic"] = traf[dom]
+        t = traf.get(dom)
+        if isinstance(t, dict) and names[dom].startswith(t.get("kernel", "?")):
+            roofline["traffic"] = t["bytes"]
 
     # the CPU baseline on this state (rank 0, N = 1): 2 steps of the OpenMP
     # transcription from the state the timed steps ended with

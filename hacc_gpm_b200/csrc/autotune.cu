@@ -287,7 +287,7 @@ extern "C" int hgpm_autotune(hgpm_ctx* c, int reps, int store, int choices[HGPM_
             ms[i] = time_kick(i, c->force) + (z2 - z1);
             CK(e);
         }
-        pick[HGPM_TUNE_KICK] = hgpm_tune_pick(ms.data(), n, 0, tol);
+        pick[HGPM_TUNE_KICK] = hgpm_tune_pick(ms.data(), n, kick_default(np, ng), tol);
         pms[HGPM_TUNE_KICK] = ms[pick[HGPM_TUNE_KICK]];
     }
     c->kick_choice = pick[HGPM_TUNE_KICK];

@@ -512,6 +512,8 @@ static MCTable multi_table(hgpm_ensemble* E) {
         c.spec = k.spec;
         c.fspec = k.fspec;
         c.spec_elems = k.spec_elems;
+        c.force = k.force;
+        c.force_elems = k.force_elems;
         c.blkwin = k.blkwin;
         c.win_stride = k.win_stride;
         c.spill = k.dep_spill;

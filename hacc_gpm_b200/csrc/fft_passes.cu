@@ -218,16 +218,84 @@ __device__ __forceinline__ void zpass_r2c_body(void* __restrict__ in_, float2* _
     }
 }
 
+// The single-class kernel: zpass_r2c_body's code with the slot prologue
+// written out (as a kernel with its own restrict-qualified parameters it
+// compiles without the body's 76 bytes of spills at 512^3).
 template <int NG, bool FIX>
 __global__ void __launch_bounds__(kThreads, 4) zpass_r2c_kernel(void* __restrict__ in_, float2* __restrict__ out,
                                                              int nlines, int zs, double mean,
                                                              const float2* __restrict__ tw, Slots sl) {
+    constexpr int M = NG / 2, L = Cfg<NG>::L, ES = L + 1;
+    float2* buf = reinterpret_cast<float2*>(hgpm_smem);
     if (slot_idle(sl, blockIdx.y)) return;
     // slot stride s0 counts input elements (int64 when FIX, float otherwise)
     in_ = FIX ? (void*)(reinterpret_cast<unsigned long long*>(in_) + (size_t)blockIdx.y * sl.s0)
               : (void*)(reinterpret_cast<float*>(in_) + (size_t)blockIdx.y * sl.s0);
     out += (size_t)blockIdx.y * sl.s1;
-    zpass_r2c_body<NG, FIX>(in_, out, nlines, zs, mean, tw, blockIdx.x);
+    const int line0 = blockIdx.x * L;
+    constexpr int TOT = L * M;
+    constexpr int PER = (TOT + kThreads - 1) / kThreads;
+    if (FIX) {
+        ulonglong2 q[PER];
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+            const int i = threadIdx.x + t * kThreads;
+            const int l = i / M, m = i % M;
+            q[t] = make_ulonglong2(0ull, 0ull);
+            if (((TOT % kThreads) == 0 || i < TOT) && line0 + l < nlines)
+                q[t] = __ldcs(reinterpret_cast<const ulonglong2*>(reinterpret_cast<unsigned long long*>(in_) +
+                                                                  (size_t)(line0 + l) * NG) + m);
+        }
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+            const int i = threadIdx.x + t * kThreads;
+            const int l = i / M, m = i % M;
+            if (((TOT % kThreads) == 0 || i < TOT)) {
+                if (line0 + l < nlines)
+                    __stcs(reinterpret_cast<ulonglong2*>(reinterpret_cast<unsigned long long*>(in_) +
+                                                         (size_t)(line0 + l) * NG) + m, make_ulonglong2(0ull, 0ull));
+                buf[m * ES + l] = make_float2((float)((double)(long long)q[t].x * kFixInv - mean),
+                                              (float)((double)(long long)q[t].y * kFixInv - mean));
+            }
+        }
+    } else {
+        float2 z[PER];
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+            const int i = threadIdx.x + t * kThreads;
+            const int l = i / M, m = i % M;
+            z[t] = make_float2(0.f, 0.f);
+            if (((TOT % kThreads) == 0 || i < TOT) && line0 + l < nlines)
+                z[t] = reinterpret_cast<const float2*>(reinterpret_cast<const float*>(in_) + (size_t)(line0 + l) * NG)[m];
+        }
+#pragma unroll
+        for (int t = 0; t < PER; ++t) {
+            const int i = threadIdx.x + t * kThreads;
+            if ((TOT % kThreads) == 0 || i < TOT) buf[(i % M) * ES + i / M] = z[t];
+        }
+    }
+    __syncthreads();
+    fft_tile<M, L, ES, false, kThreads, 2>(buf, tw);
+    constexpr int H = M / 2 + 1;
+    for (int i = threadIdx.x; i < L * H; i += kThreads) {
+        const int l = i / H, k = i % H;
+        const int line = line0 + l;
+        if (line >= nlines) continue;
+        const float2 zk = buf[k * ES + l];
+        const float2 zm = buf[((M - k) % M) * ES + l];
+        const float2 w = __ldg(&tw[k]);
+        // E = (Zk + conj Zm)/2, O = -i (Zk - conj Zm)/2, X[k] = E + w O,
+        // X[M-k] = conj(E - w O)
+        const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        const float2 o = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+        const float2 wo = cmul(w, o);
+        float2* dst = out + (size_t)line * zs;
+        dst[k] = cadd(e, wo);
+        if (k != M - k) {
+            const float2 xm = csub(e, wo);
+            dst[M - k] = make_float2(xm.x, -xm.y);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -835,9 +903,8 @@ int pk_max_bins() { return 1024; }
 }  // namespace hgpm
 
 // ===========================================================================
-// Multi-class FFT passes (multi_class.h): one persistent launch per pass over
-// the work units of every class and slot; each CTA serves one class, whose
-// unit u is slot u / per and local unit u % per.  The body is the one the
+// Multi-class FFT passes (multi_class.h): one launch per pass over the work
+// units of every class and slot, one CTA per unit.  The body is the one the
 // single-class kernel runs (the z passes with 256 threads, the y and x passes
 // with 512, for every size: a butterfly's arithmetic does not depend on which
 // thread does it).
@@ -846,16 +913,12 @@ namespace hgpm {
 
 namespace {
 
-// threads and minimum CTAs per SM of each pass: z passes 256 x 2 (the class
-// fields a CTA keeps in registers push the single-class kernels' 64 to 128
-// without spills), y and x passes 512 x 2 (as the single-class ones at 128^3
-// and above)
+// threads and minimum CTAs per SM of each pass (ptxas without spills but for
+// a few bytes, registers 80 / 62 / 64 / 62 / 128): z forward 256 x 3, z
+// inverse to pairs 256 x 2, y and x passes 512 x 2 (as the single-class ones
+// at 128^3 and above)
 template <int PASS> constexpr int mc_threads() { return PASS == 0 || PASS == 4 ? 256 : 512; }
-template <int PASS> constexpr int mc_minb() { return 2; }
-
-__device__ __forceinline__ float* mc_phi(const MCClass& c, int slot) {
-    return reinterpret_cast<float*>(c.fspec + c.spec_elems) + (size_t)slot * 6 * c.spec_elems;
-}
+template <int PASS> constexpr int mc_minb() { return PASS == 0 ? 3 : 2; }
 
 // One unit of each pass for one grid side.
 template <int NG>
@@ -878,35 +941,33 @@ __device__ __forceinline__ void mc_xpot_unit(const MCClass& c, int slot, int lu)
 }
 template <int NG>
 __device__ __forceinline__ void mc_zinv_unit(const MCClass& c, int slot, int lu) {
-    zpass_c2r_body<NG>(c.fspec + (size_t)slot * 3 * c.spec_elems, mc_phi(c, slot), NG * NG, c.zs, 1.0f, c.tw, lu);
+    zpass_c2r_body<NG, true>(c.fspec + (size_t)slot * 3 * c.spec_elems, c.force + (size_t)slot * c.force_elems,
+                             NG * NG, c.zs, 1.0f, c.tw, lu);
 }
 
 // PASS: 0 z forward, 1 y forward, 2 x with the Green's function, 3 y
-// inverse, 4 z inverse.  CTA b of nb serving class c takes units b, b + nb, ...
-template <int NG, int PASS>
-__device__ __forceinline__ void mc_fft_class(const MCClass& c, int per, int b, int nb) {
-    const int total = per * c.nslots;
-    for (int u = b; u < total; u += nb) {
-        const int slot = u / per, lu = u - slot * per;
-        if (c.active && !c.active[slot]) continue;  // the whole CTA skips
-        if (PASS == 0) mc_zfwd_unit<NG>(c, slot, lu);
-        else if (PASS == 1) mc_ypass_unit<NG, false>(c, slot, lu);
-        else if (PASS == 2) mc_xpot_unit<NG>(c, slot, lu);
-        else if (PASS == 3) mc_ypass_unit<NG, true>(c, slot, lu);
-        else mc_zinv_unit<NG>(c, slot, lu);
-        __syncthreads();  // shared memory is reused by the next unit
-    }
-}
-
+// inverse, 4 z inverse.  One CTA per unit: CTA u of the launch is unit u -
+// u0[k] of class k (slot (u - u0[k]) / per[k]).  (A persistent grid whose CTAs
+// each serve one class ran 1.7-2.2x slower at the 96-box ensemble: CTAs
+// shared out by points per unit starve the small sides, whose tiles cost
+// nearly as much as large ones; the block scheduler balances by itself.)
 template <int PASS>
 __global__ void __launch_bounds__(mc_threads<PASS>(), mc_minb<PASS>()) mc_fft_kernel(const __grid_constant__ MCTable t) {
+    const int u = blockIdx.x;
     int k = 0;
-    while (k + 1 < t.n && (int)blockIdx.x >= t.g0[k + 1]) ++k;
+    while (k + 1 < t.n && u >= t.u0[k + 1]) ++k;
     const MCClass& c = t.c[k];
-    const int b = blockIdx.x - t.g0[k], nb = t.g0[k + 1] - t.g0[k];
+    const int r = u - t.u0[k], slot = r / t.per[k], lu = r - slot * t.per[k];
+    if (c.active && !c.active[slot]) return;
     switch (c.ng) {
-#define X(n) \
-    case n: mc_fft_class<n, PASS>(c, t.per[k], b, nb); break;
+#define X(n)                                                     \
+    case n:                                                      \
+        if (PASS == 0) mc_zfwd_unit<n>(c, slot, lu);             \
+        else if (PASS == 1) mc_ypass_unit<n, false>(c, slot, lu); \
+        else if (PASS == 2) mc_xpot_unit<n>(c, slot, lu);        \
+        else if (PASS == 3) mc_ypass_unit<n, true>(c, slot, lu); \
+        else mc_zinv_unit<n>(c, slot, lu);                       \
+        break;
         HGPM_MC_SIZES(X)
 #undef X
     }
@@ -932,31 +993,19 @@ MCPassGeom mc_geom(int ng) {
     return MCPassGeom{0, 0, 0, 0, 0, 0};
 }
 
-// Persistent launch of `kern` (`threads` per CTA, `smem` bytes): the resident
-// CTAs shared out by the classes' unit counts (at least one each).
+// One launch of `kern` (`threads` per CTA, `smem` bytes), one CTA per unit
+// of every class's slots.
 cudaError_t mc_launch(const void* kern, MCTable t, const int* units, int threads, int smem, cudaStream_t s) {
-    int total = 0;
-    for (int k = 0; k < t.n; ++k) total += units[k] * t.c[k].nslots;
-    if (total == 0) return cudaSuccess;
+    t.u0[0] = 0;
+    for (int k = 0; k < t.n; ++k) {
+        t.per[k] = units[k];
+        t.u0[k + 1] = t.u0[k] + units[k] * t.c[k].nslots;
+    }
+    if (t.u0[t.n] == 0) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
-    if (e != cudaSuccess) return e;
-    const int grid = sms * (per_sm > 0 ? per_sm : 1);
-    t.g0[0] = 0;
-    for (int k = 0; k < t.n; ++k) {
-        const int uk = units[k] * t.c[k].nslots;
-        int gk = (int)((long long)grid * uk / total);
-        if (gk < 1) gk = 1;
-        if (gk > uk) gk = uk;
-        t.per[k] = units[k];
-        t.g0[k + 1] = t.g0[k] + gk;
-    }
     void* args[] = {&t};
-    return cudaLaunchKernel(kern, dim3(t.g0[t.n]), dim3(threads), args, smem, s);
+    return cudaLaunchKernel(kern, dim3(t.u0[t.n]), dim3(threads), args, smem, s);
 }
 
 }  // namespace

@@ -107,6 +107,9 @@ bool kick_uses_phi2(int choice);
 // default (used when the choice is -1).
 int deposit_candidates(int np_side, int ng);
 int deposit_default(int np_side, int ng);
+// Built-in kick candidate (without tuning): the paired potential for 16^3
+// blocks, the real potential for 8^3 blocks.
+int kick_default(int np_side, int ng);
 // Blocks too wide for a kernel's window are queued in `spill` (the deposit's
 // and the kick's own lists) and run one particle per thread after the
 // windowed pass, inside the same launcher.

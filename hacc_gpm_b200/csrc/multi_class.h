@@ -5,16 +5,16 @@
 // class (ensemble.cu).  The multi-class step launches each phase ONCE for all
 // classes: the launch's work units are the concatenation of every class's
 // units (deposit: Lagrangian blocks of every slot; FFT passes: line groups or
-// column tiles of every slot; kick: particle units of every slot), and a
-// persistent grid of CTAs walks them.  A CTA finds its unit's class in the
-// table below and runs that class's code for that unit: the same device
-// bodies the single-class kernels run (bit-identical results).  In the FFT
-// passes, whose bodies are compiled per grid side, each CTA of the
-// persistent grid serves one class (CTAs shared out by the classes' unit
-// counts), so each side's code is a loop of its own.  Per step: a counter reset, the
-// deposit, its spill pass, the five FFT passes (z, y, x with the Green's
-// function, y, z), the potential-gather kick with both drifts, and the slot
-// advance: ten launches whatever the number of classes.
+// column tiles of every slot; kick: particle units of every slot).  A CTA
+// finds its unit's class in the table below and runs that class's code for
+// that unit: the same device bodies the single-class kernels run
+// (bit-identical results), the FFT ones dispatched on the class's grid side.
+// The deposit and the kick are persistent grids walking the units; the FFT
+// passes launch one CTA per unit.  Per step: a counter reset, the deposit,
+// its spill pass, the five FFT passes (z, y, x with the Green's function, y,
+// and z to the paired potential), the kick gathering the paired potential
+// with both drifts, and the slot advance: ten launches whatever the number of
+// classes.
 #pragma once
 
 #include "hgpm_device.cuh"
@@ -41,9 +41,11 @@ struct MCClass {
     unsigned long long* rho64 = nullptr;  // slot s at s * ncell
     size_t ncell = 0;
     float2* spec = nullptr;   // forward spectrum, slot s at s * spec_elems
-    float2* fspec = nullptr;  // potential spectrum (slot stride 3 * spec_elems);
-                              // the real potential follows it at + spec_elems
+    float2* fspec = nullptr;  // potential spectrum (slot stride 3 * spec_elems)
     size_t spec_elems = 0;
+    float* force = nullptr;   // force grid space (slot stride force_elems floats):
+                              // the paired potential the kick gathers
+    size_t force_elems = 0;
     int* blkwin = nullptr;    // window records, slot stride win_stride
     size_t win_stride = 0;
     SpillList spill{};
@@ -56,10 +58,7 @@ struct MCClass {
 struct MCTable {
     int n = 0;
     int u0[kMaxMC + 1] = {};  // first global work unit of each class (per phase)
-    // FFT passes: CTAs [g0[k], g0[k+1]) of the launch work on class k, whose
-    // slots have per[k] units each
-    int g0[kMaxMC + 1] = {};
-    int per[kMaxMC] = {};
+    int per[kMaxMC] = {};     // units per slot of each class (FFT passes)
     MCClass c[kMaxMC];
 };
 

@@ -1769,6 +1769,13 @@ int kick_candidates(int np_side, int ng) {
 bool kick_uses_phi(int choice) { return choice >= kKickPhiFirst && choice < kKickCands; }
 bool kick_uses_phi2(int choice) { return choice == kKickPhi2; }
 
+// Measured mid-run, kick plus the z inverse phase that makes what it
+// gathers: 512^3 particles on 512^3 cells (16^3 blocks) 2.51 ms for the
+// paired potential, 2.73 for the real one, 2.78 for the force grid with its
+// gradient kernel; 512^3 on 1024^3 (8^3 blocks) 7.5 / 9.7 / 12.2 ms for the
+// real potential / the paired one / the force grid.
+int kick_default(int np_side, int ng) { return block_side(np_side, ng) == 16 ? kKickPhi2 : kKickPhiFirst; }
+
 int kick_kernels(int choice, int np_side, int ng) {
     (void)np_side;
     (void)ng;
@@ -1965,23 +1972,36 @@ __global__ void __launch_bounds__(1024, 1) mc_spill_kernel(const __grid_constant
                                        c.spill.items + (size_t)slot * c.spill.nblocks, cnt, blockIdx.x, gridDim.x);
 }
 
-// kick_phi_kernel's arithmetic over units of 1024 particles (a quarter of a
-// 16^3 block: four Lagrangian x-planes) of every slot of every class; the
-// slot's scalars come from its schedule row.
+// kick_phi_kernel's arithmetic (the paired potential) over units of 1024
+// particles (a quarter of a 16^3 block: four Lagrangian x-planes) of every
+// slot of every class; the slot's scalars come from its schedule row.  The
+// next unit's particle is loaded before the current one is finished.
 __global__ void __launch_bounds__(1024, 1) mc_kick_kernel(const __grid_constant__ MCTable t) {
     constexpr int B3 = 4096, SUB = 4;
-    for (int u = blockIdx.x; u < t.u0[t.n]; u += gridDim.x) {
-        int k, slot, lu;
-        if (!mc_find(t, u, k, slot, lu)) continue;
+    int u = blockIdx.x, k = 0, slot = 0, lu = 0;
+    // first unit of an active slot at or after u (u = total: none)
+    auto next_active = [&](int v) {
+        for (; v < t.u0[t.n]; v += gridDim.x)
+            if (mc_find(t, v, k, slot, lu)) break;
+        return v;
+    };
+    auto index = [&]() { return (size_t)(lu / SUB) * B3 + (lu % SUB) * 1024 + threadIdx.x; };
+    u = next_active(u);
+    if (u >= t.u0[t.n]) return;
+    PState next = load_p(offset_soa(t.c[k].p, (size_t)slot * t.c[k].part_stride), index());
+    while (u < t.u0[t.n]) {
         const MCClass& c = t.c[k];
-        ParticleSoA p = offset_soa(c.p, (size_t)slot * c.part_stride);
-        const float* phi = reinterpret_cast<const float*>(c.fspec + c.spec_elems) + (size_t)slot * 6 * c.spec_elems;
+        const int cslot = slot;
+        const size_t i = index();
+        const PState cur = next;
+        u = next_active(u + gridDim.x);
+        if (u < t.u0[t.n]) next = load_p(offset_soa(t.c[k].p, (size_t)slot * t.c[k].part_stride), index());
+        ParticleSoA p = offset_soa(c.p, (size_t)cslot * c.part_stride);
+        const float2* phi2 = reinterpret_cast<const float2*>(c.force + (size_t)cslot * c.force_elems);
         float dtf, pf_a = 0.f, pf_b = 0.f;
         int ndrift = 0;
-        kick_scalars(KickSched{c.sched, c.step, c.pitch}, slot, 0.0, 0.0, dtf, pf_a, pf_b, ndrift);
-        const size_t i = (size_t)(lu / SUB) * B3 + (lu % SUB) * 1024 + threadIdx.x;
-        const PState cur = load_p(p, i);
-        finish_p(p, i, cur, gather_phi(phi, cur, KickWeights(cur, dtf), c.ng), pf_a, pf_b, ndrift, c.ng);
+        kick_scalars(KickSched{c.sched, c.step, c.pitch}, cslot, 0.0, 0.0, dtf, pf_a, pf_b, ndrift);
+        finish_p(p, i, cur, gather_phi2(phi2, cur, KickWeights(cur, dtf), c.ng), pf_a, pf_b, ndrift, c.ng);
     }
 }
 

@@ -380,6 +380,7 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
         const char* xt = getenv("HGPM_XTMA");
         if (xt && xt[0] >= '0' && xt[0] <= '1') c->xmode = xt[0] - '0';
         const char* kv = getenv("HGPM_KICK");
+        c->kick_choice = kick_default(p->np, p->ng);
         if (kv && kv[0] >= '0' && kv[0] <= '9' && atoi(kv) < kick_candidates(p->np, p->ng)) c->kick_choice = atoi(kv);
         const char* dv = getenv("HGPM_DEPOSIT");
         if (dv && dv[0] >= '0' && dv[0] <= '9' && atoi(dv) < deposit_candidates(p->np, p->ng)) c->dep_choice = atoi(dv);

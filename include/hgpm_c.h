@@ -267,9 +267,9 @@ int hgpm_ens_release(hgpm_ensemble* ens, int cls, int slot);
 /* nsteps batched steps (slots that finish go idle on the device).         */
 int hgpm_ens_step(hgpm_ensemble* ens, int nsteps);
 int hgpm_ens_use_graph(hgpm_ensemble* ens, int on);
-/* hgpm_ens_step launches each phase once for ALL classes (one persistent
- * launch per phase over every class's and slot's work units; the
- * potential-gather kick; ten launches per step) when `on` (the default),
+/* hgpm_ens_step launches each phase once for ALL classes (one launch per
+ * phase over every class's and slot's work units; the kick gathering the
+ * paired potential; ten launches per step) when `on` (the default),
  * the ensemble has at most 8 classes and every class has 16^3 particle
  * blocks (np a multiple of 16, ng <= np) and ng in {32, 48, 64, 96, 128,
  * 192, 256}; otherwise once per phase per class, the classes on their own

@@ -17,20 +17,35 @@ def _bench():
 
 def test_step_algorithmic_bytes():
     """72 B per particle (the precision-form state read and written by the
-    kick, read by the deposit) and 56 B per cell (density, spectra, potential
-    and the float4 force grid's 12 useful bytes) per step."""
+    kick, read by the deposit) and per cell 32 B with a kick that gathers
+    the potential (density, spectra, potential) or 56 B with the force-grid
+    kick (the float4 grid's 12 useful bytes written and read)."""
     b = _bench()
     for n in (64, 256, 512):
-        a = b.alg_bytes(n ** 3, n ** 3)
-        assert sum(a.values()) == 72 * n ** 3 + 56 * n ** 3
-    assert sum(b.alg_bytes(512 ** 3, 512 ** 3).values()) == 17179869184
+        assert sum(b.alg_bytes(n ** 3, n ** 3).values()) == 72 * n ** 3 + 32 * n ** 3
+        assert sum(b.alg_bytes(n ** 3, n ** 3, False).values()) == 72 * n ** 3 + 56 * n ** 3
+    assert sum(b.alg_bytes(512 ** 3, 512 ** 3, False).values()) == 17179869184
     a = b.alg_bytes(512 ** 3, 1024 ** 3)  # more cells than particles
-    assert sum(a.values()) == 72 * 512 ** 3 + 56 * 1024 ** 3
+    assert sum(a.values()) == 72 * 512 ** 3 + 32 * 1024 ** 3
 
 
 def test_every_phase_has_kernels_named():
+    """Every phase is named for every deposit and kick candidate of both
+    block sides (the candidate lists of particles.cu)."""
     b = _bench()
-    assert set(b.KERNEL_NAMES) == set(b.alg_bytes(8, 8))
+    for np_side, ng, nd in ((512, 512, 11), (512, 1024, 7)):
+        for dep in range(nd):
+            for kick in range(8):
+                for yx in (0, 1):
+                    t = {"deposit": dep, "kick": kick, "y_pass": yx, "x_pass": yx}
+                    names = b.kernel_names(t, np_side, ng)
+                    assert set(names) == set(b.alg_bytes(8, 8)) and all("NG" not in v for v in names.values())
+    t = {"deposit": {"choice": 8, "ms": 1.0}, "kick": {"choice": 7, "ms": 2.0}, "y_pass": {"choice": 1, "ms": 0.2},
+         "x_pass": {"choice": 1, "ms": 0.5}}
+    n = b.kernel_names(t, 512, 512)
+    assert n["kick_drift"].startswith("kick_phi_kernel<16,1024,4,1>")
+    assert n["fft_z_inv"].startswith("zpass_c2r_pair_kernel<512>")
+    assert n["deposit"].startswith("deposit_col_kernel<16,4,4,1>")
 
 
 def test_help_runs_without_a_gpu():
