@@ -913,12 +913,14 @@ namespace hgpm {
 
 namespace {
 
-// threads and minimum CTAs per SM of each pass (ptxas without spills but for
-// a few bytes, registers 80 / 62 / 64 / 62 / 128): z forward 256 x 3, z
-// inverse to pairs 256 x 2, y and x passes 512 x 2 (as the single-class ones
-// at 128^3 and above)
-template <int PASS> constexpr int mc_threads() { return PASS == 0 || PASS == 4 ? 256 : 512; }
-template <int PASS> constexpr int mc_minb() { return PASS == 0 ? 3 : 2; }
+// Threads and minimum CTAs per SM of each pass.  z passes: 256 x 2 (128
+// and 90 registers; the class fields a CTA keeps in registers push the
+// single-class kernels' 64 up).  y and x passes: 512 x 2 (62 / 64 registers;
+// the single-class configuration at 128^3 and above; 256 x 2 at 101 / 104
+// registers measured the same at the 96-box ensemble).
+constexpr int kMCYX = 512;
+template <int PASS> constexpr int mc_threads() { return PASS == 0 || PASS == 4 ? 256 : kMCYX; }
+template <int PASS> constexpr int mc_minb() { return 2; }
 
 // One unit of each pass for one grid side.
 template <int NG>
@@ -930,13 +932,13 @@ template <int NG, bool INV>
 __device__ __forceinline__ void mc_ypass_unit(const MCClass& c, int slot, int lu) {
     float2* data = INV ? c.fspec + (size_t)slot * 3 * c.spec_elems : c.spec + (size_t)slot * c.spec_elems;
     constexpr int ncols = NG / 2 + 1, nch = (ncols + Cfg<NG>::CS - 1) / Cfg<NG>::CS;
-    strided_body<NG, INV, 512>(data, ncols, (size_t)c.zs, (size_t)NG * c.zs, c.tw, lu % nch, lu / nch);
+    strided_body<NG, INV, kMCYX>(data, ncols, (size_t)c.zs, (size_t)NG * c.zs, c.tw, lu % nch, lu / nch);
 }
 template <int NG>
 __device__ __forceinline__ void mc_xpot_unit(const MCClass& c, int slot, int lu) {
     constexpr int ncols = NG / 2 + 1, nch = (ncols + Cfg<NG>::CX - 1) / Cfg<NG>::CX;
     const PotentialOp op{c.cosq, 0.5 / ((double)NG * NG * NG)};
-    xone_body<NG, 512>(c.spec + (size_t)slot * c.spec_elems, c.fspec + (size_t)slot * 3 * c.spec_elems, ncols,
+    xone_body<NG, kMCYX>(c.spec + (size_t)slot * c.spec_elems, c.fspec + (size_t)slot * 3 * c.spec_elems, ncols,
                        (size_t)NG * c.zs, (size_t)c.zs, c.tw, op, lu % nch, lu / nch);
 }
 template <int NG>

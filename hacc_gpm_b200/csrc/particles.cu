@@ -1266,9 +1266,11 @@ __device__ __forceinline__ float3 gather_phi(const float* __restrict__ phi, cons
     const int xm = ix == 0 ? ng - 1 : ix - 1, x1 = ix + 1 == ng ? 0 : ix + 1, x2 = x1 + 1 == ng ? 0 : x1 + 1;
     const int ym = iy == 0 ? ng - 1 : iy - 1, y1 = iy + 1 == ng ? 0 : iy + 1, y2 = y1 + 1 == ng ? 0 : y1 + 1;
     const int zm = iz == 0 ? ng - 1 : iz - 1, z1 = iz + 1 == ng ? 0 : iz + 1, z2 = z1 + 1 == ng ? 0 : z1 + 1;
-    const size_t sx[4] = {(size_t)xm * ng * ng, (size_t)ix * ng * ng, (size_t)x1 * ng * ng, (size_t)x2 * ng * ng};
-    const size_t sy[4] = {(size_t)ym * ng, (size_t)iy * ng, (size_t)y1 * ng, (size_t)y2 * ng};
-    const int sz[4] = {zm, iz, z1, z2};
+    // 32-bit cell indices (ng^3 <= 2^30)
+    const unsigned sx[4] = {(unsigned)(xm * ng), (unsigned)(ix * ng), (unsigned)(x1 * ng), (unsigned)(x2 * ng)};
+    const unsigned sy[4] = {(unsigned)ym, (unsigned)iy, (unsigned)y1, (unsigned)y2};
+    auto row = [&](int a, int b) { return (sx[a] + sy[b]) * (unsigned)ng; };
+    const unsigned sz[4] = {(unsigned)zm, (unsigned)iz, (unsigned)z1, (unsigned)z2};
     // P[a][b][t]: phi(x_a, y_b, z_{t-1}) on the inner columns; X[e][b][cc],
     // Y[a][e][cc]: the x and y faces (e = 0: x-1 / y-1, e = 1: x+2 / y+2)
     float P[2][2][4], X[2][2][2], Y[2][2][2];
@@ -1277,15 +1279,15 @@ __device__ __forceinline__ float3 gather_phi(const float* __restrict__ phi, cons
 #pragma unroll
         for (int b = 0; b < 2; ++b)
 #pragma unroll
-            for (int t = 0; t < 4; ++t) P[a][b][t] = __ldg(&phi[sx[1 + a] + sy[1 + b] + sz[t]]);
+            for (int t = 0; t < 4; ++t) P[a][b][t] = __ldg(&phi[row(1 + a, 1 + b) + sz[t]]);
 #pragma unroll
     for (int e = 0; e < 2; ++e)
 #pragma unroll
         for (int b = 0; b < 2; ++b)
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
-                X[e][b][cc] = __ldg(&phi[sx[3 * e] + sy[1 + b] + sz[1 + cc]]);
-                Y[b][e][cc] = __ldg(&phi[sx[1 + b] + sy[3 * e] + sz[1 + cc]]);
+                X[e][b][cc] = __ldg(&phi[row(3 * e, 1 + b) + sz[1 + cc]]);
+                Y[b][e][cc] = __ldg(&phi[row(1 + b, 3 * e) + sz[1 + cc]]);
             }
     return phi_corner_kick(P, X, Y, w);
 }
@@ -1300,15 +1302,18 @@ __device__ __forceinline__ float3 gather_phi2(const float2* __restrict__ phi2, c
     const int xm = ix == 0 ? ng - 1 : ix - 1, x1 = ix + 1 == ng ? 0 : ix + 1, x2 = x1 + 1 == ng ? 0 : x1 + 1;
     const int ym = iy == 0 ? ng - 1 : iy - 1, y1 = iy + 1 == ng ? 0 : iy + 1, y2 = y1 + 1 == ng ? 0 : y1 + 1;
     const int zm = iz == 0 ? ng - 1 : iz - 1, z1 = iz + 1 == ng ? 0 : iz + 1;
-    const size_t sx[4] = {(size_t)xm * ng * ng, (size_t)ix * ng * ng, (size_t)x1 * ng * ng, (size_t)x2 * ng * ng};
-    const size_t sy[4] = {(size_t)ym * ng, (size_t)iy * ng, (size_t)y1 * ng, (size_t)y2 * ng};
+    // 32-bit cell indices (ng^3 <= 2^30): one wide multiply-add per address
+    const unsigned sx[4] = {(unsigned)(xm * ng), (unsigned)(ix * ng), (unsigned)(x1 * ng), (unsigned)(x2 * ng)};
+    const unsigned sy[4] = {(unsigned)ym, (unsigned)iy, (unsigned)y1, (unsigned)y2};
+    auto row = [&](int a, int b) { return (sx[a] + sy[b]) * (unsigned)ng; };
     float P[2][2][4], X[2][2][2], Y[2][2][2];
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
-            const float2 lo = __ldg(&phi2[sx[1 + a] + sy[1 + b] + zm]);  // z-1, z
-            const float2 hi = __ldg(&phi2[sx[1 + a] + sy[1 + b] + z1]);  // z+1, z+2
+            const unsigned r = row(1 + a, 1 + b);
+            const float2 lo = __ldg(&phi2[r + zm]);  // z-1, z
+            const float2 hi = __ldg(&phi2[r + z1]);  // z+1, z+2
             P[a][b][0] = lo.x;
             P[a][b][1] = lo.y;
             P[a][b][2] = hi.x;
@@ -1318,8 +1323,8 @@ __device__ __forceinline__ float3 gather_phi2(const float2* __restrict__ phi2, c
     for (int e = 0; e < 2; ++e)
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
-            const float2 xf = __ldg(&phi2[sx[3 * e] + sy[1 + b] + iz]);
-            const float2 yf = __ldg(&phi2[sx[1 + b] + sy[3 * e] + iz]);
+            const float2 xf = __ldg(&phi2[row(3 * e, 1 + b) + iz]);
+            const float2 yf = __ldg(&phi2[row(1 + b, 3 * e) + iz]);
             X[e][b][0] = xf.x;
             X[e][b][1] = xf.y;
             Y[b][e][0] = yf.x;
