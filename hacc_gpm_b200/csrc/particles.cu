@@ -145,7 +145,8 @@ struct WinMap {
         mz = div_magic((unsigned)wz_);
         my = div_magic((unsigned)wy_);
     }
-    __device__ __forceinline__ size_t global(int i) const {
+    // 32-bit: ng^3 <= 2^30
+    __device__ __forceinline__ unsigned global(int i) const {
         const int row = (int)div_by((unsigned)i, mz);
         const int cz = i - row * wz;
         const int cx = (int)div_by((unsigned)row, my);
@@ -154,7 +155,7 @@ struct WinMap {
         gx = gx >= ng ? gx - ng : (gx < 0 ? gx + ng : gx);
         gy = gy >= ng ? gy - ng : (gy < 0 ? gy + ng : gy);
         gz = gz >= ng ? gz - ng : (gz < 0 ? gz + ng : gz);
-        return ((size_t)gx * ng + gy) * ng + gz;
+        return ((unsigned)gx * (unsigned)ng + (unsigned)gy) * (unsigned)ng + (unsigned)gz;
     }
 };
 
@@ -503,9 +504,12 @@ __global__ void __launch_bounds__(NT, MINB) deposit_w32_kernel(ParticleSoA p, in
 // wrap check and flush; only blocks whose halves do not fit either (or that
 // wrap) go to deposit_spill_kernel.
 // Adds the column range [k0, k0 + len) into the window.  RET: each atomic
-// returns the cell's old value and a wrap (old + q < old) is recorded in
-// *wrapped; otherwise the sum of the added values is returned for the
-// caller's window-sum check.
+// returns the cell's old value, and *wrapped records whether any old value
+// had its top bit set: an add of v < 2^30 (mass <= 64) can wrap only a cell
+// already at 2^32 - v > 2^31, so every wrap is caught (a cell that passes
+// 2^31 without wrapping, 128 units of weight x mass from one block, is sent
+// to the exact pass too); otherwise the sum of the added values is returned
+// for the caller's window-sum check.
 template <int B, int PF, bool RET>
 __device__ __forceinline__ unsigned long long column_adds(const ParticleSoA& p, int i0, int k0, int len, float mass,
                                                           unsigned* __restrict__ w0, int gx0, int gy0, int gz0,
@@ -513,7 +517,7 @@ __device__ __forceinline__ unsigned long long column_adds(const ParticleSoA& p, 
     constexpr int BB = B * B;
     const int syz = wy * wz;
     unsigned long long added = 0ull;
-    bool wr = false;
+    unsigned acc = 0u;  // OR of the returned old values (RET)
     uint32_t rc[PF];
     float rx[PF], ry[PF], rz[PF];
 #pragma unroll
@@ -553,8 +557,7 @@ __device__ __forceinline__ unsigned long long column_adds(const ParticleSoA& p, 
                     for (int cc = 0; cc < 2; ++cc) {
                         const unsigned v = (unsigned)q[(a * 2 + b) * 2 + cc];
                         if (RET) {
-                            const unsigned old = atomicAdd(&w0[cw + a * syz + b * wz + cc], v);
-                            wr |= old + v < old;
+                            acc |= atomicAdd(&w0[cw + a * syz + b * wz + cc], v);
                         } else {
                             psum += v;
                             atomicAdd(&w0[cw + a * syz + b * wz + cc], v);
@@ -563,7 +566,7 @@ __device__ __forceinline__ unsigned long long column_adds(const ParticleSoA& p, 
             if (!RET) added += psum;
         }
     }
-    if (RET) *wrapped = wr;
+    if (RET) *wrapped = (acc >> 31) != 0u;
     return added;
 }
 
