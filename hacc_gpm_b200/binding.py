@@ -152,6 +152,7 @@ def lib() -> C.CDLL:
         "hgpm_ens_step": (C.c_int, [vp, C.c_int]),
         "hgpm_ens_use_graph": (C.c_int, [vp, C.c_int]),
         "hgpm_ens_multi_launch": (C.c_int, [vp, C.c_int]),
+        "hgpm_fft_c2c": (C.c_int, [vp, C.c_int, C.c_int, vp]),
         "hgpm_ens_sync": (C.c_int, [vp]),
         "hgpm_ens_status": (C.c_int, [vp, C.c_int, C.c_int, P(C.c_int), P(C.c_int)]),
         "hgpm_ens_kernel_launches": (C.c_int64, [vp, C.c_int]),
@@ -284,6 +285,13 @@ def read_ipk(path: str):
 
 def footprint_bytes(ng: int, np_side: int) -> int:
     return lib().hgpm_footprint_bytes(ng, np_side)
+
+
+def fft_c2c(data_ptr: int, ng: int, inverse: bool = False, stream: int = 0):
+    """``serial::forward_fft`` / ``backward_fft`` (ffts.cu:244-294, 397-445) on a
+    device complex64 grid [ng][ng][ng] at data_ptr, in place, unnormalised
+    (hgpm_fft_c2c); stream-ordered on the CUDA stream handle `stream`."""
+    _check(None, lib().hgpm_fft_c2c(C.c_void_p(data_ptr), ng, int(inverse), C.c_void_p(stream)))
 
 
 def write_pk(fname: str, k: np.ndarray, pk: np.ndarray, count: np.ndarray, fold: int = 0):

@@ -479,12 +479,19 @@ static bool multi_ok(const hgpm_ensemble* E) {
     return true;
 }
 
-// The classes as a multi-class table (multi_class.h).
+// The classes as a multi-class table (multi_class.h), the largest boxes
+// first: CTAs are dispatched in unit order, so the last ones to start, which
+// set a launch's tail, are the smallest.
 static MCTable multi_table(hgpm_ensemble* E) {
     MCTable t;
     t.n = (int)E->cls.size();
+    std::vector<int> order(t.n);
+    for (int i = 0; i < t.n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return (double)E->cls[a].np * E->cls[a].np * E->cls[a].np > (double)E->cls[b].np * E->cls[b].np * E->cls[b].np;
+    });
     for (int i = 0; i < t.n; ++i) {
-        EnsClass& k = E->cls[i];
+        EnsClass& k = E->cls[order[i]];
         MCClass& c = t.c[i];
         const int S = k.nslots;
         c.ng = k.ng;

@@ -391,6 +391,35 @@ __global__ void __launch_bounds__(kThreads) zpass_c2r_kernel(const float2* __res
 }
 
 // ---------------------------------------------------------------------------
+// z pass of a complex-to-complex transform of a caller's [ng][ng][ng] grid
+// (forward_fft / backward_fft on a cufftComplex grid, ffts.cu:244-294,
+// 397-445), in place: a CTA transforms CZ<NG> contiguous z lines, staged
+// transposed in shared memory ([m][l], padded) so each stage's butterflies
+// read conflict-free columns.
+template <int NG> struct CZ {
+    static constexpr int L = NG >= 1024 ? 8 : (NG >= 512 ? 16 : (NG >= 128 ? 32 : 64));
+    static constexpr int SMEM = NG * (L + 1) * 8;
+};
+
+template <int NG, bool INV>
+__global__ void __launch_bounds__(kThreads) zpass_c2c_kernel(float2* __restrict__ data, int nlines,
+                                                             const float2* __restrict__ tw) {
+    constexpr int L = CZ<NG>::L, ES = L + 1;
+    float2* buf = reinterpret_cast<float2*>(hgpm_smem);
+    const int line0 = blockIdx.x * L;
+    for (int i = threadIdx.x; i < L * NG; i += kThreads) {
+        const int l = i / NG, m = i % NG;
+        buf[m * ES + l] = line0 + l < nlines ? data[(size_t)(line0 + l) * NG + m] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    fft_tile<NG, L, ES, INV, kThreads>(buf, tw);
+    for (int i = threadIdx.x; i < L * NG; i += kThreads) {
+        const int l = i / NG, m = i % NG;
+        if (line0 + l < nlines) data[(size_t)(line0 + l) * NG + m] = buf[m * ES + l];
+    }
+}
+
+// ---------------------------------------------------------------------------
 // strided pass (y or x lines), in place,
 // blockIdx = (column chunk, plane, slot * ncomp + comp)
 // ---------------------------------------------------------------------------
@@ -815,6 +844,33 @@ cudaError_t launch_zinv(int ng, const float2* in, float* out, int nlines, int zs
     switch (ng) {
 #define X(n) \
     case n: return zinv_impl<n>(in, out, nlines, zs, in_cs, out_cs, ncomp, scale, tw, s, sl, nslots);
+        HGPM_SIZES(X)
+#undef X
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <int NG>
+static cudaError_t c2c_impl(float2* data, bool inv, const float2* tw, cudaStream_t s) {
+    constexpr int L = CZ<NG>::L;
+    const int nlines = NG * NG;
+    auto kz = inv ? zpass_c2c_kernel<NG, true> : zpass_c2c_kernel<NG, false>;
+    cudaError_t e = ensure_smem(kz, CZ<NG>::SMEM);
+    if (e != cudaSuccess) return e;
+    kz<<<cdiv(nlines, L), kThreads, CZ<NG>::SMEM, s>>>(data, nlines, tw);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    // y lines (stride ng, planes x at ng^2), then x lines (stride ng^2,
+    // planes y at ng); the z index is the contiguous column in both
+    e = strided_impl<NG>(inv, data, NG, (size_t)NG, (size_t)NG * NG, NG, 0, 1, tw, s, Slots{}, 1);
+    if (e != cudaSuccess) return e;
+    return strided_impl<NG>(inv, data, NG, (size_t)NG * NG, (size_t)NG, NG, 0, 1, tw, s, Slots{}, 1);
+}
+
+cudaError_t launch_fft_c2c(int ng, float2* data, bool inv, const float2* tw, cudaStream_t s) {
+    switch (ng) {
+#define X(n) \
+    case n: return c2c_impl<n>(data, inv, tw, s);
         HGPM_SIZES(X)
 #undef X
     }

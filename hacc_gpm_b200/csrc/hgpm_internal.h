@@ -46,6 +46,9 @@ cudaError_t launch_zfwd(int ng, void* in, bool fixed, float2* out, int nlines, i
 cudaError_t launch_zinv(int ng, const float2* in, float* out, int nlines, int zs, size_t in_cs, size_t out_cs,
                         int ncomp, float scale, const float2* tw, cudaStream_t s, const Slots& sl = Slots{},
                         int nslots = 1);
+// Unnormalised 3D complex-to-complex FFT of a [ng][ng][ng] float2 grid (z
+// fastest), in place; tw: the ng-point table exp(-2 pi i k / ng).
+cudaError_t launch_fft_c2c(int ng, float2* data, bool inv, const float2* tw, cudaStream_t s);
 // The C2R z pass of one box writing the paired potential (2 ng^3 floats:
 // cell z of a line holds (phi(z), phi(z+1 mod ng))).
 cudaError_t launch_zinv_pair(int ng, const float2* in, float* out, int zs, const float2* tw, cudaStream_t s);

@@ -1950,20 +1950,17 @@ __global__ void mc_prep_kernel(const __grid_constant__ MCTable t) {
     }
 }
 
-// deposit_col_kernel<16, 4, 4, 1> over the blocks of every slot of every class
+// deposit_col_kernel<16, 4, 4, 1> over the blocks of every slot of every
+// class, one CTA per block (a persistent grid walking the blocks took 8 %
+// longer: blocks' windows differ in size across classes)
 __global__ void __launch_bounds__(256, 4) mc_deposit_kernel(const __grid_constant__ MCTable t) {
-    for (int u = blockIdx.x; u < t.u0[t.n]; u += gridDim.x) {
-        int k, slot, blk;
-        if (mc_find(t, u, k, slot, blk)) {
-            const MCClass& c = t.c[k];
-            deposit_col_body<16, 4, 1>(offset_soa(c.p, (size_t)slot * c.part_stride), c.np, c.ng, c.mass,
-                                       c.rho64 + (size_t)slot * c.ncell, kMCDepCap,
-                                       c.blkwin + (size_t)slot * c.win_stride,
-                                       c.spill.items + (size_t)slot * c.spill.nblocks, c.spill.cnt + slot,
-                                       c.spill.over ? c.spill.over + slot : nullptr, blk);
-        }
-        __syncthreads();  // bb, wsum and the window are reused by the next unit
-    }
+    int k, slot, blk;
+    if (!mc_find(t, blockIdx.x, k, slot, blk)) return;
+    const MCClass& c = t.c[k];
+    deposit_col_body<16, 4, 1>(offset_soa(c.p, (size_t)slot * c.part_stride), c.np, c.ng, c.mass,
+                               c.rho64 + (size_t)slot * c.ncell, kMCDepCap, c.blkwin + (size_t)slot * c.win_stride,
+                               c.spill.items + (size_t)slot * c.spill.nblocks, c.spill.cnt + slot,
+                               c.spill.over ? c.spill.over + slot : nullptr, blk);
 }
 
 // deposit_spill_kernel over every slot's queue: blockIdx.y = global slot
@@ -2066,8 +2063,13 @@ cudaError_t mc_step(const MCTable& base, cudaStream_t s) {
     MCTable td = base;
     td.u0[0] = 0;
     for (int k = 0; k < base.n; ++k) td.u0[k + 1] = td.u0[k] + base.c[k].nblocks * base.c[k].nslots;
-    e = mc_persistent((const void*)mc_deposit_kernel, td, 256, kMCDepCap * 4, s);
+    e = smem_attr_once((const void*)mc_deposit_kernel, kMCDepCap * 4);
     if (e != cudaSuccess) return e;
+    {
+        void* dargs[] = {&td};
+        e = cudaLaunchKernel((const void*)mc_deposit_kernel, dim3(td.u0[td.n]), dim3(256), dargs, kMCDepCap * 4, s);
+        if (e != cudaSuccess) return e;
+    }
     {
         const int per = num_sms() / nslots > 1 ? num_sms() / nslots : 1;
         auto ks = mc_spill_kernel;

@@ -10,7 +10,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/hgpm_c.h"
@@ -1164,3 +1167,35 @@ extern "C" int64_t hgpm_kernel_launches(hgpm_ctx* c, int reset) {
 
 extern "C" size_t hgpm_sizeof_params(void) { return sizeof(hgpm_params); }
 extern "C" size_t hgpm_sizeof_timestepper(void) { return sizeof(hgpm_timestepper); }
+
+// serial::forward_fft / backward_fft on a caller's cufftComplex grid
+// (ffts.cu:244-294, 397-445).  Twiddle tables per (device, ng), made on first
+// use and kept until exit.
+extern "C" int hgpm_fft_c2c(void* data_dev, int ng, int inverse, void* stream) {
+    if (!data_dev || !fft_size_supported(ng)) return HGPM_ERR_ARG;
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, float2*> tables;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return HGPM_ERR_CUDA;
+    float2* tw = nullptr;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        auto it = tables.find({dev, ng});
+        if (it != tables.end()) {
+            tw = it->second;
+        } else {
+            const std::vector<float2> t = twiddles(ng);
+            if (cudaMalloc(&tw, ng * sizeof(float2)) != cudaSuccess) return HGPM_ERR_OOM;
+            if (cudaMemcpy(tw, t.data(), ng * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
+                cudaFree(tw);
+                return HGPM_ERR_CUDA;
+            }
+            tables[{dev, ng}] = tw;
+        }
+    }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (launch_fft_c2c(ng, reinterpret_cast<float2*>(data_dev), inverse != 0, tw, s) != cudaSuccess)
+        return HGPM_ERR_CUDA;
+    if (!stream && cudaStreamSynchronize(nullptr) != cudaSuccess) return HGPM_ERR_CUDA;
+    return HGPM_OK;
+}

@@ -14,9 +14,9 @@
 //   * MemoryManager holds an opaque context instead of raw d_pos / d_vel /
 //     d_grid / d_grad pointers (the state lives in HBM as packed cell + FP32
 //     offset; hgpm_store_state_device gives the reference's float3 layout).
-//   * forward_fft / backward_fft on caller-owned cufftComplex grids have no
-//     counterpart: the FFTs are internal to SolveGradient, GetPowerSpectrum
-//     and GenerateDisplacementIC.
+//   * forward_fft / backward_fft take single-precision cufftComplex grids
+//     (floatFFT_t); the reference's double-precision overloads (deviceFFT_t)
+//     and out-of-place forms have no counterpart.
 //   * InitGreens and fft_cache_plan are no-ops (the Green's function is
 //     computed inside the fused Poisson pass; there are no plans).
 //   * GetPowerSpectrum writes folds 0..PK_FOLDS; modes that the reference's
@@ -26,6 +26,7 @@
 
 // the headers the reference's haccgpm.hpp brings to its callers (the
 // driver calls cudaFree(0) and strlen through them)
+#include <cuComplex.h>
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <cstdint>
@@ -38,6 +39,12 @@
 // (src/haccgpm.hpp:18): microseconds since an arbitrary origin.
 typedef unsigned long long CPUTimer_t;
 CPUTimer_t CPUTimer();
+
+// src/haccgpm.hpp:28: the single-precision complex grid type (cufftComplex
+// is cuFloatComplex)
+#ifndef floatFFT_t
+#define floatFFT_t cuFloatComplex
+#endif
 
 namespace HACCGPM {
 
@@ -129,6 +136,11 @@ class MemoryManager {
 };
 
 void fft_cache_plan(int ng);
+// ffts.cu:244-294 / :397-445 with a floatFFT_t grid: the unnormalised 3D C2C
+// transform of d_grid ([ng][ng][ng], device) in place, on the legacy stream,
+// returning when done as the reference's cufftExecC2C + cudaDeviceSynchronize.
+void forward_fft(floatFFT_t* d_grid, int ng, int calls = 0);
+void backward_fft(floatFFT_t* d_grid, int ng, int calls = 0);
 void InitGreens(Params& params, MemoryManager& mem, int calls = 0);
 void GenerateDisplacementIC(MemoryManager& mem, CosmoClass& cosmo, Params& params, Timestepper& ts, int calls = 0);
 void UpdatePositions(Params& params, MemoryManager& mem, Timestepper ts, float frac, int calls = 0);

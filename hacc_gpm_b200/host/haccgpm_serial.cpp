@@ -231,6 +231,16 @@ MemoryManager::~MemoryManager() { hgpm_destroy(ctx); }
 
 void fft_cache_plan(int) {}
 
+// on the legacy stream, returning when done (hgpm_fft_c2c with no stream)
+static void fft_c2c(const char* name, floatFFT_t* d_grid, int ng, int inverse) {
+    const int rc = hgpm_fft_c2c(d_grid, ng, inverse, nullptr);
+    if (rc != HGPM_OK) die(name, rc == HGPM_ERR_ARG ? "unsupported grid size or null grid" : "CUDA error");
+}
+
+void forward_fft(floatFFT_t* d_grid, int ng, int) { fft_c2c("forward_fft", d_grid, ng, 0); }
+
+void backward_fft(floatFFT_t* d_grid, int ng, int) { fft_c2c("backward_fft", d_grid, ng, 1); }
+
 void InitGreens(Params&, MemoryManager&, int) {}
 
 void GenerateDisplacementIC(MemoryManager& mem, CosmoClass& cosmo, Params&, Timestepper&, int) {

@@ -294,6 +294,20 @@ int hgpm_ens_step_class(hgpm_ensemble* ens, int cls, int nsteps);
 int hgpm_ens_class_done(hgpm_ensemble* ens, int cls, int* done);
 int hgpm_ens_sync_class(hgpm_ensemble* ens, int cls);
 
+/* ---- 3D FFT of a caller's grid ----------------------------------------------
+ * serial::forward_fft / backward_fft on a single-precision complex grid
+ * (ffts.cu:244-294 and :397-445 with a cufftComplex grid): the unnormalised
+ * 3D complex-to-complex transform of data_dev ([ng][ng][ng] float2, z
+ * fastest, the reference's get_index order) in place, forward
+ * (exp(-2 pi i k.x / ng), CUFFT_FORWARD) or inverse (exp(+...),
+ * CUFFT_INVERSE), for ng among the supported sides.  The first call for an
+ * ng on a device uploads its twiddle table (kept until exit).  Stream-
+ * ordered on `stream` (a cudaStream_t); with NULL it runs on the legacy
+ * stream and returns when the transform is done (as the reference's
+ * cufftExecC2C + cudaDeviceSynchronize).  Double-precision grids (the
+ * reference's deviceFFT_t) are not supported.                             */
+int hgpm_fft_c2c(void* data_dev, int ng, int inverse, void* stream);
+
 /* ---- allocation-free density ------------------------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory (a host framework that owns every device allocation, or a run that

@@ -171,3 +171,24 @@ def test_footprint_model_monotone(built_lib):
     assert 4 * a < b < 9 * a
     assert 7 * b < H.footprint_bytes(256, 256) < 9 * b
     assert H.footprint_bytes(512, 512) / 2 ** 30 < 12
+
+
+def test_drop_in_header_compiles_the_reference_fft_calls(tmp_path):
+    """A caller of the reference's serial::forward_fft / backward_fft on a
+    floatFFT_t (cufftComplex) grid compiles against the drop-in header."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if not gxx:
+        pytest.skip("no g++")
+    src = tmp_path / "caller.cpp"
+    src.write_text('#include "haccgpm.hpp"\n'
+                   "void f(floatFFT_t* g, int ng) {\n"
+                   "    HACCGPM::serial::forward_fft(g, ng);\n"
+                   "    HACCGPM::serial::backward_fft(g, ng, 1);\n"
+                   "}\n")
+    cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), "-I",
+                        os.path.join(ROOT, "hacc_gpm_b200", "host"), "-I", cuda_inc, str(src)],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
