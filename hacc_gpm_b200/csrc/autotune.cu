@@ -144,7 +144,7 @@ int ctx_apply_tuned(hgpm_ctx* c) {
     if (!getenv("HGPM_KICK") && ch[HGPM_TUNE_KICK] >= 0 && ch[HGPM_TUNE_KICK] < kick_candidates(c->np, c->ng))
         c->kick_choice = ch[HGPM_TUNE_KICK];
     if (!getenv("HGPM_NO_TMA")) c->tma = ch[HGPM_TUNE_YPASS] != 0;
-    if (!getenv("HGPM_XTMA") && ch[HGPM_TUNE_XPASS] >= 0 && ch[HGPM_TUNE_XPASS] <= 1) c->xmode = ch[HGPM_TUNE_XPASS];
+    if (!getenv("HGPM_XTMA") && ch[HGPM_TUNE_XPASS] >= 0 && ch[HGPM_TUNE_XPASS] <= 2) c->xmode = ch[HGPM_TUNE_XPASS];
     return 1;
 }
 
@@ -221,20 +221,25 @@ extern "C" int hgpm_autotune(hgpm_ctx* c, int reps, int store, int choices[HGPM_
         pick[HGPM_TUNE_YPASS] = hgpm_tune_pick(ms, 2, 1, tol);
         pms[HGPM_TUNE_YPASS] = ms[pick[HGPM_TUNE_YPASS]];
     }
-    // x pass with the Green's function: 0 = plain, 1 = TMA-fed
+    // x pass with the Green's function: 0 = plain, 1 = TMA-fed, 2 = plain
+    // with twice the columns per CTA
     {
-        double ms[2];
+        double ms[3];
         const double coeff = 0.5 / ((double)ng * ng * ng);
-        for (int t = 0; t < 2; ++t) {
+        for (int t = 0; t < 3; ++t) {
             ms[t] = time_launches(c, reps, [&] {
-                return t ? launch_xpotential_tma(ng, c->spec, c->fspec, M + 1, c->zs, c->tw_ng, c->cosq, coeff,
-                                                 c->d_err + 1, c->stream)
-                         : launch_xpotential(ng, c->spec, c->fspec, M + 1, (size_t)ng * c->zs, (size_t)c->zs, ng,
-                                             c->tw_ng, c->cosq, coeff, c->stream);
+                if (t == 1)
+                    return launch_xpotential_tma(ng, c->spec, c->fspec, M + 1, c->zs, c->tw_ng, c->cosq, coeff,
+                                                 c->d_err + 1, c->stream);
+                if (t == 2)
+                    return launch_xpotential_wide(ng, c->spec, c->fspec, M + 1, (size_t)ng * c->zs, (size_t)c->zs,
+                                                  ng, c->tw_ng, c->cosq, coeff, c->stream);
+                return launch_xpotential(ng, c->spec, c->fspec, M + 1, (size_t)ng * c->zs, (size_t)c->zs, ng,
+                                         c->tw_ng, c->cosq, coeff, c->stream);
             }, &e);
             CK(e);
         }
-        pick[HGPM_TUNE_XPASS] = hgpm_tune_pick(ms, 2, 1, tol);
+        pick[HGPM_TUNE_XPASS] = hgpm_tune_pick(ms, 3, 1, tol);
         pms[HGPM_TUNE_XPASS] = ms[pick[HGPM_TUNE_XPASS]];
     }
     c->dep_choice = pick[HGPM_TUNE_DEPOSIT];

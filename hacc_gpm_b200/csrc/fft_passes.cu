@@ -461,29 +461,42 @@ __global__ void __launch_bounds__(Cfg<NG>::NTS, 2) strided_kernel(float2* __rest
 // One-output x pass on a loaded tile: forward x FFT, pre() in registers,
 // inverse x FFT, the same stages and arithmetic as xpotential_tma_kernel (bit
 // for bit).
-template <int NG, int NT, class Op>
+template <int NG, int NT, class Op, int C = Cfg<NG>::CX>
 __device__ __forceinline__ void xone_after_load(float2* __restrict__ tile, float2* __restrict__ out, size_t rs,
                                                 int nvalid, const float2* __restrict__ tw, const Op& op, int iy,
                                                 int col0) {
-    constexpr int C = Cfg<NG>::CX;
     fft_tile_fwd_op_inv<NG, C, C, NT, 1, true>(tile, tw,
                                               [&](int ix, int c, float2 v) { return op.pre(ix, iy, col0 + c, v); });
     store_tile<NG, C, NT>(tile, out, rs, nvalid);
 }
 
-// The one-output x pass of column chunk bx of plane (ky) by of one box.
-template <int NG, int NT, class Op>
+// The one-output x pass of column chunk bx (C columns) of plane (ky) by of
+// one box.
+template <int NG, int NT, class Op, int C = Cfg<NG>::CX>
 __device__ __forceinline__ void xone_body(const float2* __restrict__ in, float2* __restrict__ out, int ncols,
                                           size_t rs, size_t ps, const float2* __restrict__ tw, const Op& op, int bx,
                                           int by) {
-    constexpr int C = Cfg<NG>::CX;
     float2* tile = reinterpret_cast<float2*>(hgpm_smem);
     const int col0 = bx * C;
     const size_t off = (size_t)by * ps + col0;
     const int nvalid = ncols - col0;
     load_tile<NG, C, NT>(tile, in + off, rs, nvalid);
     __syncthreads();
-    xone_after_load<NG, NT>(tile, out + off, rs, nvalid, tw, op, by, col0);
+    xone_after_load<NG, NT, Op, C>(tile, out + off, rs, nvalid, tw, op, by, col0);
+}
+
+// The Poisson x pass with twice the columns per CTA (one tile in shared
+// memory, 2 CTAs of 512 threads per SM): more columns in flight per SM for
+// the long lines (1024^3: 8 columns of 1024 points against 4).  Columns stay
+// within the grid side (the Green's function indexes its table by column).
+template <int NG> struct XW {
+    static constexpr int C = 2 * Cfg<NG>::CX <= NG ? 2 * Cfg<NG>::CX : Cfg<NG>::CX;
+};
+template <int NG>
+__global__ void __launch_bounds__(512, 2) xpot_wide_kernel(const float2* __restrict__ in, float2* __restrict__ out,
+                                                           int ncols, size_t rs, size_t ps,
+                                                           const float2* __restrict__ tw, PotentialOp op) {
+    xone_body<NG, 512, PotentialOp, XW<NG>::C>(in, out, ncols, rs, ps, tw, op, blockIdx.x, blockIdx.y);
 }
 
 template <int NG, class Op>
@@ -923,6 +936,29 @@ cudaError_t launch_xpotential(int ng, const float2* in, float2* out, int ncols, 
     switch (ng) {
 #define X(n) \
     case n: return xfused_impl<n, PotentialOp>(in, out, ncols, rs, ps, nplanes, 0, tw, op, s, sl, nslots);
+        HGPM_SIZES(X)
+#undef X
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <int NG>
+static cudaError_t xpot_wide_impl(const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
+                                  const float2* tw, const PotentialOp& op, cudaStream_t s) {
+    constexpr int C = XW<NG>::C, SMEM = NG * C * 8;
+    auto k = xpot_wide_kernel<NG>;
+    cudaError_t e = ensure_smem(k, SMEM);
+    if (e != cudaSuccess) return e;
+    k<<<dim3(cdiv(ncols, C), nplanes), 512, SMEM, s>>>(in, out, ncols, rs, ps, tw, op);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_xpotential_wide(int ng, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
+                                   const float2* tw, const double* cosq, double coeff, cudaStream_t s) {
+    PotentialOp op{cosq, coeff};
+    switch (ng) {
+#define X(n) \
+    case n: return xpot_wide_impl<n>(in, out, ncols, rs, ps, nplanes, tw, op, s);
         HGPM_SIZES(X)
 #undef X
     }

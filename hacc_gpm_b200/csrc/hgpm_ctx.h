@@ -51,8 +51,8 @@ struct hgpm_ctx {
     bool force_valid = false;
     bool phi2_valid = false;  // the paired potential, in the force grid's space
     // kernel variants (environment, read at creation): HGPM_NO_TMA=1 selects the
-    // plain strided y passes, HGPM_XTMA=0|1 the fused x pass: plain or TMA-fed
-    // (the default; 0.48 against 0.53 ms at 512^3).  The deposit
+    // plain strided y passes, HGPM_XTMA=0|1|2 the fused x pass: plain, TMA-fed
+    // (the default) or plain with twice the columns per CTA.  The deposit
     // and kick candidates (bit-identical results) are chosen by the autotuner
     // (hgpm_autotune, or its cache), else HGPM_DEPOSIT / HGPM_KICK, else the
     // built-in defaults (-1 / 0).

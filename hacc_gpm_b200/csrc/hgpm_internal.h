@@ -59,6 +59,9 @@ cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs,
 cudaError_t launch_xpotential(int ng, const float2* in, float2* out, int ncols, size_t rs, size_t ps, int nplanes,
                               const float2* tw, const double* cosq, double coeff, cudaStream_t s,
                               const Slots& sl = Slots{}, int nslots = 1);
+// The same pass with twice the columns per CTA (x pass choice 2).
+cudaError_t launch_xpotential_wide(int ng, const float2* in, float2* out, int ncols, size_t rs, size_t ps,
+                                   int nplanes, const float2* tw, const double* cosq, double coeff, cudaStream_t s);
 // Force grid (F_x, F_y, F_z, 0) from the real potential by central
 // differences (the reference's -i sin(k) gradient, applied in real space).
 cudaError_t launch_gradient(int ng, const float* phi, float4* f, cudaStream_t s, const Slots& sl = Slots{},

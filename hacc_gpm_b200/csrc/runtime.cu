@@ -381,7 +381,7 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
         const char* nt = getenv("HGPM_NO_TMA");
         c->tma = !(nt && nt[0] == '1');
         const char* xt = getenv("HGPM_XTMA");
-        if (xt && xt[0] >= '0' && xt[0] <= '1') c->xmode = xt[0] - '0';
+        if (xt && xt[0] >= '0' && xt[0] <= '2') c->xmode = xt[0] - '0';
         const char* kv = getenv("HGPM_KICK");
         c->kick_choice = kick_default(p->np, p->ng);
         if (kv && kv[0] >= '0' && kv[0] <= '9' && atoi(kv) < kick_candidates(p->np, p->ng)) c->kick_choice = atoi(kv);
@@ -758,9 +758,12 @@ extern "C" int hgpm_solve_gradient(hgpm_ctx* c) {
     {
         PhaseScope ps(c, PH_POISSON);
         const double coeff = 0.5 / ((double)ng * ng * ng);
-        if (c->xmode)
+        if (c->xmode == 1)
             CK(launch_xpotential_tma(ng, c->spec, c->fspec, M + 1, c->zs, c->tw_ng, c->cosq, coeff, c->d_err + 1,
                                      c->stream));
+        else if (c->xmode == 2)
+            CK(launch_xpotential_wide(ng, c->spec, c->fspec, M + 1, (size_t)ng * c->zs, (size_t)c->zs, ng, c->tw_ng,
+                                      c->cosq, coeff, c->stream));
         else
             CK(launch_xpotential(ng, c->spec, c->fspec, M + 1, (size_t)ng * c->zs, (size_t)c->zs, ng, c->tw_ng,
                                  c->cosq, coeff, c->stream));

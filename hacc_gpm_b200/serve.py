@@ -47,9 +47,9 @@ def request_stream(n: int, rate: float = 20.0, seed: int = 7, sizes=(32, 48, 64,
 
 
 # GPU milliseconds of one PM step per particle + cell, for the concurrency
-# cap below: the mid-run 512^3 step on one B200 (5.7 ms for 512^3 particles
+# cap below: the mid-run 512^3 step on one B200 (5.2 ms for 512^3 particles
 # on a 512^3 grid, bench.py).
-STEP_MS_PER_UNIT = 5.7 / (2 * 512 ** 3)
+STEP_MS_PER_UNIT = 5.2 / (2 * 512 ** 3)
 
 
 def class_capacity(sizes, hbm_budget: float, max_slots: int = 64, step_ms: float = None,

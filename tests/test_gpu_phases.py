@@ -114,11 +114,11 @@ def test_tma_and_plain_strided_passes_bit_identical(ng, monkeypatch):
 
 @pytest.mark.parametrize("ng", [32, 64, 128, 80, 96])
 def test_fused_x_pass_variants_bit_identical(ng, monkeypatch):
-    """The persistent TMA-fed Poisson x pass and the plain fused x pass give
-    bit-identical forces."""
+    """The persistent TMA-fed Poisson x pass and the plain fused x pass (with
+    its own or twice the columns per CTA) give bit-identical forces."""
     x, v = lattice_state(ng, ng, disp=1.1, seed=ng + 3)
     out = []
-    for flag in ("0", "1"):
+    for flag in ("0", "1", "2"):
         monkeypatch.setenv("HGPM_XTMA", flag)
         with make(ng) as s:
             s.load_state(x, v)
@@ -126,7 +126,7 @@ def test_fused_x_pass_variants_bit_identical(ng, monkeypatch):
             s.solve_gradient()
             out.append(s.get_force())
             s.sync()
-    assert np.array_equal(out[0], out[1])
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
 
 
 @pytest.mark.parametrize("ng,np_side,disp", [(32, 32, 0.3), (64, 64, 0.3), (64, 64, 2.0), (64, 64, 6.0),
