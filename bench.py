@@ -107,10 +107,11 @@ DEPOSIT_NAMES = {
          "deposit_w32_kernel<16,512,2,1>", "deposit_w32_kernel<16,256,4,1,4>", "deposit_col_kernel<16,4,4,0>",
          "deposit_col_kernel<16,4,2,0>", "deposit_col_kernel<16,3,4,0>",
          "deposit_col_kernel<16,4,4,1> (32-bit windows, x-half split, wraps from the atomics' returned values)",
-         "deposit_direct_kernel<16,S,512>", "deposit_col_kernel<16,4,4,2>"],
+         "deposit_direct_kernel<16,S,512>", "deposit_col_kernel<16,4,4,2>",
+         "deposit_col_kernel<16,4,4,1,1> (32-bit windows, x-half split, returned-value wraps, x-chain merge)"],
     8: ["deposit_tiled_kernel<8,S,256,3>", "deposit_w32_kernel<8,256,4,1,2> (32-bit windows, 13312 cells)",
         "deposit_col_kernel<8,12,4,0>", "deposit_w32_kernel<8,512,2,1,1>", "deposit_col_kernel<8,12,4,1>",
-        "deposit_direct_kernel<8,S,256>", "deposit_col_kernel<8,12,4,2>"],
+        "deposit_direct_kernel<8,S,256>", "deposit_col_kernel<8,12,4,2>", "deposit_col_kernel<8,12,4,1,1>"],
 }
 KICK_NAMES = {
     16: ["kick_flat_nt_kernel<16,1024,4> (float4 force gathers)", "kick_flat_nt_kernel<16,1024,2>",

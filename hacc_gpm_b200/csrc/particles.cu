@@ -510,7 +510,11 @@ __global__ void __launch_bounds__(NT, MINB) deposit_w32_kernel(ParticleSoA p, in
 // 2^31 without wrapping, 128 units of weight x mass from one block, is sent
 // to the exact pass too); otherwise the sum of the added values is returned
 // for the caller's window-sum check.
-template <int B, int PF, bool RET>
+// CHAIN: a particle's 4 upper-x corners are held in registers and merged
+// into the next particle's lower-x corners when its cell is the next in x (the
+// column walks Lagrangian x), saving 4 shared atomics; merged values stay
+// below 2^31 (mass <= 64), so the wrap argument above holds.
+template <int B, int PF, bool RET, bool CHAIN = false>
 __device__ __forceinline__ unsigned long long column_adds(const ParticleSoA& p, int i0, int k0, int len, float mass,
                                                           unsigned* __restrict__ w0, int gx0, int gy0, int gz0,
                                                           int wy, int wz, int ng, bool* wrapped) {
@@ -518,6 +522,12 @@ __device__ __forceinline__ unsigned long long column_adds(const ParticleSoA& p, 
     const int syz = wy * wz;
     unsigned long long added = 0ull;
     unsigned acc = 0u;  // OR of the returned old values (RET)
+    unsigned pend[4] = {0u, 0u, 0u, 0u};  // CHAIN: pending upper-x corners at window cell pw
+    int pw = -1;
+    auto add = [&](int w, unsigned v) {
+        if (RET) acc |= atomicAdd(&w0[w], v);
+        else atomicAdd(&w0[w], v);
+    };
     uint32_t rc[PF];
     float rx[PF], ry[PF], rz[PF];
 #pragma unroll
@@ -547,24 +557,48 @@ __device__ __forceinline__ unsigned long long column_adds(const ParticleSoA& p, 
             cic_q24<true>(cx, cy, cz, mass, q);
             const int cw = (win_rel(cell_x(c), gx0, ng) * wy + win_rel(cell_y(c), gy0, ng)) * wz +
                            win_rel(cell_z(c), gz0, ng);
-            // a particle's 8 values sum to about mass * 2^24 (< 2^31 for mass <= 64)
-            unsigned psum = 0u;
+            unsigned v[8];
 #pragma unroll
-            for (int a = 0; a < 2; ++a)
+            for (int m = 0; m < 8; ++m) v[m] = (unsigned)q[m];
+            if (!RET) {
+                // a particle's 8 values sum to about mass * 2^24 (< 2^31 for mass <= 64)
+                unsigned psum = 0u;
+#pragma unroll
+                for (int m = 0; m < 8; ++m) psum += v[m];
+                added += psum;
+            }
+            if (CHAIN) {
+                if (cw == pw) {
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) v[m] += pend[m];
+                } else if (pw >= 0) {
+#pragma unroll
+                    for (int b = 0; b < 2; ++b)
+#pragma unroll
+                        for (int cc = 0; cc < 2; ++cc) add(pw + b * wz + cc, pend[b * 2 + cc]);
+                }
 #pragma unroll
                 for (int b = 0; b < 2; ++b)
 #pragma unroll
-                    for (int cc = 0; cc < 2; ++cc) {
-                        const unsigned v = (unsigned)q[(a * 2 + b) * 2 + cc];
-                        if (RET) {
-                            acc |= atomicAdd(&w0[cw + a * syz + b * wz + cc], v);
-                        } else {
-                            psum += v;
-                            atomicAdd(&w0[cw + a * syz + b * wz + cc], v);
-                        }
-                    }
-            if (!RET) added += psum;
+                    for (int cc = 0; cc < 2; ++cc) add(cw + b * wz + cc, v[b * 2 + cc]);
+#pragma unroll
+                for (int m = 0; m < 4; ++m) pend[m] = v[4 + m];
+                pw = cw + syz;
+            } else {
+#pragma unroll
+                for (int a = 0; a < 2; ++a)
+#pragma unroll
+                    for (int b = 0; b < 2; ++b)
+#pragma unroll
+                        for (int cc = 0; cc < 2; ++cc) add(cw + a * syz + b * wz + cc, v[(a * 2 + b) * 2 + cc]);
+            }
         }
+    }
+    if (CHAIN && pw >= 0) {
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) add(pw + b * wz + cc, pend[b * 2 + cc]);
     }
     if (RET) *wrapped = (acc >> 31) != 0u;
     return added;
@@ -580,7 +614,7 @@ __device__ __forceinline__ unsigned long long column_adds(const ParticleSoA& p, 
 //      (in practice never at the workloads' densities) is taken back out of
 //      the grid by adding the negated values, so the grid's integers are
 //      those of the other checks.
-template <int B, int PF, int CHK>
+template <int B, int PF, int CHK, bool CHAIN = false>
 __device__ __forceinline__ bool column_pass(const ParticleSoA& p, int i0, int k0, int len, float mass,
                                             unsigned* __restrict__ w0, long long* wsum, const int* box, int ox,
                                             int oy, int oz, int ng, unsigned long long* __restrict__ rho) {
@@ -594,7 +628,7 @@ __device__ __forceinline__ bool column_pass(const ParticleSoA& p, int i0, int k0
     __syncthreads();
     bool wrapped = false;
     const unsigned long long added =
-        column_adds<B, PF, RET>(p, i0, k0, len, mass, w0, gx0, gy0, gz0, wy, wz, ng, &wrapped);
+        column_adds<B, PF, RET, CHAIN>(p, i0, k0, len, mass, w0, gx0, gy0, gz0, wy, wz, ng, &wrapped);
     long long tot = 0;
     if (CHK == 2) {
         __syncthreads();
@@ -647,7 +681,7 @@ __device__ __forceinline__ bool column_pass(const ParticleSoA& p, int i0, int k0
 // Block blk of one box: p, rho, recs (window records, may be null), the
 // box's spill queue (items, cnt) and wide-window counter (over, may be
 // null).  The single-class kernel below and the multi-class deposit run it.
-template <int B, int PF, int CHK>
+template <int B, int PF, int CHK, bool CHAIN = false>
 __device__ __forceinline__ void deposit_col_body(ParticleSoA p, int np_side, int ng, float mass,
                                                  unsigned long long* __restrict__ rho, int cap_cells,
                                                  int* __restrict__ recs, int* __restrict__ items, int* cnt,
@@ -719,15 +753,15 @@ __device__ __forceinline__ void deposit_col_body(ParticleSoA p, int np_side, int
     // flushed); at most one item per block
     int queue = -1;
     if (vol <= cap_cells) {
-        if (!column_pass<B, PF, CHK>(p, tid, 0, B, mass, w0, wsum, bb, ox, oy, oz, ng, rho)) queue = 0;
+        if (!column_pass<B, PF, CHK, CHAIN>(p, tid, 0, B, mass, w0, wsum, bb, ox, oy, oz, ng, rho)) queue = 0;
     } else {
         auto hvol = [&](int h) {
             const int* q = bb + 6 + 6 * h;
             return (long long)(q[3] - q[0] + 2) * (q[4] - q[1] + 2) * (q[5] - q[2] + 2);
         };
         if (hvol(0) <= cap_cells && hvol(1) <= cap_cells) {
-            if (!column_pass<B, PF, CHK>(p, tid, 0, B / 2, mass, w0, wsum, bb + 6, ox, oy, oz, ng, rho)) queue = 0;
-            else if (!column_pass<B, PF, CHK>(p, tid, B / 2, B / 2, mass, w0, wsum, bb + 12, ox, oy, oz, ng, rho))
+            if (!column_pass<B, PF, CHK, CHAIN>(p, tid, 0, B / 2, mass, w0, wsum, bb + 6, ox, oy, oz, ng, rho)) queue = 0;
+            else if (!column_pass<B, PF, CHK, CHAIN>(p, tid, B / 2, B / 2, mass, w0, wsum, bb + 12, ox, oy, oz, ng, rho))
                 queue = 2;
         } else {
             queue = 0;
@@ -736,13 +770,13 @@ __device__ __forceinline__ void deposit_col_body(ParticleSoA p, int np_side, int
     if (queue >= 0 && tid == 0) items[atomicAdd(cnt, 1)] = blk * 4 + queue;
 }
 
-template <int B, int MINB, int PF, int CHK = 0>
+template <int B, int MINB, int PF, int CHK = 0, bool CHAIN = false>
 __global__ void __launch_bounds__(B * B, MINB) deposit_col_kernel(ParticleSoA p, int np_side, int ng, float mass,
                                                                   unsigned long long* __restrict__ rho, int cap_cells,
                                                                   int* __restrict__ blkwin, SpillList spill, Slots sl) {
     const int slot = blockIdx.y;
     if (slot_idle(sl, slot)) return;
-    deposit_col_body<B, PF, CHK>(offset_soa(p, (size_t)slot * sl.s0), np_side, ng, mass, rho + (size_t)slot * sl.s1,
+    deposit_col_body<B, PF, CHK, CHAIN>(offset_soa(p, (size_t)slot * sl.s0), np_side, ng, mass, rho + (size_t)slot * sl.s1,
                                  cap_cells, blkwin ? blkwin + (size_t)slot * sl.s2 : nullptr,
                                  spill.items + (size_t)slot * spill.nblocks, spill.cnt + slot,
                                  spill.over ? spill.over + slot : nullptr, blockIdx.x);
@@ -1633,7 +1667,7 @@ struct DepositCfg {
     int nt, cap, cell_bytes;
 };
 
-constexpr int kDepositCands = 11;
+constexpr int kDepositCands = 12;
 
 // Candidates per block side; index = HGPM_DEPOSIT (or the tuned choice).
 //   16^3 blocks: 0-2 (lo, hi) 16-bit-split windows (deposit_tiled_kernel) with
@@ -1643,11 +1677,13 @@ constexpr int kDepositCands = 11;
 //   with a 4- or 2-deep ring, 3 CTAs per SM with 18432-cell windows, and 4
 //   CTAs per SM detecting wraps from the atomics' returned values; 9 direct
 //   (deposit_direct_kernel: no window, every weight to the int64 grid); 10
-//   the column kernel with the wrap check folded into the flush.
+//   the column kernel with the wrap check folded into the flush; 11 the
+//   default column kernel with the x-chain merge (column_adds CHAIN).
 //   8^3 blocks: 0 split window, 1 32-bit window (256 threads, 13312 cells),
 //   2 column kernel (64 threads, 4096 cells), 3 32-bit window (512 threads,
 //   kBigCap cells), 4 column kernel with returned-value wrap detection, 5
-//   direct, 6 column kernel with the check in the flush.
+//   direct, 6 column kernel with the check in the flush, 7 column kernel with
+//   returned-value wraps and the x-chain merge.
 // The 32-bit windows need mass <= 64; otherwise the split window of the same
 // thread count runs.
 template <int B, bool SMALL>
@@ -1672,6 +1708,7 @@ static int deposit_candidates(int cap_default, bool w32, DepositCfg* out) {
         }
         out[n++] = {deposit_direct_kernel<B, SMALL, 512>, 512, 0, 0};
         out[n++] = w32 ? DepositCfg{deposit_col_kernel<B, 4, 4, 2>, 256, 13312, 4} : out[0];
+        out[n++] = w32 ? DepositCfg{deposit_col_kernel<B, 4, 4, 1, true>, 256, 13312, 4} : out[0];
     } else {
         out[n++] = {deposit_tiled_kernel<B, SMALL, 256, 3>, 256, cap_default, 8};
         if (w32) {
@@ -1684,6 +1721,7 @@ static int deposit_candidates(int cap_default, bool w32, DepositCfg* out) {
         }
         out[n++] = {deposit_direct_kernel<B, SMALL, 256>, 256, 0, 0};
         out[n++] = w32 ? DepositCfg{deposit_col_kernel<B, 12, 4, 2>, B * B, 4096, 4} : out[0];
+        out[n++] = w32 ? DepositCfg{deposit_col_kernel<B, 12, 4, 1, true>, B * B, 4096, 4} : out[0];
     }
     return n;
 }
@@ -1731,7 +1769,7 @@ static cudaError_t deposit_impl(const ParticleSoA& p, int np_side, int ng, float
     return cudaGetLastError();
 }
 
-int deposit_candidates(int np_side, int ng) { return block_side(np_side, ng) == 16 ? kDepositCands : 7; }
+int deposit_candidates(int np_side, int ng) { return block_side(np_side, ng) == 16 ? kDepositCands : 8; }
 
 int deposit_default(int np_side, int ng) {
     return block_side(np_side, ng) == 16 ? deposit_default_choice<16>(np_side, ng)

@@ -33,7 +33,7 @@ def test_every_phase_has_kernels_named():
     """Every phase is named for every deposit and kick candidate of both
     block sides (the candidate lists of particles.cu)."""
     b = _bench()
-    for np_side, ng, nd in ((512, 512, 11), (512, 1024, 7)):
+    for np_side, ng, nd in ((512, 512, 12), (512, 1024, 8)):
         for dep in range(nd):
             for kick in range(8):
                 for yx in (0, 1):

@@ -61,7 +61,7 @@ def test_deposit_deterministic_and_matches_oracle(ng, np_side):
     assert r1.astype(np.float64).sum() == pytest.approx(ro.sum(), rel=1e-7)
 
 
-@pytest.mark.parametrize("ng,np_side,ncand", [(32, 32, 11), (64, 32, 7)])
+@pytest.mark.parametrize("ng,np_side,ncand", [(32, 32, 12), (64, 32, 8)])
 def test_deposit_hot_cell_exact(ng, np_side, ncand, monkeypatch):
     """All particles in one cell (late-time clustering extreme): the 32-bit
     windows wrap, every candidate detects it and sends the block to the
@@ -138,7 +138,7 @@ def test_deposit_configurations_bit_identical(ng, np_side, disp, monkeypatch):
     (np = ng = 32, 48, 64) and 8^3 blocks (np < ng)."""
     x, v = lattice_state(np_side, ng, disp=disp, vel=1.0, seed=23)
     out = []
-    n = 11 if np_side % 16 == 0 and ng <= np_side else 7
+    n = 12 if np_side % 16 == 0 and ng <= np_side else 8
     for flag in range(n):
         monkeypatch.setenv("HGPM_DEPOSIT", str(flag))
         with make(ng, np_side) as s:
