@@ -140,7 +140,8 @@ def kernel_names(tuned, np_side, ng):
         "deposit": "%s + %s (queued blocks)" % (DEPOSIT_NAMES[blk][dep], spill),
         "fft_z_fwd": "zpass_r2c_kernel<NG,1>",
         "fft_y_fwd": "strided_tma_kernel<NG,0,0>" if ypass else "strided_kernel<NG,0>",
-        "poisson_x": ("xpotential_tma_kernel<NG,256>" if xpass else "xfused_kernel<NG,PotentialOp>") +
+        "poisson_x": {0: "xfused_kernel<NG,PotentialOp>", 1: "xpotential_tma_kernel<NG,256>"}.get(
+            xpass, "xpot_wide_kernel<NG> (twice the columns per CTA)") +
                      " (forward x, Green's function, inverse x)",
         "fft_y_inv": "strided_tma_kernel<NG,1,0>" if ypass else "strided_kernel<NG,1>",
         "fft_z_inv": zinv,

@@ -239,7 +239,7 @@ extern "C" int hgpm_autotune(hgpm_ctx* c, int reps, int store, int choices[HGPM_
             }, &e);
             CK(e);
         }
-        pick[HGPM_TUNE_XPASS] = hgpm_tune_pick(ms, 3, 1, tol);
+        pick[HGPM_TUNE_XPASS] = hgpm_tune_pick(ms, 3, 2, tol);
         pms[HGPM_TUNE_XPASS] = ms[pick[HGPM_TUNE_XPASS]];
     }
     c->dep_choice = pick[HGPM_TUNE_DEPOSIT];

@@ -51,13 +51,14 @@ struct hgpm_ctx {
     bool force_valid = false;
     bool phi2_valid = false;  // the paired potential, in the force grid's space
     // kernel variants (environment, read at creation): HGPM_NO_TMA=1 selects the
-    // plain strided y passes, HGPM_XTMA=0|1|2 the fused x pass: plain, TMA-fed
-    // (the default) or plain with twice the columns per CTA.  The deposit
+    // plain strided y passes, HGPM_XTMA=0|1|2 the fused x pass: plain, TMA-fed,
+    // or plain with twice the columns per CTA (the default: 0.43 ms against
+    // 0.48 TMA-fed at 512^3, 4.3 against 6.2 plain at 1024^3).  The deposit
     // and kick candidates (bit-identical results) are chosen by the autotuner
     // (hgpm_autotune, or its cache), else HGPM_DEPOSIT / HGPM_KICK, else the
     // built-in defaults (-1 / 0).
     bool tma = true;
-    int xmode = 1;
+    int xmode = 2;
     int dep_choice = -1;
     int kick_choice = 0;
     float* stage = nullptr;     // AoS float3 x, v staging (lazy)

@@ -335,8 +335,8 @@ int hgpm_cic_density_noalloc(const float* x_dev, int np_side, int ng, float* rho
  *   HGPM_TUNE_DEPOSIT  deposit window kernel / CTA shape / window cap,
  *   HGPM_TUNE_KICK     kick gather scheme / CTA shape / units per CTA turn,
  *   HGPM_TUNE_YPASS    1 = TMA-fed persistent y pass, 0 = plain strided,
- *   HGPM_TUNE_XPASS    1 = TMA-fed persistent x pass, 0 = plain, 2 = plain
- *                      with twice the columns per CTA.
+ *   HGPM_TUNE_XPASS    2 = plain x pass with twice the columns per CTA (the
+ *                      default), 1 = TMA-fed persistent, 0 = plain.
  * hgpm_autotune times every candidate `reps` times on the context's current
  * particle state (which it leaves unchanged), keeps a knob's default unless
  * another candidate is faster by more than 2 %, applies the winners to the

@@ -36,8 +36,8 @@ def test_every_phase_has_kernels_named():
     for np_side, ng, nd in ((512, 512, 12), (512, 1024, 8)):
         for dep in range(nd):
             for kick in range(8):
-                for yx in (0, 1):
-                    t = {"deposit": dep, "kick": kick, "y_pass": yx, "x_pass": yx}
+                for yx in (0, 1, 2):
+                    t = {"deposit": dep, "kick": kick, "y_pass": min(yx, 1), "x_pass": yx}
                     names = b.kernel_names(t, np_side, ng)
                     assert set(names) == set(b.alg_bytes(8, 8)) and all("NG" not in v for v in names.values())
     t = {"deposit": {"choice": 8, "ms": 1.0}, "kick": {"choice": 7, "ms": 2.0}, "y_pass": {"choice": 1, "ms": 0.2},
