@@ -1028,9 +1028,9 @@ __device__ __forceinline__ void mc_ypass_unit(const MCClass& c, int slot, int lu
 }
 template <int NG>
 __device__ __forceinline__ void mc_xpot_unit(const MCClass& c, int slot, int lu) {
-    constexpr int ncols = NG / 2 + 1, nch = (ncols + Cfg<NG>::CX - 1) / Cfg<NG>::CX;
+    constexpr int ncols = NG / 2 + 1, nch = (ncols + XW<NG>::C - 1) / XW<NG>::C;
     const PotentialOp op{c.cosq, 0.5 / ((double)NG * NG * NG)};
-    xone_body<NG, kMCYX>(c.spec + (size_t)slot * c.spec_elems, c.fspec + (size_t)slot * 3 * c.spec_elems, ncols,
+    xone_body<NG, kMCYX, PotentialOp, XW<NG>::C>(c.spec + (size_t)slot * c.spec_elems, c.fspec + (size_t)slot * 3 * c.spec_elems, ncols,
                        (size_t)NG * c.zs, (size_t)c.zs, c.tw, op, lu % nch, lu / nch);
 }
 template <int NG>
@@ -1078,8 +1078,8 @@ MCPassGeom mc_geom(int ng) {
     case n: {                                                                                           \
         const int ncols = n / 2 + 1;                                                                    \
         return MCPassGeom{(n * n + Cfg<n>::L - 1) / Cfg<n>::L, (ncols + Cfg<n>::CS - 1) / Cfg<n>::CS * n, \
-                          (ncols + Cfg<n>::CX - 1) / Cfg<n>::CX * n, Cfg<n>::ZSMEM, Cfg<n>::SSMEM,        \
-                          n * Cfg<n>::CX * 8};                                                          \
+                          (ncols + XW<n>::C - 1) / XW<n>::C * n, Cfg<n>::ZSMEM, Cfg<n>::SSMEM,            \
+                          n * XW<n>::C * 8};                                                            \
     }
         HGPM_MC_SIZES(X)
 #undef X
