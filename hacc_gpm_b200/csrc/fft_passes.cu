@@ -304,12 +304,8 @@ __global__ void __launch_bounds__(kThreads, 4) zpass_r2c_kernel(void* __restrict
 // X[0] and X[ng/2] are taken as real (Hermitian extension), which makes the
 // result equal to the real part of the reference's full C2C inverse.
 // ---------------------------------------------------------------------------
-// PAIR: out holds the paired potential the pair-gathering kick reads
-// (pair_row / hgpm_device.cuh): line l's row starts at pair 1 + l (NG + 2);
-// its pair k, 0 <= k <= NG + 1, is (phi(k - 1), phi(k)) with z taken mod NG,
-// so the pairs a particle at z needs, (z-1, z), (z, z+1) and (z+1, z+2), are
-// pairs z, z + 1 and z + 2 with no wrap; a thread's two pairs 2m + 1, 2m + 2
-// are one aligned 16-byte store.
+// PAIR: out holds nlines * NG pairs, cell z of a line (phi(z), phi(z+1 mod
+// NG)) (the paired potential the pair-gathering kick reads).
 template <int NG, bool PAIR = false>
 __device__ __forceinline__ void zpass_c2r_body(const float2* __restrict__ in, float* __restrict__ out, int nlines,
                                                int zs, float scale, const float2* __restrict__ tw, int bx) {
@@ -365,15 +361,10 @@ __device__ __forceinline__ void zpass_c2r_body(const float2* __restrict__ in, fl
         if (line >= nlines) continue;
         const float2 z = buf[m * ES + l];
         if (PAIR) {
-            // pairs 2m + 1, 2m + 2: (phi(2m), phi(2m+1)), (phi(2m+1), phi(2m+2))
-            float2* row = reinterpret_cast<float2*>(out) + pair_row(line, NG);
+            // cells 2m and 2m+1: (phi(2m), phi(2m+1)), (phi(2m+1), phi(2m+2))
             const float nx = buf[(m + 1 == M ? 0 : m + 1) * ES + l].x * scale;
-            *reinterpret_cast<float4*>(row + 2 * m + 1) = make_float4(z.x * scale, z.y * scale, z.y * scale, nx);
-            if (m == 0) {
-                // the row's ends: pair 0 = (phi(NG-1), phi(0)), pair NG+1 = (phi(0), phi(1))
-                row[0] = make_float2(buf[(M - 1) * ES + l].y * scale, z.x * scale);
-                row[NG + 1] = make_float2(z.x * scale, z.y * scale);
-            }
+            reinterpret_cast<float4*>(out + (size_t)line * NG * 2)[m] =
+                make_float4(z.x * scale, z.y * scale, z.y * scale, nx);
         } else {
             reinterpret_cast<float2*>(out + (size_t)line * NG)[m] = make_float2(z.x * scale, z.y * scale);
         }

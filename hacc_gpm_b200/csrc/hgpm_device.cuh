@@ -74,15 +74,6 @@ struct KickSched {
     int pitch = 0;
 };
 
-// First pair of line l = x * ng + y in the paired potential: a row of ng + 2
-// pairs per line after one leading pad pair, so the row's pair 1 (and every
-// odd pair) starts on a 16-byte boundary.
-__host__ __device__ __forceinline__ unsigned pair_row(unsigned l, int ng) { return 1u + l * (unsigned)(ng + 2); }
-// Floats of the paired potential of an ng^3 grid.
-__host__ __device__ __forceinline__ size_t pair_floats(int ng) {
-    return 2 * (1 + (size_t)ng * ng * (size_t)(ng + 2));
-}
-
 // Signed mode index as get_kmodes maps it (src/haccgpm.hpp:255-274).
 __host__ __device__ __forceinline__ int signed_mode(int i, int n) { return i > n / 2 - 1 ? i - n : i; }
 

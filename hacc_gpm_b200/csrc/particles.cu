@@ -1329,28 +1329,28 @@ __device__ __forceinline__ float3 gather_phi(const float* __restrict__ phi, cons
     return phi_corner_kick(P, X, Y, w);
 }
 
-// The paired potential (zpass_c2r_kernel with PAIR; rows of ng + 2 pairs,
-// pair k of a row = (phi(k - 1), phi(k)), pair_row): the 4 z values of an
-// inner column are pairs z and z + 2 of its row, the 2 of a face column pair
-// z + 1, with no wrap in z: 16 loads instead of 32 and one address per row,
-// the same values, the same forces (bit-identical to gather_phi).
+// The paired potential (zpass_c2r_kernel with PAIR): cell z holds
+// (phi(z), phi(z+1)), so the 4 z values of an inner column are two 8-byte
+// loads and the 2 of a face column one: 16 loads instead of 32, the same
+// values, the same forces (bit-identical to gather_phi).
 __device__ __forceinline__ float3 gather_phi2(const float2* __restrict__ phi2, const PState& c, const KickWeights& w,
                                               int ng) {
     const int ix = cell_x(c.c), iy = cell_y(c.c), iz = cell_z(c.c);
     const int xm = ix == 0 ? ng - 1 : ix - 1, x1 = ix + 1 == ng ? 0 : ix + 1, x2 = x1 + 1 == ng ? 0 : x1 + 1;
     const int ym = iy == 0 ? ng - 1 : iy - 1, y1 = iy + 1 == ng ? 0 : iy + 1, y2 = y1 + 1 == ng ? 0 : y1 + 1;
-    // 32-bit pair indices (ng^2 (ng + 2) < 2^31 for ng <= 1024)
+    const int zm = iz == 0 ? ng - 1 : iz - 1, z1 = iz + 1 == ng ? 0 : iz + 1;
+    // 32-bit cell indices (ng^3 <= 2^30): one wide multiply-add per address
     const unsigned sx[4] = {(unsigned)(xm * ng), (unsigned)(ix * ng), (unsigned)(x1 * ng), (unsigned)(x2 * ng)};
     const unsigned sy[4] = {(unsigned)ym, (unsigned)iy, (unsigned)y1, (unsigned)y2};
-    auto col = [&](int a, int b) { return phi2 + (pair_row(sx[a] + sy[b], ng) + (unsigned)iz); };
+    auto row = [&](int a, int b) { return (sx[a] + sy[b]) * (unsigned)ng; };
     float P[2][2][4], X[2][2][2], Y[2][2][2];
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
-            const float2* q = col(1 + a, 1 + b);
-            const float2 lo = __ldg(q);      // z-1, z
-            const float2 hi = __ldg(q + 2);  // z+1, z+2
+            const unsigned r = row(1 + a, 1 + b);
+            const float2 lo = __ldg(&phi2[r + zm]);  // z-1, z
+            const float2 hi = __ldg(&phi2[r + z1]);  // z+1, z+2
             P[a][b][0] = lo.x;
             P[a][b][1] = lo.y;
             P[a][b][2] = hi.x;
@@ -1360,8 +1360,8 @@ __device__ __forceinline__ float3 gather_phi2(const float2* __restrict__ phi2, c
     for (int e = 0; e < 2; ++e)
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
-            const float2 xf = __ldg(col(3 * e, 1 + b) + 1);  // z, z+1
-            const float2 yf = __ldg(col(1 + b, 3 * e) + 1);
+            const float2 xf = __ldg(&phi2[row(3 * e, 1 + b) + iz]);
+            const float2 yf = __ldg(&phi2[row(1 + b, 3 * e) + iz]);
             X[e][b][0] = xf.x;
             X[e][b][1] = xf.y;
             Y[b][e][0] = yf.x;
