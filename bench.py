@@ -126,7 +126,9 @@ KICK_NAMES = {
 }
 
 
-def kernel_names(tuned, np_side, ng):
+def kernel_names(tuned, np_side, ng, plane=None):
+    if plane is None:
+        plane = os.environ.get("HGPM_PLANE") == "1"
     blk = 16 if np_side % 16 == 0 and ng <= np_side else 8
     dep, kick = tuned["deposit"]["choice"] if isinstance(tuned["deposit"], dict) else tuned["deposit"], \
         tuned["kick"]["choice"] if isinstance(tuned["kick"], dict) else tuned["kick"]
@@ -147,6 +149,13 @@ def kernel_names(tuned, np_side, ng):
         "fft_z_inv": zinv,
         "kick_drift": KICK_NAMES[blk][kick],
     }
+    if plane and ng in (256, 512, 1024):
+        # HGPM_PLANE=1: the z and y passes in one kernel, a cluster per x plane
+        names["fft_z_fwd"] = "zy_fwd_kernel<NG,3> (z and y passes, an 8-CTA cluster per x plane)"
+        names["fft_y_fwd"] = "(in zy_fwd_kernel)"
+        if kick == 7:
+            names["fft_z_inv"] = "yz_inv_pair_kernel<NG,3> (y and z inverse passes, the paired potential)"
+            names["fft_y_inv"] = "(in yz_inv_pair_kernel)"
     small = "1" if ng <= np_side else "0"
     return {k: v.replace("NG", str(ng)).replace(",S,", "," + small + ",") for k, v in names.items()}
 

@@ -14,6 +14,9 @@
 #include <stdint.h>
 #include <math.h>
 
+#include <map>
+#include <mutex>
+
 #include "fft_engine.cuh"
 #include "hgpm_device.cuh"
 #include "hgpm_internal.h"
@@ -46,8 +49,9 @@ template <int NG> struct Cfg {
 // ---------------------------------------------------------------------------
 // Rows e in [0, N) at g + e*rs; columns [0, nvalid) valid (nvalid may be < C).
 // All of a thread's global loads are issued before any shared store
-// (register staging) so each CTA keeps its whole tile in flight.
-template <int N, int C, int NT = kThreads>
+// (register staging) so each CTA keeps its whole tile in flight.  CG: loads
+// from L2 (ld.global.cg), for data other CTAs of the same kernel wrote.
+template <int N, int C, int NT = kThreads, bool CG = false>
 __device__ __forceinline__ void load_tile(float2* __restrict__ tile, const float2* __restrict__ g,
                                           size_t rs, int nvalid) {
     constexpr int TPR = C / 2;  // float4 (two complex) per row chunk
@@ -60,7 +64,8 @@ __device__ __forceinline__ void load_tile(float2* __restrict__ tile, const float
             const int i = threadIdx.x + t * NT;
             if ((TOT % NT) == 0 || i < TOT) {
                 const int e = i / TPR, c = 2 * (i % TPR);
-                v[t] = __ldcs(reinterpret_cast<const float4*>(g + (size_t)e * rs + c));
+                const float4* src = reinterpret_cast<const float4*>(g + (size_t)e * rs + c);
+                v[t] = CG ? __ldcg(src) : __ldcs(src);
             }
         }
     } else {
@@ -72,9 +77,9 @@ __device__ __forceinline__ void load_tile(float2* __restrict__ tile, const float
                 const int e = i / TPR, c = 2 * (i % TPR);
                 const float2* src = g + (size_t)e * rs + c;
                 if (c + 1 < nvalid) {
-                    v[t] = *reinterpret_cast<const float4*>(src);
+                    v[t] = CG ? __ldcg(reinterpret_cast<const float4*>(src)) : *reinterpret_cast<const float4*>(src);
                 } else if (c < nvalid) {
-                    const float2 s = src[0];
+                    const float2 s = CG ? __ldcg(src) : src[0];
                     v[t] = make_float4(s.x, s.y, 0.f, 0.f);
                 }
             }
@@ -90,7 +95,9 @@ __device__ __forceinline__ void load_tile(float2* __restrict__ tile, const float
     }
 }
 
-template <int N, int C, int NT = kThreads>
+// WB: write-back stores (kept in L2 for a read later in the same kernel)
+// instead of streaming ones.
+template <int N, int C, int NT = kThreads, bool WB = false>
 __device__ __forceinline__ void store_tile(const float2* __restrict__ tile, float2* __restrict__ g,
                                            size_t rs, int nvalid) {
     constexpr int TPR = C / 2;
@@ -104,7 +111,8 @@ __device__ __forceinline__ void store_tile(const float2* __restrict__ tile, floa
             float2* dst = g + (size_t)e * rs + c;
             const float4 v = *reinterpret_cast<const float4*>(&tile[e * C + c]);
             if (c + 1 < nvalid) {
-                __stcs(reinterpret_cast<float4*>(dst), v);
+                if (WB) *reinterpret_cast<float4*>(dst) = v;
+                else __stcs(reinterpret_cast<float4*>(dst), v);
             } else if (c < nvalid) {
                 dst[0] = make_float2(v.x, v.y);
             }
@@ -306,7 +314,8 @@ __global__ void __launch_bounds__(kThreads, 4) zpass_r2c_kernel(void* __restrict
 // ---------------------------------------------------------------------------
 // PAIR: out holds nlines * NG pairs, cell z of a line (phi(z), phi(z+1 mod
 // NG)) (the paired potential the pair-gathering kick reads).
-template <int NG, bool PAIR = false>
+// CG: the spectrum is read from L2 (written earlier in the same kernel).
+template <int NG, bool PAIR = false, bool CG = false>
 __device__ __forceinline__ void zpass_c2r_body(const float2* __restrict__ in, float* __restrict__ out, int nlines,
                                                int zs, float scale, const float2* __restrict__ tw, int bx) {
     constexpr int M = NG / 2, L = Cfg<NG>::L, ES = L + 1;
@@ -326,8 +335,8 @@ __device__ __forceinline__ void zpass_c2r_body(const float2* __restrict__ in, fl
         rm[t] = make_float2(0.f, 0.f);
         if (i < TOT && line0 + l < nlines) {
             const float2* src = in + (size_t)(line0 + l) * zs;
-            rk[t] = __ldcs(&src[k]);
-            rm[t] = __ldcs(&src[M - k]);
+            rk[t] = CG ? __ldcg(&src[k]) : __ldcs(&src[k]);
+            rm[t] = CG ? __ldcg(&src[M - k]) : __ldcs(&src[M - k]);
         }
     }
 #pragma unroll
@@ -388,6 +397,150 @@ __global__ void __launch_bounds__(kThreads) zpass_c2r_kernel(const float2* __res
     in += (size_t)slot * sl.s0 + (size_t)comp * in_cs;
     out += (size_t)slot * sl.s1 + (size_t)comp * out_cs;
     zpass_c2r_body<NG>(in, out, nlines, zs, scale, tw, blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// z and y passes of the x planes with a thread-block cluster per plane.
+//
+// A cluster of kPlaneCTAs CTAs works on one x plane at a time, planes
+// cid, cid + G, cid + 2G, ... (G clusters, as many as are resident at once).
+// Forward (zy_fwd_kernel): the R2C z pass of a plane's L-line tiles (int64
+// density in and zeroed, as zpass_r2c_kernel<NG,1>; every kPlaneCTAs-th tile
+// per CTA), the cluster barrier (release / acquire at cluster scope) that
+// makes the plane's half spectrum visible to every CTA of the cluster, then
+// the y transform of the plane's PlaneCfg-column tiles in place.  The plane
+// (ng x zs complex, 1.1 MB at 512^3) was written microseconds earlier by
+// write-back stores and is read back from L2 (.cg loads), so DRAM sees the
+// z pass's traffic and one write of the spectrum instead of the y pass's
+// extra read and write.  Each CTA interleaves the next plane's z tiles
+// (DRAM-bound) with the current plane's y tiles (L2 and shared memory), one
+// barrier per plane.  Inverse (yz_inv_pair_kernel), the same pipeline with
+// the roles swapped: the y inverse of the next plane's columns (DRAM in,
+// write-back stores) interleaved with the C2R z pass of the current plane's
+// lines into the paired potential (as zpass_c2r_pair_kernel<NG>).  Every
+// transform runs the same stages in the same order as the separate passes,
+// so the results are bit-identical to theirs.
+// ---------------------------------------------------------------------------
+constexpr int kPlaneCTAs = 8;
+template <int NG> struct PlaneCfg {
+    static constexpr int CY = NG >= 768 ? 4 : 8;  // y columns per tile
+    static constexpr int L = Cfg<NG>::L;
+    static constexpr int ZT = NG / L;                                  // z tiles per plane
+    static constexpr int YT = (NG / 2 + 1 + CY - 1) / CY;             // y tiles per plane
+    static constexpr int SMEM = Cfg<NG>::ZSMEM > NG * CY * 8 ? Cfg<NG>::ZSMEM : NG * CY * 8;
+    static_assert(NG % L == 0 && ZT >= kPlaneCTAs, "a plane holds whole z tiles, one or more per CTA");
+};
+
+// Every thread of every CTA of the cluster arrives; the writes before it
+// are visible to the reads after it in every CTA of the cluster.  A
+// hardware barrier over CTAs the cluster launch co-schedules: no polling.
+__device__ __forceinline__ void plane_cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// The R2C z pass of lines [line0, line0 + L) of the int64 density: the
+// arithmetic of zpass_r2c_kernel<NG, true>, the half spectrum written with
+// write-back stores.  Returns synchronised (the tile may be reused).
+template <int NG>
+__device__ __forceinline__ void zr2c_fix_tile(unsigned long long* __restrict__ in, float2* __restrict__ out, int line0,
+                                              int zs, double mean, const float2* __restrict__ tw, float2* buf) {
+    constexpr int M = NG / 2, L = Cfg<NG>::L, ES = L + 1;
+    constexpr int TOT = L * M;
+    constexpr int PER = (TOT + kThreads - 1) / kThreads;
+    static_assert(TOT % kThreads == 0, "whole tiles");
+    ulonglong2 q[PER];
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int i = threadIdx.x + t * kThreads;
+        const int l = i / M, m = i % M;
+        q[t] = __ldcs(reinterpret_cast<const ulonglong2*>(in + (size_t)(line0 + l) * NG) + m);
+    }
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int i = threadIdx.x + t * kThreads;
+        const int l = i / M, m = i % M;
+        __stcs(reinterpret_cast<ulonglong2*>(in + (size_t)(line0 + l) * NG) + m, make_ulonglong2(0ull, 0ull));
+        buf[m * ES + l] = make_float2((float)((double)(long long)q[t].x * kFixInv - mean),
+                                      (float)((double)(long long)q[t].y * kFixInv - mean));
+    }
+    __syncthreads();
+    fft_tile<M, L, ES, false, kThreads, 2>(buf, tw);
+    constexpr int H = M / 2 + 1;
+    for (int i = threadIdx.x; i < L * H; i += kThreads) {
+        const int l = i / H, k = i % H;
+        const float2 zk = buf[k * ES + l];
+        const float2 zm = buf[((M - k) % M) * ES + l];
+        const float2 w = __ldg(&tw[k]);
+        const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        const float2 o = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+        const float2 wo = cmul(w, o);
+        float2* dst = out + (size_t)(line0 + l) * zs;
+        dst[k] = cadd(e, wo);
+        if (k != M - k) {
+            const float2 xm = csub(e, wo);
+            dst[M - k] = make_float2(xm.x, -xm.y);
+        }
+    }
+    __syncthreads();
+}
+
+// One y-column tile (columns [c0, c0 + CY)) of plane g transformed in place.
+// CG: read from L2 (the plane was written earlier in the same kernel); WB:
+// written back through L2 (read later in the same kernel).
+template <int NG, bool INV, bool CG, bool WB>
+__device__ __forceinline__ void plane_y_tile(float2* __restrict__ g, int c0, int zs, const float2* __restrict__ tw,
+                                             float2* buf) {
+    constexpr int CY = PlaneCfg<NG>::CY, H = NG / 2 + 1;
+    load_tile<NG, CY, kThreads, CG>(buf, g + c0, zs, H - c0);
+    __syncthreads();
+    fft_tile<NG, CY, CY, INV, kThreads>(buf, tw);
+    store_tile<NG, CY, kThreads, WB>(buf, g + c0, zs, H - c0);
+    __syncthreads();
+}
+
+template <int NG, int MINB>
+__global__ void __cluster_dims__(kPlaneCTAs, 1, 1) __launch_bounds__(kThreads, MINB)
+    zy_fwd_kernel(unsigned long long* __restrict__ rho, float2* __restrict__ spec, int zs, double mean,
+                  const float2* __restrict__ tw) {
+    using P = PlaneCfg<NG>;
+    constexpr int TMAX = P::ZT > P::YT ? P::ZT : P::YT;
+    float2* buf = reinterpret_cast<float2*>(hgpm_smem);
+    const int nclu = gridDim.x / kPlaneCTAs, cid = blockIdx.x / kPlaneCTAs, r = blockIdx.x % kPlaneCTAs;
+    for (int t = r; t < P::ZT; t += kPlaneCTAs) zr2c_fix_tile<NG>(rho, spec, cid * NG + t * P::L, zs, mean, tw, buf);
+    plane_cluster_sync();
+    for (int x = cid; x < NG; x += nclu) {
+        const int xn = x + nclu;
+        float2* g = spec + (size_t)x * NG * zs;
+        for (int t = r; t < TMAX; t += kPlaneCTAs) {
+            if (xn < NG && t < P::ZT) zr2c_fix_tile<NG>(rho, spec, xn * NG + t * P::L, zs, mean, tw, buf);
+            if (t < P::YT) plane_y_tile<NG, false, true, false>(g, t * P::CY, zs, tw, buf);
+        }
+        plane_cluster_sync();
+    }
+}
+
+template <int NG, int MINB>
+__global__ void __cluster_dims__(kPlaneCTAs, 1, 1) __launch_bounds__(kThreads, MINB)
+    yz_inv_pair_kernel(float2* __restrict__ spec, float* __restrict__ out, int zs, const float2* __restrict__ tw) {
+    using P = PlaneCfg<NG>;
+    constexpr int TMAX = P::ZT > P::YT ? P::ZT : P::YT;
+    float2* buf = reinterpret_cast<float2*>(hgpm_smem);
+    const int nclu = gridDim.x / kPlaneCTAs, cid = blockIdx.x / kPlaneCTAs, r = blockIdx.x % kPlaneCTAs;
+    for (int t = r; t < P::YT; t += kPlaneCTAs)
+        plane_y_tile<NG, true, false, true>(spec + (size_t)cid * NG * zs, t * P::CY, zs, tw, buf);
+    plane_cluster_sync();
+    for (int x = cid; x < NG; x += nclu) {
+        const int xn = x + nclu;
+        for (int t = r; t < TMAX; t += kPlaneCTAs) {
+            if (xn < NG && t < P::YT)
+                plane_y_tile<NG, true, false, true>(spec + (size_t)xn * NG * zs, t * P::CY, zs, tw, buf);
+            if (t < P::ZT) {
+                zpass_c2r_body<NG, true, true>(spec, out, NG * NG, zs, 1.0f, tw, x * P::ZT + t);
+                __syncthreads();
+            }
+        }
+        plane_cluster_sync();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -770,6 +923,46 @@ static cudaError_t zinv_impl(const float2* in, float* out, int nlines, int zs, s
     return cudaGetLastError();
 }
 
+// Clusters of `func` (kPlaneCTAs CTAs of kThreads threads, smem bytes each)
+// resident at once on the current device, queried once per (device,
+// kernel); 0 if the query fails.
+static int plane_clusters_once(const void* func, int smem) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, int> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> g(mu);
+    auto it = done.find({dev, func});
+    if (it != done.end()) return it->second;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kPlaneCTAs, 1, 1);
+    cfg.blockDim = dim3(kThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, func, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    done[{dev, func}] = n;
+    return n;
+}
+
+template <int NG, int MINB>
+static cudaError_t plane_impl(bool inv, void* a, float2* spec, int zs, double mean, const float2* tw, cudaStream_t s) {
+    constexpr int SMEM = PlaneCfg<NG>::SMEM;
+    const void* fn = inv ? (const void*)yz_inv_pair_kernel<NG, MINB> : (const void*)zy_fwd_kernel<NG, MINB>;
+    cudaError_t e = smem_attr_once(fn, SMEM);
+    if (e != cudaSuccess) return e;
+    int nclu = plane_clusters_once(fn, SMEM);
+    if (nclu < 1 || nclu > NG) nclu = NG;  // one plane per cluster
+    if (inv)
+        yz_inv_pair_kernel<NG, MINB><<<nclu * kPlaneCTAs, kThreads, SMEM, s>>>(spec, reinterpret_cast<float*>(a), zs, tw);
+    else
+        zy_fwd_kernel<NG, MINB><<<nclu * kPlaneCTAs, kThreads, SMEM, s>>>(reinterpret_cast<unsigned long long*>(a), spec,
+                                                                          zs, mean, tw);
+    return cudaGetLastError();
+}
+
 template <int NG>
 static cudaError_t zinv_pair_impl(const float2* in, float* out, int nlines, int zs, const float2* tw, cudaStream_t s) {
     using G = Cfg<NG>;
@@ -850,6 +1043,38 @@ cudaError_t launch_zfwd(int ng, void* in, bool fixed, float2* out, int nlines, i
 #undef X
     }
     return cudaErrorInvalidValue;
+}
+
+bool plane_fft_supported(int ng) {
+    switch (ng) {
+#define X(n) \
+    case n:  \
+        return true;
+        HGPM_PLANE_SIZES(X)
+#undef X
+    }
+    return false;
+}
+
+static cudaError_t launch_plane(int ng, bool inv, void* a, float2* spec, int zs, double mean,
+                                const float2* tw, cudaStream_t s) {
+    switch (ng) {
+#define X(n)                                                                          \
+    case n:                                                                           \
+        return plane_impl<n, 3>(inv, a, spec, zs, mean, tw, s);
+        HGPM_PLANE_SIZES(X)
+#undef X
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_zy_fwd(int ng, unsigned long long* rho, float2* spec, int zs, double mean, const float2* tw,
+                          cudaStream_t s) {
+    return launch_plane(ng, false, rho, spec, zs, mean, tw, s);
+}
+
+cudaError_t launch_yz_inv_pair(int ng, float2* spec, float* out, int zs, const float2* tw, cudaStream_t s) {
+    return launch_plane(ng, true, out, spec, zs, 0.0, tw, s);
 }
 
 cudaError_t launch_zinv(int ng, const float2* in, float* out, int nlines, int zs, size_t in_cs, size_t out_cs,

@@ -59,6 +59,10 @@ struct hgpm_ctx {
     // built-in defaults (-1 / 0).
     bool tma = true;
     int xmode = 2;
+    // HGPM_PLANE=1: the z and y passes as one kernel with a thread-block
+    // cluster per x plane (launch_zy_fwd / launch_yz_inv_pair) at the sides
+    // that have it; 0 (the default, faster) the separate passes
+    bool plane = false;
     int dep_choice = -1;
     int kick_choice = 0;
     float* stage = nullptr;     // AoS float3 x, v staging (lazy)

@@ -52,6 +52,18 @@ cudaError_t launch_fft_c2c(int ng, float2* data, bool inv, const float2* tw, cud
 // The C2R z pass of one box writing the paired potential (2 ng^3 floats:
 // cell z of a line holds (phi(z), phi(z+1 mod ng))).
 cudaError_t launch_zinv_pair(int ng, const float2* in, float* out, int zs, const float2* tw, cudaStream_t s);
+// The z and y passes of one box with a thread-block cluster per x plane
+// (sides in HGPM_PLANE_SIZES): the forward R2C z + y passes of the int64
+// density (zeroed) into the half spectrum, and the inverse y + C2R z passes
+// of a half spectrum (y-inverted in place) into the paired potential;
+// bit-identical to launch_zfwd + the y pass and the y pass +
+// launch_zinv_pair.  Measured slower than the separate passes (512^3: 0.77
+// against 0.65 ms forward, 0.77 against 0.49 inverse), so opt-in.
+#define HGPM_PLANE_SIZES(X) X(256) X(512) X(1024)
+bool plane_fft_supported(int ng);
+cudaError_t launch_zy_fwd(int ng, unsigned long long* rho, float2* spec, int zs, double mean, const float2* tw,
+                          cudaStream_t s);
+cudaError_t launch_yz_inv_pair(int ng, float2* spec, float* out, int zs, const float2* tw, cudaStream_t s);
 cudaError_t launch_strided(int ng, bool inv, float2* data, int ncols, size_t rs, size_t ps, int nplanes, size_t cs,
                            int ncomp, const float2* tw, cudaStream_t s, const Slots& sl = Slots{}, int nslots = 1);
 // x pass fused with the Green's function: the potential's spectrum

@@ -382,6 +382,8 @@ extern "C" int hgpm_create(const hgpm_params* p, int device, hgpm_ctx** out) {
         c->tma = !(nt && nt[0] == '1');
         const char* xt = getenv("HGPM_XTMA");
         if (xt && xt[0] >= '0' && xt[0] <= '2') c->xmode = xt[0] - '0';
+        const char* pv = getenv("HGPM_PLANE");
+        if (pv && (pv[0] == '0' || pv[0] == '1')) c->plane = pv[0] == '1';
         const char* kv = getenv("HGPM_KICK");
         c->kick_choice = kick_default(p->np, p->ng);
         if (kv && kv[0] >= '0' && kv[0] <= '9' && atoi(kv) < kick_candidates(p->np, p->ng)) c->kick_choice = atoi(kv);
@@ -730,6 +732,13 @@ extern "C" int hgpm_get_density(hgpm_ctx* c, float* rho) {
 // zeroes the accumulator)
 static int forward_zy(hgpm_ctx* c) {
     const int ng = c->ng, M = ng / 2;
+    if (c->plane && plane_fft_supported(ng)) {
+        PhaseScope ps(c, PH_ZFWD);
+        CK(launch_zy_fwd(ng, c->rho64, c->spec, c->zs, mean_density(c), c->tw_ng, c->stream));
+        c->rho_dirty = false;
+        count(c, PH_ZFWD, 1);
+        return HGPM_OK;
+    }
     {
         PhaseScope ps(c, PH_ZFWD);
         CK(launch_zfwd(ng, c->rho64, true, c->spec, ng * ng, c->zs, mean_density(c), c->tw_ng, c->stream));
@@ -769,7 +778,8 @@ extern "C" int hgpm_solve_gradient(hgpm_ctx* c) {
                                  c->cosq, coeff, c->stream));
         count(c, PH_POISSON, 1);
     }
-    {
+    const bool plane_inv = c->plane && plane_fft_supported(ng) && kick_uses_phi2(c->kick_choice);
+    if (!plane_inv) {
         PhaseScope ps(c, PH_YINV);
         if (c->tma)
             CK(launch_strided_tma(ng, true, false, c->fspec, M + 1, c->zs, 0, 1, c->tw_ng, c->d_err + 1, c->stream));
@@ -786,8 +796,10 @@ extern "C" int hgpm_solve_gradient(hgpm_ctx* c) {
         float* phi = reinterpret_cast<float*>(c->fspec + cs);
         c->force_valid = false;
         if (kick_uses_phi2(c->kick_choice)) {
-            // the paired potential, in the force grid's space
-            CK(launch_zinv_pair(ng, c->fspec, c->force, c->zs, c->tw_ng, c->stream));
+            // the paired potential, in the force grid's space (with the
+            // inverse y pass when the plane kernels run)
+            if (plane_inv) CK(launch_yz_inv_pair(ng, c->fspec, c->force, c->zs, c->tw_ng, c->stream));
+            else CK(launch_zinv_pair(ng, c->fspec, c->force, c->zs, c->tw_ng, c->stream));
             c->phi_valid = false;
             c->phi2_valid = true;
         } else {

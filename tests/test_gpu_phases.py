@@ -112,6 +112,38 @@ def test_tma_and_plain_strided_passes_bit_identical(ng, monkeypatch):
     assert np.array_equal(out[0], out[1])
 
 
+@pytest.mark.parametrize("ng,np_side", [(256, 256), (512, 256), (1024, 128)])
+def test_plane_cluster_passes_bit_identical(ng, np_side, monkeypatch):
+    """The z and y passes as one kernel with a thread-block cluster per x
+    plane (HGPM_PLANE=1) give the spectrum, the force formed on demand, the
+    paired-potential kick and P(k) of the separate passes bit for bit."""
+    rng = np.random.default_rng(ng + np_side)
+    x = (rng.random((np_side ** 3, 3), dtype=np.float32) * np.float32(ng)).astype(np.float32)
+    x = np.minimum(x, np.float32(ng) * np.float32(1 - 2 ** -23))
+    v = rng.standard_normal((np_side ** 3, 3), dtype=np.float32)
+    monkeypatch.setenv("HGPM_KICK", "7")
+    ref = None
+    for flag in ("0", "1"):
+        monkeypatch.setenv("HGPM_PLANE", flag)
+        with make(ng, np_side) as s:
+            s.load_state(x, v)
+            s.cic()
+            pk = s.power_spectrum(nbins=64, log_bins=True)[1]
+            s.cic()
+            s.solve_gradient()
+            s.kick_drift(0.0123, 1.7, 0.3, 0.25, 2)
+            xs, vs = s.store_state()
+            # the force grid formed on demand from the y-inverted spectrum
+            # (not at 1024^3: 13 GB on the host)
+            f = s.get_force() if ng <= 512 else None
+            got = (pk, xs, vs, f)
+        if ref is None:
+            ref = got
+            continue
+        for a, b in zip(ref, got):
+            assert (a is None and b is None) or np.array_equal(a, b), flag
+
+
 @pytest.mark.parametrize("ng", [32, 64, 128, 80, 96])
 def test_fused_x_pass_variants_bit_identical(ng, monkeypatch):
     """The persistent TMA-fed Poisson x pass and the plain fused x pass (with
@@ -240,7 +272,7 @@ def test_autotune_leaves_state_and_results_unchanged(ng, np_side, tmp_path, monk
     the same afterwards, the picks are valid, steps after tuning equal steps
     without it bit for bit, and a stored pick is applied to the next context
     of that size."""
-    for k in ("HGPM_DEPOSIT", "HGPM_KICK", "HGPM_NO_TMA", "HGPM_XTMA"):
+    for k in ("HGPM_DEPOSIT", "HGPM_KICK", "HGPM_NO_TMA", "HGPM_XTMA", "HGPM_PLANE"):
         monkeypatch.delenv(k, raising=False)
     monkeypatch.setenv("HGPM_TUNE_CACHE", str(tmp_path / "tune.txt"))
     hp = H.parse_params(params_text(ng, np_side))
