@@ -148,7 +148,8 @@ def test_plane_cluster_passes_bit_identical(ng, np_side, monkeypatch):
                                         (256, 128), (384, 128), (512, 256)])
 def test_fused_x_pass_variants_bit_identical(ng, np_side, monkeypatch):
     """The persistent TMA-fed Poisson x pass and the plain fused x pass (with
-    its own or twice the columns per CTA) give bit-identical forces."""
+    its own or twice the columns per CTA) give bit-identical forces, and the
+    next deposit after the solve starts from a zeroed accumulator."""
     x, v = lattice_state(np_side, ng, disp=1.1, seed=ng + 3)
     out = []
     for flag in ("0", "1", "2"):
@@ -158,11 +159,13 @@ def test_fused_x_pass_variants_bit_identical(ng, np_side, monkeypatch):
             s.cic()
             s.solve_gradient()
             f = s.get_force()
+            s.cic()
+            rho = s.get_density()
             s.sync()
         if out:
-            assert np.array_equal(out[0], f), flag
+            assert np.array_equal(out[0][0], f) and np.array_equal(out[0][1], rho), flag
         else:
-            out.append(f)
+            out.append((f, rho))
 
 
 @pytest.mark.parametrize("ng,np_side,disp", [(32, 32, 0.3), (64, 64, 0.3), (64, 64, 2.0), (64, 64, 6.0),
