@@ -190,13 +190,14 @@ def test_deposit_configurations_bit_identical(ng, np_side, disp, monkeypatch):
 
 
 @pytest.mark.parametrize("ng,np_side,disp", [(32, 32, 1.0), (48, 48, 1.0), (64, 32, 1.0), (32, 64, 1.0), (64, 64, 0.3),
-                                             (64, 64, 4.0)])
+                                             (64, 64, 4.0), (128, 128, 1.5)])
 def test_kick_variants_bit_identical(ng, np_side, disp, monkeypatch):
     """Every kick candidate (flat global gathers with different CTA shapes
     and unit runs, the float4-window kick, the gathers of the real or the
     paired potential that form each corner's force as the gradient kernel
     does) runs the same FP32 arithmetic in the same order; disp 4 spreads
-    blocks past the window caps (global-gather fallback)."""
+    blocks past the window caps (global-gather fallback); at 128^3 the grid
+    has more blocks than resident CTAs."""
     x, v = lattice_state(np_side, ng, disp=disp, vel=1.0, seed=17)
     out = []
     for flag in ("0", "1", "2", "3", "4", "5", "6", "7"):
