@@ -346,7 +346,10 @@ int hgpm_cic_density_noalloc(const float* x_dev, int np_side, int ng, float* rho
  * its size and device unless HGPM_NO_TUNE_CACHE is set (or the knob's
  * environment variable HGPM_DEPOSIT / HGPM_KICK / HGPM_NO_TMA / HGPM_XTMA
  * pins it).  choices / best_ms (may be NULL) receive the picks and their
- * ms per launch.                                                          */
+ * ms per launch.  HGPM_PLANE=1 (not tuned; sides 256, 512, 1024) runs the
+ * z and y passes of the step's transforms as one kernel with an 8-CTA
+ * thread-block cluster per x plane: bit-identical, slower than the
+ * separate passes on B200.                                                */
 #define HGPM_TUNE_KNOBS 4
 #define HGPM_TUNE_DEPOSIT 0
 #define HGPM_TUNE_KICK 1
