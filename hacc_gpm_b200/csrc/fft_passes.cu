@@ -868,18 +868,28 @@ __global__ void __launch_bounds__(kThreads) xpk_kernel(const float2* __restrict_
     }
 }
 
+// Bin b's partial sums: one warp per bin, lane l adding partials l, l + 32,
+// ... in order, then the 32 lane sums combined by a fixed shuffle tree (a
+// fixed order: deterministic run to run).
 __global__ void pk_reduce_kernel(const double* __restrict__ part_sum, const unsigned long long* __restrict__ part_cnt,
                                  int nparts, int nbins, double* __restrict__ sum, unsigned long long* __restrict__ cnt) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nbins) return;
+    const int b = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (b >= nbins) return;  // whole warps
     double s = 0.0;
     unsigned long long n = 0;
-    for (int p = 0; p < nparts; ++p) {
+    for (int p = lane; p < nparts; p += 32) {
         s += part_sum[(size_t)p * nbins + b];
         n += part_cnt[(size_t)p * nbins + b];
     }
-    sum[b] = s;
-    cnt[b] = n;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        n += __shfl_down_sync(0xffffffffu, n, o);
+    }
+    if (lane == 0) {
+        sum[b] = s;
+        cnt[b] = n;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1019,7 +1029,7 @@ static cudaError_t xpk_impl(const float2* in, int ncols, size_t rs, size_t ps, c
     k<<<nparts, kThreads, smem, s>>>(in, ncols, rs, ps, nchunks, tw, a, part_sum, part_cnt);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    pk_reduce_kernel<<<cdiv(a.nbins, 128), 128, 0, s>>>(part_sum, part_cnt, nparts, a.nbins, sum, cnt);
+    pk_reduce_kernel<<<cdiv((size_t)a.nbins * 32, 256), 256, 0, s>>>(part_sum, part_cnt, nparts, a.nbins, sum, cnt);
     return cudaGetLastError();
 }
 

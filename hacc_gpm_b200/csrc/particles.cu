@@ -1943,10 +1943,15 @@ cudaError_t launch_ktables(int ng, double* cosq, float* sk, float* pkw, cudaStre
 cudaError_t launch_noise(float* out, size_t n, int seed, int kind, cudaStream_t s) {
     if (kind == 0) {
         if (n > 0x7fffffffu) return cudaErrorInvalidValue;  // the reference's int cell index
-        // threads: the largest power of two <= n / 16 (at least 32, at most 2^20)
-        int T = 32;
-        while (T < (1 << 20) && (size_t)T * 2 * 16 <= n) T *= 2;
-        noise_curand_kernel<<<nblk(T, 256), 256, 0, s>>>(out, (int)n, seed, T);
+        // threads T, a power of two (which thread draws a cell does not change
+        // the cell's state): about n / 64, so a thread's one curand_init is
+        // shared by ~64 cells that each cost one skip, but at least
+        // min(n, 32768) so that small grids still spread over the GPU (at
+        // least 32)
+        const size_t target = n / 64 > (n < 32768 ? n : 32768) ? n / 64 : (n < 32768 ? n : 32768);
+        size_t T = 32;
+        while (T * 2 <= target) T *= 2;
+        noise_curand_kernel<<<nblk(T, 256), 256, 0, s>>>(out, (int)n, seed, (int)T);
     } else {
         noise_kernel<<<nblk(n, 256), 256, 0, s>>>(out, n, (uint32_t)seed);
     }

@@ -38,6 +38,19 @@ def test_curand_noise_is_the_references(case):
     assert np.array_equal(g, case["noise"])
 
 
+def test_curand_noise_of_a_larger_box_starts_with_the_references():
+    """A cell's draw depends only on SEED and its linear index (its state is
+    curand_init(seed, cell, 0)), so the first 32^3 cells of a 128^3 box's
+    noise are the reference's 32^3 noise; at 128^3 each thread draws 8 cells,
+    reaching each next one by skipahead_sequence, where 32^3 draws one."""
+    case = R.Case("a32")
+    from tests.helpers import params_text
+    with H.Simulation(H.parse_params(params_text(128, seed=case.p.seed))) as s:
+        g = s.ic_noise().reshape(-1)
+    ref = case["noise"].reshape(-1)
+    assert np.array_equal(g[:ref.size], ref)
+
+
 def test_seeded_ics_are_the_references(case):
     """hgpm_ic_generate from the params file and .ipk alone (no noise
     replay) lands on the reference's ICs within the IC bars."""
