@@ -219,10 +219,15 @@ constexpr int kWinRec = 8;
 constexpr int kWin4Cap = 6912;
 
 // 8 corner weights ((w_x w_y) w_z) * mass rounded to 2^-24, index (a*2+b)*2+c
-// for corner (+a, +b, +c).  Q32: every value < 2^32 (mass < 256).
+// for corner (+a, +b, +c).  Q32: every value < 2^32 (mass < 256).  The x
+// weights are scaled by 2^24 first: a power-of-two factor commutes with
+// every rounding of the products while they stay normal, and a weight whose
+// products leave the normal range (below 2^-126) rounds to 0 either way, so
+// the integers are those of scaling the finished product.
 template <bool Q32>
 __device__ __forceinline__ void cic_q24(float dx, float dy, float dz, float mass, unsigned long long q[8]) {
-    const float wx[2] = {1.f - dx, dx}, wy[2] = {1.f - dy, dy}, wz[2] = {1.f - dz, dz};
+    const float wx[2] = {__fmul_rn(1.f - dx, kQ24F), __fmul_rn(dx, kQ24F)}, wy[2] = {1.f - dy, dy},
+                wz[2] = {1.f - dz, dz};
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -231,9 +236,8 @@ __device__ __forceinline__ void cic_q24(float dx, float dy, float dz, float mass
             for (int cc = 0; cc < 2; ++cc) {
                 float mul = __fmul_rn(__fmul_rn(wx[a], wy[b]), wz[cc]);
                 if (mass != 1.f) mul = __fmul_rn(mul, mass);  // exact when mass is 1 (ng = np)
-                // the product by 2^24 is exact, so only the rounding to an integer rounds
-                q[(a * 2 + b) * 2 + cc] = Q32 ? (unsigned long long)__float2uint_rn(mul * kQ24F)
-                                              : (unsigned long long)__float2ull_rn(mul * kQ24F);
+                q[(a * 2 + b) * 2 + cc] = Q32 ? (unsigned long long)__float2uint_rn(mul)
+                                              : (unsigned long long)__float2ull_rn(mul);
             }
 }
 
