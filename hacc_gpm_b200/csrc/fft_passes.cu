@@ -577,10 +577,9 @@ __global__ void __launch_bounds__(kThreads) zpass_c2c_kernel(float2* __restrict_
 // blockIdx = (column chunk, plane, slot * ncomp + comp)
 // ---------------------------------------------------------------------------
 // Column chunk bx of plane by of one component of one box, NT threads.
-template <int NG, bool INV, int NT>
+template <int NG, bool INV, int NT, int C = Cfg<NG>::CS>
 __device__ __forceinline__ void strided_body(float2* __restrict__ data, int ncols, size_t rs, size_t ps,
                                              const float2* __restrict__ tw, int bx, int by) {
-    constexpr int C = Cfg<NG>::CS;
     float2* tile = reinterpret_cast<float2*>(hgpm_smem);
     const int col0 = bx * C;
     float2* g = data + (size_t)by * ps + col0;
@@ -1249,6 +1248,19 @@ constexpr int kMCYX = 512;
 template <int PASS> constexpr int mc_threads() { return PASS == 0 || PASS == 4 ? 256 : kMCYX; }
 template <int PASS> constexpr int mc_minb() { return 2; }
 
+// Columns per y / x tile.  Up to 128 a plane's ng/2 + 1 columns are split
+// into the fewest even-width tiles that keep a stage at about two radix-8
+// butterflies per thread (NG C <= 8192): the Nyquist column gets no tile of
+// its own, which left most of a last tile empty (at 64: 33 columns in tiles
+// of 16 or 32).  Larger sides keep the single-class widths.
+template <int NG> struct MCCols {
+    static constexpr int NC = NG / 2 + 1;
+    static constexpr int TILES = ((NC + 1) / 2 * 2 * NG + 8191) / 8192;
+    static constexpr int EVEN = ((NC + TILES - 1) / TILES + 1) / 2 * 2;
+    static constexpr int Y = NG <= 128 ? EVEN : Cfg<NG>::CS;
+    static constexpr int X = NG <= 128 ? EVEN : XW<NG>::C;
+};
+
 // One unit of each pass for one grid side.
 template <int NG>
 __device__ __forceinline__ void mc_zfwd_unit(const MCClass& c, int slot, int lu) {
@@ -1258,14 +1270,15 @@ __device__ __forceinline__ void mc_zfwd_unit(const MCClass& c, int slot, int lu)
 template <int NG, bool INV>
 __device__ __forceinline__ void mc_ypass_unit(const MCClass& c, int slot, int lu) {
     float2* data = INV ? c.fspec + (size_t)slot * 3 * c.spec_elems : c.spec + (size_t)slot * c.spec_elems;
-    constexpr int ncols = NG / 2 + 1, nch = (ncols + Cfg<NG>::CS - 1) / Cfg<NG>::CS;
-    strided_body<NG, INV, kMCYX>(data, ncols, (size_t)c.zs, (size_t)NG * c.zs, c.tw, lu % nch, lu / nch);
+    constexpr int ncols = NG / 2 + 1, nch = (ncols + MCCols<NG>::Y - 1) / MCCols<NG>::Y;
+    strided_body<NG, INV, kMCYX, MCCols<NG>::Y>(data, ncols, (size_t)c.zs, (size_t)NG * c.zs, c.tw, lu % nch,
+                                                 lu / nch);
 }
 template <int NG>
 __device__ __forceinline__ void mc_xpot_unit(const MCClass& c, int slot, int lu) {
-    constexpr int ncols = NG / 2 + 1, nch = (ncols + XW<NG>::C - 1) / XW<NG>::C;
+    constexpr int ncols = NG / 2 + 1, nch = (ncols + MCCols<NG>::X - 1) / MCCols<NG>::X;
     const PotentialOp op{c.cosq, 0.5 / ((double)NG * NG * NG)};
-    xone_body<NG, kMCYX, PotentialOp, XW<NG>::C>(c.spec + (size_t)slot * c.spec_elems, c.fspec + (size_t)slot * 3 * c.spec_elems, ncols,
+    xone_body<NG, kMCYX, PotentialOp, MCCols<NG>::X>(c.spec + (size_t)slot * c.spec_elems, c.fspec + (size_t)slot * 3 * c.spec_elems, ncols,
                        (size_t)NG * c.zs, (size_t)c.zs, c.tw, op, lu % nch, lu / nch);
 }
 template <int NG>
@@ -1312,9 +1325,10 @@ MCPassGeom mc_geom(int ng) {
 #define X(n)                                                                                            \
     case n: {                                                                                           \
         const int ncols = n / 2 + 1;                                                                    \
-        return MCPassGeom{(n * n + Cfg<n>::L - 1) / Cfg<n>::L, (ncols + Cfg<n>::CS - 1) / Cfg<n>::CS * n, \
-                          (ncols + XW<n>::C - 1) / XW<n>::C * n, Cfg<n>::ZSMEM, Cfg<n>::SSMEM,            \
-                          n * XW<n>::C * 8};                                                            \
+        return MCPassGeom{(n * n + Cfg<n>::L - 1) / Cfg<n>::L,                                          \
+                          (ncols + MCCols<n>::Y - 1) / MCCols<n>::Y * n,                                 \
+                          (ncols + MCCols<n>::X - 1) / MCCols<n>::X * n, Cfg<n>::ZSMEM,                   \
+                          n * MCCols<n>::Y * 8, n * MCCols<n>::X * 8};                                   \
     }
         HGPM_MC_SIZES(X)
 #undef X
