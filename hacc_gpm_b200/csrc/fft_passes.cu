@@ -1239,14 +1239,15 @@ namespace hgpm {
 
 namespace {
 
-// Threads and minimum CTAs per SM of each pass.  z passes: 256 x 2 (128
-// and 90 registers; the class fields a CTA keeps in registers push the
-// single-class kernels' 64 up).  y and x passes: 512 x 2 (62 / 64 registers;
+// Threads and minimum CTAs per SM of each pass.  z passes: 256 threads, 2
+// CTAs per SM forward (128 registers; the class fields a CTA keeps in
+// registers push the single-class kernels' 64 up, and 3 per SM spills) and 3
+// inverse (80 registers: 0.156 against 0.184 ms per ensemble step).  y and x passes: 512 x 2 (62 / 64 registers;
 // the single-class configuration at 128^3 and above; 256 x 2 at 101 / 104
 // registers measured the same at the 96-box ensemble).
 constexpr int kMCYX = 512;
 template <int PASS> constexpr int mc_threads() { return PASS == 0 || PASS == 4 ? 256 : kMCYX; }
-template <int PASS> constexpr int mc_minb() { return 2; }
+template <int PASS> constexpr int mc_minb() { return PASS == 4 ? 3 : 2; }
 
 // Columns per y / x tile.  Up to 128 a plane's ng/2 + 1 columns are split
 // into the fewest even-width tiles that keep a stage at about two radix-8
