@@ -155,10 +155,10 @@ __device__ __forceinline__ void store_tile_comp(const float2* __restrict__ tile,
 // The CTA's work (line group bx of one box) as a device function: the
 // single-class kernel below and the multi-class pass (mc_zfwd_kernel) run
 // the same code.
-template <int NG, bool FIX>
+template <int NG, bool FIX, int L = Cfg<NG>::L>
 __device__ __forceinline__ void zpass_r2c_body(void* __restrict__ in_, float2* __restrict__ out, int nlines, int zs,
                                                double mean, const float2* __restrict__ tw, int bx) {
-    constexpr int M = NG / 2, L = Cfg<NG>::L, ES = L + 1;
+    constexpr int M = NG / 2, ES = L + 1;
     float2* buf = reinterpret_cast<float2*>(hgpm_smem);
     const int line0 = bx * L;
     constexpr int TOT = L * M;
@@ -1239,15 +1239,16 @@ namespace hgpm {
 
 namespace {
 
-// Threads and minimum CTAs per SM of each pass.  z passes: 256 threads, 2
-// CTAs per SM forward (128 registers; the class fields a CTA keeps in
-// registers push the single-class kernels' 64 up, and 3 per SM spills) and 3
-// inverse (80 registers: 0.156 against 0.184 ms per ensemble step).  y and x passes: 512 x 2 (62 / 64 registers;
+// Threads and minimum CTAs per SM of each pass.  z passes: 256 threads, 3
+// CTAs per SM (80 registers; the forward pass with half-height tiles from
+// 192 up, MCCols::ZL, which bounds its register staging: 0.283 against
+// 0.326 ms per ensemble step at 2 CTAs of 128 registers; the inverse 0.156
+// against 0.184).  y and x passes: 512 x 2 (62 / 64 registers;
 // the single-class configuration at 128^3 and above; 256 x 2 at 101 / 104
 // registers measured the same at the 96-box ensemble).
 constexpr int kMCYX = 512;
 template <int PASS> constexpr int mc_threads() { return PASS == 0 || PASS == 4 ? 256 : kMCYX; }
-template <int PASS> constexpr int mc_minb() { return PASS == 4 ? 3 : 2; }
+template <int PASS> constexpr int mc_minb() { return PASS == 0 || PASS == 4 ? 3 : 2; }
 
 // Columns per y / x tile.  Up to 128 a plane's ng/2 + 1 columns are split
 // into the fewest even-width tiles that keep a stage at about two radix-8
@@ -1260,13 +1261,16 @@ template <int NG> struct MCCols {
     static constexpr int EVEN = ((NC + TILES - 1) / TILES + 1) / 2 * 2;
     static constexpr int Y = NG <= 128 ? EVEN : Cfg<NG>::CS;
     static constexpr int X = NG <= 128 ? EVEN : XW<NG>::C;
+    // z lines per forward z tile: half the single-class count from 192 up,
+    // which bounds the pass's register staging by the smaller sides'
+    static constexpr int ZL = NG >= 192 ? Cfg<NG>::L / 2 : Cfg<NG>::L;
 };
 
 // One unit of each pass for one grid side.
 template <int NG>
 __device__ __forceinline__ void mc_zfwd_unit(const MCClass& c, int slot, int lu) {
-    zpass_r2c_body<NG, true>(c.rho64 + (size_t)slot * c.ncell, c.spec + (size_t)slot * c.spec_elems, NG * NG, c.zs,
-                             c.mean, c.tw, lu);
+    zpass_r2c_body<NG, true, MCCols<NG>::ZL>(c.rho64 + (size_t)slot * c.ncell, c.spec + (size_t)slot * c.spec_elems,
+                                             NG * NG, c.zs, c.mean, c.tw, lu);
 }
 template <int NG, bool INV>
 __device__ __forceinline__ void mc_ypass_unit(const MCClass& c, int slot, int lu) {
@@ -1318,7 +1322,7 @@ __global__ void __launch_bounds__(mc_threads<PASS>(), mc_minb<PASS>()) mc_fft_ke
 
 // Per-size unit counts and shared memory of the passes (host).
 struct MCPassGeom {
-    int zunits, yunits, xunits;  // per slot
+    int zfunits, zunits, yunits, xunits;  // per slot (z forward, z inverse, y, x)
     int zsmem, ysmem, xsmem;
 };
 MCPassGeom mc_geom(int ng) {
@@ -1326,7 +1330,7 @@ MCPassGeom mc_geom(int ng) {
 #define X(n)                                                                                            \
     case n: {                                                                                           \
         const int ncols = n / 2 + 1;                                                                    \
-        return MCPassGeom{(n * n + Cfg<n>::L - 1) / Cfg<n>::L,                                          \
+        return MCPassGeom{(n * n + MCCols<n>::ZL - 1) / MCCols<n>::ZL, (n * n + Cfg<n>::L - 1) / Cfg<n>::L,  \
                           (ncols + MCCols<n>::Y - 1) / MCCols<n>::Y * n,                                 \
                           (ncols + MCCols<n>::X - 1) / MCCols<n>::X * n, Cfg<n>::ZSMEM,                   \
                           n * MCCols<n>::Y * 8, n * MCCols<n>::X * 8};                                   \
@@ -1334,7 +1338,7 @@ MCPassGeom mc_geom(int ng) {
         HGPM_MC_SIZES(X)
 #undef X
     }
-    return MCPassGeom{0, 0, 0, 0, 0, 0};
+    return MCPassGeom{0, 0, 0, 0, 0, 0, 0};
 }
 
 // One launch of `kern` (`threads` per CTA, `smem` bytes), one CTA per unit
@@ -1355,11 +1359,12 @@ cudaError_t mc_launch(const void* kern, MCTable t, const int* units, int threads
 }  // namespace
 
 cudaError_t mc_launch_fft_passes(const MCTable& base, cudaStream_t s) {
-    int zu[kMaxMC], yu[kMaxMC], xu[kMaxMC];
+    int zf[kMaxMC], zu[kMaxMC], yu[kMaxMC], xu[kMaxMC];
     int zs = 0, ys = 0, xs = 0;
     for (int k = 0; k < base.n; ++k) {
         const MCPassGeom g = mc_geom(base.c[k].ng);
         if (!g.zunits) return cudaErrorInvalidValue;
+        zf[k] = g.zfunits;
         zu[k] = g.zunits;
         yu[k] = g.yunits;
         xu[k] = g.xunits;
@@ -1367,7 +1372,7 @@ cudaError_t mc_launch_fft_passes(const MCTable& base, cudaStream_t s) {
         ys = g.ysmem > ys ? g.ysmem : ys;
         xs = g.xsmem > xs ? g.xsmem : xs;
     }
-    cudaError_t e = mc_launch((const void*)mc_fft_kernel<0>, base, zu, mc_threads<0>(), zs, s);
+    cudaError_t e = mc_launch((const void*)mc_fft_kernel<0>, base, zf, mc_threads<0>(), zs, s);
     if (e == cudaSuccess) e = mc_launch((const void*)mc_fft_kernel<1>, base, yu, mc_threads<1>(), ys, s);
     if (e == cudaSuccess) e = mc_launch((const void*)mc_fft_kernel<2>, base, xu, mc_threads<2>(), xs, s);
     if (e == cudaSuccess) e = mc_launch((const void*)mc_fft_kernel<3>, base, yu, mc_threads<3>(), ys, s);
